@@ -1,0 +1,337 @@
+/*
+ * ryoanji-b200 — C ABI of the single-GPU Barnes-Hut gravity path for NVIDIA B200 (sm_100a).
+ *
+ * Plain pointers and sizes only. Every device array argument is device memory of the current device unless the
+ * comment says "host". Each entry point names the reference interface it replaces (paths relative to the
+ * reference project root, tischwab0911/ryoanji). Functions return a ryo_status and never exit the process.
+ *
+ * Conventions shared with the reference:
+ *   - 64-bit Hilbert keys, 21 levels; keys equal to 2^63 mark removed particles.
+ *   - cornerstone leaf arrays (numLeaves + 1 keys), Warren-Salmon placeholder-bit node prefixes, nodes sorted
+ *     level-major; childOffsets is 0 for leaves; parents[(i - 1) / 8] is the parent of node i.
+ *   - multipoles: 8 floats per node (mass, qxx, qxy, qxz, qyy, qyz, qzz, trace), traceless quadrupole times 3;
+ *     source centres: 4 floats per node (x, y, z, squared MAC radius).
+ *   - traversal outputs are ACCUMULATED into p, ax, ay, az.
+ */
+#ifndef RYOANJI_B200_H
+#define RYOANJI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C"
+{
+#endif
+
+#define RYO_API __attribute__((visibility("default")))
+
+    typedef struct CUstream_st* ryo_stream_t; /* a cudaStream_t; NULL is the legacy default stream */
+
+    typedef enum ryo_status
+    {
+        RYO_OK                              = 0,
+        RYO_ERR_CUDA                        = 1, /* a CUDA call failed; see ryo_ctx_last_error */
+        RYO_ERR_BAD_ARG                     = 2,
+        RYO_ERR_OOM                         = 3,
+        RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE = 4, /* a single target still overflowed the traversal stack */
+        RYO_ERR_TIMEOUT                     = 5, /* a bounded device wait gave up (error flag set by a kernel) */
+        RYO_ERR_CAPACITY                    = 6, /* a caller-provided buffer is too small; see the size out-arg */
+        RYO_ERR_NOT_CUBIC                   = 7, /* Ewald needs a cubic periodic box */
+        RYO_ERR_NO_DEVICE                   = 8
+    } ryo_status;
+
+    /* cstone::BoundaryType (cstone/include/cstone/sfc/box.hpp:84-90) */
+    enum
+    {
+        RYO_BOUNDARY_OPEN       = 0,
+        RYO_BOUNDARY_PERIODIC   = 1,
+        RYO_BOUNDARY_FIXED      = 2,
+        RYO_BOUNDARY_CUBIC_OPEN = 3
+    };
+
+    /* cstone::Box<float> / Box<double> (cstone/include/cstone/sfc/box.hpp:99-214): xmin,xmax,ymin,ymax,zmin,zmax */
+    typedef struct ryo_box_f32
+    {
+        float limits[6];
+        int boundary[3];
+    } ryo_box_f32;
+
+    typedef struct ryo_box_f64
+    {
+        double limits[6];
+        int boundary[3];
+    } ryo_box_f64;
+
+    /* cstone::GroupView (cstone/include/cstone/traversal/groups.hpp:28-35); groupStart/groupEnd are device arrays */
+    typedef struct ryo_group_view
+    {
+        uint32_t firstBody, lastBody, numGroups;
+        const uint32_t* groupStart;
+        const uint32_t* groupEnd;
+    } ryo_group_view;
+
+    /* ryoanji::EwaldSettings (ryoanji/src/ryoanji/nbody/ewald.h:23-31) */
+    typedef struct ryo_ewald_settings
+    {
+        int numReplicaShells;        /* 1 */
+        double lCut;                 /* 2.6 */
+        double hCut;                 /* 2.8 */
+        double alpha_scale;          /* 2.0 */
+        double small_R_scale_factor; /* 3.0e-3 */
+    } ryo_ewald_settings;
+
+    typedef struct ryo_ctx ryo_ctx_t;
+    typedef struct ryo_treebuilder ryo_treebuilder_t;
+
+    /* ------------------------------------------------------------------------------------------ context */
+
+    RYO_API const char* ryo_status_string(ryo_status s);
+    /* library version "major.minor.patch" */
+    RYO_API const char* ryo_version(void);
+    /* A context owns scratch memory, per-call counters and statistics on one device (no global device state, so
+     * several contexts may run concurrently on different streams). */
+    RYO_API ryo_status ryo_ctx_create(int device, ryo_ctx_t** out);
+    RYO_API void ryo_ctx_destroy(ryo_ctx_t* ctx);
+    RYO_API const char* ryo_ctx_last_error(const ryo_ctx_t* ctx);
+
+    /* ------------------------------------------------------------------------------------------ cstone layer */
+
+    /* cstone::computeSfcKeys (cstone/include/cstone/sfc/sfc_gpu.h:100-102, sfc_gpu.cu:35-44): Hilbert keys of
+     * x, y, z in @p box; keys already equal to 2^63 are left unchanged. */
+    RYO_API ryo_status ryo_compute_sfc_keys_f32(const float* x, const float* y, const float* z, uint64_t* keys,
+                                                size_t n, const ryo_box_f32* box, ryo_stream_t stream);
+    RYO_API ryo_status ryo_compute_sfc_keys_f64(const double* x, const double* y, const double* z, uint64_t* keys,
+                                                size_t n, const ryo_box_f64* box, ryo_stream_t stream);
+
+    /* bounding box of the coordinates (min/max per axis, exact), written to host @p limits6 */
+    RYO_API ryo_status ryo_compute_bounding_box_f32(ryo_ctx_t* ctx, const float* x, const float* y, const float* z,
+                                                    size_t n, float* limits6, ryo_stream_t stream);
+
+    /* cstone::sequence (cstone/include/cstone/primitives/primitives_gpu.h): v[i] = first + i */
+    RYO_API ryo_status ryo_sequence(uint32_t* v, size_t n, uint32_t first, ryo_stream_t stream);
+
+    /* cstone::sortByKey with caller buffers (cstone/include/cstone/primitives/primitives_gpu.cu:311-356): stable
+     * ascending sort of keys[0:n) carrying values along; keyBuf/valueBuf hold n elements each; tmp holds
+     * ryo_sort_by_key_temp_bytes(n) bytes. Onesweep radix sort over bits [0, 64). */
+    RYO_API size_t ryo_sort_by_key_temp_bytes(size_t n);
+    RYO_API ryo_status ryo_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf,
+                                       uint32_t* valueBuf, void* tmp, size_t tmpBytes, ryo_stream_t stream);
+
+    /* cstone::computeOctree / updateOctreeGpu to convergence (cstone/include/cstone/tree/csarray.hpp:409-440,
+     * update_gpu.cuh:43-68): the cornerstone leaf array of sorted keys with at most @p bucketSize particles per
+     * leaf. Built in one pass (no host-synchronised rebalance loop); identical to the reference's fixed point.
+     * Writes leaves[numLeaves + 1] and counts[numLeaves] if numLeaves <= capacity; *numLeaves (host) always. */
+    RYO_API ryo_status ryo_compute_octree(ryo_ctx_t* ctx, const uint64_t* sortedKeys, size_t n, unsigned bucketSize,
+                                          uint64_t* leaves, uint32_t* counts, int capacity, int* numLeaves,
+                                          ryo_stream_t stream);
+
+    /* cstone::buildOctreeGpu (cstone/include/cstone/tree/octree_gpu.cu:138-200): internal octree of a leaf array.
+     * numNodes = numLeaves + (numLeaves - 1) / 7; parents holds max(1, (numNodes - 1) / 8) entries; levelRange is
+     * HOST memory (23 entries), d_levelRange device memory (23 entries, may be NULL). */
+    RYO_API ryo_status ryo_build_octree(ryo_ctx_t* ctx, const uint64_t* leaves, int numLeaves, uint64_t* prefixes,
+                                        int* childOffsets, int* parents, int* levelRange, int* d_levelRange,
+                                        int* internalToLeaf, int* leafToInternal, ryo_stream_t stream);
+
+    /* cstone::computeFixedGroups (cstone/include/cstone/traversal/groups_gpu.cu:45-58): groups[0:numGroups+1] of
+     * groupSize consecutive bodies in [first, last); groupStart = groups, groupEnd = groups + 1 */
+    RYO_API ryo_status ryo_compute_fixed_groups(uint32_t first, uint32_t last, unsigned groupSize, uint32_t* groups,
+                                                ryo_stream_t stream);
+
+    /* ------------------------------------------------------------------------------------------ upsweep
+     * The individual steps of the reference's upward pass. Sums run in double precision on the device; stored
+     * values are float. centers: 4 floats per node, multipoles: 8 floats per node. */
+
+    /* cstone::computeLeafSourceCenterGpu (cstone/include/cstone/focus/source_center_gpu.h:65-80) */
+    RYO_API ryo_status ryo_compute_leaf_source_center_f32(const float* x, const float* y, const float* z,
+                                                          const float* m, const int* leafToInternal, int numLeaves,
+                                                          const uint32_t* layout, float* centers,
+                                                          ryo_stream_t stream);
+    /* cstone::upsweepCentersGpu (source_center_gpu.h:82-92); levelRange is HOST memory */
+    RYO_API ryo_status ryo_upsweep_centers_f32(int numLevels, const int* levelRange, const int* childOffsets,
+                                               float* centers, ryo_stream_t stream);
+    /* ryoanji::computeLeafMultipoles (ryoanji/src/ryoanji/nbody/upsweep_gpu.h:24-31) */
+    RYO_API ryo_status ryo_compute_leaf_multipoles_f32(const float* x, const float* y, const float* z, const float* m,
+                                                       const int* leafToInternal, int numLeaves,
+                                                       const uint32_t* layout, const float* centers,
+                                                       float* multipoles, ryo_stream_t stream);
+    /* ryoanji::upsweepMultipoles (upsweep_gpu.h:33-41): M2M for cells [firstCell, lastCell) */
+    RYO_API ryo_status ryo_upsweep_multipoles_f32(int firstCell, int lastCell, const int* childOffsets,
+                                                  const float* centers, float* multipoles, ryo_stream_t stream);
+    /* cstone::setMacGpu (source_center_gpu.h:104-116): centers[i][3] = squared vector-MAC radius, 0 if massless */
+    RYO_API ryo_status ryo_set_mac_f32(const uint64_t* prefixes, int numNodes, float* centers, float invTheta,
+                                       const ryo_box_f32* box, ryo_stream_t stream);
+
+    /* ------------------------------------------------------------------------------------------ traversal */
+
+    /* ryoanji::bhMaxTargetSize (ryoanji/src/ryoanji/nbody/traversal_gpu.h:58-59): 64 */
+    RYO_API int ryo_bh_max_target_size(void);
+    /* ryoanji::stackSize (traversal_gpu.h:61-62): size of the caller stack pool in ints. The B200 traversal keeps
+     * its stacks in shared memory, so this is 0; a pool passed by a caller is not used. */
+    RYO_API uint32_t ryo_stack_size(uint32_t numGroups);
+
+    /* ryoanji::traverse (ryoanji/src/ryoanji/nbody/traversal_gpu.h:51-56), float instantiation: Barnes-Hut
+     * accelerations of the targets grouped by @p grp from the tree of the sources. Starts with the 8 siblings at
+     * initNodeIdx. numShells > 0 adds the (2 numShells + 1)^3 periodic replicas of edge boxL (3 floats, host).
+     * Accumulates G m phi into p (if not NULL) and G a into ax, ay, az. *totalPotential (host, may be NULL)
+     * receives 0.5 G sum(m phi) over the traversed targets. Groups whose traversal overflows the stack are split
+     * and traversed again (ryoanji/src/ryoanji/nbody/traversal_gpu.cu:582-618). */
+    RYO_API ryo_status ryo_traverse_f32(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const float* xt,
+                                        const float* yt, const float* zt, const float* mt, const float* ht,
+                                        const float* xs, const float* ys, const float* zs, const float* ms,
+                                        const float* hs, const int* childOffsets, const int* internalToLeaf,
+                                        const uint32_t* layout, const float* sourceCenter, const float* multipoles,
+                                        float G, int numShells, const float* boxL, float* p, float* ax, float* ay,
+                                        float* az, double* totalPotential, ryo_stream_t stream);
+
+    /* options of the extended traversal (not in the reference): per-group interaction counts and stack depth */
+    typedef struct ryo_traverse_options
+    {
+        uint32_t* groupM2P; /* device, numGroups entries (may be NULL): approximated cells per group */
+        uint32_t* groupP2P; /* device, numGroups entries (may be NULL): directly summed source bodies per group */
+        int stackCapacity;  /* traversal stack entries per warp, 0 = default (1024); small values force splits */
+    } ryo_traverse_options;
+
+    RYO_API ryo_status ryo_traverse_ex_f32(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx,
+                                           const float* xt, const float* yt, const float* zt, const float* mt,
+                                           const float* ht, const float* xs, const float* ys, const float* zs,
+                                           const float* ms, const float* hs, const int* childOffsets,
+                                           const int* internalToLeaf, const uint32_t* layout,
+                                           const float* sourceCenter, const float* multipoles, float G, int numShells,
+                                           const float* boxL, float* p, float* ax, float* ay, float* az,
+                                           double* totalPotential, const ryo_traverse_options* options,
+                                           ryo_stream_t stream);
+
+    /* ryoanji::readBhStats (traversal_gpu.h:64-65): {sumP2P, maxP2P, sumM2P, maxM2P, maxStack} of the last
+     * traversal on this context; maxP2P is 0xFFFFFFFF if a single target could not be traversed */
+    RYO_API ryo_status ryo_read_bh_stats(ryo_ctx_t* ctx, uint64_t* stats5);
+    /* ryoanji::readTraversalRetries (traversal_gpu.h:67-68) */
+    RYO_API uint64_t ryo_read_traversal_retries(ryo_ctx_t* ctx);
+
+    /* ------------------------------------------------------------------------------------------ Ewald */
+
+    /* ryoanji::computeGravityEwaldGpu (ryoanji/src/ryoanji/interface/ewald.cuh:24-27): root-multipole Ewald
+     * correction of the targets in @p grp; rootCenter (3) and Mroot (8) are HOST arrays; *ugravTot (host) is
+     * incremented by 0.5 G sum(m phi_ewald). The k-space sum runs in double precision. */
+    RYO_API ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float* rootCenter, const float* Mroot,
+                                                     const ryo_group_view* grp, const float* x, const float* y,
+                                                     const float* z, const float* m, const ryo_box_f32* box, float G,
+                                                     float* ugrav, float* ax, float* ay, float* az, double* ugravTot,
+                                                     const ryo_ewald_settings* settings, ryo_stream_t stream);
+
+    /* ------------------------------------------------------------------------------------------ direct sums */
+
+    /* ryoanji::directSum (ryoanji/src/ryoanji/nbody/direct.cuh:87-107): all-pairs sum for targets [first, last)
+     * over numBodies sources with (2 numShells + 1)^3 replicas; adds m phi to p and a to ax, ay, az (no G). */
+    RYO_API ryo_status ryo_direct_sum_f32(size_t first, size_t last, size_t numBodies, const float* boxL,
+                                          int numShells, const float* x, const float* y, const float* z,
+                                          const float* m, const float* h, float* p, float* ax, float* ay, float* az,
+                                          ryo_stream_t stream);
+    RYO_API ryo_status ryo_direct_sum_f64(size_t first, size_t last, size_t numBodies, const double* boxL,
+                                          int numShells, const double* x, const double* y, const double* z,
+                                          const double* m, const double* h, double* p, double* ax, double* ay,
+                                          double* az, ryo_stream_t stream);
+    /* accuracy reference: double-precision direct sum for selected targets of float data, exact 1/sqrt
+     * (the P2P<true> form, ryoanji/src/ryoanji/nbody/kernel.hpp:55-120); writes G m phi and G a per target */
+    RYO_API ryo_status ryo_direct_targets_f64(const int64_t* targets, size_t numTargets, const float* x,
+                                              const float* y, const float* z, const float* m, const float* h,
+                                              size_t numBodies, double G, const double* boxL, int numShells,
+                                              double* pot, double* ax, double* ay, double* az, ryo_stream_t stream);
+
+    /* ------------------------------------------------------------------------------------------ TreeBuilder
+     * ryoanji::TreeBuilder<uint64_t> (ryoanji/src/ryoanji/interface/treebuilder.cuh:34-125) */
+
+    RYO_API ryo_status ryo_treebuilder_create(ryo_ctx_t* ctx, unsigned ncrit, ryo_treebuilder_t** out);
+    RYO_API void ryo_treebuilder_destroy(ryo_treebuilder_t* tb);
+    /* TreeBuilder::update: sorts x, y, z in place into SFC order and builds the tree; *numNodes (host) receives
+     * the total node count. Like the reference, only x, y, z are permuted; ryo_treebuilder_order gives the
+     * permutation for other per-particle arrays. */
+    RYO_API ryo_status ryo_treebuilder_update_f32(ryo_treebuilder_t* tb, float* x, float* y, float* z, size_t n,
+                                                  const ryo_box_f32* box, int* numNodes, ryo_stream_t stream);
+    RYO_API ryo_status ryo_treebuilder_update_f64(ryo_treebuilder_t* tb, double* x, double* y, double* z, size_t n,
+                                                  const ryo_box_f64* box, int* numNodes, ryo_stream_t stream);
+
+    /* device arrays of the last update, valid until the next update (TreeBuilder accessors, treebuilder.cuh:103-112) */
+    typedef struct ryo_tree_view
+    {
+        int numLeafNodes, numInternalNodes, numNodes;
+        unsigned maxTreeLevel;        /* 21 */
+        const uint32_t* layout;       /* numLeafNodes + 1 */
+        const uint64_t* nodeKeys;     /* prefixes, numNodes */
+        const int* childOffsets;      /* numNodes */
+        const int* leafToInternal;    /* the leaf part: numLeafNodes entries */
+        const int* internalToLeaf;    /* numNodes */
+        const int* parents;           /* max(1, (numNodes - 1) / 8) */
+        const uint64_t* leaves;       /* numLeafNodes + 1 */
+        const uint32_t* order;        /* numBodies: original index of each sorted body */
+        const uint64_t* sortedKeys;   /* numBodies */
+        int levelRange[23];           /* host copy */
+    } ryo_tree_view;
+    RYO_API ryo_status ryo_treebuilder_view(const ryo_treebuilder_t* tb, ryo_tree_view* out);
+
+    /* ------------------------------------------------------------------------------------------ fused solve
+     * The B200 plain path for one system: keys, sort, gather, leaves, links, fused FP64 upsweep with MAC radii,
+     * fixed groups, traversal, Ewald if periodic. Not in the reference; it composes the functions above with the
+     * reference's semantics except that it permutes every per-particle array (TreeBuilder permutes only x, y, z). */
+    typedef struct ryo_solve_params
+    {
+        unsigned bucketSize;         /* leaf capacity, reference ncrit (64) */
+        unsigned groupSize;          /* target group size, <= 64 (64) */
+        float theta;                 /* opening angle (0.5) */
+        float G;                     /* gravitational constant (1) */
+        int useBox;                  /* 1: use @p box; 0: bounding box of the data (open boundaries) */
+        ryo_box_f32 box;             /* coordinate box; periodic boundary on all axes enables replicas + Ewald */
+        int numShells;               /* periodic replica shells when periodic (1) */
+        ryo_ewald_settings ewald;    /* Ewald settings when periodic */
+        int stackCapacity;           /* 0 = default */
+    } ryo_solve_params;
+
+    typedef struct ryo_solve_stats
+    {
+        int numLeaves, numNodes, numGroups;
+        uint64_t sumP2P, maxP2P, sumM2P, maxM2P, maxStack, retries;
+        double potentialEnergy; /* 0.5 G sum(m phi), tree + Ewald */
+        float box[6];           /* the box used */
+    } ryo_solve_stats;
+
+    RYO_API void ryo_solve_params_default(ryo_solve_params* p);
+
+    /* x, y, z, m, h: in any order on entry, SFC-sorted on return; vx, vy, vz (may be NULL) are permuted along;
+     * p, ax, ay, az are overwritten with the potential (G m phi) and acceleration in sorted order; order (may be
+     * NULL) receives the original index of each sorted body. stats (host, may be NULL). */
+    RYO_API ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* params, float* x, float* y, float* z,
+                                     float* m, float* h, float* vx, float* vy, float* vz, size_t n, float* p,
+                                     float* ax, float* ay, float* az, uint32_t* order, ryo_solve_stats* stats,
+                                     ryo_stream_t stream);
+
+    /* device arrays of the last ryo_solve_f32 on this context (valid until the next solve on it): the sorted keys,
+     * permutation, tree and the packed node records the traversal read (16 floats per node: centre x, y, z, squared
+     * MAC radius; multipole mass, qxx, qxy, qxz, qyy, qyz, qzz, trace; then 4 ints: first child, first body, body
+     * count, unused), plus the double-precision root expansion the Ewald correction used. */
+    typedef struct ryo_solve_arrays
+    {
+        int numLeaves, numNodes, numGroups;
+        const uint64_t* sortedKeys;
+        const uint32_t* order;
+        const uint64_t* leaves;
+        const uint32_t* layout;
+        const uint64_t* prefixes;
+        const int* childOffsets;
+        const int* internalToLeaf;
+        const int* leafToInternal; /* full array: numNodes entries */
+        const int* parents;
+        const float* nodeData;
+        const uint32_t* groups;
+        const uint32_t* groupM2P; /* per target group: approximated cells (all replicas) */
+        const uint32_t* groupP2P; /* per target group: directly summed source bodies */
+        int levelRange[23];
+        double rootCenter[3];
+        double rootMultipole[8];
+    } ryo_solve_arrays;
+    RYO_API ryo_status ryo_solve_arrays_get(ryo_ctx_t* ctx, ryo_solve_arrays* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RYOANJI_B200_H */

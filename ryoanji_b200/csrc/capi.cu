@@ -1,0 +1,994 @@
+/*
+ * ryoanji-b200: the C ABI (include/ryoanji_b200.h) over the kernels.
+ *
+ * Every entry point catches CUDA failures and turns them into a ryo_status with a message (the reference exits
+ * the process instead, cstone/include/cstone/cuda/errorcheck.cuh:15-27). Scratch memory is owned by the context
+ * (or the TreeBuilder) and grows on demand; nothing is kept in global device symbols, so contexts are independent.
+ */
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+#include "internal.hpp"
+
+using namespace ryo;
+
+namespace
+{
+thread_local std::string tlsError;
+
+struct ApiError
+{
+    ryo_status status;
+    std::string what;
+};
+
+ryo_status fromCuda(const CudaError& e, std::string& msg)
+{
+    msg = std::string(e.what) + ": " + cudaGetErrorString(e.err);
+    if (e.err == cudaErrorMemoryAllocation) return RYO_ERR_OOM;
+    if (e.err == cudaErrorInvalidValue) return RYO_ERR_BAD_ARG;
+    if (e.err == cudaErrorNoDevice || e.err == cudaErrorInvalidDevice) return RYO_ERR_NO_DEVICE;
+    return RYO_ERR_CUDA;
+}
+
+template<class F>
+ryo_status guarded(std::string& msg, F&& f)
+{
+    try
+    {
+        f();
+        return RYO_OK;
+    }
+    catch (const CudaError& e)
+    {
+        return fromCuda(e, msg);
+    }
+    catch (const ApiError& e)
+    {
+        msg = e.what;
+        return e.status;
+    }
+    catch (const std::bad_alloc&)
+    {
+        msg = "host allocation failed";
+        return RYO_ERR_OOM;
+    }
+}
+
+#define REQUIRE(cond, msg)                                                                                             \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        if (!(cond)) throw ApiError{RYO_ERR_BAD_ARG, msg};                                                             \
+    } while (0)
+
+DevBox<float> boxOf(const ryo_box_f32* b)
+{
+    int periodic = b->boundary[0] == RYO_BOUNDARY_PERIODIC && b->boundary[1] == RYO_BOUNDARY_PERIODIC &&
+                   b->boundary[2] == RYO_BOUNDARY_PERIODIC;
+    return makeDevBox<float>(b->limits, periodic);
+}
+
+DevBox<double> boxOf(const ryo_box_f64* b)
+{
+    int periodic = b->boundary[0] == RYO_BOUNDARY_PERIODIC && b->boundary[1] == RYO_BOUNDARY_PERIODIC &&
+                   b->boundary[2] == RYO_BOUNDARY_PERIODIC;
+    return makeDevBox<double>(b->limits, periodic);
+}
+
+void checkBox(const float* l)
+{
+    for (int d = 0; d < 3; ++d)
+        REQUIRE(l[2 * d + 1] > l[2 * d], "box: every axis needs max > min");
+}
+
+void checkBox(const double* l)
+{
+    for (int d = 0; d < 3; ++d)
+        REQUIRE(l[2 * d + 1] > l[2 * d], "box: every axis needs max > min");
+}
+
+//! raise RYO_ERR_TIMEOUT if a kernel gave up a bounded wait
+void checkDeviceError(ryo_ctx* ctx, cudaStream_t s)
+{
+    unsigned int err = 0;
+    RYO_CUDA(cudaMemcpyAsync(&err, &ctx->ctl->error, sizeof(err), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaStreamSynchronize(s));
+    if (err)
+    {
+        RYO_CUDA(cudaMemsetAsync(&ctx->ctl->error, 0, sizeof(unsigned int), s));
+        throw ApiError{RYO_ERR_TIMEOUT, "a device-side bounded wait timed out"};
+    }
+}
+
+} // namespace
+
+// ==================================================================================================== context
+
+extern "C" const char* ryo_status_string(ryo_status s)
+{
+    switch (s)
+    {
+        case RYO_OK: return "ok";
+        case RYO_ERR_CUDA: return "CUDA error";
+        case RYO_ERR_BAD_ARG: return "bad argument";
+        case RYO_ERR_OOM: return "out of device memory";
+        case RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE: return "traversal stack overflow for a single target";
+        case RYO_ERR_TIMEOUT: return "device wait timed out";
+        case RYO_ERR_CAPACITY: return "buffer capacity too small";
+        case RYO_ERR_NOT_CUBIC: return "Ewald needs a cubic periodic box";
+        case RYO_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" const char* ryo_version(void) { return "0.1.0"; }
+
+extern "C" ryo_status ryo_ctx_create(int device, ryo_ctx_t** out)
+{
+    if (!out) return RYO_ERR_BAD_ARG;
+    *out = nullptr;
+    ryo_ctx* ctx = new ryo_ctx();
+    ryo_status st = guarded(tlsError,
+                            [&]
+                            {
+                                RYO_CUDA(cudaSetDevice(device));
+                                ctx->device = device;
+                                RYO_CUDA(cudaDeviceGetAttribute(&ctx->smCount, cudaDevAttrMultiProcessorCount, device));
+                                RYO_CUDA(cudaMalloc(&ctx->ctl, sizeof(Control)));
+                                RYO_CUDA(cudaMemset(ctx->ctl, 0, sizeof(Control)));
+                            });
+    if (st != RYO_OK)
+    {
+        delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return RYO_OK;
+}
+
+extern "C" void ryo_ctx_destroy(ryo_ctx_t* ctx)
+{
+    if (!ctx) return;
+    cudaDeviceSynchronize();
+    ctx->releaseAll();
+    if (ctx->ctl) cudaFree(ctx->ctl);
+    delete ctx;
+}
+
+extern "C" const char* ryo_ctx_last_error(const ryo_ctx_t* ctx) { return ctx ? ctx->lastError.c_str() : tlsError.c_str(); }
+
+// ==================================================================================================== cstone layer
+
+extern "C" ryo_status ryo_compute_sfc_keys_f32(const float* x, const float* y, const float* z, uint64_t* keys,
+                                               size_t n, const ryo_box_f32* box, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       REQUIRE(box && (n == 0 || (x && y && z && keys)), "compute_sfc_keys: null argument");
+                       checkBox(box->limits);
+                       launchKeys<float>(x, y, z, keys, n, boxOf(box), true, stream);
+                   });
+}
+
+extern "C" ryo_status ryo_compute_sfc_keys_f64(const double* x, const double* y, const double* z, uint64_t* keys,
+                                               size_t n, const ryo_box_f64* box, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       REQUIRE(box && (n == 0 || (x && y && z && keys)), "compute_sfc_keys: null argument");
+                       checkBox(box->limits);
+                       launchKeys<double>(x, y, z, keys, n, boxOf(box), true, stream);
+                   });
+}
+
+extern "C" ryo_status ryo_compute_bounding_box_f32(ryo_ctx_t* ctx, const float* x, const float* y, const float* z,
+                                                   size_t n, float* limits6, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(limits6 && n > 0 && x && y && z, "compute_bounding_box: bad argument");
+                       double* mm = ctx->scratch<double>("bbox", 6, stream);
+                       launchBoundingBox(x, y, z, n, mm, stream);
+                       double h[6];
+                       RYO_CUDA(cudaMemcpyAsync(h, mm, sizeof(h), cudaMemcpyDeviceToHost, stream));
+                       RYO_CUDA(cudaStreamSynchronize(stream));
+                       for (int i = 0; i < 6; ++i)
+                           limits6[i] = float(h[i]);
+                   });
+}
+
+extern "C" ryo_status ryo_sequence(uint32_t* v, size_t n, uint32_t first, ryo_stream_t stream)
+{
+    return guarded(tlsError, [&] { launchSequence(v, n, first, stream); });
+}
+
+extern "C" size_t ryo_sort_by_key_temp_bytes(size_t n) { return sortTempBytes(n) + 64; }
+
+namespace
+{
+__global__ void sortErrorFlagInit(unsigned int* f) { *f = 0; }
+} // namespace
+
+extern "C" ryo_status ryo_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf, uint32_t* valueBuf,
+                                      void* tmp, size_t tmpBytes, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       if (n == 0) return;
+                       REQUIRE(keys && values && keyBuf && valueBuf && tmp, "sort_by_key: null argument");
+                       if (tmpBytes < ryo_sort_by_key_temp_bytes(n))
+                           throw ApiError{RYO_ERR_CAPACITY, "sort_by_key: temporary storage too small"};
+                       // the last 64 bytes of tmp hold the wait-timeout flag
+                       unsigned int* flag = reinterpret_cast<unsigned int*>(static_cast<char*>(tmp) + sortTempBytes(n));
+                       sortErrorFlagInit<<<1, 1, 0, stream>>>(flag);
+                       RYO_LAUNCH_CHECK();
+                       bool alt = radixSortPairs(keys, values, keyBuf, valueBuf, n, 0, 64, tmp, sortTempBytes(n), flag,
+                                                 stream, false);
+                       if (alt)
+                       {
+                           RYO_CUDA(cudaMemcpyAsync(keys, keyBuf, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice,
+                                                    stream));
+                           RYO_CUDA(cudaMemcpyAsync(values, valueBuf, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                                    stream));
+                       }
+                       unsigned int err = 0;
+                       RYO_CUDA(cudaMemcpyAsync(&err, flag, sizeof(err), cudaMemcpyDeviceToHost, stream));
+                       RYO_CUDA(cudaStreamSynchronize(stream));
+                       if (err) throw ApiError{RYO_ERR_TIMEOUT, "sort_by_key: look-back wait timed out"};
+                   });
+}
+
+extern "C" ryo_status ryo_compute_octree(ryo_ctx_t* ctx, const uint64_t* sortedKeys, size_t n, unsigned bucketSize,
+                                         uint64_t* leaves, uint32_t* counts, int capacity, int* numLeaves,
+                                         ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(numLeaves && bucketSize > 0 && (n == 0 || sortedKeys), "compute_octree: bad argument");
+                       int nl     = buildLeaves(ctx, sortedKeys, n, bucketSize, leaves, counts, nullptr, capacity,
+                                                stream);
+                       *numLeaves = nl;
+                       RYO_CUDA(cudaStreamSynchronize(stream));
+                       if (nl > capacity) throw ApiError{RYO_ERR_CAPACITY, "compute_octree: leaf capacity too small"};
+                   });
+}
+
+extern "C" ryo_status ryo_build_octree(ryo_ctx_t* ctx, const uint64_t* leaves, int numLeaves, uint64_t* prefixes,
+                                       int* childOffsets, int* parents, int* levelRange, int* d_levelRange,
+                                       int* internalToLeaf, int* leafToInternal, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(numLeaves >= 1 && leaves && prefixes && childOffsets && parents && levelRange &&
+                                   internalToLeaf && leafToInternal,
+                               "build_octree: bad argument");
+                       OctreeArrays o{prefixes, childOffsets, parents, internalToLeaf, leafToInternal, d_levelRange};
+                       linkOctree(ctx, leaves, numLeaves, o, levelRange, stream);
+                       checkDeviceError(ctx, stream);
+                   });
+}
+
+extern "C" ryo_status ryo_compute_fixed_groups(uint32_t first, uint32_t last, unsigned groupSize, uint32_t* groups,
+                                               ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       REQUIRE(groupSize > 0 && last >= first && groups, "compute_fixed_groups: bad argument");
+                       launchFixedGroups(first, last, groupSize, groups, stream);
+                   });
+}
+
+// ==================================================================================================== upsweep
+
+extern "C" ryo_status ryo_compute_leaf_source_center_f32(const float* x, const float* y, const float* z,
+                                                         const float* m, const int* leafToInternal, int numLeaves,
+                                                         const uint32_t* layout, float* centers, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       launchLeafCenters(x, y, z, m, leafToInternal, numLeaves, layout,
+                                         reinterpret_cast<float4*>(centers), stream);
+                   });
+}
+
+extern "C" ryo_status ryo_upsweep_centers_f32(int numLevels, const int* levelRange, const int* childOffsets,
+                                              float* centers, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       REQUIRE(levelRange && numLevels <= kMaxLevel + 1, "upsweep_centers: bad argument");
+                       for (int level = numLevels - 1; level >= 0; --level)
+                           launchUpsweepCenters(levelRange[level], levelRange[level + 1], childOffsets,
+                                                reinterpret_cast<float4*>(centers), stream);
+                   });
+}
+
+extern "C" ryo_status ryo_compute_leaf_multipoles_f32(const float* x, const float* y, const float* z, const float* m,
+                                                      const int* leafToInternal, int numLeaves,
+                                                      const uint32_t* layout, const float* centers,
+                                                      float* multipoles, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       launchLeafMultipoles(x, y, z, m, leafToInternal, numLeaves, layout,
+                                            reinterpret_cast<const float4*>(centers), multipoles, stream);
+                   });
+}
+
+extern "C" ryo_status ryo_upsweep_multipoles_f32(int firstCell, int lastCell, const int* childOffsets,
+                                                 const float* centers, float* multipoles, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       launchUpsweepMultipoles(firstCell, lastCell, childOffsets,
+                                               reinterpret_cast<const float4*>(centers), multipoles, stream);
+                   });
+}
+
+extern "C" ryo_status ryo_set_mac_f32(const uint64_t* prefixes, int numNodes, float* centers, float invTheta,
+                                      const ryo_box_f32* box, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       REQUIRE(box, "set_mac: null box");
+                       checkBox(box->limits);
+                       launchSetMac(prefixes, numNodes, reinterpret_cast<float4*>(centers), invTheta, boxOf(box),
+                                    stream);
+                   });
+}
+
+// ==================================================================================================== traversal
+
+extern "C" int ryo_bh_max_target_size(void) { return 64; }
+extern "C" uint32_t ryo_stack_size(uint32_t) { return 0; }
+
+namespace
+{
+
+__global__ void splitGroupsKernel(const uint32_t* failed, uint32_t numFailed, const uint32_t* starts,
+                                  const uint32_t* ends, uint32_t* newStart, uint32_t* newEnd, unsigned int* unsplit,
+                                  unsigned int* numNew)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numFailed) return;
+    uint32_t g = failed[i];
+    uint32_t a = starts[g], b = ends[g];
+    if (b - a < 2)
+    {
+        atomicAdd(unsplit, 1u);
+        return;
+    }
+    uint32_t mid  = a + (b - a) / 2;
+    unsigned slot = atomicAdd(numNew, 2u);
+    newStart[slot]     = a;
+    newEnd[slot]       = mid;
+    newStart[slot + 1] = mid;
+    newEnd[slot + 1]   = b;
+}
+
+/*! run a traversal to completion: groups that overflow the stack are split in two along the SFC and traversed
+ *  again until none fails (traversal_gpu.cu:572-623); counts per group refer to the groups of @p t */
+void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potentialOut)
+{
+    const uint32_t numGroups = uint32_t(t.numGroups);
+    t.ctl                    = ctx->ctl;
+    if (t.stackCapacity <= 0) t.stackCapacity = 1024;
+    launchTraversalReset(ctx->ctl, true, s);
+    ctx->retries          = 0;
+    bool unsplittable     = false;
+    uint32_t* failed      = ctx->scratch<uint32_t>("trav.failed", std::max<uint32_t>(numGroups, 1), s);
+    t.failedGroups        = failed;
+    t.failedCapacity      = numGroups;
+    bool first            = true;
+    while (t.numGroups > 0)
+    {
+        if (!first) launchTraversalReset(ctx->ctl, false, s);
+        launchTraverse(t, ctx->smCount, s);
+        unsigned int numFailed = 0;
+        RYO_CUDA(cudaMemcpyAsync(&numFailed, &ctx->ctl->failedCount, sizeof(numFailed), cudaMemcpyDeviceToHost, s));
+        RYO_CUDA(cudaStreamSynchronize(s));
+        if (numFailed == 0) break;
+        ctx->retries += numFailed;
+        // split the failed groups on the device: halves along the SFC
+        uint32_t cap        = 2 * numFailed;
+        uint32_t* nStart    = ctx->scratch<uint32_t>(first ? "trav.splitA" : "trav.splitB", cap, s);
+        uint32_t* nEnd      = ctx->scratch<uint32_t>(first ? "trav.splitEndA" : "trav.splitEndB", cap, s);
+        unsigned int* cnt   = ctx->ctl->counters;
+        RYO_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), s));
+        splitGroupsKernel<<<ceilDiv(numFailed, 256), 256, 0, s>>>(failed, numFailed, t.groupStart, t.groupEnd, nStart,
+                                                                   nEnd, cnt + 1, cnt);
+        RYO_LAUNCH_CHECK();
+        unsigned int h[2];
+        RYO_CUDA(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
+        RYO_CUDA(cudaStreamSynchronize(s));
+        if (h[1] > 0) unsplittable = true;
+        // the new groups are traversed into fresh buffers of the other name so that starts/ends stay valid
+        uint32_t* keepStart = ctx->scratch<uint32_t>(first ? "trav.curA" : "trav.curB", std::max(h[0], 1u), s);
+        uint32_t* keepEnd   = ctx->scratch<uint32_t>(first ? "trav.curEndA" : "trav.curEndB", std::max(h[0], 1u), s);
+        RYO_CUDA(cudaMemcpyAsync(keepStart, nStart, h[0] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        RYO_CUDA(cudaMemcpyAsync(keepEnd, nEnd, h[0] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        t.groupStart = keepStart;
+        t.groupEnd   = keepEnd;
+        t.numGroups  = int(h[0]);
+        t.groupM2P   = nullptr; // per-group counts are reported for unsplit groups only
+        t.groupP2P   = nullptr;
+        first        = !first;
+        if (t.numGroups == 0) break;
+        failed           = ctx->scratch<uint32_t>(first ? "trav.failed" : "trav.failed2", t.numGroups, s);
+        t.failedGroups   = failed;
+        t.failedCapacity = uint32_t(t.numGroups);
+    }
+    Control hc;
+    RYO_CUDA(cudaMemcpyAsync(&hc, ctx->ctl, sizeof(Control), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < 5; ++i)
+        ctx->hostStats[i] = hc.stats[i];
+    if (unsplittable) ctx->hostStats[kMaxP2P] = 0xFFFFFFFFull;
+    if (potentialOut) *potentialOut = hc.potential;
+    if (hc.error) throw ApiError{RYO_ERR_TIMEOUT, "traversal: a device-side bounded wait timed out"};
+}
+
+} // namespace
+
+extern "C" ryo_status ryo_traverse_ex_f32(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const float* xt,
+                                          const float* yt, const float* zt, const float* mt, const float* ht,
+                                          const float* xs, const float* ys, const float* zs, const float* ms,
+                                          const float* hs, const int* childOffsets, const int* internalToLeaf,
+                                          const uint32_t* layout, const float* sourceCenter, const float* multipoles,
+                                          float G, int numShells, const float* boxL, float* p, float* ax, float* ay,
+                                          float* az, double* totalPotential, const ryo_traverse_options* options,
+                                          ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(grp && xt && yt && zt && mt && ht && xs && ys && zs && ms && hs && childOffsets &&
+                                   internalToLeaf && layout && sourceCenter && multipoles && ax && ay && az,
+                               "traverse: null argument");
+                       REQUIRE(numShells >= 0 && (numShells == 0 || boxL), "traverse: replicas need boxL");
+                       TraverseLaunch t{};
+                       t.groupStart     = grp->groupStart;
+                       t.groupEnd       = grp->groupEnd;
+                       t.numGroups      = int(grp->numGroups);
+                       t.initNode       = initNodeIdx;
+                       t.numNodes       = initNodeIdx == 0 ? 1 : 2;
+                       t.nodes          = nullptr;
+                       t.centers        = reinterpret_cast<const float4*>(sourceCenter);
+                       t.multipoles     = multipoles;
+                       t.childOffsets   = childOffsets;
+                       t.internalToLeaf = internalToLeaf;
+                       t.layout         = layout;
+                       t.xt = xt, t.yt = yt, t.zt = zt, t.mt = mt, t.ht = ht;
+                       t.xs = xs, t.ys = ys, t.zs = zs, t.ms = ms, t.hs = hs;
+                       t.G         = G;
+                       t.numShells = numShells;
+                       for (int d = 0; d < 3; ++d)
+                           t.boxL[d] = numShells > 0 ? boxL[d] : 0.f;
+                       t.p  = p;
+                       t.ax = ax;
+                       t.ay = ay;
+                       t.az = az;
+                       t.groupM2P      = options ? options->groupM2P : nullptr;
+                       t.groupP2P      = options ? options->groupP2P : nullptr;
+                       t.stackCapacity = options ? options->stackCapacity : 0;
+                       double pot      = 0;
+                       runTraversal(ctx, t, stream, &pot);
+                       if (totalPotential) *totalPotential = 0.5 * double(G) * pot;
+                       if (ctx->hostStats[kMaxP2P] == 0xFFFFFFFFull)
+                           throw ApiError{RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE,
+                                          "traverse: a single target overflowed the stack"};
+                   });
+}
+
+extern "C" ryo_status ryo_traverse_f32(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const float* xt,
+                                       const float* yt, const float* zt, const float* mt, const float* ht,
+                                       const float* xs, const float* ys, const float* zs, const float* ms,
+                                       const float* hs, const int* childOffsets, const int* internalToLeaf,
+                                       const uint32_t* layout, const float* sourceCenter, const float* multipoles,
+                                       float G, int numShells, const float* boxL, float* p, float* ax, float* ay,
+                                       float* az, double* totalPotential, ryo_stream_t stream)
+{
+    return ryo_traverse_ex_f32(ctx, grp, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
+                               internalToLeaf, layout, sourceCenter, multipoles, G, numShells, boxL, p, ax, ay, az,
+                               totalPotential, nullptr, stream);
+}
+
+extern "C" ryo_status ryo_read_bh_stats(ryo_ctx_t* ctx, uint64_t* stats5)
+{
+    if (!ctx || !stats5) return RYO_ERR_BAD_ARG;
+    for (int i = 0; i < 5; ++i)
+        stats5[i] = ctx->hostStats[i];
+    return RYO_OK;
+}
+
+extern "C" uint64_t ryo_read_traversal_retries(ryo_ctx_t* ctx) { return ctx ? ctx->retries : 0; }
+
+// ==================================================================================================== Ewald
+
+extern "C" ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float* rootCenter, const float* Mroot,
+                                                    const ryo_group_view* grp, const float* x, const float* y,
+                                                    const float* z, const float* m, const ryo_box_f32* box, float G,
+                                                    float* ugrav, float* ax, float* ay, float* az, double* ugravTot,
+                                                    const ryo_ewald_settings* settings, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(rootCenter && Mroot && grp && x && y && z && m && box && ax && ay && az && settings,
+                               "compute_gravity_ewald: null argument");
+                       float lx = box->limits[1] - box->limits[0], ly = box->limits[3] - box->limits[2],
+                             lz = box->limits[5] - box->limits[4];
+                       if (!(lx == ly && ly == lz)) throw ApiError{RYO_ERR_NOT_CUBIC, "Ewald needs a cubic box"};
+                       double mr[8], c[3];
+                       for (int i = 0; i < 8; ++i)
+                           mr[i] = Mroot[i];
+                       for (int i = 0; i < 3; ++i)
+                           c[i] = rootCenter[i];
+                       EwaldHost e = ewaldSetup(mr, c, settings->numReplicaShells, double(lx), settings->lCut,
+                                                settings->hCut, settings->alpha_scale,
+                                                settings->small_R_scale_factor);
+                       double* pot = &ctx->ctl->ewaldPotential;
+                       RYO_CUDA(cudaMemsetAsync(pot, 0, sizeof(double), stream));
+                       launchEwaldGroups(e, grp->groupStart, grp->groupEnd, grp->numGroups, x, y, z, m, G, ugrav, ax,
+                                         ay, az, pot, stream);
+                       double h = 0;
+                       RYO_CUDA(cudaMemcpyAsync(&h, pot, sizeof(double), cudaMemcpyDeviceToHost, stream));
+                       RYO_CUDA(cudaStreamSynchronize(stream));
+                       if (ugravTot) *ugravTot += 0.5 * double(G) * h;
+                   });
+}
+
+// ==================================================================================================== direct sums
+
+extern "C" ryo_status ryo_direct_sum_f32(size_t first, size_t last, size_t numBodies, const float* boxL,
+                                         int numShells, const float* x, const float* y, const float* z,
+                                         const float* m, const float* h, float* p, float* ax, float* ay, float* az,
+                                         ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&] { launchDirect<float>(first, last, numBodies, boxL, numShells, x, y, z, m, h, p, ax, ay, az,
+                                             stream); });
+}
+
+extern "C" ryo_status ryo_direct_sum_f64(size_t first, size_t last, size_t numBodies, const double* boxL,
+                                         int numShells, const double* x, const double* y, const double* z,
+                                         const double* m, const double* h, double* p, double* ax, double* ay,
+                                         double* az, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&] { launchDirect<double>(first, last, numBodies, boxL, numShells, x, y, z, m, h, p, ax, ay, az,
+                                              stream); });
+}
+
+extern "C" ryo_status ryo_direct_targets_f64(const int64_t* targets, size_t numTargets, const float* x, const float* y,
+                                             const float* z, const float* m, const float* h, size_t numBodies,
+                                             double G, const double* boxL, int numShells, double* pot, double* ax,
+                                             double* ay, double* az, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       launchDirectTargets(targets, numTargets, x, y, z, m, h, numBodies, G, boxL, numShells, pot, ax,
+                                           ay, az, stream);
+                   });
+}
+
+// ==================================================================================================== TreeBuilder
+
+struct ryo_treebuilder
+{
+    ryo_ctx* ctx;
+    unsigned ncrit;
+    std::string tag;
+    size_t numBodies = 0;
+    int numLeaves = 0, numInternal = 0, numNodes = 0;
+    int levelRange[kMaxLevel + 2] = {};
+    uint64_t* sortedKeys = nullptr;
+    uint32_t* order      = nullptr;
+    uint64_t* leaves     = nullptr;
+    uint32_t* counts     = nullptr;
+    uint32_t* layout     = nullptr;
+    OctreeArrays oct{};
+
+    template<class T>
+    T* buf(const char* name, size_t count, cudaStream_t s)
+    {
+        return ctx->scratch<T>(tag + name, count, s);
+    }
+};
+
+namespace
+{
+template<class T>
+void treebuilderUpdate(ryo_treebuilder* tb, T* x, T* y, T* z, size_t n, const DevBox<T>& box, cudaStream_t s)
+{
+    ryo_ctx* ctx = tb->ctx;
+    REQUIRE(n > 0 && n < (size_t(1) << 32), "treebuilder: body count must be in [1, 2^32)");
+    uint64_t* keys     = tb->buf<uint64_t>(".keys", n, s);
+    uint64_t* keysAlt  = tb->buf<uint64_t>(".keysAlt", n, s);
+    uint32_t* order    = tb->buf<uint32_t>(".order", n, s);
+    uint32_t* orderAlt = tb->buf<uint32_t>(".orderAlt", n, s);
+    size_t tmpBytes    = sortTempBytes(n);
+    void* tmp          = tb->buf<char>(".sorttmp", tmpBytes, s);
+    T* scratch         = tb->buf<T>(".coord", n, s);
+
+    launchKeys<T>(x, y, z, keys, n, box, false, s);
+    bool alt       = radixSortPairs(keys, order, keysAlt, orderAlt, n, 0, 64, tmp, tmpBytes, &ctx->ctl->error, s, true);
+    tb->sortedKeys = alt ? keysAlt : keys;
+    tb->order      = alt ? orderAlt : order;
+    for (T* a : {x, y, z})
+    {
+        launchGatherT<T>(tb->order, a, scratch, n, s);
+        RYO_CUDA(cudaMemcpyAsync(a, scratch, n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    }
+
+    int cap     = int(std::min<size_t>(n / 2 + 64, size_t(1) << 30));
+    tb->leaves  = tb->buf<uint64_t>(".leaves", size_t(cap) + 1, s);
+    tb->counts  = tb->buf<uint32_t>(".counts", cap, s);
+    tb->layout  = tb->buf<uint32_t>(".layout", size_t(cap) + 1, s);
+    int nl      = buildLeaves(ctx, tb->sortedKeys, n, tb->ncrit, tb->leaves, tb->counts, tb->layout, cap, s);
+    if (nl > cap)
+    {
+        cap        = nl;
+        tb->leaves = tb->buf<uint64_t>(".leaves", size_t(cap) + 1, s);
+        tb->counts = tb->buf<uint32_t>(".counts", cap, s);
+        tb->layout = tb->buf<uint32_t>(".layout", size_t(cap) + 1, s);
+        nl         = buildLeaves(ctx, tb->sortedKeys, n, tb->ncrit, tb->leaves, tb->counts, tb->layout, cap, s);
+    }
+    tb->numLeaves   = nl;
+    tb->numInternal = (nl - 1) / 7;
+    tb->numNodes    = nl + tb->numInternal;
+    int nn          = tb->numNodes;
+    tb->oct.prefixes       = tb->buf<uint64_t>(".prefixes", nn, s);
+    tb->oct.childOffsets   = tb->buf<int>(".childOffsets", size_t(nn) + 1, s);
+    tb->oct.parents        = tb->buf<int>(".parents", std::max(1, (nn - 1) / 8), s);
+    tb->oct.internalToLeaf = tb->buf<int>(".internalToLeaf", nn, s);
+    tb->oct.leafToInternal = tb->buf<int>(".leafToInternal", nn, s);
+    tb->oct.d_levelRange   = tb->buf<int>(".levelRange", kMaxLevel + 2, s);
+    linkOctree(ctx, tb->leaves, nl, tb->oct, tb->levelRange, s);
+    tb->numBodies = n;
+    checkDeviceError(ctx, s);
+}
+} // namespace
+
+extern "C" ryo_status ryo_treebuilder_create(ryo_ctx_t* ctx, unsigned ncrit, ryo_treebuilder_t** out)
+{
+    if (!ctx || !out || ncrit == 0) return RYO_ERR_BAD_ARG;
+    static unsigned long long counter = 0;
+    auto* tb  = new ryo_treebuilder();
+    tb->ctx   = ctx;
+    tb->ncrit = ncrit;
+    tb->tag   = "tb" + std::to_string(++counter);
+    *out      = tb;
+    return RYO_OK;
+}
+
+extern "C" void ryo_treebuilder_destroy(ryo_treebuilder_t* tb)
+{
+    if (!tb) return;
+    cudaDeviceSynchronize();
+    for (auto it = tb->ctx->buffers.begin(); it != tb->ctx->buffers.end();)
+    {
+        if (it->first.rfind(tb->tag + ".", 0) == 0)
+        {
+            if (it->second.ptr) cudaFree(it->second.ptr);
+            it = tb->ctx->buffers.erase(it);
+        }
+        else ++it;
+    }
+    delete tb;
+}
+
+extern "C" ryo_status ryo_treebuilder_update_f32(ryo_treebuilder_t* tb, float* x, float* y, float* z, size_t n,
+                                                 const ryo_box_f32* box, int* numNodes, ryo_stream_t stream)
+{
+    if (!tb) return RYO_ERR_BAD_ARG;
+    return guarded(tb->ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(x && y && z && box, "treebuilder_update: null argument");
+                       checkBox(box->limits);
+                       treebuilderUpdate<float>(tb, x, y, z, n, boxOf(box), stream);
+                       if (numNodes) *numNodes = tb->numNodes;
+                   });
+}
+
+extern "C" ryo_status ryo_treebuilder_update_f64(ryo_treebuilder_t* tb, double* x, double* y, double* z, size_t n,
+                                                 const ryo_box_f64* box, int* numNodes, ryo_stream_t stream)
+{
+    if (!tb) return RYO_ERR_BAD_ARG;
+    return guarded(tb->ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(x && y && z && box, "treebuilder_update: null argument");
+                       checkBox(box->limits);
+                       treebuilderUpdate<double>(tb, x, y, z, n, boxOf(box), stream);
+                       if (numNodes) *numNodes = tb->numNodes;
+                   });
+}
+
+extern "C" ryo_status ryo_treebuilder_view(const ryo_treebuilder_t* tb, ryo_tree_view* out)
+{
+    if (!tb || !out) return RYO_ERR_BAD_ARG;
+    out->numLeafNodes     = tb->numLeaves;
+    out->numInternalNodes = tb->numInternal;
+    out->numNodes         = tb->numNodes;
+    out->maxTreeLevel     = kMaxLevel;
+    out->layout           = tb->layout;
+    out->nodeKeys         = tb->oct.prefixes;
+    out->childOffsets     = tb->oct.childOffsets;
+    out->leafToInternal   = tb->oct.leafToInternal ? tb->oct.leafToInternal + tb->numInternal : nullptr;
+    out->internalToLeaf   = tb->oct.internalToLeaf;
+    out->parents          = tb->oct.parents;
+    out->leaves           = tb->leaves;
+    out->order            = tb->order;
+    out->sortedKeys       = tb->sortedKeys;
+    for (int i = 0; i < kMaxLevel + 2; ++i)
+        out->levelRange[i] = tb->levelRange[i];
+    return RYO_OK;
+}
+
+// ==================================================================================================== fused solve
+
+extern "C" void ryo_solve_params_default(ryo_solve_params* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->bucketSize                 = 64;
+    p->groupSize                  = 64;
+    p->theta                      = 0.5f;
+    p->G                          = 1.0f;
+    p->useBox                     = 0;
+    p->numShells                  = 1;
+    p->ewald.numReplicaShells     = 1;
+    p->ewald.lCut                 = 2.6;
+    p->ewald.hCut                 = 2.8;
+    p->ewald.alpha_scale          = 2.0;
+    p->ewald.small_R_scale_factor = 3.0e-3;
+    p->stackCapacity              = 0;
+}
+
+namespace
+{
+__global__ void packSolveBodies(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                                const float* __restrict__ m, const float* __restrict__ h, size_t n,
+                                float4* __restrict__ xyzm, float4* __restrict__ xyzh)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        float px = x[i], py = y[i], pz = z[i];
+        xyzm[i]  = make_float4(px, py, pz, m[i]);
+        xyzh[i]  = make_float4(px, py, pz, h[i]);
+    }
+}
+} // namespace
+
+extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, float* x, float* y, float* z, float* m,
+                                    float* h, float* vx, float* vy, float* vz, size_t n, float* p, float* ax,
+                                    float* ay, float* az, uint32_t* orderOut, ryo_solve_stats* stats,
+                                    ryo_stream_t stream)
+{
+    if (!ctx || !P) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(x && y && z && m && h && p && ax && ay && az, "solve: null argument");
+                       REQUIRE(n > 0 && n < (size_t(1) << 32), "solve: body count must be in [1, 2^32)");
+                       REQUIRE(P->groupSize >= 1 && P->groupSize <= 64, "solve: groupSize must be in [1, 64]");
+                       REQUIRE(P->bucketSize >= 1 && P->theta > 0.f, "solve: bad bucketSize or theta");
+                       cudaStream_t s = stream;
+
+                       // box: given, or the cube enclosing the data (exact min/max)
+                       ryo_box_f32 box{};
+                       if (P->useBox) { box = P->box; }
+                       else
+                       {
+                           double* mm = ctx->scratch<double>("solve.bbox", 6, s);
+                           launchBoundingBox(x, y, z, n, mm, s);
+                           double hb[6];
+                           RYO_CUDA(cudaMemcpyAsync(hb, mm, sizeof(hb), cudaMemcpyDeviceToHost, s));
+                           RYO_CUDA(cudaStreamSynchronize(s));
+                           double ext = std::max({hb[1] - hb[0], hb[3] - hb[2], hb[5] - hb[4]});
+                           if (!(ext > 0)) ext = 1.0;
+                           for (int d = 0; d < 3; ++d)
+                           {
+                               box.limits[2 * d]     = float(hb[2 * d]);
+                               box.limits[2 * d + 1] = float(hb[2 * d] + ext);
+                               if (!(box.limits[2 * d + 1] >= float(hb[2 * d + 1])))
+                                   box.limits[2 * d + 1] = std::nextafter(float(hb[2 * d + 1]), 3.4e38f);
+                               box.boundary[d] = RYO_BOUNDARY_OPEN;
+                           }
+                       }
+                       checkBox(box.limits);
+                       DevBox<float> dbox = boxOf(&box);
+                       bool periodic      = dbox.periodic;
+
+                       // keys and sort
+                       uint64_t* keys    = ctx->scratch<uint64_t>("solve.keys", n, s);
+                       uint64_t* keysAlt = ctx->scratch<uint64_t>("solve.keysAlt", n, s);
+                       uint32_t* ord     = ctx->scratch<uint32_t>("solve.order", n, s);
+                       uint32_t* ordAlt  = ctx->scratch<uint32_t>("solve.orderAlt", n, s);
+                       size_t tmpBytes   = sortTempBytes(n);
+                       void* tmp         = ctx->scratch<char>("solve.sorttmp", tmpBytes, s);
+                       launchKeys<float>(x, y, z, keys, n, dbox, false, s);
+                       bool alt = radixSortPairs(keys, ord, keysAlt, ordAlt, n, 0, 64, tmp, tmpBytes, &ctx->ctl->error,
+                                                 s, true);
+                       const uint64_t* sorted = alt ? keysAlt : keys;
+                       const uint32_t* order  = alt ? ordAlt : ord;
+
+                       // permute every per-particle array
+                       float* tmpF = ctx->scratch<float>("solve.tmpf", n, s);
+                       for (float* a : {x, y, z, m, h, vx, vy, vz})
+                       {
+                           if (!a) continue;
+                           launchGather(order, a, tmpF, n, s);
+                           RYO_CUDA(cudaMemcpyAsync(a, tmpF, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+                       }
+                       if (orderOut)
+                           RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+                       float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
+                       float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
+                       packSolveBodies<<<ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
+                                                                                        : unsigned(ctx->smCount * 16),
+                                         256, 0, s>>>(x, y, z, m, h, n, xyzm, xyzh);
+                       RYO_LAUNCH_CHECK();
+
+                       // leaves, links
+                       int cap           = int(std::min<size_t>(n / 2 + 64, size_t(1) << 30));
+                       uint64_t* leaves  = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
+                       uint32_t* counts  = ctx->scratch<uint32_t>("solve.counts", cap, s);
+                       uint32_t* layout  = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
+                       int nl = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s);
+                       if (nl > cap)
+                       {
+                           cap    = nl;
+                           leaves = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
+                           counts = ctx->scratch<uint32_t>("solve.counts", cap, s);
+                           layout = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
+                           nl     = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s);
+                       }
+                       int ni = (nl - 1) / 7, nn = nl + ni;
+                       OctreeArrays oct;
+                       oct.prefixes       = ctx->scratch<uint64_t>("solve.prefixes", nn, s);
+                       oct.childOffsets   = ctx->scratch<int>("solve.childOffsets", size_t(nn) + 1, s);
+                       oct.parents        = ctx->scratch<int>("solve.parents", std::max(1, (nn - 1) / 8), s);
+                       oct.internalToLeaf = ctx->scratch<int>("solve.internalToLeaf", nn, s);
+                       oct.leafToInternal = ctx->scratch<int>("solve.leafToInternal", nn, s);
+                       oct.d_levelRange   = ctx->scratch<int>("solve.levelRange", kMaxLevel + 2, s);
+                       int levelRange[kMaxLevel + 2];
+                       linkOctree(ctx, leaves, nl, oct, levelRange, s);
+
+                       // fused upsweep: node records + FP64 root expansion
+                       NodeRecord* records = ctx->scratch<NodeRecord>("solve.records", nn, s);
+                       double* root        = ctx->scratch<double>("solve.root", 16, s);
+                       launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
+                                          oct.parents, oct.prefixes, 1.0f / P->theta, dbox, records, nullptr, nullptr,
+                                          root, s);
+
+                       // groups and traversal
+                       uint32_t numGroups = uint32_t((n + P->groupSize - 1) / P->groupSize);
+                       uint32_t* groups   = ctx->scratch<uint32_t>("solve.groups", size_t(numGroups) + 1, s);
+                       launchFixedGroups(0, uint32_t(n), P->groupSize, groups, s);
+                       for (float* a : {p, ax, ay, az})
+                           RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
+                       TraverseLaunch t{};
+                       t.groupStart    = groups;
+                       t.groupEnd      = groups + 1;
+                       t.numGroups     = int(numGroups);
+                       t.initNode      = nn == 1 ? 0 : 1;
+                       t.numNodes      = nn;
+                       t.nodes         = records;
+                       t.tgtXYZH       = xyzh;
+                       t.tgtM          = m;
+                       t.srcXYZM       = xyzm;
+                       t.srcH          = h;
+                       t.G             = P->G;
+                       t.numShells     = periodic ? P->numShells : 0;
+                       for (int d = 0; d < 3; ++d)
+                           t.boxL[d] = dbox.len[d];
+                       t.p  = p;
+                       t.ax = ax;
+                       t.ay = ay;
+                       t.az = az;
+                       t.stackCapacity = P->stackCapacity;
+                       uint32_t* gm2p  = ctx->scratch<uint32_t>("solve.groupM2P", numGroups, s);
+                       uint32_t* gp2p  = ctx->scratch<uint32_t>("solve.groupP2P", numGroups, s);
+                       t.groupM2P      = gm2p;
+                       t.groupP2P      = gp2p;
+                       double pot      = 0;
+                       runTraversal(ctx, t, s, &pot);
+                       double energy = 0.5 * double(P->G) * pot;
+
+                       if (periodic)
+                       {
+                           if (!(dbox.len[0] == dbox.len[1] && dbox.len[1] == dbox.len[2]))
+                               throw ApiError{RYO_ERR_NOT_CUBIC, "solve: Ewald needs a cubic periodic box"};
+                           double hr[16];
+                           RYO_CUDA(cudaMemcpyAsync(hr, root, sizeof(double) * 11, cudaMemcpyDeviceToHost, s));
+                           RYO_CUDA(cudaStreamSynchronize(s));
+                           EwaldHost e = ewaldSetup(hr + 3, hr, P->ewald.numReplicaShells, double(dbox.len[0]),
+                                                    P->ewald.lCut, P->ewald.hCut, P->ewald.alpha_scale,
+                                                    P->ewald.small_R_scale_factor);
+                           double* ep = &ctx->ctl->ewaldPotential;
+                           RYO_CUDA(cudaMemsetAsync(ep, 0, sizeof(double), s));
+                           launchEwaldGroups(e, groups, groups + 1, numGroups, x, y, z, m, P->G, p, ax, ay, az, ep, s);
+                           double he = 0;
+                           RYO_CUDA(cudaMemcpyAsync(&he, ep, sizeof(double), cudaMemcpyDeviceToHost, s));
+                           RYO_CUDA(cudaStreamSynchronize(s));
+                           energy += 0.5 * double(P->G) * he;
+                       }
+                       {
+                           ryo_solve_arrays& a = ctx->lastSolve;
+                           a.numLeaves         = nl;
+                           a.numNodes          = nn;
+                           a.numGroups         = int(numGroups);
+                           a.sortedKeys        = sorted;
+                           a.order             = order;
+                           a.leaves            = leaves;
+                           a.layout            = layout;
+                           a.prefixes          = oct.prefixes;
+                           a.childOffsets      = oct.childOffsets;
+                           a.internalToLeaf    = oct.internalToLeaf;
+                           a.leafToInternal    = oct.leafToInternal;
+                           a.parents           = oct.parents;
+                           a.nodeData          = reinterpret_cast<const float*>(records);
+                           a.groups            = groups;
+                           a.groupM2P          = gm2p;
+                           a.groupP2P          = gp2p;
+                           for (int i = 0; i < kMaxLevel + 2; ++i)
+                               a.levelRange[i] = levelRange[i];
+                           double hr[11];
+                           RYO_CUDA(cudaMemcpyAsync(hr, root, sizeof(hr), cudaMemcpyDeviceToHost, s));
+                           RYO_CUDA(cudaStreamSynchronize(s));
+                           for (int i = 0; i < 3; ++i)
+                               a.rootCenter[i] = hr[i];
+                           for (int i = 0; i < 8; ++i)
+                               a.rootMultipole[i] = hr[3 + i];
+                       }
+                       if (ctx->hostStats[kMaxP2P] == 0xFFFFFFFFull)
+                           throw ApiError{RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE, "solve: a single target overflowed"};
+                       checkDeviceError(ctx, s);
+                       if (stats)
+                       {
+                           stats->numLeaves       = nl;
+                           stats->numNodes        = nn;
+                           stats->numGroups       = int(numGroups);
+                           stats->sumP2P          = ctx->hostStats[kSumP2P];
+                           stats->maxP2P          = ctx->hostStats[kMaxP2P];
+                           stats->sumM2P          = ctx->hostStats[kSumM2P];
+                           stats->maxM2P          = ctx->hostStats[kMaxM2P];
+                           stats->maxStack        = ctx->hostStats[kMaxStack];
+                           stats->retries         = ctx->retries;
+                           stats->potentialEnergy = energy;
+                           for (int i = 0; i < 6; ++i)
+                               stats->box[i] = box.limits[i];
+                       }
+                   });
+}
+
+extern "C" ryo_status ryo_solve_arrays_get(ryo_ctx_t* ctx, ryo_solve_arrays* out)
+{
+    if (!ctx || !out) return RYO_ERR_BAD_ARG;
+    *out = ctx->lastSolve;
+    return RYO_OK;
+}

@@ -1,0 +1,626 @@
+/*
+ * ryoanji-b200: device-side building blocks shared by all kernels.
+ *
+ * Key arithmetic, the mixed-dimension Hilbert curve (encode and decode), the coordinate box and warp helpers.
+ * Everything that feeds an integer output (keys, node boxes, MAC radii) keeps the reference's rounding points
+ * exactly: products and sums are issued with explicit round-to-nearest intrinsics so that the compiler cannot
+ * contract them into FMAs, which the reference CPU build does not do either.
+ */
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ryoanji_b200.h"
+
+namespace ryo
+{
+
+constexpr int kMaxLevel    = 21;                     // 64-bit SFC keys: 21 octal digits
+constexpr uint64_t kKeyEnd = uint64_t(1) << 63;      // end of the key range, also the "remove" marker key
+constexpr int kWarp        = 32;
+
+// ------------------------------------------------------------------------------------------------ error handling
+
+struct CudaError
+{
+    cudaError_t err;
+    const char* what;
+};
+
+#define RYO_CUDA(call)                                                                                                 \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t e_ = (call);                                                                                       \
+        if (e_ != cudaSuccess) throw ::ryo::CudaError{e_, #call};                                                      \
+    } while (0)
+
+#define RYO_LAUNCH_CHECK() RYO_CUDA(cudaGetLastError())
+
+inline unsigned ceilDiv(size_t a, size_t b) { return unsigned((a + b - 1) / b); }
+
+// ------------------------------------------------------------------------------------------------ key arithmetic
+
+__host__ __device__ inline int clz64(uint64_t v)
+{
+#ifdef __CUDA_ARCH__
+    return __clzll((long long)v);
+#else
+    return v ? __builtin_clzll(v) : 64;
+#endif
+}
+
+//! key range covered by one node on @p level
+__host__ __device__ inline uint64_t nodeRange(unsigned level) { return uint64_t(1) << (3 * (kMaxLevel - level)); }
+
+//! level of a power-of-8 key range
+__host__ __device__ inline unsigned rangeLevel(uint64_t range) { return unsigned(clz64(range - 1) - 1) / 3; }
+
+//! number of leading key bits (excluding the unused top bit) shared by two keys
+__host__ __device__ inline int commonBits(uint64_t a, uint64_t b) { return clz64(a ^ b) - 1; }
+
+__host__ __device__ inline unsigned octalDigit(uint64_t key, unsigned level)
+{
+    return unsigned(key >> (3 * (kMaxLevel - level))) & 7u;
+}
+
+//! Warren-Salmon placeholder-bit prefix: the first @p len key bits behind a leading 1
+__host__ __device__ inline uint64_t encodePrefix(uint64_t key, int len)
+{
+    return (key >> (63 - len)) | (uint64_t(1) << len);
+}
+
+__host__ __device__ inline int prefixLength(uint64_t prefix) { return 63 - clz64(prefix); }
+
+__host__ __device__ inline uint64_t prefixStart(uint64_t prefix)
+{
+    int len = prefixLength(prefix);
+    return (prefix ^ (uint64_t(1) << len)) << (63 - len);
+}
+
+//! position (level) of the last non-zero octal digit, kMaxLevel for 0
+__host__ __device__ inline int lastNonZeroLevel(uint64_t key)
+{
+#ifdef __CUDA_ARCH__
+    return key ? kMaxLevel - (__ffsll((long long)key) - 1) / 3 : kMaxLevel;
+#else
+    return key ? kMaxLevel - __builtin_ctzll(key) / 3 : kMaxLevel;
+#endif
+}
+
+/*! @brief the minimal sequence of aligned octree nodes covering [a, b), written to @p out if not null
+ *
+ * Nodes grow while walking up from a's last non-zero digit to the first digit where a and b differ, then shrink
+ * towards b. Returns the number of nodes. Same node sequence as cstone's spanSfcRange (cstone/sfc/common.hpp:412-451).
+ */
+__host__ __device__ inline int spanKeyRange(uint64_t a, uint64_t b, uint64_t* out)
+{
+    int num      = 0;
+    int diffLvl  = (clz64(a ^ b) + 3 - 1) / 3;
+    for (int lvl = lastNonZeroLevel(a); lvl > diffLvl; --lvl)
+    {
+        int reps = (8 - int(octalDigit(a, lvl))) % 8;
+        for (int r = 0; r < reps; ++r)
+        {
+            if (out) out[num] = a;
+            ++num;
+            a += nodeRange(lvl);
+        }
+    }
+    int bLast = lastNonZeroLevel(b);
+    for (int lvl = diffLvl; lvl <= bLast; ++lvl)
+    {
+        int reps = int(octalDigit(b, lvl)) - int(octalDigit(a, lvl));
+        for (int r = 0; r < reps; ++r)
+        {
+            if (out) out[num] = a;
+            ++num;
+            a += nodeRange(lvl);
+        }
+    }
+    return num;
+}
+
+// ------------------------------------------------------------------------------------------------ Hilbert curve
+
+/*! 3D Hilbert index of the @p order low bits of (px, py, pz). The digit of an octant and the re-orientation of the
+ *  remaining bits per level define the curve of cstone/sfc/hilbert.hpp:43-94; the same curve is required for
+ *  bit-identical keys. */
+__host__ __device__ inline uint64_t hilbert3(unsigned px, unsigned py, unsigned pz, int order)
+{
+    // octant (x<<2|y<<1|z) -> Hilbert digit {0,1,3,2,7,6,4,5}, packed 3 bits per entry
+    constexpr uint32_t digitOf = 0u | (1u << 3) | (3u << 6) | (2u << 9) | (7u << 12) | (6u << 15) | (4u << 18) |
+                                 (5u << 21);
+    uint64_t key = 0;
+    for (int lvl = order - 1; lvl >= 0; --lvl)
+    {
+        unsigned bx = (px >> lvl) & 1u, by = (py >> lvl) & 1u, bz = (pz >> lvl) & 1u;
+        unsigned oct = (bx << 2) | (by << 1) | bz;
+        key          = (key << 3) | ((digitOf >> (3 * oct)) & 7u);
+        unsigned nby = by ^ 1u, nbz = bz ^ 1u;
+        px ^= 0u - (bx & (nby | bz));
+        py ^= 0u - ((bx & (by | bz)) | (by & nbz));
+        pz ^= 0u - ((bx & nby & nbz) | (by & nbz));
+        if (bz)
+        {
+            unsigned t = px;
+            px         = py;
+            py         = pz;
+            pz         = t;
+        }
+        else if (!by)
+        {
+            unsigned t = px;
+            px         = pz;
+            pz         = t;
+        }
+    }
+    return key;
+}
+
+__host__ __device__ inline uint64_t hilbert2(unsigned px, unsigned py, int order)
+{
+    uint64_t key = 0;
+    for (int lvl = order - 1; lvl >= 0; --lvl)
+    {
+        unsigned bx = (px >> lvl) & 1u, by = (py >> lvl) & 1u;
+        if (by == 0)
+        {
+            unsigned t = px;
+            px         = py ^ (0u - bx);
+            py         = t ^ (0u - bx);
+        }
+        key = 4 * key + 2 * bx + (bx ^ by);
+    }
+    return key;
+}
+
+//! descending sort of the axis bit depths with the axis permutation (hilbert.hpp:128-157)
+__host__ __device__ inline void sortAxes(unsigned b[3], int p[3])
+{
+    auto cswap = [&](int i, int j)
+    {
+        if (b[i] < b[j])
+        {
+            unsigned t = b[i];
+            b[i]       = b[j];
+            b[j]       = t;
+            int tp     = p[i];
+            p[i]       = p[j];
+            p[j]       = tp;
+        }
+    };
+    cswap(0, 1);
+    cswap(0, 2);
+    cswap(1, 2);
+}
+
+//! mixed-dimension Hilbert key for boxes whose axes have different bit depths (hilbert.hpp:117-244)
+__host__ __device__ inline uint64_t hilbertKey(unsigned px, unsigned py, unsigned pz, const unsigned bits[3])
+{
+    if (bits[0] == kMaxLevel && bits[1] == kMaxLevel && bits[2] == kMaxLevel) { return hilbert3(px, py, pz, kMaxLevel); }
+    unsigned b[3] = {bits[0], bits[1], bits[2]};
+    int p[3]      = {0, 1, 2};
+    sortAxes(b, p);
+    uint64_t c[3] = {px, py, pz};
+    uint64_t s[3] = {c[p[0]], c[p[1]], c[p[2]]};
+    uint64_t key  = 0;
+    if (b[0] > b[1])
+    {
+        int n = b[0] - b[1];
+        for (int i = 0; i < n; ++i)
+        {
+            unsigned bit = b[0] - i - 1;
+            key |= ((s[0] >> bit) & 1) << (3 * bit);
+        }
+        s[0] &= (uint64_t(1) << b[1]) - 1;
+        b[0] -= n;
+    }
+    if (b[1] > b[2])
+    {
+        int n          = b[1] - b[2];
+        uint64_t mask  = (uint64_t(1) << b[2]) - 1;
+        uint64_t key2d = hilbert2(unsigned(s[0] >> b[2]), unsigned(s[1] >> b[2]), n);
+        uint64_t lx = s[0] & mask, ly = s[1] & mask;
+        for (int lvl = n - 1; lvl >= 0; --lvl)
+        {
+            unsigned q  = unsigned(key2d >> (2 * lvl)) & 3u;
+            unsigned qx = (q >> 1) & 1u;
+            unsigned qy = qx ^ (q & 1u);
+            if (qy == 0)
+            {
+                uint64_t t = lx;
+                lx         = ly;
+                ly         = t;
+                if (qx == 1)
+                {
+                    lx = mask - lx;
+                    ly = mask - ly;
+                }
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            key |= ((key2d >> (2 * (n - 1 - i))) & 3) << (3 * (b[1] - 1 - i));
+        s[0] = lx;
+        s[1] = ly;
+        b[0] -= n;
+        b[1] -= n;
+    }
+    return key | hilbert3(unsigned(s[0]), unsigned(s[1]), unsigned(s[2]), b[2]);
+}
+
+__host__ __device__ inline void unhilbert3(uint64_t key, unsigned order, unsigned& ox, unsigned& oy, unsigned& oz)
+{
+    unsigned px = 0, py = 0, pz = 0;
+    for (unsigned lvl = 0; lvl < order; ++lvl)
+    {
+        unsigned oct = unsigned(key >> (3 * lvl)) & 7u;
+        unsigned bx = oct >> 2, by = (oct >> 1) & 1u, bz = oct & 1u;
+        if (by ^ bz)
+        {
+            unsigned t = px;
+            px         = pz;
+            pz         = py;
+            py         = t;
+        }
+        else if ((!bx && !by && !bz) || (bx && by && bz))
+        {
+            unsigned t = px;
+            px         = pz;
+            pz         = t;
+        }
+        unsigned mask = (1u << lvl) - 1;
+        unsigned nbx = bx ^ 1u, nby = by ^ 1u, nbz = bz ^ 1u;
+        px ^= mask & (0u - (bx & (by | bz)));
+        py ^= mask & (0u - ((bx & (nby | nbz)) | (nbx & by & bz)));
+        pz ^= mask & (0u - ((bx & nby & nbz) | (by & bz)));
+        px |= bx << lvl;
+        py |= (bx ^ by) << lvl;
+        pz |= (by ^ bz) << lvl;
+    }
+    ox = px;
+    oy = py;
+    oz = pz;
+}
+
+__host__ __device__ inline void unhilbert2(uint64_t key, unsigned order, unsigned& ox, unsigned& oy)
+{
+    unsigned x = 0, y = 0;
+    for (unsigned lvl = 0; lvl < 2 * order; lvl += 2)
+    {
+        unsigned sa = unsigned(key >> (lvl + 1)) & 1u;
+        unsigned sb = unsigned(key >> lvl) & 1u;
+        if ((sa ^ sb) == 0)
+        {
+            unsigned t = x;
+            x          = y ^ (0u - sa);
+            y          = t ^ (0u - sa);
+        }
+        x = (x >> 1) | (sa << 31);
+        y = (y >> 1) | ((sa ^ sb) << 31);
+    }
+    ox = x >> (32 - order);
+    oy = y >> (32 - order);
+}
+
+//! inverse of hilbertKey (hilbert.hpp:362-471)
+__host__ __device__ inline void unhilbertKey(uint64_t key, const unsigned bits[3], unsigned out[3])
+{
+    unsigned b[3] = {bits[0], bits[1], bits[2]};
+    int p[3]      = {0, 1, 2};
+    sortAxes(b, p);
+    uint64_t c[3] = {0, 0, 0};
+    if (b[0] > b[1])
+    {
+        int n = b[0] - b[1];
+        for (int i = 0; i < n; ++i)
+        {
+            unsigned bit = b[0] - 1 - i;
+            c[0] |= ((key >> (3 * bit)) & 1) << bit;
+        }
+        key &= (uint64_t(1) << (3 * b[1])) - 1;
+    }
+    uint64_t key2d = 0;
+    if (b[1] > b[2])
+    {
+        int n = b[1] - b[2];
+        for (int i = 0; i < n; ++i)
+            key2d |= ((key >> (3 * (b[1] - 1 - i))) & 3) << (2 * (n - 1 - i));
+        unsigned ux, uy;
+        unhilbert2(key2d, n, ux, uy);
+        uint64_t nm = (uint64_t(1) << n) - 1;
+        c[0] |= (uint64_t(ux) & nm) << b[2];
+        c[1] |= (uint64_t(uy) & nm) << b[2];
+        key &= (uint64_t(1) << (3 * b[2])) - 1;
+    }
+    unsigned shift = kMaxLevel - b[2];
+    unsigned ux, uy, uz;
+    unhilbert3(key << (3 * shift), kMaxLevel, ux, uy, uz);
+    uint64_t x3 = ux >> shift, y3 = uy >> shift, z3 = uz >> shift;
+    uint64_t maxc = (uint64_t(1) << b[2]) - 1;
+    int n2        = b[1] > b[2] ? int(b[1] - b[2]) : 0;
+    for (int i = 0; i < n2; ++i)
+    {
+        unsigned q  = unsigned(key2d >> (2 * i)) & 3u;
+        unsigned qx = (q >> 1) & 1u;
+        unsigned qy = qx ^ (q & 1u);
+        if (qy == 0)
+        {
+            uint64_t t = x3;
+            x3         = y3;
+            y3         = t;
+            if (qx == 1)
+            {
+                x3 = maxc - x3;
+                y3 = maxc - y3;
+            }
+        }
+    }
+    c[0] |= x3;
+    c[1] |= y3;
+    c[2] |= z3;
+    out[p[0]] = unsigned(c[0]);
+    out[p[1]] = unsigned(c[1]);
+    out[p[2]] = unsigned(c[2]);
+}
+
+//! digits above a short axis' depth may only use the axes present there (hilbert.hpp:516-552)
+__host__ __device__ inline bool validMixDKey(uint64_t key, const unsigned bits[3])
+{
+    unsigned lo = bits[0], mid = bits[1], hi = bits[2];
+    if (lo > mid) { unsigned t = lo; lo = mid; mid = t; }
+    if (lo > hi) { unsigned t = lo; lo = hi; hi = t; }
+    if (mid > hi) { unsigned t = mid; mid = hi; hi = t; }
+    for (unsigned i = lo + 1; i <= unsigned(kMaxLevel); ++i)
+    {
+        unsigned d = unsigned(key >> (3 * (i - 1))) & 7u;
+        if (i <= mid) { if (d > 3u) return false; }
+        else if (i <= hi) { if (d > 1u) return false; }
+    }
+    return true;
+}
+
+// ------------------------------------------------------------------------------------------------ exact float ops
+
+template<class T>
+struct Fp;
+
+template<>
+struct Fp<float>
+{
+    __host__ __device__ static float mul(float a, float b)
+    {
+#ifdef __CUDA_ARCH__
+        return __fmul_rn(a, b);
+#else
+        return a * b;
+#endif
+    }
+    __host__ __device__ static float add(float a, float b)
+    {
+#ifdef __CUDA_ARCH__
+        return __fadd_rn(a, b);
+#else
+        return a + b;
+#endif
+    }
+    __host__ __device__ static float sub(float a, float b)
+    {
+#ifdef __CUDA_ARCH__
+        return __fsub_rn(a, b);
+#else
+        return a - b;
+#endif
+    }
+};
+
+template<>
+struct Fp<double>
+{
+    __host__ __device__ static double mul(double a, double b)
+    {
+#ifdef __CUDA_ARCH__
+        return __dmul_rn(a, b);
+#else
+        return a * b;
+#endif
+    }
+    __host__ __device__ static double add(double a, double b)
+    {
+#ifdef __CUDA_ARCH__
+        return __dadd_rn(a, b);
+#else
+        return a + b;
+#endif
+    }
+    __host__ __device__ static double sub(double a, double b)
+    {
+#ifdef __CUDA_ARCH__
+        return __dsub_rn(a, b);
+#else
+        return a - b;
+#endif
+    }
+};
+
+//! x*x + (y*y + z*z), each product and sum rounded once (the reference's right-folded norm2)
+template<class T>
+__host__ __device__ inline T norm2Exact(T x, T y, T z)
+{
+    using F = Fp<T>;
+    return F::add(F::mul(x, x), F::add(F::mul(y, y), F::mul(z, z)));
+}
+
+// ------------------------------------------------------------------------------------------------ coordinate box
+
+/*! @brief the coordinate box in the form the kernels use (cstone/sfc/box.hpp:99-214)
+ *
+ * lo/len/inv follow Box<T>'s constructor; bits are the per-axis key depths of the mixed-dimension curve.
+ */
+template<class T>
+struct DevBox
+{
+    T lo[3];
+    T len[3];
+    T inv[3];
+    unsigned bits[3];
+    int periodic;
+};
+
+template<class T>
+inline DevBox<T> makeDevBox(const T* limits6, int periodic)
+{
+    DevBox<T> b;
+    T maxDim = T(0);
+    for (int d = 0; d < 3; ++d)
+    {
+        b.lo[d]  = limits6[2 * d];
+        b.len[d] = limits6[2 * d + 1] - limits6[2 * d];
+        b.inv[d] = T(1.) / (limits6[2 * d + 1] - limits6[2 * d]);
+    }
+    maxDim       = b.len[0] > b.len[1] ? b.len[0] : b.len[1];
+    maxDim       = maxDim > b.len[2] ? maxDim : b.len[2];
+    const T bias = T(0.5849625007211563); // 1 - log2(1 / 0.75): box.hpp:193
+    for (int d = 0; d < 3; ++d)
+    {
+        T ratio   = maxDim / b.len[d];
+        T l2      = sizeof(T) == 4 ? T(log2f(float(ratio))) : T(log2(double(ratio)));
+        b.bits[d] = kMaxLevel - static_cast<unsigned>(floor(l2 + bias));
+    }
+    b.periodic = periodic;
+    return b;
+}
+
+//! integer cell of x along one axis: floor(x*m) - floor(xmin*m) with exact fractional-part comparison (sfc.hpp:153-159)
+template<class T>
+__host__ __device__ inline int cellIndex(T x, T xmin, T m)
+{
+    using F = Fp<T>;
+    T a = F::mul(x, m), b = F::mul(xmin, m);
+    T fa = floor(a), fb = floor(b);
+    return int(F::sub(fa, fb)) - int(F::sub(a, fa) < F::sub(b, fb));
+}
+
+//! SFC key of a point (sfc.hpp:161-207); coordinates outside the box are clamped into it
+template<class T>
+__host__ __device__ inline uint64_t pointKey(T x, T y, T z, const DevBox<T>& box)
+{
+    const T v[3] = {x, y, z};
+    unsigned ic[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        T m   = Fp<T>::mul(T(1u << box.bits[d]), box.inv[d]);
+        int c = cellIndex(v[d], box.lo[d], m);
+        int cm = int((1u << box.bits[d]) - 1);
+        c      = c < cm ? c : cm;
+        ic[d]  = unsigned(c > 0 ? c : 0);
+    }
+    return hilbertKey(ic[0], ic[1], ic[2], box.bits);
+}
+
+//! geometric centre and half size of the node with start key @p key on @p level (hilbert.hpp:562-585, box.hpp:357-381)
+template<class T>
+__host__ __device__ inline void nodeGeometry(uint64_t key, unsigned level, const DevBox<T>& box, T center[3], T size[3])
+{
+    using F = Fp<T>;
+    if (!validMixDKey(key, box.bits))
+    {
+        for (int d = 0; d < 3; ++d)
+        {
+            center[d] = box.lo[d];
+            size[d]   = T(0);
+        }
+        return;
+    }
+    unsigned fromRight = kMaxLevel - level;
+    unsigned p[3];
+    unhilbertKey(key, box.bits, p);
+    const T unit = T(1.) / T(1u << kMaxLevel);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        unsigned len = 1u << (box.bits[d] < fromRight ? box.bits[d] : fromRight);
+        int i0       = int(p[d] & ~(len - 1));
+        int i1       = i0 + int(len);
+        T half       = F::mul(F::mul(F::mul(T(0.5), unit), box.len[d]), T(1u << (kMaxLevel - box.bits[d])));
+        center[d]    = F::add(box.lo[d], F::mul(T(i1 + i0), half));
+        size[d]      = F::mul(T(i1 - i0), half);
+    }
+}
+
+//! squared MAC radius (2*max edge/theta + |com - geometric centre|)^2 of a node (macs.hpp:64-82)
+template<class T>
+__host__ __device__ inline T vecMacR2(uint64_t prefix, const T com[3], float invTheta, const DevBox<T>& box)
+{
+    using F      = Fp<T>;
+    uint64_t key = prefixStart(prefix);
+    unsigned lvl = unsigned(prefixLength(prefix)) / 3;
+    T gc[3], gs[3];
+    nodeGeometry(key, lvl, box, gc, gs);
+    T s   = sqrt(norm2Exact(F::sub(com[0], gc[0]), F::sub(com[1], gc[1]), F::sub(com[2], gc[2])));
+    T mx  = gs[0] > gs[1] ? gs[0] : gs[1];
+    mx    = mx > gs[2] ? mx : gs[2];
+    T l   = F::mul(T(2.0), mx);
+    T mac = F::add(F::mul(l, T(invTheta)), s);
+    return F::mul(mac, mac);
+}
+
+// ------------------------------------------------------------------------------------------------ warp helpers
+
+__device__ inline unsigned laneId() { return threadIdx.x & (kWarp - 1); }
+
+__device__ inline unsigned lanemaskLt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+template<class T>
+__device__ inline T warpMin(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v   = w < v ? w : v;
+    }
+    return v;
+}
+
+template<class T>
+__device__ inline T warpMax(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v   = w > v ? w : v;
+    }
+    return v;
+}
+
+template<class T>
+__device__ inline T warpSum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+//! inclusive warp scan of ints
+__device__ inline int warpInclusiveScan(int v)
+{
+    unsigned lane = laneId();
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1)
+    {
+        int w = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= unsigned(o)) v += w;
+    }
+    return v;
+}
+
+} // namespace ryo

@@ -1,0 +1,248 @@
+/*
+ * ryoanji-b200: Ewald correction for periodic boxes (root-multipole form).
+ *
+ * Reference: ryoanji/src/ryoanji/nbody/ewald.hpp:90-389 and ryoanji/src/ryoanji/interface/ewald.cu:31-99. The tree
+ * traversal covers the (2 numReplicaShells + 1)^3 replica boxes; the correction adds, per target, the real-space
+ * images of the root multipole with erfc weights (-erf inside the replicated region) and the reciprocal-space sum.
+ *
+ * B200 form: one warp per target group, lanes over its targets. Real space runs in float. The reciprocal sum runs in
+ * double: per target the three phase factors exp(2 pi i dx_d / L) are computed once and every wave vector's
+ * exp(i k.r) is a product of their integer powers, so no trigonometric call is made per wave vector.
+ */
+#include <cmath>
+
+#include "internal.hpp"
+
+namespace ryo
+{
+
+struct EwaldKernelParams
+{
+    float mroot[8];
+    float center[3];
+    double centerD[3];
+    float L, lCut2, alpha, alpha2, k1, ka, smallR2;
+    int replicaShells, ewaldShells;
+    int numK;
+    double twoPiOverL;
+    signed char h[343][3];
+    double fc[343];
+    double fs[343];
+};
+
+//! ewaldEvalMultipoleComplete (ewald.hpp:90-115)
+template<class T>
+__host__ __device__ inline void ewaldEval(T acc[4], const T r[3], const T g[6], const T* M)
+{
+    T m   = M[0];
+    T qxx = (M[1] + M[7]) / T(3), qyy = (M[4] + M[7]) / T(3), qzz = (M[6] + M[7]) / T(3);
+    T qxy = M[2] / T(3), qxz = M[3] / T(3), qyz = M[5] / T(3);
+    T Qr[3] = {r[0] * qxx + r[1] * qxy + r[2] * qxz, r[0] * qxy + r[1] * qyy + r[2] * qyz,
+               r[0] * qxz + r[1] * qyz + r[2] * qzz};
+    T rQr = T(0.5) * (r[0] * Qr[0] + r[1] * Qr[1] + r[2] * Qr[2]);
+    T Qtr = T(0.5) * M[7];
+    T u   = -g[0] * m + g[1] * Qtr - g[2] * rQr;
+    T f   = g[1] * m - g[2] * Qtr + g[3] * rQr;
+    acc[0] += u;
+    for (int d = 0; d < 3; ++d)
+        acc[d + 1] += g[2] * Qr[d] - r[d] * f;
+}
+
+EwaldHost ewaldSetup(const double* mroot, const double* center, int replicaShells, double L, double lCut, double hCut,
+                     double alphaScale, double smallR)
+{
+    EwaldHost e{};
+    for (int i = 0; i < 8; ++i)
+        e.mroot[i] = mroot[i];
+    for (int i = 0; i < 3; ++i)
+        e.center[i] = center[i];
+    if (lCut == 0 && hCut == 0 && alphaScale == 0) replicaShells = 0;
+    e.replicaShells = replicaShells;
+    e.ewaldShells   = std::max(int(std::ceil(lCut)), replicaShells);
+    e.L             = L;
+    e.lCut          = lCut;
+    e.hCut          = hCut;
+    e.alphaScale    = alphaScale;
+    e.smallR        = smallR;
+    e.numK          = 0;
+    if (e.ewaldShells == 0) return e;
+    // ewaldInitParameters (ewald.hpp:133-198)
+    int hReps    = int(std::ceil(hCut));
+    double alpha = alphaScale / L;
+    double k4    = M_PI * M_PI / (alpha * alpha * L * L);
+    for (int hx = -hReps; hx <= hReps; ++hx)
+        for (int hy = -hReps; hy <= hReps; ++hy)
+            for (int hz = -hReps; hz <= hReps; ++hz)
+            {
+                double hr[3] = {double(hx), double(hy), double(hz)};
+                double h2    = hr[0] * hr[0] + (hr[1] * hr[1] + hr[2] * hr[2]);
+                if (h2 == 0 || h2 > hCut * hCut) continue;
+                double g0 = std::exp(-k4 * h2) / (M_PI * h2 * L);
+                double g1 = 2 * M_PI / L * g0;
+                double g2 = -2 * M_PI / L * g1;
+                double g3 = 2 * M_PI / L * g2;
+                double g4 = -2 * M_PI / L * g3;
+                double g5 = 2 * M_PI / L * g4;
+                double gc[6] = {g0, 0.0, g2, 0.0, g4, 0.0};
+                double gs[6] = {0.0, g1, 0.0, g3, 0.0, g5};
+                double a1[4] = {0, 0, 0, 0}, a2[4] = {0, 0, 0, 0};
+                ewaldEval<double>(a1, hr, gc, mroot);
+                ewaldEval<double>(a2, hr, gs, mroot);
+                double* k = e.kdata + 5 * e.numK;
+                k[0]      = hx;
+                k[1]      = hy;
+                k[2]      = hz;
+                k[3]      = a1[0];
+                k[4]      = a2[0];
+                e.numK++;
+            }
+    return e;
+}
+
+__device__ inline double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+__global__ void ewaldKernel(const __grid_constant__ EwaldKernelParams E, const uint32_t* __restrict__ groupStart,
+                            const uint32_t* __restrict__ groupEnd, uint32_t numGroups, const float* __restrict__ x,
+                            const float* __restrict__ y, const float* __restrict__ z, const float* __restrict__ m,
+                            float G, float* ugrav, float* ax, float* ay, float* az, double* potential)
+{
+    int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+    int lane       = laneId();
+    double upot    = 0.0;
+    if (warpGlobal < int(numGroups))
+    {
+        uint32_t b = groupStart[warpGlobal], e = groupEnd[warpGlobal];
+        for (uint32_t i = b + lane; i < e; i += kWarp)
+        {
+            float pos[3]  = {x[i], y[i], z[i]};
+            float acc[4]  = {E.k1 * E.mroot[0], 0.f, 0.f, 0.f};
+            float r[3]    = {pos[0] - E.center[0], pos[1] - E.center[1], pos[2] - E.center[2]};
+            int S         = E.ewaldShells, Rs = E.replicaShells;
+            // real space (ewald.hpp:200-301)
+            for (int ix = -S; ix <= S; ++ix)
+                for (int iy = -S; iy <= S; ++iy)
+                    for (int iz = -S; iz <= S; ++iz)
+                    {
+                        bool pre  = (-Rs <= ix && ix <= Rs) && (-Rs <= iy && iy <= Rs) && (-Rs <= iz && iz <= Rs);
+                        float R[3] = {r[0] + ix * E.L, r[1] + iy * E.L, r[2] + iz * E.L};
+                        float R2   = R[0] * R[0] + (R[1] * R[1] + R[2] * R[2]);
+                        if (R2 > E.lCut2 && !pre) continue;
+                        float g[6];
+                        if (R2 < E.smallR2 && E.ka > 0.f)
+                        {
+                            float c0 = E.ka, a2 = R2 * E.alpha2;
+                            g[0] = c0 * (a2 / 3.f - 1.f);
+                            c0 *= 2 * E.alpha2;
+                            g[1] = c0 * (a2 / 5.f - 1.f / 3.f);
+                            c0 *= 2 * E.alpha2;
+                            g[2] = c0 * (a2 / 7.f - 1.f / 5.f);
+                            c0 *= 2 * E.alpha2;
+                            g[3] = c0 * (a2 / 9.f - 1.f / 7.f);
+                            c0 *= 2 * E.alpha2;
+                            g[4] = c0 * (a2 / 11.f - 1.f / 9.f);
+                            c0 *= 2 * E.alpha2;
+                            g[5] = c0 * (a2 / 13.f - 1.f / 11.f);
+                        }
+                        else
+                        {
+                            float Rm = sqrtf(R2), iR = 1.f / Rm, iR2 = iR * iR;
+                            float a  = expf(-R2 * E.alpha2) * E.ka * iR2;
+                            float an = 1.f;
+                            float fn = pre ? -erff(E.alpha * Rm) : erfcf(E.alpha * Rm);
+                            g[0] = fn * iR;
+                            g[1] = g[0] * iR2 + a;
+                            an *= 2 * E.alpha2;
+                            g[2] = 3 * g[1] * iR2 + an * a;
+                            an *= 2 * E.alpha2;
+                            g[3] = 5 * g[2] * iR2 + an * a;
+                            an *= 2 * E.alpha2;
+                            g[4] = 7 * g[3] * iR2 + an * a;
+                            an *= 2 * E.alpha2;
+                            g[5] = 9 * g[4] * iR2 + an * a;
+                        }
+                        ewaldEval<float>(acc, R, g, E.mroot);
+                    }
+            // reciprocal space (ewald.hpp:303-327), double, exp(i k.r) from powers of the per-axis phases
+            double dr[3] = {double(pos[0]) - E.centerD[0], double(pos[1]) - E.centerD[1],
+                            double(pos[2]) - E.centerD[2]};
+            double2 pw[3][7];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+            {
+                double sn, cs;
+                sincos(E.twoPiOverL * dr[d], &sn, &cs);
+                double2 e1 = make_double2(cs, sn), e1c = make_double2(cs, -sn);
+                pw[d][3]   = make_double2(1.0, 0.0);
+                pw[d][4]   = e1;
+                pw[d][2]   = e1c;
+                pw[d][5]   = cmul(e1, e1);
+                pw[d][1]   = cmul(e1c, e1c);
+                pw[d][6]   = cmul(pw[d][5], e1);
+                pw[d][0]   = cmul(pw[d][1], e1c);
+            }
+            double kp = 0.0, ka3[3] = {0.0, 0.0, 0.0};
+            for (int q = 0; q < E.numK; ++q)
+            {
+                int hx = E.h[q][0], hy = E.h[q][1], hz = E.h[q][2];
+                double2 w = cmul(cmul(pw[0][hx + 3], pw[1][hy + 3]), pw[2][hz + 3]);
+                double c = w.x, s = w.y;
+                double sum  = E.fc[q] * c + E.fs[q] * s;
+                double diff = E.fc[q] * s - E.fs[q] * c;
+                kp -= sum;
+                ka3[0] += diff * (E.twoPiOverL * hx);
+                ka3[1] += diff * (E.twoPiOverL * hy);
+                ka3[2] += diff * (E.twoPiOverL * hz);
+            }
+            double phi = double(acc[0]) + kp;
+            double mi  = m[i];
+            upot += phi * mi;
+            if (ugrav) ugrav[i] += float(G * phi * mi);
+            ax[i] += float(G * (double(acc[1]) + ka3[0]));
+            ay[i] += float(G * (double(acc[2]) + ka3[1]));
+            az[i] += float(G * (double(acc[3]) + ka3[2]));
+        }
+    }
+    upot = warpSum(upot);
+    if (lane == 0 && upot != 0.0) atomicAdd(potential, upot);
+}
+
+void launchEwaldGroups(const EwaldHost& h, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
+                       const float* x, const float* y, const float* z, const float* m, float G, float* ugrav,
+                       float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s)
+{
+    if (h.ewaldShells == 0 || numGroups == 0) return;
+    EwaldKernelParams E{};
+    for (int i = 0; i < 8; ++i)
+        E.mroot[i] = float(h.mroot[i]);
+    for (int i = 0; i < 3; ++i)
+    {
+        E.center[i]  = float(h.center[i]);
+        E.centerD[i] = h.center[i];
+    }
+    double alpha    = h.alphaScale / h.L;
+    E.L             = float(h.L);
+    E.lCut2         = float(h.lCut * h.lCut * h.L * h.L);
+    E.alpha         = float(alpha);
+    E.alpha2        = float(alpha * alpha);
+    E.k1            = float(M_PI / (alpha * alpha * h.L * h.L * h.L));
+    E.ka            = float(2.0 * alpha / std::sqrt(M_PI));
+    E.smallR2       = float(h.smallR * h.L * h.L);
+    E.replicaShells = h.replicaShells;
+    E.ewaldShells   = h.ewaldShells;
+    E.numK          = h.numK;
+    E.twoPiOverL    = 2 * M_PI / h.L;
+    for (int q = 0; q < h.numK; ++q)
+    {
+        for (int d = 0; d < 3; ++d)
+            E.h[q][d] = (signed char)h.kdata[5 * q + d];
+        E.fc[q] = h.kdata[5 * q + 3];
+        E.fs[q] = h.kdata[5 * q + 4];
+    }
+    unsigned threads = 128;
+    unsigned blocks  = ceilDiv(size_t(numGroups) * kWarp, threads);
+    ewaldKernel<<<blocks, threads, 0, s>>>(E, groupStart, groupEnd, numGroups, x, y, z, m, G, ugrav, ax, ay, az,
+                                           potentialOut);
+    RYO_LAUNCH_CHECK();
+}
+
+} // namespace ryo

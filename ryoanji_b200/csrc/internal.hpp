@@ -1,0 +1,231 @@
+/*
+ * ryoanji-b200: host-side internals shared by the translation units (context, scratch memory, launchers).
+ */
+#pragma once
+
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "common.cuh"
+
+namespace ryo
+{
+
+//! per-context device control block: work counters, statistics and error flags of the last calls
+struct Control
+{
+    unsigned int workCounter;  // traversal work queue head
+    unsigned int failedCount;  // groups that overflowed the traversal stack in the current pass
+    unsigned int error;        // non-zero: a bounded device wait gave up
+    unsigned int tileCounter;  // onesweep tile ticket of the current pass
+    unsigned long long stats[5]; // sumP2P, maxP2P, sumM2P, maxM2P, maxStack
+    double potential;          // sum m * phi of the traversal (no G)
+    double ewaldPotential;     // sum m * phi of the Ewald correction (no G)
+    unsigned int counters[8];  // scratch counters for other kernels
+};
+
+enum BhStat
+{
+    kSumP2P = 0,
+    kMaxP2P,
+    kSumM2P,
+    kMaxM2P,
+    kMaxStack
+};
+
+} // namespace ryo
+
+struct ryo_ctx
+{
+    int device   = 0;
+    int smCount  = 148;
+    std::string lastError;
+    ryo::Control* ctl = nullptr; // device
+    unsigned long long hostStats[5] = {0, 0, 0, 0, 0};
+    uint64_t retries                = 0;
+    ryo_solve_arrays lastSolve      = {};
+
+    struct Buffer
+    {
+        void* ptr    = nullptr;
+        size_t bytes = 0;
+    };
+    std::unordered_map<std::string, Buffer> buffers;
+
+    //! grow-only named scratch buffer of at least @p count elements
+    template<class T>
+    T* scratch(const std::string& name, size_t count, cudaStream_t s)
+    {
+        size_t bytes = count * sizeof(T);
+        if (bytes == 0) bytes = 256;
+        Buffer& b = buffers[name];
+        if (b.bytes < bytes)
+        {
+            // growth is rare: wait for work that may still use the old buffer, then reallocate
+            if (b.ptr)
+            {
+                RYO_CUDA(cudaStreamSynchronize(s));
+                RYO_CUDA(cudaFree(b.ptr));
+                b.ptr   = nullptr;
+                b.bytes = 0;
+            }
+            size_t grow = bytes + bytes / 8;
+            RYO_CUDA(cudaMalloc(&b.ptr, grow));
+            b.bytes = grow;
+        }
+        return static_cast<T*>(b.ptr);
+    }
+
+    void releaseAll()
+    {
+        for (auto& kv : buffers)
+            if (kv.second.ptr) cudaFree(kv.second.ptr);
+        buffers.clear();
+    }
+};
+
+namespace ryo
+{
+
+// ---------------------------------------------------------------------------------------------------- sfc.cu
+template<class T>
+void launchKeys(const T* x, const T* y, const T* z, uint64_t* keys, size_t n, const DevBox<T>& box, bool keepRemoved,
+                cudaStream_t s);
+void launchBoundingBox(const float* x, const float* y, const float* z, size_t n, double* minmax6, cudaStream_t s);
+void launchSequence(uint32_t* v, size_t n, uint32_t first, cudaStream_t s);
+//! out[i] = in[order[i]] for float arrays
+void launchGather(const uint32_t* order, const float* in, float* out, size_t n, cudaStream_t s);
+template<class T>
+void launchGatherT(const uint32_t* order, const T* in, T* out, size_t n, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- scan / sort
+//! out[i] = sum(in[0:i]) for i in [0, n]; out has n + 1 entries (out[n] = total); in-place allowed
+void exclusiveScanU32(ryo_ctx* ctx, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s);
+
+size_t sortTempBytes(size_t n);
+/*! stable LSD sort of (keys, values) on bits [beginBit, endBit). Ping-pongs between (keys, values) and
+ *  (keysAlt, valuesAlt), all four buffers of n elements; returns true if the result is in the Alt buffers.
+ *  iotaValues: ignore the input values and sort (key, input index) pairs. */
+bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_t* valuesAlt, size_t n, int beginBit,
+                    int endBit, void* tmp, size_t tmpBytes, unsigned int* errorFlag, cudaStream_t s,
+                    bool iotaValues = false);
+
+// ---------------------------------------------------------------------------------------------------- octree.cu
+//! cornerstone leaves of sorted keys; returns numLeaves (host), writes only if numLeaves <= capacity
+int buildLeaves(ryo_ctx* ctx, const uint64_t* sortedKeys, size_t n, unsigned bucket, uint64_t* leaves,
+                uint32_t* counts, uint32_t* layout, int capacity, cudaStream_t s);
+
+struct OctreeArrays
+{
+    uint64_t* prefixes;
+    int* childOffsets;
+    int* parents;
+    int* internalToLeaf;
+    int* leafToInternal;
+    int* d_levelRange; // 23, device
+};
+//! internal octree of a leaf array; fills hostLevelRange[23]
+void linkOctree(ryo_ctx* ctx, const uint64_t* leaves, int numLeaves, const OctreeArrays& out, int* hostLevelRange,
+                cudaStream_t s);
+void launchFixedGroups(uint32_t first, uint32_t last, unsigned groupSize, uint32_t* groups, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- upsweep.cu
+void launchLeafCenters(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
+                       int numLeaves, const uint32_t* layout, float4* centers, cudaStream_t s);
+void launchUpsweepCenters(int first, int last, const int* childOffsets, float4* centers, cudaStream_t s);
+void launchLeafMultipoles(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
+                          int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
+                          cudaStream_t s);
+void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const float4* centers, float* multipoles,
+                             cudaStream_t s);
+void launchSetMac(const uint64_t* prefixes, int numNodes, float4* centers, float invTheta, const DevBox<float>& box,
+                  cudaStream_t s);
+
+//! node record used by the traversal: 64 bytes, one cache line half per node
+struct alignas(16) NodeRecord
+{
+    float4 center; // x, y, z, mac^2
+    float4 q0;     // mass, qxx, qxy, qxz
+    float4 q1;     // qyy, qyz, qzz, trace
+    int4 link;     // child (global node index, 0 = leaf), first body, body count, unused
+};
+
+/*! fused upsweep of the solver path: per leaf FP64 centre of mass and P2M in one pass over the bodies, then M2M
+ *  bottom-up by last-arriving child, MAC radius, and the traversal node records. Also writes the reference-layout
+ *  centers (4 floats) and multipoles (8 floats) if not null. */
+void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
+                        const int* leafToInternal, const int* childOffsets, const int* parents,
+                        const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
+                        float4* centers, float* multipoles, double* rootCenterMultipole, cudaStream_t s);
+
+//! pack reference-layout tree arrays into node records (for the reference-signature traverse)
+void launchPackNodes(int numNodes, const float4* centers, const float* multipoles, const int* childOffsets,
+                     const int* internalToLeaf, const uint32_t* layout, NodeRecord* records, cudaStream_t s);
+void launchPackBodies(const float* x, const float* y, const float* z, const float* w, size_t n, float4* out,
+                      cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- traverse.cu
+struct TraverseLaunch
+{
+    const uint32_t* groupStart;
+    const uint32_t* groupEnd;
+    int numGroups;
+    int initNode;
+    int numNodes; // 1 means the root is the only (leaf) node; any larger value otherwise
+    // packed form (solver path): node records and (x,y,z,h) targets / (x,y,z,m) sources
+    const NodeRecord* nodes;
+    const float4* tgtXYZH;
+    const float* tgtM;
+    const float4* srcXYZM;
+    const float* srcH;
+    // reference form, used when nodes == nullptr
+    const float4* centers;
+    const float* multipoles;
+    const int* childOffsets;
+    const int* internalToLeaf;
+    const uint32_t* layout;
+    const float *xt, *yt, *zt, *mt, *ht;
+    const float *xs, *ys, *zs, *ms, *hs;
+    float G;
+    int numShells;
+    float boxL[3];
+    float* p;
+    float* ax;
+    float* ay;
+    float* az;
+    uint32_t* groupM2P;
+    uint32_t* groupP2P;
+    uint32_t* failedGroups;
+    uint32_t failedCapacity;
+    int stackCapacity;
+    Control* ctl;
+};
+void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s);
+void launchTraversalReset(Control* ctl, bool resetStats, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- ewald.cu
+struct EwaldHost
+{
+    double mroot[8];
+    double center[3];
+    int replicaShells, ewaldShells;
+    double L, lCut, hCut, alphaScale, smallR;
+    int numK;
+    double kdata[343 * 5]; // per k vector: hs[3], fc, fs
+};
+EwaldHost ewaldSetup(const double* mroot, const double* center, int replicaShells, double L, double lCut,
+                     double hCut, double alphaScale, double smallR);
+void launchEwaldGroups(const EwaldHost& e, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
+                       const float* x, const float* y, const float* z, const float* m, float G, float* ugrav,
+                       float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- direct.cu
+template<class T>
+void launchDirect(size_t first, size_t last, size_t numBodies, const T* boxL, int numShells, const T* x, const T* y,
+                  const T* z, const T* m, const T* h, T* p, T* ax, T* ay, T* az, cudaStream_t s);
+void launchDirectTargets(const int64_t* targets, size_t numTargets, const float* x, const float* y, const float* z,
+                         const float* m, const float* h, size_t numBodies, double G, const double* boxL,
+                         int numShells, double* pot, double* ax, double* ay, double* az, cudaStream_t s);
+
+} // namespace ryo

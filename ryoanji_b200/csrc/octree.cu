@@ -1,0 +1,343 @@
+/*
+ * ryoanji-b200: cornerstone leaf array, internal octree links and fixed target groups.
+ *
+ * Leaves. The reference converges a leaf array by repeated split/merge rounds with three host synchronisations
+ * each (cstone/include/cstone/tree/csarray.hpp:266-440, csarray_gpu.cu:86-231). Its fixed point is unique: a node
+ * is internal exactly when it holds more than bucketSize particles (and lies above level 21), and every child of
+ * an internal node that is not itself internal is a leaf. Both facts follow from the rebalance rules (a node with
+ * too many particles always splits; eight sibling leaves whose total fits always merge), so the fixed point can be
+ * built directly from the sorted keys in one pass:
+ *   - a node holds more than B particles iff it contains some window k[j], k[j+B] of B+1 consecutive sorted keys,
+ *     so the deepest internal node containing particle i is the deepest common node of the windows covering i;
+ *   - particle i lies in the child of that node containing it: the non-empty leaves;
+ *   - the empty leaves are the minimal aligned node sequence filling the key gaps between non-empty leaves.
+ * The result is bit-identical to the reference's converged leaves and counts.
+ *
+ * Links. The internal nodes and the level-sorted node order follow cstone/include/cstone/tree/octree.hpp:40-196
+ * (the node numbering is part of the reference's output: internalToLeaf/leafToInternal are compared bit for bit).
+ */
+#include "internal.hpp"
+
+namespace ryo
+{
+
+constexpr int kLeafBlock = 256;
+
+/*! level of the leaf that contains each sorted particle
+ *
+ * w[j] = min(commonLevel(k[j], k[j+B]), 20) is the level of the deepest internal node holding the window j; the
+ * particle's leaf is one level below the deepest window level among the windows that contain it.
+ */
+__global__ void __launch_bounds__(kLeafBlock) leafLevels(const uint64_t* __restrict__ keys, uint32_t n,
+                                                         uint32_t bucket, uint8_t* __restrict__ level)
+{
+    extern __shared__ unsigned char smem[];
+    uint8_t* w = smem; // window levels for j in [i0 - B, i0 + blockDim)
+    const uint32_t i0     = blockIdx.x * kLeafBlock;
+    const int64_t jFirst  = int64_t(i0) - int64_t(bucket);
+    const uint32_t span   = kLeafBlock + bucket;
+    const int64_t numWin  = int64_t(n) - int64_t(bucket); // windows j in [0, n - B)
+    for (uint32_t t = threadIdx.x; t < span; t += kLeafBlock)
+    {
+        int64_t j = jFirst + t;
+        uint8_t v = 0;
+        if (j >= 0 && j < numWin)
+        {
+            int cb  = commonBits(keys[j], keys[j + bucket]);
+            int lvl = cb / 3;
+            v       = uint8_t(lvl < kMaxLevel - 1 ? lvl : kMaxLevel - 1);
+        }
+        w[t] = v;
+    }
+    __syncthreads();
+    uint32_t i = i0 + threadIdx.x;
+    if (i >= n) return;
+    // windows covering i: j in [max(0, i - B), min(i, n - B - 1)], at w[j - jFirst]
+    int64_t jlo = int64_t(i) - bucket;
+    if (jlo < 0) jlo = 0;
+    int64_t jhi = int64_t(i) < numWin - 1 ? int64_t(i) : numWin - 1;
+    uint8_t mx  = 0;
+    for (int64_t j = jlo; j <= jhi; ++j)
+    {
+        uint8_t v = w[j - jFirst];
+        mx        = v > mx ? v : mx;
+    }
+    level[i] = uint8_t(mx + 1);
+}
+
+//! 1 where a particle starts a new non-empty leaf
+__global__ void leafHeads(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ level, uint32_t n,
+                          uint32_t* __restrict__ head)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t s = keys[i] & ~(nodeRange(level[i]) - 1);
+    uint32_t h = 1;
+    if (i > 0)
+    {
+        uint64_t sp = keys[i - 1] & ~(nodeRange(level[i - 1]) - 1);
+        h           = sp != s;
+    }
+    head[i] = h;
+}
+
+__global__ void leafCompact(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ level,
+                            const uint32_t* __restrict__ rank, uint32_t n, uint64_t* __restrict__ leafStart,
+                            uint8_t* __restrict__ leafLvl, uint32_t* __restrict__ leafFirst)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (rank[i + 1] != rank[i])
+    {
+        uint32_t q   = rank[i];
+        leafStart[q] = keys[i] & ~(nodeRange(level[i]) - 1);
+        leafLvl[q]   = level[i];
+        leafFirst[q] = i;
+    }
+}
+
+//! number of output leaves contributed by non-empty leaf q: the gap before it plus itself (q == numNE: final gap)
+__global__ void leafSlots(const uint64_t* __restrict__ leafStart, const uint8_t* __restrict__ leafLvl, uint32_t numNE,
+                          uint32_t* __restrict__ slots)
+{
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q > numNE) return;
+    uint64_t prevEnd = q == 0 ? 0 : leafStart[q - 1] + nodeRange(leafLvl[q - 1]);
+    uint64_t start   = q == numNE ? kKeyEnd : leafStart[q];
+    slots[q]         = uint32_t(spanKeyRange(prevEnd, start, nullptr)) + (q < numNE ? 1u : 0u);
+}
+
+__global__ void leafWrite(const uint64_t* __restrict__ leafStart, const uint8_t* __restrict__ leafLvl,
+                          const uint32_t* __restrict__ leafFirst, const uint32_t* __restrict__ offsets, uint32_t numNE,
+                          uint32_t n, uint64_t* __restrict__ leaves, uint32_t* __restrict__ counts,
+                          uint32_t* __restrict__ layout)
+{
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q > numNE) return;
+    uint64_t prevEnd = q == 0 ? 0 : leafStart[q - 1] + nodeRange(leafLvl[q - 1]);
+    uint64_t start   = q == numNE ? kKeyEnd : leafStart[q];
+    uint32_t o       = offsets[q];
+    uint32_t first   = q == numNE ? n : leafFirst[q];
+    int gap          = spanKeyRange(prevEnd, start, leaves + o);
+    for (int g = 0; g < gap; ++g)
+    {
+        counts[o + g] = 0;
+        if (layout) layout[o + g] = first;
+    }
+    if (q < numNE)
+    {
+        uint32_t last          = q + 1 < numNE ? leafFirst[q + 1] : n;
+        counts[o + gap]        = last - first;
+        if (layout) layout[o + gap] = first;
+    }
+    else
+    {
+        leaves[o] = kKeyEnd;
+        if (layout) layout[o] = n;
+    }
+}
+
+__global__ void singleLeaf(uint64_t* leaves, uint32_t* counts, uint32_t* layout, uint32_t n)
+{
+    leaves[0] = 0;
+    leaves[1] = kKeyEnd;
+    counts[0] = n;
+    if (layout)
+    {
+        layout[0] = 0;
+        layout[1] = n;
+    }
+}
+
+int buildLeaves(ryo_ctx* ctx, const uint64_t* keys, size_t n64, unsigned bucket, uint64_t* leaves, uint32_t* counts,
+                uint32_t* layout, int capacity, cudaStream_t s)
+{
+    uint32_t n = uint32_t(n64);
+    if (n <= bucket)
+    {
+        if (capacity >= 1)
+        {
+            singleLeaf<<<1, 1, 0, s>>>(leaves, counts, layout, n);
+            RYO_LAUNCH_CHECK();
+        }
+        return 1;
+    }
+    if (bucket > 16384) throw CudaError{cudaErrorInvalidValue, "bucket size above 16384 is not supported"};
+
+    uint8_t* level  = ctx->scratch<uint8_t>("leaf.level", n, s);
+    uint32_t* head  = ctx->scratch<uint32_t>("leaf.head", size_t(n) + 1, s);
+    size_t smemBytes = kLeafBlock + bucket;
+    if (smemBytes > 48 * 1024)
+        RYO_CUDA(cudaFuncSetAttribute(leafLevels, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemBytes)));
+    leafLevels<<<ceilDiv(n, kLeafBlock), kLeafBlock, smemBytes, s>>>(keys, n, bucket, level);
+    RYO_LAUNCH_CHECK();
+    leafHeads<<<ceilDiv(n, 256), 256, 0, s>>>(keys, level, n, head);
+    RYO_LAUNCH_CHECK();
+    exclusiveScanU32(ctx, head, head, n, s);
+    uint32_t numNE = 0;
+    RYO_CUDA(cudaMemcpyAsync(&numNE, head + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaStreamSynchronize(s));
+
+    uint64_t* leafStart = ctx->scratch<uint64_t>("leaf.start", numNE, s);
+    uint8_t* leafLvl    = ctx->scratch<uint8_t>("leaf.lvl", numNE, s);
+    uint32_t* leafFirst = ctx->scratch<uint32_t>("leaf.first", numNE, s);
+    uint32_t* slots     = ctx->scratch<uint32_t>("leaf.slots", size_t(numNE) + 2, s);
+    leafCompact<<<ceilDiv(n, 256), 256, 0, s>>>(keys, level, head, n, leafStart, leafLvl, leafFirst);
+    RYO_LAUNCH_CHECK();
+    leafSlots<<<ceilDiv(numNE + 1, 256), 256, 0, s>>>(leafStart, leafLvl, numNE, slots);
+    RYO_LAUNCH_CHECK();
+    exclusiveScanU32(ctx, slots, slots, size_t(numNE) + 1, s);
+    uint32_t numLeaves = 0;
+    RYO_CUDA(cudaMemcpyAsync(&numLeaves, slots + numNE + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaStreamSynchronize(s));
+    if (int64_t(numLeaves) <= int64_t(capacity))
+    {
+        leafWrite<<<ceilDiv(numNE + 1, 256), 256, 0, s>>>(leafStart, leafLvl, leafFirst, slots, numNE, n, leaves,
+                                                           counts, layout);
+        RYO_LAUNCH_CHECK();
+    }
+    return int(numLeaves);
+}
+
+// ------------------------------------------------------------------------------------------------ links
+
+//! weight of the digits on levels 1..level+1 in the binary-radix-tree to octree index map (octree.hpp:55-65)
+__device__ inline int treeIndexWeight(uint64_t key, unsigned level)
+{
+    int w = 0;
+    for (unsigned l = 1; l <= level + 1; ++l)
+    {
+        int d = int(octalDigit(key, l));
+        w += d >= 4 ? 7 - d : -d;
+    }
+    return w;
+}
+
+/*! unsorted node layout: internal nodes first, numbered as in the reference's binary-radix-tree map (node of the
+ *  leaf pair whose common prefix ends on a level boundary), then the leaves (octree_gpu.cu:41-64) */
+__global__ void unsortedLayout(const uint64_t* __restrict__ leaves, int numInternal, int numLeaves,
+                               uint64_t* __restrict__ prefixes)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= numLeaves) return;
+    uint64_t key              = leaves[t];
+    uint64_t next             = leaves[t + 1];
+    prefixes[t + numInternal] = encodePrefix(key, 3 * int(rangeLevel(next - key)));
+    int common                = commonBits(key, next);
+    if (t < numLeaves - 1 && common % 3 == 0)
+    {
+        int at       = (t + treeIndexWeight(key, common / 3)) / 7;
+        prefixes[at] = encodePrefix(key, common);
+    }
+}
+
+__global__ void invertOrder(const uint32_t* __restrict__ order, int numNodes, int numInternal,
+                            int* __restrict__ internalToLeaf, int* __restrict__ leafToInternal)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numNodes) return;
+    int o             = int(order[i]);
+    leafToInternal[o] = i;
+    internalToLeaf[i] = o - numInternal;
+}
+
+__global__ void levelBounds(const uint64_t* __restrict__ prefixes, int numNodes, int* __restrict__ levelRange)
+{
+    int l = threadIdx.x;
+    if (l > kMaxLevel + 1) return;
+    if (l == kMaxLevel + 1)
+    {
+        levelRange[l] = numNodes;
+        return;
+    }
+    uint64_t target = encodePrefix(0, 3 * l);
+    int lo = 0, hi = numNodes;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) / 2;
+        if (prefixes[mid] < target) lo = mid + 1;
+        else hi = mid;
+    }
+    levelRange[l] = lo;
+}
+
+__global__ void linkNodes(const uint64_t* __restrict__ prefixes, int numInternal, const int* __restrict__ leafToInternal,
+                          const int* __restrict__ levelRange, int* __restrict__ childOffsets, int* __restrict__ parents)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= numInternal) return;
+    int a         = leafToInternal[t];
+    uint64_t pre  = prefixes[a];
+    int len       = prefixLength(pre);
+    int lvl       = len / 3;
+    uint64_t cpre = encodePrefix(prefixStart(pre), len + 3);
+    int lo = levelRange[lvl + 1], hi = levelRange[lvl + 2];
+    int end = hi;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) / 2;
+        if (prefixes[mid] < cpre) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo != end && prefixes[lo] == cpre)
+    {
+        childOffsets[a]       = lo;
+        parents[(lo - 1) / 8] = a;
+    }
+}
+
+void linkOctree(ryo_ctx* ctx, const uint64_t* leaves, int numLeaves, const OctreeArrays& out, int* hostLevelRange,
+                cudaStream_t s)
+{
+    int numInternal = (numLeaves - 1) / 7;
+    int numNodes    = numLeaves + numInternal;
+    uint64_t* pre   = ctx->scratch<uint64_t>("link.prefix", numNodes, s);
+    uint64_t* preB  = ctx->scratch<uint64_t>("link.prefixB", numNodes, s);
+    uint32_t* ord   = ctx->scratch<uint32_t>("link.order", numNodes, s);
+    uint32_t* ordB  = ctx->scratch<uint32_t>("link.orderB", numNodes, s);
+    size_t tmpBytes = sortTempBytes(numNodes);
+    void* tmp       = ctx->scratch<char>("link.sorttmp", tmpBytes, s);
+
+    unsortedLayout<<<ceilDiv(numLeaves, 256), 256, 0, s>>>(leaves, numInternal, numLeaves, pre);
+    RYO_LAUNCH_CHECK();
+    // prefixes are unique, so any correct sort gives the reference's order
+    bool alt = radixSortPairs(pre, ord, preB, ordB, numNodes, 0, 64, tmp, tmpBytes, &ctx->ctl->error, s, true);
+    const uint64_t* sortedPre = alt ? preB : pre;
+    const uint32_t* order     = alt ? ordB : ord;
+    RYO_CUDA(cudaMemcpyAsync(out.prefixes, sortedPre, sizeof(uint64_t) * numNodes, cudaMemcpyDeviceToDevice, s));
+    invertOrder<<<ceilDiv(numNodes, 256), 256, 0, s>>>(order, numNodes, numInternal, out.internalToLeaf,
+                                                        out.leafToInternal);
+    RYO_LAUNCH_CHECK();
+    int* dlr = out.d_levelRange ? out.d_levelRange : ctx->scratch<int>("link.levelRange", kMaxLevel + 2, s);
+    levelBounds<<<1, 32, 0, s>>>(out.prefixes, numNodes, dlr);
+    RYO_LAUNCH_CHECK();
+    RYO_CUDA(cudaMemsetAsync(out.childOffsets, 0, sizeof(int) * numNodes, s));
+    int numParents = (numNodes - 1) / 8 > 1 ? (numNodes - 1) / 8 : 1;
+    RYO_CUDA(cudaMemsetAsync(out.parents, 0, sizeof(int) * numParents, s));
+    if (numInternal > 0)
+    {
+        linkNodes<<<ceilDiv(numInternal, 256), 256, 0, s>>>(out.prefixes, numInternal, out.leafToInternal, dlr,
+                                                             out.childOffsets, out.parents);
+        RYO_LAUNCH_CHECK();
+    }
+    RYO_CUDA(cudaMemcpyAsync(hostLevelRange, dlr, sizeof(int) * (kMaxLevel + 2), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaStreamSynchronize(s));
+}
+
+// ------------------------------------------------------------------------------------------------ groups
+
+__global__ void fixedGroups(uint32_t first, uint32_t last, unsigned groupSize, uint32_t numGroups, uint32_t* groups)
+{
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < numGroups) groups[g] = first + g * groupSize;
+    if (g == numGroups) groups[g] = last;
+}
+
+void launchFixedGroups(uint32_t first, uint32_t last, unsigned groupSize, uint32_t* groups, cudaStream_t s)
+{
+    uint32_t numGroups = (last - first + groupSize - 1) / groupSize;
+    fixedGroups<<<ceilDiv(numGroups + 1, 256), 256, 0, s>>>(first, last, groupSize, numGroups, groups);
+    RYO_LAUNCH_CHECK();
+}
+
+} // namespace ryo

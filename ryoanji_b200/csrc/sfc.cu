@@ -1,0 +1,224 @@
+/*
+ * ryoanji-b200: SFC keys, bounding box, sequences and gathers.
+ *
+ * computeSfcKeys (reference cstone/include/cstone/sfc/sfc_gpu.cu:23-44) is HBM-light and integer-heavy: each key
+ * costs 21 Hilbert levels of bit arithmetic on 12 input bytes. Threads process four consecutive points with 128-bit
+ * loads when the arrays allow it; the grid is a multiple of the SM count and strides over the data.
+ */
+#include "internal.hpp"
+
+namespace ryo
+{
+
+template<class T>
+__global__ void keysKernel(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
+                           uint64_t* __restrict__ keys, size_t n, DevBox<T> box, bool keepRemoved)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        if (keepRemoved && keys[i] == kKeyEnd) continue;
+        keys[i] = pointKey(x[i], y[i], z[i], box);
+    }
+}
+
+//! four points per thread with 16-byte loads, keys written as two 16-byte stores
+__global__ void keysKernelVec4(const float4* __restrict__ x, const float4* __restrict__ y,
+                               const float4* __restrict__ z, ulonglong2* __restrict__ keys, size_t n4,
+                               DevBox<float> box)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n4; i += stride)
+    {
+        float4 px = x[i], py = y[i], pz = z[i];
+        ulonglong2 a, b;
+        a.x         = pointKey(px.x, py.x, pz.x, box);
+        a.y         = pointKey(px.y, py.y, pz.y, box);
+        b.x         = pointKey(px.z, py.z, pz.z, box);
+        b.y         = pointKey(px.w, py.w, pz.w, box);
+        keys[2 * i]     = a;
+        keys[2 * i + 1] = b;
+    }
+}
+
+static unsigned streamGrid(size_t work, unsigned block)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t want = (work + block - 1) / block;
+    size_t cap  = size_t(sms) * 8;
+    return unsigned(want < cap ? (want ? want : 1) : cap);
+}
+
+template<class T>
+void launchKeys(const T* x, const T* y, const T* z, uint64_t* keys, size_t n, const DevBox<T>& box, bool keepRemoved,
+                cudaStream_t s)
+{
+    if (n == 0) return;
+    constexpr unsigned block = 256;
+    bool aligned = (reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) |
+                    reinterpret_cast<uintptr_t>(z) | reinterpret_cast<uintptr_t>(keys)) % 16 == 0;
+    if constexpr (std::is_same_v<T, float>)
+    {
+        if (aligned && !keepRemoved && n >= 4)
+        {
+            size_t n4 = n / 4;
+            keysKernelVec4<<<streamGrid(n4, block), block, 0, s>>>(
+                reinterpret_cast<const float4*>(x), reinterpret_cast<const float4*>(y),
+                reinterpret_cast<const float4*>(z), reinterpret_cast<ulonglong2*>(keys), n4, box);
+            RYO_LAUNCH_CHECK();
+            size_t done = n4 * 4;
+            if (done < n)
+            {
+                keysKernel<<<1, 32, 0, s>>>(x + done, y + done, z + done, keys + done, n - done, box, false);
+                RYO_LAUNCH_CHECK();
+            }
+            return;
+        }
+    }
+    keysKernel<<<streamGrid(n, block), block, 0, s>>>(x, y, z, keys, n, box, keepRemoved);
+    RYO_LAUNCH_CHECK();
+}
+
+template void launchKeys<float>(const float*, const float*, const float*, uint64_t*, size_t, const DevBox<float>&,
+                                bool, cudaStream_t);
+template void launchKeys<double>(const double*, const double*, const double*, uint64_t*, size_t,
+                                 const DevBox<double>&, bool, cudaStream_t);
+
+// ------------------------------------------------------------------------------------------------ bounding box
+
+__device__ inline void atomicMinDouble(double* addr, double v)
+{
+    unsigned long long* a = reinterpret_cast<unsigned long long*>(addr);
+    unsigned long long old = *a;
+    while (v < __longlong_as_double(old))
+    {
+        unsigned long long prev = atomicCAS(a, old, __double_as_longlong(v));
+        if (prev == old) break;
+        old = prev;
+    }
+}
+
+__device__ inline void atomicMaxDouble(double* addr, double v)
+{
+    unsigned long long* a = reinterpret_cast<unsigned long long*>(addr);
+    unsigned long long old = *a;
+    while (v > __longlong_as_double(old))
+    {
+        unsigned long long prev = atomicCAS(a, old, __double_as_longlong(v));
+        if (prev == old) break;
+        old = prev;
+    }
+}
+
+__global__ void bboxInit(double* mm)
+{
+    if (threadIdx.x < 3)
+    {
+        mm[2 * threadIdx.x]     = 1e300;
+        mm[2 * threadIdx.x + 1] = -1e300;
+    }
+}
+
+//! per-axis min and max (exact in any precision), reduced per block and combined with double atomics
+__global__ void bboxKernel(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                           size_t n, double* mm)
+{
+    float lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        float v[3] = {x[i], y[i], z[i]};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            lo[d] = fminf(lo[d], v[d]);
+            hi[d] = fmaxf(hi[d], v[d]);
+        }
+    }
+    __shared__ float slo[3][32], shi[3][32];
+    int w = threadIdx.x / kWarp, l = laneId();
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        lo[d] = warpMin(lo[d]);
+        hi[d] = warpMax(hi[d]);
+        if (l == 0)
+        {
+            slo[d][w] = lo[d];
+            shi[d][w] = hi[d];
+        }
+    }
+    __syncthreads();
+    if (w == 0)
+    {
+        int nw = blockDim.x / kWarp;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            float a = l < nw ? slo[d][l] : 3.4e38f, b = l < nw ? shi[d][l] : -3.4e38f;
+            a = warpMin(a);
+            b = warpMax(b);
+            if (l == 0)
+            {
+                atomicMinDouble(mm + 2 * d, double(a));
+                atomicMaxDouble(mm + 2 * d + 1, double(b));
+            }
+        }
+    }
+}
+
+void launchBoundingBox(const float* x, const float* y, const float* z, size_t n, double* minmax6, cudaStream_t s)
+{
+    bboxInit<<<1, 32, 0, s>>>(minmax6);
+    RYO_LAUNCH_CHECK();
+    if (n == 0) return;
+    bboxKernel<<<streamGrid(n, 256), 256, 0, s>>>(x, y, z, n, minmax6);
+    RYO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------------------------------------------ sequences, gathers
+
+__global__ void sequenceKernel(uint32_t* v, size_t n, uint32_t first)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        v[i] = first + uint32_t(i);
+}
+
+void launchSequence(uint32_t* v, size_t n, uint32_t first, cudaStream_t s)
+{
+    if (n == 0) return;
+    sequenceKernel<<<streamGrid(n, 256), 256, 0, s>>>(v, n, first);
+    RYO_LAUNCH_CHECK();
+}
+
+template<class T>
+__global__ void gatherKernel(const uint32_t* __restrict__ order, const T* __restrict__ in, T* __restrict__ out,
+                             size_t n)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = in[order[i]];
+}
+
+template<class T>
+void launchGatherT(const uint32_t* order, const T* in, T* out, size_t n, cudaStream_t s)
+{
+    if (n == 0) return;
+    gatherKernel<<<streamGrid(n, 256), 256, 0, s>>>(order, in, out, n);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchGather(const uint32_t* order, const float* in, float* out, size_t n, cudaStream_t s)
+{
+    launchGatherT<float>(order, in, out, n, s);
+}
+
+template void launchGatherT<float>(const uint32_t*, const float*, float*, size_t, cudaStream_t);
+template void launchGatherT<double>(const uint32_t*, const double*, double*, size_t, cudaStream_t);
+template void launchGatherT<float4>(const uint32_t*, const float4*, float4*, size_t, cudaStream_t);
+template void launchGatherT<uint64_t>(const uint32_t*, const uint64_t*, uint64_t*, size_t, cudaStream_t);
+
+} // namespace ryo

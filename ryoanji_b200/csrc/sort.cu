@@ -1,0 +1,389 @@
+/*
+ * ryoanji-b200: device-wide exclusive scan and the onesweep LSD radix sort.
+ *
+ * Replaces the CUB DeviceRadixSort::SortPairs call of the reference (cstone/include/cstone/primitives/
+ * primitives_gpu.cu:311-356). One upfront pass histograms every digit position; each 8-bit digit pass then reads
+ * the keys once and writes them once: tiles rank their keys with warp match/ballot, publish per-digit tile counts
+ * with decoupled look-back (bounded waits), stage the tile in shared memory in digit order and write coalesced runs.
+ * The sort is stable (keys and payload indices keep their input order within equal keys), as the reference needs.
+ */
+#include "internal.hpp"
+
+namespace ryo
+{
+
+// ------------------------------------------------------------------------------------------------ scan
+
+constexpr int kScanBlock = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile  = kScanBlock * kScanItems;
+
+//! inclusive block scan of one value per thread (blockDim.x <= 1024, multiple of 32)
+template<class T>
+__device__ T blockInclusiveScan(T v, T* sWarp, T* total)
+{
+    int lane = laneId(), warp = threadIdx.x / kWarp, nw = blockDim.x / kWarp;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1)
+    {
+        T w = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += w;
+    }
+    if (lane == kWarp - 1) sWarp[warp] = v;
+    __syncthreads();
+    if (warp == 0)
+    {
+        T s = lane < nw ? sWarp[lane] : T(0);
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1)
+        {
+            T w = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += w;
+        }
+        if (lane < nw) sWarp[lane] = s;
+    }
+    __syncthreads();
+    if (warp > 0) v += sWarp[warp - 1];
+    if (total) *total = sWarp[nw - 1];
+    __syncthreads();
+    return v;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scanTileSums(const uint32_t* __restrict__ in, size_t n,
+                                                           uint32_t* __restrict__ tileSums)
+{
+    __shared__ uint32_t sWarp[32];
+    size_t base  = size_t(blockIdx.x) * kScanTile + size_t(threadIdx.x) * kScanItems;
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i)
+        if (base + i < n) sum += in[base + i];
+    uint32_t tot;
+    blockInclusiveScan(sum, sWarp, &tot);
+    if (threadIdx.x == 0) tileSums[blockIdx.x] = tot;
+}
+
+//! exclusive scan of the tile sums in one block; tileSums[numTiles] receives the grand total
+__global__ void __launch_bounds__(1024) scanTileOffsets(uint32_t* tileSums, uint32_t numTiles)
+{
+    __shared__ uint32_t sWarp[32];
+    uint32_t carry = 0;
+    for (uint32_t b = 0; b < numTiles; b += blockDim.x)
+    {
+        uint32_t i = b + threadIdx.x;
+        uint32_t v = i < numTiles ? tileSums[i] : 0;
+        uint32_t tot;
+        uint32_t incl = blockInclusiveScan(v, sWarp, &tot);
+        if (i < numTiles) tileSums[i] = carry + incl - v;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) tileSums[numTiles] = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scanApply(const uint32_t* in, size_t n,
+                                                        const uint32_t* __restrict__ tileOffsets, uint32_t* out,
+                                                        uint32_t numTiles)
+{
+    __shared__ uint32_t sWarp[32];
+    size_t base = size_t(blockIdx.x) * kScanTile + size_t(threadIdx.x) * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i)
+    {
+        v[i] = base + i < n ? in[base + i] : 0;
+        sum += v[i];
+    }
+    uint32_t incl = blockInclusiveScan(sum, sWarp, (uint32_t*)nullptr);
+    uint32_t run  = tileOffsets[blockIdx.x] + incl - sum;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i)
+    {
+        if (base + i < n) out[base + i] = run;
+        run += v[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tileOffsets[numTiles];
+}
+
+void exclusiveScanU32(ryo_ctx* ctx, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s)
+{
+    uint32_t numTiles = uint32_t((n + kScanTile - 1) / kScanTile);
+    if (numTiles == 0)
+    {
+        RYO_CUDA(cudaMemsetAsync(out, 0, sizeof(uint32_t), s));
+        return;
+    }
+    uint32_t* sums = ctx->scratch<uint32_t>("scan.sums", numTiles + 1, s);
+    scanTileSums<<<numTiles, kScanBlock, 0, s>>>(in, n, sums);
+    RYO_LAUNCH_CHECK();
+    scanTileOffsets<<<1, 1024, 0, s>>>(sums, numTiles);
+    RYO_LAUNCH_CHECK();
+    scanApply<<<numTiles, kScanBlock, 0, s>>>(in, n, sums, out, numTiles);
+    RYO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------------------------------------------ radix sort
+
+constexpr int kSortBlock  = 256;
+constexpr int kSortWarps  = kSortBlock / kWarp;
+constexpr int kSortItems  = 12;
+constexpr int kSortTile   = kSortBlock * kSortItems;
+constexpr int kDigits     = 256;
+constexpr int kMaxPasses  = 8;
+constexpr unsigned long long kFlagAggregate = 1ull << 62;
+constexpr unsigned long long kFlagInclusive = 2ull << 62;
+constexpr int kSpinLimit  = 1 << 22;
+
+struct SortTemp
+{
+    uint32_t* hist;     // kMaxPasses x 256
+    uint32_t* base;     // kMaxPasses x 256
+    unsigned int* tile; // kMaxPasses tile tickets
+    unsigned long long* status;
+    size_t headBytes;
+    size_t numTiles;
+};
+
+static SortTemp sortLayout(void* tmp, size_t n)
+{
+    SortTemp t;
+    t.numTiles   = (n + kSortTile - 1) / kSortTile;
+    char* p      = static_cast<char*>(tmp);
+    t.hist       = reinterpret_cast<uint32_t*>(p);
+    t.base       = t.hist + kMaxPasses * kDigits;
+    t.tile       = reinterpret_cast<unsigned int*>(t.base + kMaxPasses * kDigits);
+    t.headBytes  = 2 * kMaxPasses * kDigits * sizeof(uint32_t) + 256;
+    t.status     = reinterpret_cast<unsigned long long*>(p + t.headBytes);
+    return t;
+}
+
+size_t sortTempBytes(size_t n)
+{
+    size_t tiles = (n + kSortTile - 1) / kSortTile;
+    return 2 * kMaxPasses * kDigits * sizeof(uint32_t) + 256 + (tiles + 1) * kDigits * sizeof(unsigned long long);
+}
+
+//! all digit histograms in one read of the keys; warp-aggregated shared-memory counts
+__global__ void __launch_bounds__(256) digitHistogram(const uint64_t* __restrict__ keys, size_t n, int beginBit,
+                                                      int numPasses, uint32_t* hist)
+{
+    __shared__ uint32_t sh[kMaxPasses][kDigits];
+    for (int i = threadIdx.x; i < kMaxPasses * kDigits; i += blockDim.x)
+        (&sh[0][0])[i] = 0;
+    __syncthreads();
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i0 = size_t(blockIdx.x) * blockDim.x; i0 < n; i0 += stride)
+    {
+        size_t i       = i0 + threadIdx.x;
+        bool valid     = i < n;
+        uint64_t key   = valid ? keys[i] : 0;
+        unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        for (int p = 0; p < numPasses; ++p)
+        {
+            unsigned d     = valid ? unsigned(key >> (beginBit + 8 * p)) & 255u : 256u;
+            unsigned peers = __match_any_sync(0xffffffffu, d) & vmask;
+            if (valid && (peers & lanemaskLt()) == 0) atomicAdd(&sh[p][d], __popc(peers));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < numPasses * kDigits; i += blockDim.x)
+    {
+        uint32_t c = (&sh[0][0])[i];
+        if (c) atomicAdd(hist + i, c);
+    }
+}
+
+__global__ void digitBases(const uint32_t* hist, uint32_t* base, int numPasses)
+{
+    __shared__ uint32_t sWarp[32];
+    for (int p = 0; p < numPasses; ++p)
+    {
+        uint32_t v    = hist[p * kDigits + threadIdx.x];
+        uint32_t incl = blockInclusiveScan(v, sWarp, (uint32_t*)nullptr);
+        base[p * kDigits + threadIdx.x] = incl - v;
+    }
+}
+
+__global__ void __launch_bounds__(kSortBlock) onesweepPass(const uint64_t* __restrict__ keysIn,
+                                                           const uint32_t* __restrict__ valsIn,
+                                                           uint64_t* __restrict__ keysOut,
+                                                           uint32_t* __restrict__ valsOut, size_t n, int shift,
+                                                           int nbits, const uint32_t* __restrict__ digitBase,
+                                                           unsigned long long* status, unsigned int* tileTicket,
+                                                           uint32_t epoch, unsigned int* errorFlag)
+{
+    __shared__ uint32_t sTile;
+    __shared__ uint32_t sHist[kSortWarps][kDigits];
+    __shared__ uint32_t sStart[kDigits];
+    __shared__ uint32_t sGlobal[kDigits];
+    __shared__ uint32_t sWarp[32];
+    __shared__ uint64_t sKeys[kSortTile];
+    __shared__ uint8_t sDig[kSortTile];
+
+    const int tid = threadIdx.x, lane = laneId(), warp = tid / kWarp;
+    for (int i = tid; i < kSortWarps * kDigits; i += kSortBlock)
+        (&sHist[0][0])[i] = 0;
+    if (tid == 0) sTile = atomicAdd(tileTicket, 1u);
+    __syncthreads();
+
+    const uint32_t tile  = sTile;
+    const size_t base    = size_t(tile) * kSortTile;
+    const uint32_t dmask = (1u << nbits) - 1;
+    const size_t wbase   = base + size_t(warp) * (kSortItems * kWarp);
+
+    uint64_t k[kSortItems];
+    uint32_t v[kSortItems], d[kSortItems], r[kSortItems];
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i)
+    {
+        size_t idx = wbase + size_t(i) * kWarp + lane;
+        if (idx < n)
+        {
+            k[i] = keysIn[idx];
+            v[i] = valsIn ? valsIn[idx] : uint32_t(idx);
+            d[i] = uint32_t(k[i] >> shift) & dmask;
+        }
+        else
+        {
+            k[i] = 0;
+            v[i] = 0;
+            d[i] = kDigits;
+        }
+    }
+
+    // rank within the warp: items in (item, lane) order, which is this warp's input order
+    const unsigned lt = lanemaskLt();
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i)
+    {
+        unsigned peers = __match_any_sync(0xffffffffu, d[i]);
+        int leader     = __ffs(peers) - 1;
+        uint32_t before = 0;
+        if (lane == leader && d[i] < kDigits)
+        {
+            before              = sHist[warp][d[i]];
+            sHist[warp][d[i]] = before + __popc(peers);
+        }
+        before = __shfl_sync(0xffffffffu, before, leader);
+        r[i]   = before + __popc(peers & lt);
+    }
+    __syncthreads();
+
+    // digit tid: warp-exclusive offsets and the tile count
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w)
+    {
+        uint32_t c   = sHist[w][tid];
+        sHist[w][tid] = total;
+        total += c;
+    }
+
+    // decoupled look-back over earlier tiles for digit tid
+    const unsigned long long tag = (unsigned long long)epoch << 32;
+    volatile unsigned long long* mine = status + size_t(tile) * kDigits + tid;
+    uint32_t excl = 0;
+    if (tile == 0) { *mine = kFlagInclusive | tag | total; }
+    else
+    {
+        *mine = kFlagAggregate | tag | total;
+        long t    = long(tile) - 1;
+        int spins = 0;
+        while (t >= 0)
+        {
+            unsigned long long s = *(volatile unsigned long long*)(status + size_t(t) * kDigits + tid);
+            unsigned long long flag = s & (3ull << 62);
+            if (flag == 0 || uint32_t((s >> 32) & 0x3FFFFFFFu) != epoch)
+            {
+                if (++spins > kSpinLimit)
+                {
+                    atomicExch(errorFlag, 1u);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            excl += uint32_t(s);
+            if (flag == kFlagInclusive) break;
+            --t;
+        }
+        *mine = kFlagInclusive | tag | uint32_t(excl + total);
+    }
+    sGlobal[tid] = digitBase[tid] + excl;
+    uint32_t incl = blockInclusiveScan(total, sWarp, (uint32_t*)nullptr);
+    sStart[tid]   = incl - total;
+    __syncthreads();
+
+    // stage the tile in digit order
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i)
+    {
+        if (d[i] < kDigits)
+        {
+            uint32_t pos = sStart[d[i]] + sHist[warp][d[i]] + r[i];
+            sKeys[pos]   = k[i];
+            r[i]         = pos;
+        }
+    }
+    __syncthreads();
+    const uint32_t count = uint32_t(n - base < size_t(kSortTile) ? n - base : size_t(kSortTile));
+    for (uint32_t p = tid; p < count; p += kSortBlock)
+    {
+        uint64_t key = sKeys[p];
+        uint32_t dig = uint32_t(key >> shift) & dmask;
+        sDig[p]      = uint8_t(dig);
+        keysOut[sGlobal[dig] + (p - sStart[dig])] = key;
+    }
+    __syncthreads();
+    uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys);
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i)
+        if (d[i] < kDigits) sVals[r[i]] = v[i];
+    __syncthreads();
+    for (uint32_t p = tid; p < count; p += kSortBlock)
+    {
+        uint32_t dig = sDig[p];
+        valsOut[sGlobal[dig] + (p - sStart[dig])] = sVals[p];
+    }
+}
+
+bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_t* valuesAlt, size_t n, int beginBit,
+                    int endBit, void* tmp, size_t tmpBytes, unsigned int* errorFlag, cudaStream_t s, bool iotaValues)
+{
+    if (n == 0) return false;
+    if (tmpBytes < sortTempBytes(n)) throw CudaError{cudaErrorInvalidValue, "radix sort: temporary storage too small"};
+    int numPasses = (endBit - beginBit + 7) / 8;
+    SortTemp t    = sortLayout(tmp, n);
+    RYO_CUDA(cudaMemsetAsync(tmp, 0, t.headBytes, s));
+    RYO_CUDA(cudaMemsetAsync(t.status, 0, t.numTiles * kDigits * sizeof(unsigned long long), s));
+
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t hb = (n + 255) / 256;
+    unsigned histBlocks = unsigned(hb < size_t(sms) * 4 ? hb : size_t(sms) * 4);
+    digitHistogram<<<histBlocks, 256, 0, s>>>(keys, n, beginBit, numPasses, t.hist);
+    RYO_LAUNCH_CHECK();
+    digitBases<<<1, kDigits, 0, s>>>(t.hist, t.base, numPasses);
+    RYO_LAUNCH_CHECK();
+
+    // pass p reads buffer set p % 2 and writes the other
+    bool inAlt = false;
+    for (int p = 0; p < numPasses; ++p)
+    {
+        int shift          = beginBit + 8 * p;
+        int nbits          = endBit - shift < 8 ? endBit - shift : 8;
+        uint64_t* kin      = inAlt ? keysAlt : keys;
+        uint64_t* kout     = inAlt ? keys : keysAlt;
+        const uint32_t* vin = (p == 0 && iotaValues) ? nullptr : (inAlt ? valuesAlt : values);
+        uint32_t* vout     = inAlt ? values : valuesAlt;
+        onesweepPass<<<unsigned(t.numTiles), kSortBlock, 0, s>>>(kin, vin, kout, vout, n, shift, nbits,
+                                                                  t.base + p * kDigits, t.status, t.tile + p,
+                                                                  uint32_t(p + 1), errorFlag);
+        RYO_LAUNCH_CHECK();
+        inAlt = !inAlt;
+    }
+    return inAlt;
+}
+
+} // namespace ryo

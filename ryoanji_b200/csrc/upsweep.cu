@@ -1,0 +1,519 @@
+/*
+ * ryoanji-b200: upward pass — centres of mass, cartesian quadrupoles, MAC radii, traversal node records.
+ *
+ * Reference: cstone/include/cstone/focus/source_center_gpu.cu:103-310 (centres, setMac) and
+ * ryoanji/src/ryoanji/nbody/upsweep_gpu.cu:33-128 (P2M, M2M), with the formulas of
+ * ryoanji/src/ryoanji/nbody/cartesian_qpole.hpp:67-235. Sums run in double precision and are rounded to float once
+ * per stored value; the MAC radius is computed in float from the stored float centre, as the reference does.
+ *
+ * The solver path uses one fused pass: eight lanes per leaf read the leaf's bodies once and accumulate, relative to
+ * the leaf's first body, the fourteen sums that give both the centre of mass (weights |m|) and the second moments
+ * about it; the last of eight siblings to finish combines them into the parent (parallel-axis theorem in double)
+ * and climbs on, so the whole tree is reduced in one launch without per-level host loops.
+ */
+#include "internal.hpp"
+
+namespace ryo
+{
+
+constexpr int kTpl = 8; // lanes per leaf
+
+template<class T>
+__device__ inline T groupSum8(T v)
+{
+#pragma unroll
+    for (int o = 1; o < kTpl; o <<= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------------------------------------ reference steps
+
+__global__ void leafCentersKernel(const float* __restrict__ x, const float* __restrict__ y,
+                                  const float* __restrict__ z, const float* __restrict__ m,
+                                  const int* __restrict__ leafToInternal, int numLeaves,
+                                  const uint32_t* __restrict__ layout, float4* __restrict__ centers)
+{
+    int tid  = blockIdx.x * blockDim.x + threadIdx.x;
+    int leaf = tid / kTpl;
+    double c[4] = {0, 0, 0, 0};
+    if (leaf < numLeaves)
+    {
+        for (uint32_t i = layout[leaf] + tid % kTpl; i < layout[leaf + 1]; i += kTpl)
+        {
+            double w = fabs(double(m[i]));
+            c[0] += w * x[i];
+            c[1] += w * y[i];
+            c[2] += w * z[i];
+            c[3] += w;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        c[k] = groupSum8(c[k]);
+    if (leaf < numLeaves && tid % kTpl == 0)
+    {
+        double inv = c[3] != 0.0 ? 1.0 / c[3] : 1.0;
+        centers[leafToInternal[leaf]] = make_float4(float(c[0] * inv), float(c[1] * inv), float(c[2] * inv),
+                                                    float(c[3]));
+    }
+}
+
+__global__ void upsweepCentersKernel(int first, int last, const int* __restrict__ childOffsets, float4* centers)
+{
+    int i = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= last) return;
+    int fc = childOffsets[i];
+    if (!fc) return;
+    double c[4] = {0, 0, 0, 0};
+    for (int k = fc; k < fc + 8; ++k)
+    {
+        float4 ck = centers[k];
+        double w  = fabs(double(ck.w));
+        c[0] += w * ck.x;
+        c[1] += w * ck.y;
+        c[2] += w * ck.z;
+        c[3] += w;
+    }
+    double inv = c[3] != 0.0 ? 1.0 / c[3] : 1.0;
+    centers[i] = make_float4(float(c[0] * inv), float(c[1] * inv), float(c[2] * inv), float(c[3]));
+}
+
+//! traceless x3 form with the trace in the last slot (cartesian_qpole.hpp:92-108)
+__device__ inline void finalizeQuad(const double raw[7], float* out)
+{
+    double tr = raw[1] + raw[4] + raw[6];
+    out[0]    = float(raw[0]);
+    out[1]    = float(3 * raw[1] - tr);
+    out[2]    = float(3 * raw[2]);
+    out[3]    = float(3 * raw[3]);
+    out[4]    = float(3 * raw[4] - tr);
+    out[5]    = float(3 * raw[5]);
+    out[6]    = float(3 * raw[6] - tr);
+    out[7]    = float(tr);
+}
+
+__global__ void leafMultipolesKernel(const float* __restrict__ x, const float* __restrict__ y,
+                                     const float* __restrict__ z, const float* __restrict__ m,
+                                     const int* __restrict__ leafToInternal, int numLeaves,
+                                     const uint32_t* __restrict__ layout, const float4* __restrict__ centers,
+                                     float* __restrict__ multipoles)
+{
+    int tid  = blockIdx.x * blockDim.x + threadIdx.x;
+    int leaf = tid / kTpl;
+    double q[7] = {0, 0, 0, 0, 0, 0, 0}; // mass, xx, xy, xz, yy, yz, zz
+    int node    = 0;
+    if (leaf < numLeaves)
+    {
+        node     = leafToInternal[leaf];
+        float4 c = centers[node];
+        for (uint32_t i = layout[leaf] + tid % kTpl; i < layout[leaf + 1]; i += kTpl)
+        {
+            double rx = double(x[i]) - c.x, ry = double(y[i]) - c.y, rz = double(z[i]) - c.z, mi = m[i];
+            q[0] += mi;
+            q[1] += rx * rx * mi;
+            q[2] += rx * ry * mi;
+            q[3] += rx * rz * mi;
+            q[4] += ry * ry * mi;
+            q[5] += ry * rz * mi;
+            q[6] += rz * rz * mi;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        q[k] = groupSum8(q[k]);
+    if (leaf < numLeaves && tid % kTpl == 0) finalizeQuad(q, multipoles + 8 * size_t(node));
+}
+
+//! M2M of cells [first, last) from their eight children (cartesian_qpole.hpp:187-235), double sums
+__global__ void upsweepMultipolesKernel(int first, int last, const int* __restrict__ childOffsets,
+                                        const float4* __restrict__ centers, float* multipoles)
+{
+    int i = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= last) return;
+    int fc = childOffsets[i];
+    if (!fc) return;
+    float4 cp = centers[i];
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = fc; k < fc + 8; ++k)
+    {
+        float4 ck      = centers[k];
+        const float* a = multipoles + 8 * size_t(k);
+        double rx = double(cp.x) - ck.x, ry = double(cp.y) - ck.y, rz = double(cp.z) - ck.z;
+        double r2 = (rx * rx + ry * ry + rz * rz) * (1.0 / 3.0);
+        double ml = double(a[0]) * 3;
+        acc[7] += a[7] + ml * r2;
+        acc[0] += a[0];
+        acc[1] += a[1] + ml * (rx * rx - r2);
+        acc[2] += a[2] + ml * rx * ry;
+        acc[3] += a[3] + ml * rx * rz;
+        acc[4] += a[4] + ml * (ry * ry - r2);
+        acc[5] += a[5] + ml * ry * rz;
+        acc[6] += a[6] + ml * (rz * rz - r2);
+    }
+    float* o = multipoles + 8 * size_t(i);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        o[k] = float(acc[k]);
+}
+
+__global__ void setMacKernel(const uint64_t* __restrict__ prefixes, int numNodes, float4* centers, float invTheta,
+                             DevBox<float> box)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numNodes) return;
+    float4 c      = centers[i];
+    float com[3]  = {c.x, c.y, c.z};
+    float mac     = vecMacR2(prefixes[i], com, invTheta, box);
+    centers[i].w  = (c.w != 0.f) ? mac : 0.f;
+}
+
+void launchLeafCenters(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
+                       int numLeaves, const uint32_t* layout, float4* centers, cudaStream_t s)
+{
+    if (numLeaves <= 0) return;
+    leafCentersKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(x, y, z, m, leafToInternal, numLeaves,
+                                                                              layout, centers);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchUpsweepCenters(int first, int last, const int* childOffsets, float4* centers, cudaStream_t s)
+{
+    if (last <= first) return;
+    upsweepCentersKernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets, centers);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchLeafMultipoles(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
+                          int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
+                          cudaStream_t s)
+{
+    if (numLeaves <= 0) return;
+    leafMultipolesKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(x, y, z, m, leafToInternal,
+                                                                                 numLeaves, layout, centers,
+                                                                                 multipoles);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const float4* centers, float* multipoles,
+                             cudaStream_t s)
+{
+    if (last <= first) return;
+    upsweepMultipolesKernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets, centers,
+                                                                       multipoles);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchSetMac(const uint64_t* prefixes, int numNodes, float4* centers, float invTheta, const DevBox<float>& box,
+                  cudaStream_t s)
+{
+    if (numNodes <= 0) return;
+    setMacKernel<<<ceilDiv(numNodes, 256), 256, 0, s>>>(prefixes, numNodes, centers, invTheta, box);
+    RYO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------------------------------------------ fused path
+
+//! double-precision node summary kept during the fused upsweep (128 bytes, one line per node)
+struct alignas(128) DNode
+{
+    double c[3]; // centre of mass (weights |m|)
+    double w;    // sum |m|
+    double m;    // sum m
+    double q[6]; // second moments about c: xx, xy, xz, yy, yz, zz
+    double pad[5];
+};
+
+__device__ inline void storeDNode(DNode* d, const double c[3], double w, double m, const double q[6])
+{
+    double2* p = reinterpret_cast<double2*>(d);
+    __stcg(p + 0, make_double2(c[0], c[1]));
+    __stcg(p + 1, make_double2(c[2], w));
+    __stcg(p + 2, make_double2(m, q[0]));
+    __stcg(p + 3, make_double2(q[1], q[2]));
+    __stcg(p + 4, make_double2(q[3], q[4]));
+    __stcg(p + 5, make_double2(q[5], 0.0));
+}
+
+__device__ inline void loadDNode(const DNode* d, double c[3], double& w, double& m, double q[6])
+{
+    const double2* p = reinterpret_cast<const double2*>(d);
+    double2 a = __ldcg(p + 0), b = __ldcg(p + 1), e = __ldcg(p + 2), f = __ldcg(p + 3), g = __ldcg(p + 4),
+            k = __ldcg(p + 5);
+    c[0] = a.x;
+    c[1] = a.y;
+    c[2] = b.x;
+    w    = b.y;
+    m    = e.x;
+    q[0] = e.y;
+    q[1] = f.x;
+    q[2] = f.y;
+    q[3] = g.x;
+    q[4] = g.y;
+    q[5] = k.x;
+}
+
+struct FusedArgs
+{
+    const float4* xyzm;
+    const uint32_t* layout;
+    const int* leafToInternal;
+    const int* childOffsets;
+    const int* parents;
+    const uint64_t* prefixes;
+    int numLeaves;
+    int numNodes;
+    float invTheta;
+    DevBox<float> box;
+    DNode* dn;
+    unsigned int* arrivals;
+    NodeRecord* records;
+    float4* centers;
+    float* multipoles;
+    double* root; // 11 doubles: centre (3) + finalized multipole (8)
+};
+
+//! write the float outputs of a finished node
+__device__ void emitNode(const FusedArgs& A, int node, const double c[3], double w, double m, const double q[6],
+                         int child, uint32_t firstBody, uint32_t count)
+{
+    float com[3] = {float(c[0]), float(c[1]), float(c[2])};
+    float mac    = w != 0.0 && float(w) != 0.f ? vecMacR2(A.prefixes[node], com, A.invTheta, A.box) : 0.f;
+    double raw[7] = {m, q[0], q[1], q[2], q[3], q[4], q[5]};
+    float qf[8];
+    finalizeQuad(raw, qf);
+    float4 cen = make_float4(com[0], com[1], com[2], mac);
+    NodeRecord r;
+    r.center = cen;
+    r.q0     = make_float4(qf[0], qf[1], qf[2], qf[3]);
+    r.q1     = make_float4(qf[4], qf[5], qf[6], qf[7]);
+    r.link   = make_int4(child, int(firstBody), int(count), 0);
+    A.records[node] = r;
+    if (A.centers) A.centers[node] = cen;
+    if (A.multipoles)
+    {
+        float4* mp = reinterpret_cast<float4*>(A.multipoles + 8 * size_t(node));
+        mp[0]      = r.q0;
+        mp[1]      = r.q1;
+    }
+    if (node == 0 && A.root)
+    {
+        A.root[0] = c[0];
+        A.root[1] = c[1];
+        A.root[2] = c[2];
+        double tr = raw[1] + raw[4] + raw[6];
+        A.root[3] = raw[0];
+        A.root[4] = 3 * raw[1] - tr;
+        A.root[5] = 3 * raw[2];
+        A.root[6] = 3 * raw[3];
+        A.root[7] = 3 * raw[4] - tr;
+        A.root[8] = 3 * raw[5];
+        A.root[9] = 3 * raw[6] - tr;
+        A.root[10] = tr;
+    }
+}
+
+//! combine the eight children of @p node (parallel-axis theorem, double)
+__device__ void combineChildren(const FusedArgs& A, int node, int fc)
+{
+    double cc[8][3], cw[8], cm[8], cq[8][6];
+    double W = 0, M = 0, sx = 0, sy = 0, sz = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+    {
+        loadDNode(A.dn + fc + k, cc[k], cw[k], cm[k], cq[k]);
+        double w = fabs(cw[k]);
+        W += w;
+        M += cm[k];
+        sx += w * cc[k][0];
+        sy += w * cc[k][1];
+        sz += w * cc[k][2];
+    }
+    double c[3];
+    double inv = W != 0.0 ? 1.0 / W : 1.0;
+    c[0]       = sx * inv;
+    c[1]       = sy * inv;
+    c[2]       = sz * inv;
+    double q[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+    {
+        double dx = cc[k][0] - c[0], dy = cc[k][1] - c[1], dz = cc[k][2] - c[2];
+        q[0] += cq[k][0] + cm[k] * dx * dx;
+        q[1] += cq[k][1] + cm[k] * dx * dy;
+        q[2] += cq[k][2] + cm[k] * dx * dz;
+        q[3] += cq[k][3] + cm[k] * dy * dy;
+        q[4] += cq[k][4] + cm[k] * dy * dz;
+        q[5] += cq[k][5] + cm[k] * dz * dz;
+    }
+    storeDNode(A.dn + node, c, W, M, q);
+    emitNode(A, node, c, W, M, q, fc, 0, 0);
+}
+
+/*! eight lanes per leaf: one pass over the bodies, then the last-arriving sibling climbs to combine parents */
+__global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
+{
+    int tid     = blockIdx.x * blockDim.x + threadIdx.x;
+    int leaf    = tid / kTpl;
+    int sub     = tid % kTpl;
+    bool active = leaf < A.numLeaves;
+    uint32_t b0 = 0, b1 = 0;
+    float4 p0   = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (active)
+    {
+        b0 = A.layout[leaf];
+        b1 = A.layout[leaf + 1];
+        if (b1 > b0) p0 = A.xyzm[b0];
+    }
+    // sums relative to the first body: sum|m|, sum|m|d, sum m, sum m d, sum m d d^T
+    double s[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t i = b0 + sub; i < b1; i += kTpl)
+    {
+        float4 b  = A.xyzm[i];
+        double dx = double(b.x) - p0.x, dy = double(b.y) - p0.y, dz = double(b.z) - p0.z;
+        double mi = b.w, wi = fabs(mi);
+        s[0] += wi;
+        s[1] += wi * dx;
+        s[2] += wi * dy;
+        s[3] += wi * dz;
+        s[4] += mi;
+        s[5] += mi * dx;
+        s[6] += mi * dy;
+        s[7] += mi * dz;
+        s[8] += mi * dx * dx;
+        s[9] += mi * dx * dy;
+        s[10] += mi * dx * dz;
+        s[11] += mi * dy * dy;
+        s[12] += mi * dy * dz;
+        s[13] += mi * dz * dz;
+    }
+#pragma unroll
+    for (int k = 0; k < 14; ++k)
+        s[k] = groupSum8(s[k]);
+    if (!active || sub != 0) return;
+
+    int node = A.leafToInternal[leaf];
+    double W = s[0], M = s[4];
+    double c[3], q[6];
+    if (W != 0.0)
+    {
+        double inv = 1.0 / W;
+        double ex = s[1] * inv, ey = s[2] * inv, ez = s[3] * inv; // centre relative to p0
+        c[0] = double(p0.x) + ex;
+        c[1] = double(p0.y) + ey;
+        c[2] = double(p0.z) + ez;
+        // sum m (d - e)(d - e)^T
+        q[0] = s[8] - 2 * ex * s[5] + M * ex * ex;
+        q[1] = s[9] - ex * s[6] - ey * s[5] + M * ex * ey;
+        q[2] = s[10] - ex * s[7] - ez * s[5] + M * ex * ez;
+        q[3] = s[11] - 2 * ey * s[6] + M * ey * ey;
+        q[4] = s[12] - ey * s[7] - ez * s[6] + M * ey * ez;
+        q[5] = s[13] - 2 * ez * s[7] + M * ez * ez;
+    }
+    else
+    {
+        // zero total |m|: centre at the origin like the reference's normalisation; moments about it
+        c[0] = c[1] = c[2] = 0.0;
+        double ox = p0.x, oy = p0.y, oz = p0.z; // p0 - 0
+        q[0] = s[8] + 2 * ox * s[5] + M * ox * ox;
+        q[1] = s[9] + ox * s[6] + oy * s[5] + M * ox * oy;
+        q[2] = s[10] + ox * s[7] + oz * s[5] + M * ox * oz;
+        q[3] = s[11] + 2 * oy * s[6] + M * oy * oy;
+        q[4] = s[12] + oy * s[7] + oz * s[6] + M * oy * oz;
+        q[5] = s[13] + 2 * oz * s[7] + M * oz * oz;
+    }
+    storeDNode(A.dn + node, c, W, M, q);
+    emitNode(A, node, c, W, M, q, 0, b0, b1 - b0);
+
+    // climb: the eighth sibling to arrive combines the parent
+    while (node > 0)
+    {
+        int parent = A.parents[(node - 1) / 8];
+        __threadfence();
+        unsigned prev = atomicAdd(A.arrivals + parent, 1u);
+        if (prev != 7) break;
+        __threadfence();
+        combineChildren(A, parent, A.childOffsets[parent]);
+        node = parent;
+    }
+}
+
+void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
+                        const int* leafToInternal, const int* childOffsets, const int* parents,
+                        const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
+                        float4* centers, float* multipoles, double* root, cudaStream_t s)
+{
+    FusedArgs A;
+    A.xyzm           = xyzm;
+    A.layout         = layout;
+    A.leafToInternal = leafToInternal;
+    A.childOffsets   = childOffsets;
+    A.parents        = parents;
+    A.prefixes       = prefixes;
+    A.numLeaves      = numLeaves;
+    A.numNodes       = numNodes;
+    A.invTheta       = invTheta;
+    A.box            = box;
+    A.dn             = ctx->scratch<DNode>("up.dnode", numNodes, s);
+    A.arrivals       = ctx->scratch<unsigned int>("up.arrivals", numNodes, s);
+    A.records        = records;
+    A.centers        = centers;
+    A.multipoles     = multipoles;
+    A.root           = root;
+    RYO_CUDA(cudaMemsetAsync(A.arrivals, 0, sizeof(unsigned int) * numNodes, s));
+    fusedUpsweepKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(A);
+    RYO_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------------------------------------------ packing
+
+__global__ void packNodesKernel(int numNodes, const float4* __restrict__ centers, const float* __restrict__ multipoles,
+                                const int* __restrict__ childOffsets, const int* __restrict__ internalToLeaf,
+                                const uint32_t* __restrict__ layout, NodeRecord* __restrict__ records)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numNodes) return;
+    const float4* mp = reinterpret_cast<const float4*>(multipoles + 8 * size_t(i));
+    NodeRecord r;
+    r.center = centers[i];
+    r.q0     = mp[0];
+    r.q1     = mp[1];
+    int leaf = internalToLeaf[i];
+    int fc   = childOffsets[i];
+    uint32_t first = 0, count = 0;
+    if (leaf >= 0)
+    {
+        first = layout[leaf];
+        count = layout[leaf + 1] - first;
+    }
+    r.link     = make_int4(fc, int(first), int(count), leaf);
+    records[i] = r;
+}
+
+void launchPackNodes(int numNodes, const float4* centers, const float* multipoles, const int* childOffsets,
+                     const int* internalToLeaf, const uint32_t* layout, NodeRecord* records, cudaStream_t s)
+{
+    if (numNodes <= 0) return;
+    packNodesKernel<<<ceilDiv(numNodes, 256), 256, 0, s>>>(numNodes, centers, multipoles, childOffsets,
+                                                           internalToLeaf, layout, records);
+    RYO_LAUNCH_CHECK();
+}
+
+__global__ void packBodiesKernel(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                                 const float* __restrict__ w, size_t n, float4* __restrict__ out)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = make_float4(x[i], y[i], z[i], w[i]);
+}
+
+void launchPackBodies(const float* x, const float* y, const float* z, const float* w, size_t n, float4* out,
+                      cudaStream_t s)
+{
+    if (n == 0) return;
+    size_t blocks = (n + 255) / 256;
+    packBodiesKernel<<<unsigned(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, s>>>(x, y, z, w, n, out);
+    RYO_LAUNCH_CHECK();
+}
+
+} // namespace ryo

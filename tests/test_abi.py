@@ -1,0 +1,78 @@
+"""CPU checks of the drop-in boundary: the library loads, exports every function the header declares, and reports
+errors as statuses (no GPU needed)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+import torch
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "ryoanji_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    return re.findall(r"RYO_API\s+[\w\s\*]+?\b(ryo_\w+)\s*\(", text)
+
+
+def test_header_declares_functions():
+    names = declared_functions()
+    assert len(names) >= 30
+    assert "ryo_traverse_f32" in names and "ryo_treebuilder_update_f32" in names
+
+
+def test_library_exports_every_declared_symbol():
+    from ryoanji_b200._abi import LIB_PATH, SIGNATURES
+    lib = C.CDLL(LIB_PATH)
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    # the Python bindings cover the whole header
+    assert set(declared_functions()) == set(SIGNATURES)
+
+
+def test_only_c_abi_is_exported():
+    from ryoanji_b200._abi import LIB_PATH
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB_PATH], capture_output=True, text=True).stdout
+    exported = [l.split()[-1] for l in out.splitlines() if " T " in l]
+    assert exported and all(n.startswith("ryo_") for n in exported), [n for n in exported if not n.startswith("ryo_")]
+
+
+def test_status_strings_and_version():
+    import ryoanji_b200 as ryo
+    assert ryo.lib.ryo_version() == b"0.1.0"
+    assert ryo.lib.ryo_status_string(0) == b"ok"
+    assert b"stack" in ryo.lib.ryo_status_string(4)
+    assert ryo.bh_max_target_size() == 64
+    assert ryo.stack_size(1000) == 0
+
+
+def test_bad_arguments_return_status_not_crash():
+    import ryoanji_b200 as ryo
+    assert ryo.lib.ryo_ctx_create(0, None) == 2
+    assert ryo.lib.ryo_read_bh_stats(None, None) == 2
+    assert ryo.lib.ryo_treebuilder_create(None, 64, None) == 2
+    args = [None, None, 1] + [None] * 15 + [1.0, 0, None, None, None, None, None, None, None]
+    assert ryo.lib.ryo_traverse_f32(*args) == 2
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-device path")
+def test_context_without_device_fails_cleanly():
+    import ryoanji_b200 as ryo
+    h = C.c_void_p()
+    st = ryo.lib.ryo_ctx_create(0, C.byref(h))
+    assert st != 0 and not h.value
+    assert len(ryo.lib.ryo_ctx_last_error(None)) > 0
+
+
+def test_cpp_shim_headers_compile():
+    """the C++ drop-in headers (reference signatures) compile against the C ABI"""
+    shim = os.path.join(ROOT, "include", "ryoanji_b200", "ryoanji.hpp")
+    if not os.path.exists(shim):
+        pytest.skip("no C++ shim")
+    src = f'#include "{shim}"\nint main() {{ return 0; }}\n'
+    r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-x",
+                        "c++", "-"], input=src, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

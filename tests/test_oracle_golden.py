@@ -1,0 +1,180 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures written by tests/golden/make_golden.py).
+
+Integer outputs are compared bit for bit; the float upsweep too (same operation order); the CPU tree walk,
+direct sum and Ewald to round-off.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases
+
+CASES = golden_cases()
+
+
+@pytest.fixture(scope="module", params=CASES, ids=[os.path.basename(c)[5:-4] for c in CASES])
+def case(request):
+    return dict(np.load(request.param))
+
+
+def test_keys(oracle, case):
+    keys = oracle.sfc_keys(case["x"], case["y"], case["z"], case["box"])
+    assert np.array_equal(keys, case["keys"])
+    assert np.array_equal(oracle.box_dim_bits(case["box"]), case["bits"])
+
+
+def test_sort(oracle, case):
+    sk, order = oracle.sort_keys(case["keys"])
+    assert np.array_equal(sk, case["sorted_keys"])
+    assert np.array_equal(order, case["order"])
+
+
+def test_leaves(oracle, case):
+    leaves, counts = oracle.octree_leaves(case["sorted_keys"], int(case["bucket"]))
+    assert np.array_equal(leaves, case["leaves"])
+    assert np.array_equal(counts, case["counts"])
+
+
+def test_link(oracle, case):
+    t = oracle.octree_link(case["leaves"])
+    for k in ("prefixes", "childOffsets", "parents", "levelRange", "internalToLeaf", "leafToInternal"):
+        assert np.array_equal(t[k], case["tree_" + k]), k
+
+
+def _sorted(case):
+    o = case["order"]
+    return [case[k][o] for k in ("x", "y", "z", "m", "h")]
+
+
+def _tree(oracle, case):
+    return oracle.octree_link(case["leaves"])
+
+
+def test_upsweep_float_order_is_bit_exact(oracle, case):
+    xs, ys, zs, ms, hs = _sorted(case)
+    t = _tree(oracle, case)
+    centers, mp = oracle.upsweep(xs, ys, zs, ms, case["layout"], t, float(case["theta"]), case["box"], mode=0)
+    assert np.array_equal(centers, case["centers"])
+    assert np.array_equal(mp, case["multipoles"])
+
+
+def test_upsweep_double_close_to_reference(oracle, case):
+    xs, ys, zs, ms, hs = _sorted(case)
+    t = _tree(oracle, case)
+    c1, m1 = oracle.upsweep(xs, ys, zs, ms, case["layout"], t, float(case["theta"]), case["box"], mode=1)
+    c0 = case["centers"]
+    scale = np.abs(c0[:, :3]).max()
+    assert np.abs(c1[:, :3] - c0[:, :3]).max() <= 2e-6 * scale
+    m0 = case["multipoles"]
+    assert np.allclose(m1[:, 0], m0[:, 0], rtol=1e-5, atol=0)
+
+
+def test_gravity_cpu(oracle, case):
+    if "grav_ax" not in case:
+        pytest.skip("no CPU walk for this case")
+    xs, ys, zs, ms, hs = _sorted(case)
+    t = _tree(oracle, case)
+    u, pot, ax, ay, az = oracle.gravity_cpu(t, case["centers"], case["multipoles"], case["layout"], xs, ys, zs, hs, ms,
+                                            case["box"])
+    for a, k in ((ax, "grav_ax"), (ay, "grav_ay"), (az, "grav_az"), (pot, "grav_pot")):
+        assert np.array_equal(a, case[k]), k
+    assert abs(u - float(case["grav_u"])) <= 1e-5 * abs(float(case["grav_u"]))
+
+
+def test_direct_sum(oracle, case):
+    if "direct_ax" not in case:
+        pytest.skip("no direct sum for this case")
+    x, y, z, m, h = _sorted(case)
+    idx = np.arange(0, len(x), 7)
+    pot, ax, ay, az = oracle.direct(x, y, z, h, m, idx, G=1.0)
+    for a, k in ((pot, "direct_pot"), (ax, "direct_ax"), (ay, "direct_ay"), (az, "direct_az")):
+        ref = case[k][idx]
+        assert np.allclose(a, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max()), k
+
+
+def test_ewald(oracle, case):
+    if "ewald_ax" not in case:
+        pytest.skip("not periodic")
+    xs, ys, zs, ms, hs = (a.astype(np.float64) for a in _sorted(case))
+    rc = case["centers"][0, :3].astype(np.float64)
+    mr = case["multipoles"][0].astype(np.float64)
+    u, pot, ax, ay, az = oracle.ewald(rc, mr, xs, ys, zs, ms, case["box"].astype(np.float64), G=1.0)
+    for a, k in ((ax, "ewald_ax"), (ay, "ewald_ay"), (az, "ewald_az"), (pot, "ewald_pot")):
+        assert np.allclose(a, case[k], rtol=1e-12, atol=1e-12 * np.abs(case[k]).max()), k
+    assert abs(u - float(case["ewald_u"])) <= 1e-12 * abs(float(case["ewald_u"]))
+
+
+def test_known_answers(oracle, known):
+    h1, h2 = known["p2p_h"]
+    for h, ref in ((h1, known["p2p_base"]), (h2, known["p2p_soft"])):
+        a = oracle.p2p([1, 1, 1], [2, 2, 2], 1.0, h, h)
+        a = oracle.p2p([1, 1, 1], [-2, -2, -2], 1.0, h, h, a)
+        assert np.allclose(a, ref, rtol=0, atol=1e-10)
+    # self interaction is exactly zero for non-zero softening (ryoanji/test/nbody/kernel.cpp:68-78)
+    assert np.array_equal(oracle.p2p([0, 0, 0], [0, 0, 0], 1.0, 0.1, 0.1), np.zeros(4))
+    e1 = oracle.ewald_single_particle_energy(1.0, 1, 1.0)
+    e2 = oracle.ewald_single_particle_energy(1.0, 1, 2.0)
+    assert abs(e1 - known["ewald_single"][0]) < 1e-10 and abs(e2 - known["ewald_single"][1]) < 1e-10
+
+
+def test_m2p_matches_p2p_far_away(oracle):
+    """the cartesian quadrupole reproduces the direct sum of its sources far away (cartesian_qpole.cpp:27-76)"""
+    rng = np.random.default_rng(11)
+    x, y, z = (rng.uniform(-1, 1, 100) for _ in range(3))
+    m = rng.uniform(0, 1, 100)
+    c, q = oracle.p2m(x, y, z, m)
+    target = np.array([-8.0, 0.0, 0.0])
+    ref = np.zeros(4)
+    for s in range(100):
+        ref = oracle.p2p(target, [x[s], y[s], z[s]], m[s], 0.0, 0.0, ref)
+    approx = oracle.m2p(target, c[:3], q)
+    assert np.abs(approx - ref).max() < 1e-3
+
+
+def test_mixed_dimension_cell_contains_point(oracle):
+    """the fork's cell index puts every point inside its key's cell for fitted boxes (sfc.cpp:69-100)"""
+    box = np.array([-0.0011882485223581088, 0.0011884225944410061, -0.0011882157500425073, 0.001188368630643466,
+                    -0.012426126792806139, 0.045320500145225831])
+    bits = None
+    import ctypes as C
+    rng = np.random.default_rng(42)
+    n = 20000
+    x = rng.uniform(box[0], box[1], n)
+    y = rng.uniform(box[2], box[3], n)
+    z = rng.uniform(box[4], box[5], n)
+    x[0], y[0], z[0] = -2.3742214883045176e-05, 9.6842915978489733e-08, 0.010289945748438454
+    keys = oracle.sfc_keys(x, y, z, box)
+    b = (C.c_uint * 3)()
+    oracle.lib.orc_box_dim_bits_f64(box.ctypes.data_as(C.c_void_p), b)
+    bits = list(b)
+    assert bits[0] == 16 and bits[2] == 21
+    L = box[1::2] - box[0::2]
+    outside = 0
+    for i in range(0, n, 37):
+        ib = oracle.hilbert_ibox(int(keys[i]), 21, bits)
+        half = [0.5 / 2 ** 21 * L[d] * 2 ** (21 - bits[d]) for d in range(3)]
+        c = [box[2 * d] + (ib[2 * d + 1] + ib[2 * d]) * half[d] for d in range(3)]
+        s = [(ib[2 * d + 1] - ib[2 * d]) * half[d] for d in range(3)]
+        p = (x[i], y[i], z[i])
+        tol = 1e-12 * L.max()
+        outside += any(abs(p[d] - c[d]) > s[d] + tol for d in range(3))
+    assert outside == 0
+
+
+def test_reference_wrapper_agrees_when_present(oracle):
+    """if the reference compiled here, the restatement equals it on a fresh random case (not only the fixtures)"""
+    from pyoracle import Oracle, have_reference
+    if not have_reference():
+        pytest.skip("reference not built here")
+    ref = Oracle(reference=True)
+    rng = np.random.default_rng(99)
+    n = 3000
+    x, y, z = (rng.standard_normal(n).astype(np.float32) * 0.2 for _ in range(3))
+    box = np.array([-2, 2, -1.5, 1.5, -1, 1], np.float32)
+    k1, k2 = oracle.sfc_keys(x, y, z, box), ref.sfc_keys(x, y, z, box)
+    assert np.array_equal(k1, k2)
+    s1, _ = oracle.sort_keys(k1)
+    l1, c1 = oracle.octree_leaves(s1, 12)
+    l2, c2 = ref.octree_leaves(s1, 12)
+    assert np.array_equal(l1, l2) and np.array_equal(c1, c2)
