@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the single-GPU Barnes-Hut solve: Mparticles/s of one full build + upsweep + traversal.
+
+Workload (default): N = 2^26 bodies i.i.d. uniform in [-1, 1]^3, masses 1/N, theta = 0.5, cartesian quadrupoles,
+leaf bucket 64, 64-body target groups, fixed box [-1, 1]^3, FP32 with the FP64 steps of the design. The reference
+P2P is singular for a body with itself at zero softening, so every body gets h = 1e-6 (the reference's own overflow
+test does the same), far below the mean spacing 2.5e-3.
+
+One "step" is one complete solve from unsorted, device-resident coordinates: SFC keys, radix sort, gathers, leaf
+array, octree links, upsweep, target groups, traversal. Inputs (>> L2) are restored from a pristine copy before each
+step, outside the timed interval of that step; each step is timed with CUDA events on the launching stream.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank solves its own system (replicas, weak scaling; a single system is not sharded).
+`--impl reference` times the reference's own CPU implementation of the path (oracle/_ref, compiled from the
+reference sources) on the host cores for a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BASELINE_PUBLISHED_MPS = 62.2  # reference, 1x A100, theta 0.5, 67 M particles (README.md:60)
+P2P_FLOPS, M2P_FLOPS = 23, 65  # the reference's flop convention (ryoanji/test/demo.cu:108)
+METRIC = "BH solve throughput (build + upsweep + traversal), theta 0.5, 1st-pct acc err vs FP64 direct"
+
+
+def workload_config(args, world):
+    return {"workload": f"uniform cube N=2^{args.log2n} in [-1,1]^3, masses 1/N, h=1e-6, theta={args.theta}, "
+                        "cartesian quadrupole, bucket 64, groups 64, one full solve per step",
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2": "inputs of 256 MiB per array (> 126 MB L2) restored before every step",
+            "vs_baseline_note": "published 62.2 Mparticles/s: reference on 1x A100, README.md:60"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--log2n", type=int, default=26)
+    ap.add_argument("--theta", type=float, default=0.5)
+    ap.add_argument("--accuracy-targets", type=int, default=16384)
+    ap.add_argument("--cpu-log2n", type=int, default=21, help="CPU baseline sample size")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while the timed region runs"""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------------ arms
+
+def cpu_reference_solve(log2n: int, theta: float, seed: int = 0):
+    """the reference's CPU path (oracle/_ref) or, where it could not be built, the restated oracle"""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import Oracle, have_reference
+    from ryoanji_b200 import datasets as ds
+    kind = "reference" if have_reference() else "port"
+    orc = Oracle(reference=(kind == "reference"))
+    p = ds.uniform_cube(1 << log2n, seed=seed)
+    t0 = time.perf_counter()
+    u, *_ , sec = orc.solve(p.x, p.y, p.z, p.m, p.h, [-1, 1, -1, 1, -1, 1], bucket=64, theta=theta, G=1.0)
+    dt = time.perf_counter() - t0
+    return kind, dt, sec
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_reference_solve(args.cpu_log2n, args.theta, seed=1)
+    times = []
+    kind = "port"
+    for i in range(args.steps):
+        kind, dt, _ = cpu_reference_solve(args.cpu_log2n, args.theta, seed=2 + i)
+        times.append(dt)
+    n = 1 << args.cpu_log2n
+    value = n * len(times) / sum(times) / 1e6
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value,
+        "unit": "Mparticles/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args, args.gpus),
+        "cpu_baseline": {"value": value, "unit": "Mparticles/s", "cores": cores, "kind": kind,
+                         "sample": f"each step: one full CPU solve (keys, sort, computeOctree, links, upsweep, "
+                                   f"computeGravity) of N=2^{args.cpu_log2n} bodies of the same uniform-cube "
+                                   f"distribution, OpenMP on {cores} threads"},
+        "e2e": {"value": value, "unit": "Mparticles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import ryoanji_b200 as ryo
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = 1 << args.log2n
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    pristine = [torch.rand(n, device=dev, generator=gen) * 2 - 1 for _ in range(3)]
+    pristine += [torch.full((n,), 1.0 / n, device=dev), torch.full((n,), 1e-6, device=dev)]
+    work = [t.clone() for t in pristine]
+    out = [torch.empty(n, device=dev) for _ in range(4)]
+    ctx = ryo.Context(local_rank)
+    params = ryo.SolveParams(theta=args.theta, bucket_size=64, group_size=64, box=ryo.Box.cube(-1.0, 1.0),
+                             timing=True)
+    peaks = ryo.measure_peaks(ctx)
+
+    def restore():
+        for w, p in zip(work, pristine):
+            w.copy_(p)
+
+    def solve():
+        return ryo.solve(*work, *out, params=params, ctx=ctx)
+
+    for _ in range(args.warmup):
+        restore()
+        solve()
+    barrier()
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    launches0 = ryo.kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    results = []
+    with ClockSampler(uuid) as clocks:
+        barrier()
+        for i in range(args.steps):
+            restore()
+            ev[i][0].record()
+            results.append(solve())
+            ev[i][1].record()
+        barrier()
+    launches = ryo.kernel_launches() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = max_over_ranks(sum(step_ms))
+    value = world * n * args.steps / (total_ms * 1e-3) / 1e6
+    res = results[-1]
+    flops = P2P_FLOPS * res.sum_p2p + M2P_FLOPS * res.sum_m2p
+    trav_ms = float(np.mean([r.ms["traverse"] for r in results]))
+    achieved = flops / (trav_ms * 1e-3) / 1e12
+    phase = {k: float(np.mean([r.ms[k] for r in results])) for k in ("sort", "tree", "upsweep", "traverse",
+                                                                      "total")}
+
+    line = {
+        "metric": METRIC,
+        "value": value, "unit": "Mparticles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / world / BASELINE_PUBLISHED_MPS, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args, world),
+        "phase_ms": phase,
+        "interactions": {"p2p_per_body": res.sum_p2p / n, "m2p_per_body": res.sum_m2p / n, "max_p2p": res.max_p2p,
+                         "max_m2p": res.max_m2p, "leaves": res.num_leaves, "nodes": res.num_nodes,
+                         "retries": res.retries, "counted_tflops_traversal": achieved},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+                     "frac": achieved / peaks["fp32_tflops"], "traffic": None,
+                     "kernel": "traverseKernel (M2P + P2P), 23 flops per P2P and 65 per M2P per target",
+                     "peak_source": "measured FP32 FMA peak of this GPU in this run (ryo_measure_peaks)",
+                     "peak_fp32x2": peaks["fp32x2_tflops"]},
+        "build_hbm": {"bytes_per_body": 296, "gbs": 296 * n / ((phase["sort"] + phase["tree"] + phase["upsweep"])
+                                                              * 1e-3) / 1e9,
+                      "peak_gbs": _measured_hbm(peaks)},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+
+    # accuracy against the FP64 direct sum on random targets of the last solve (sorted order)
+    if args.accuracy_targets > 0:
+        rng = np.random.default_rng(7)
+        tgt = torch.from_numpy(rng.choice(n, args.accuracy_targets, replace=False)).to(dev)
+        rp, rx, ry, rz = ryo.direct_targets_f64(tgt, *work)
+        a = torch.stack([out[1][tgt], out[2][tgt], out[3][tgt]], 1).double()
+        r = torch.stack([rx, ry, rz], 1)
+        err = (torch.linalg.norm(a - r, dim=1) / torch.linalg.norm(r, dim=1)).cpu().numpy()
+        pt, pd = float(out[0][tgt].double().sum()), float(rp.sum())
+        line["accuracy"] = {"targets": args.accuracy_targets, "err_p99_1st_pct": float(np.percentile(err, 99)),
+                            "err_max": float(err.max()), "err_median": float(np.median(err)),
+                            "potential_sample_rel_diff": abs(pt - pd) / abs(pd),
+                            "potential_energy_tree": res.potential_energy}
+
+    # end to end through the public API: host buffers in, host results out
+    if not args.no_e2e:
+        host_in = [t.cpu().pin_memory() for t in pristine]
+        host_out = [torch.empty(n).pin_memory() for _ in range(4)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            for w, h in zip(work, host_in):
+                w.copy_(h, non_blocking=True)
+            solve()
+        barrier()
+        e0.record()
+        for _ in range(args.steps):
+            for w, h in zip(work, host_in):
+                w.copy_(h, non_blocking=True)
+            solve()
+            for h, o in zip(host_out, out):
+                h.copy_(o, non_blocking=True)
+        e1.record()
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        line["e2e"] = {"value": world * n * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mparticles/s",
+                       "h2d_bytes_per_step": 5 * 4 * n, "d2h_bytes_per_step": 4 * 4 * n}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        kind, dt, sec = cpu_reference_solve(args.cpu_log2n, args.theta, seed=3)
+        line["cpu_baseline"] = {"value": (1 << args.cpu_log2n) / dt / 1e6, "unit": "Mparticles/s",
+                                "cores": os.cpu_count(), "kind": kind,
+                                "sample": f"one solve of N=2^{args.cpu_log2n} uniform cube (bounded sample), "
+                                          f"OpenMP on {os.cpu_count()} threads; build/upsweep/gravity s = "
+                                          f"{[round(float(s), 3) for s in sec]}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _measured_hbm(peaks):
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return peaks["copy_gbs"]
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

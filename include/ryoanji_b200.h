@@ -284,6 +284,7 @@ extern "C"
         int numShells;               /* periodic replica shells when periodic (1) */
         ryo_ewald_settings ewald;    /* Ewald settings when periodic */
         int stackCapacity;           /* 0 = default */
+        int timing;                  /* 1: record per-phase device times into ryo_solve_stats.ms */
     } ryo_solve_params;
 
     typedef struct ryo_solve_stats
@@ -292,6 +293,9 @@ extern "C"
         uint64_t sumP2P, maxP2P, sumM2P, maxM2P, maxStack, retries;
         double potentialEnergy; /* 0.5 G sum(m phi), tree + Ewald */
         float box[6];           /* the box used */
+        /* with params.timing: device milliseconds of keys+sort+gather, leaves+links, upsweep, traversal (all
+         * passes), Ewald, and the whole solve */
+        float ms[6];
     } ryo_solve_stats;
 
     RYO_API void ryo_solve_params_default(ryo_solve_params* p);
@@ -329,6 +333,14 @@ extern "C"
         double rootMultipole[8];
     } ryo_solve_arrays;
     RYO_API ryo_status ryo_solve_arrays_get(ryo_ctx_t* ctx, ryo_solve_arrays* out);
+
+    /* ------------------------------------------------------------------------------------------ measurement */
+
+    /* number of kernels this library has launched in the process so far (every launch is counted) */
+    RYO_API uint64_t ryo_kernel_launches(void);
+    /* calibration for roofline denominators (about 0.2 s): out3 = {FP32 FMA TFLOP/s, packed f32x2 FMA TFLOP/s,
+     * streaming copy GB/s (read + write)} at the clocks of the call */
+    RYO_API ryo_status ryo_measure_peaks(ryo_ctx_t* ctx, double* out3, ryo_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -23,6 +23,7 @@ __all__ = [
     "compute_fixed_groups", "compute_leaf_source_center", "upsweep_centers", "compute_leaf_multipoles",
     "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries",
     "compute_gravity_ewald", "direct_sum", "direct_targets_f64", "solve", "solve_arrays", "bh_max_target_size",
+    "kernel_launches", "measure_peaks",
     "stack_size",
     "BOUNDARY_OPEN", "BOUNDARY_PERIODIC", "BOUNDARY_FIXED", "BOUNDARY_CUBIC_OPEN", "MAX_TREE_LEVEL",
 ]
@@ -465,6 +466,7 @@ class SolveParams:
     num_shells: int = 1
     ewald: EwaldSettings | None = None
     stack_capacity: int = 0
+    timing: bool = False
 
     def c(self) -> _abi.SolveParams:
         p = _abi.SolveParams()
@@ -480,6 +482,7 @@ class SolveParams:
         if self.ewald is not None:
             p.ewald = self.ewald.c()
         p.stackCapacity = self.stack_capacity
+        p.timing = int(self.timing)
         return p
 
 
@@ -496,6 +499,7 @@ class SolveResult:
     retries: int
     potential_energy: float
     box: list
+    ms: dict
 
 
 def solve(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, v=None, order=None,
@@ -511,8 +515,9 @@ def solve(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, v=Non
                              _ptr(vz), C.c_size_t(x.numel()), _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), _ptr(order),
                              C.byref(st), _stream(stream)), ctx)
     _solve_n[id(ctx)] = x.numel()
+    ms = dict(zip(("sort", "tree", "upsweep", "traverse", "ewald", "total"), list(st.ms)))
     return SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
-                       st.maxStack, st.retries, st.potentialEnergy, list(st.box))
+                       st.maxStack, st.retries, st.potentialEnergy, list(st.box), ms)
 
 
 _solve_n: dict = {}
@@ -520,6 +525,19 @@ _solve_n: dict = {}
 
 def _last_n(ctx) -> int:
     return _solve_n.get(id(ctx), 0)
+
+
+def kernel_launches() -> int:
+    """kernels launched by the library in this process"""
+    return int(lib.ryo_kernel_launches())
+
+
+def measure_peaks(ctx: Context | None = None, stream=None) -> dict:
+    """FP32 FMA peak (scalar and packed f32x2) in TFLOP/s and streaming-copy GB/s, measured now"""
+    ctx = ctx or default_context()
+    out = (C.c_double * 3)()
+    _check(lib.ryo_measure_peaks(ctx.handle, out, _stream(stream)), ctx)
+    return dict(fp32_tflops=out[0], fp32x2_tflops=out[1], copy_gbs=out[2])
 
 
 def solve_arrays(ctx: Context | None = None, device=None) -> dict:

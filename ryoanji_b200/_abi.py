@@ -58,13 +58,14 @@ class TreeView(C.Structure):
 class SolveParams(C.Structure):
     _fields_ = [("bucketSize", C.c_uint), ("groupSize", C.c_uint), ("theta", C.c_float), ("G", C.c_float),
                 ("useBox", C.c_int), ("box", BoxF32), ("numShells", C.c_int), ("ewald", EwaldSettings),
-                ("stackCapacity", C.c_int)]
+                ("stackCapacity", C.c_int), ("timing", C.c_int)]
 
 
 class SolveStats(C.Structure):
     _fields_ = [("numLeaves", C.c_int), ("numNodes", C.c_int), ("numGroups", C.c_int), ("sumP2P", C.c_uint64),
                 ("maxP2P", C.c_uint64), ("sumM2P", C.c_uint64), ("maxM2P", C.c_uint64), ("maxStack", C.c_uint64),
-                ("retries", C.c_uint64), ("potentialEnergy", C.c_double), ("box", C.c_float * 6)]
+                ("retries", C.c_uint64), ("potentialEnergy", C.c_double), ("box", C.c_float * 6),
+                ("ms", C.c_float * 6)]
 
 
 class SolveArrays(C.Structure):
@@ -128,6 +129,8 @@ SIGNATURES = {
     "ryo_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "ryo_solve_f32": (_i, [_p, C.POINTER(SolveParams)] + [_p] * 8 + [_sz] + [_p] * 5 + [C.POINTER(SolveStats), _p]),
     "ryo_solve_arrays_get": (_i, [_p, C.POINTER(SolveArrays)]),
+    "ryo_kernel_launches": (C.c_uint64, []),
+    "ryo_measure_peaks": (_i, [_p, C.POINTER(_d), _p]),
 }
 
 

@@ -396,10 +396,12 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
     uint32_t* failed      = ctx->scratch<uint32_t>("trav.failed", std::max<uint32_t>(numGroups, 1), s);
     t.failedGroups        = failed;
     t.failedCapacity      = numGroups;
-    bool first            = true;
+    int pass              = 0;
+    bool flip             = false; // alternates the scratch buffers of successive split passes
     while (t.numGroups > 0)
     {
-        if (!first) launchTraversalReset(ctx->ctl, false, s);
+        if (pass > 0) launchTraversalReset(ctx->ctl, false, s);
+        ++pass;
         launchTraverse(t, ctx->smCount, s);
         unsigned int numFailed = 0;
         RYO_CUDA(cudaMemcpyAsync(&numFailed, &ctx->ctl->failedCount, sizeof(numFailed), cudaMemcpyDeviceToHost, s));
@@ -407,10 +409,10 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
         if (numFailed == 0) break;
         ctx->retries += numFailed;
         // split the failed groups on the device: halves along the SFC
-        uint32_t cap        = 2 * numFailed;
-        uint32_t* nStart    = ctx->scratch<uint32_t>(first ? "trav.splitA" : "trav.splitB", cap, s);
-        uint32_t* nEnd      = ctx->scratch<uint32_t>(first ? "trav.splitEndA" : "trav.splitEndB", cap, s);
-        unsigned int* cnt   = ctx->ctl->counters;
+        uint32_t cap      = 2 * numFailed;
+        uint32_t* nStart  = ctx->scratch<uint32_t>(flip ? "trav.splitB" : "trav.splitA", cap, s);
+        uint32_t* nEnd    = ctx->scratch<uint32_t>(flip ? "trav.splitEndB" : "trav.splitEndA", cap, s);
+        unsigned int* cnt = ctx->ctl->counters;
         RYO_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), s));
         splitGroupsKernel<<<ceilDiv(numFailed, 256), 256, 0, s>>>(failed, numFailed, t.groupStart, t.groupEnd, nStart,
                                                                    nEnd, cnt + 1, cnt);
@@ -419,9 +421,9 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
         RYO_CUDA(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
         RYO_CUDA(cudaStreamSynchronize(s));
         if (h[1] > 0) unsplittable = true;
-        // the new groups are traversed into fresh buffers of the other name so that starts/ends stay valid
-        uint32_t* keepStart = ctx->scratch<uint32_t>(first ? "trav.curA" : "trav.curB", std::max(h[0], 1u), s);
-        uint32_t* keepEnd   = ctx->scratch<uint32_t>(first ? "trav.curEndA" : "trav.curEndB", std::max(h[0], 1u), s);
+        // the new groups go to the buffer set not read by this pass
+        uint32_t* keepStart = ctx->scratch<uint32_t>(flip ? "trav.curB" : "trav.curA", std::max(h[0], 1u), s);
+        uint32_t* keepEnd   = ctx->scratch<uint32_t>(flip ? "trav.curEndB" : "trav.curEndA", std::max(h[0], 1u), s);
         RYO_CUDA(cudaMemcpyAsync(keepStart, nStart, h[0] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         RYO_CUDA(cudaMemcpyAsync(keepEnd, nEnd, h[0] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         t.groupStart = keepStart;
@@ -429,9 +431,9 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
         t.numGroups  = int(h[0]);
         t.groupM2P   = nullptr; // per-group counts are reported for unsplit groups only
         t.groupP2P   = nullptr;
-        first        = !first;
+        flip         = !flip;
         if (t.numGroups == 0) break;
-        failed           = ctx->scratch<uint32_t>(first ? "trav.failed" : "trav.failed2", t.numGroups, s);
+        failed           = ctx->scratch<uint32_t>(flip ? "trav.failedB" : "trav.failedA", t.numGroups, s);
         t.failedGroups   = failed;
         t.failedCapacity = uint32_t(t.numGroups);
     }
@@ -783,6 +785,17 @@ __global__ void packSolveBodies(const float* __restrict__ x, const float* __rest
 }
 } // namespace
 
+namespace
+{
+//! phase marks of a timed solve: 0 start, 1 sorted, 2 tree, 3 upsweep, 4 traversal, 5 Ewald, 6 end
+void mark(ryo_ctx* ctx, const ryo_solve_params* P, int i, cudaStream_t s)
+{
+    if (!P->timing) return;
+    if (!ctx->phaseEvents[i]) RYO_CUDA(cudaEventCreate(&ctx->phaseEvents[i]));
+    RYO_CUDA(cudaEventRecord(ctx->phaseEvents[i], s));
+}
+} // namespace
+
 extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, float* x, float* y, float* z, float* m,
                                     float* h, float* vx, float* vy, float* vz, size_t n, float* p, float* ax,
                                     float* ay, float* az, uint32_t* orderOut, ryo_solve_stats* stats,
@@ -797,6 +810,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                        REQUIRE(P->groupSize >= 1 && P->groupSize <= 64, "solve: groupSize must be in [1, 64]");
                        REQUIRE(P->bucketSize >= 1 && P->theta > 0.f, "solve: bad bucketSize or theta");
                        cudaStream_t s = stream;
+                       mark(ctx, P, 0, s);
 
                        // box: given, or the cube enclosing the data (exact min/max)
                        ryo_box_f32 box{};
@@ -846,6 +860,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                        }
                        if (orderOut)
                            RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+                       mark(ctx, P, 1, s);
                        float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
                        float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
                        packSolveBodies<<<ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
@@ -878,6 +893,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                        int levelRange[kMaxLevel + 2];
                        linkOctree(ctx, leaves, nl, oct, levelRange, s);
 
+                       mark(ctx, P, 2, s);
                        // fused upsweep: node records + FP64 root expansion
                        NodeRecord* records = ctx->scratch<NodeRecord>("solve.records", nn, s);
                        double* root        = ctx->scratch<double>("solve.root", 16, s);
@@ -885,6 +901,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                                           oct.parents, oct.prefixes, 1.0f / P->theta, dbox, records, nullptr, nullptr,
                                           root, s);
 
+                       mark(ctx, P, 3, s);
                        // groups and traversal
                        uint32_t numGroups = uint32_t((n + P->groupSize - 1) / P->groupSize);
                        uint32_t* groups   = ctx->scratch<uint32_t>("solve.groups", size_t(numGroups) + 1, s);
@@ -913,11 +930,14 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                        t.stackCapacity = P->stackCapacity;
                        uint32_t* gm2p  = ctx->scratch<uint32_t>("solve.groupM2P", numGroups, s);
                        uint32_t* gp2p  = ctx->scratch<uint32_t>("solve.groupP2P", numGroups, s);
+                       RYO_CUDA(cudaMemsetAsync(gm2p, 0, sizeof(uint32_t) * numGroups, s));
+                       RYO_CUDA(cudaMemsetAsync(gp2p, 0, sizeof(uint32_t) * numGroups, s));
                        t.groupM2P      = gm2p;
                        t.groupP2P      = gp2p;
                        double pot      = 0;
                        runTraversal(ctx, t, s, &pot);
                        double energy = 0.5 * double(P->G) * pot;
+                       mark(ctx, P, 4, s);
 
                        if (periodic)
                        {
@@ -936,6 +956,16 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                            RYO_CUDA(cudaMemcpyAsync(&he, ep, sizeof(double), cudaMemcpyDeviceToHost, s));
                            RYO_CUDA(cudaStreamSynchronize(s));
                            energy += 0.5 * double(P->G) * he;
+                       }
+                       mark(ctx, P, 5, s);
+                       mark(ctx, P, 6, s);
+                       float ms[6] = {0, 0, 0, 0, 0, 0};
+                       if (P->timing)
+                       {
+                           RYO_CUDA(cudaEventSynchronize(ctx->phaseEvents[6]));
+                           for (int i = 0; i < 5; ++i)
+                               RYO_CUDA(cudaEventElapsedTime(&ms[i], ctx->phaseEvents[i], ctx->phaseEvents[i + 1]));
+                           RYO_CUDA(cudaEventElapsedTime(&ms[5], ctx->phaseEvents[0], ctx->phaseEvents[6]));
                        }
                        {
                            ryo_solve_arrays& a = ctx->lastSolve;
@@ -981,7 +1011,10 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                            stats->retries         = ctx->retries;
                            stats->potentialEnergy = energy;
                            for (int i = 0; i < 6; ++i)
+                           {
                                stats->box[i] = box.limits[i];
+                               stats->ms[i]  = ms[i];
+                           }
                        }
                    });
 }
@@ -991,4 +1024,20 @@ extern "C" ryo_status ryo_solve_arrays_get(ryo_ctx_t* ctx, ryo_solve_arrays* out
     if (!ctx || !out) return RYO_ERR_BAD_ARG;
     *out = ctx->lastSolve;
     return RYO_OK;
+}
+
+// ==================================================================================================== measurement
+
+uint64_t& ryo::launchCounter()
+{
+    static uint64_t counter = 0;
+    return counter;
+}
+
+extern "C" uint64_t ryo_kernel_launches(void) { return ryo::launchCounter(); }
+
+extern "C" ryo_status ryo_measure_peaks(ryo_ctx_t* ctx, double* out3, ryo_stream_t stream)
+{
+    if (!ctx || !out3) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError, [&] { measurePeaks(ctx->smCount, out3, out3 + 1, out3 + 2, stream); });
 }

@@ -35,7 +35,15 @@ struct CudaError
         if (e_ != cudaSuccess) throw ::ryo::CudaError{e_, #call};                                                      \
     } while (0)
 
-#define RYO_LAUNCH_CHECK() RYO_CUDA(cudaGetLastError())
+//! counts every kernel launch of the library (reported by ryo_kernel_launches)
+uint64_t& launchCounter();
+
+#define RYO_LAUNCH_CHECK()                                                                                             \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        ++::ryo::launchCounter();                                                                                      \
+        RYO_CUDA(cudaGetLastError());                                                                                  \
+    } while (0)
 
 inline unsigned ceilDiv(size_t a, size_t b) { return unsigned((a + b - 1) / b); }
 

@@ -45,6 +45,7 @@ struct ryo_ctx
     unsigned long long hostStats[5] = {0, 0, 0, 0, 0};
     uint64_t retries                = 0;
     ryo_solve_arrays lastSolve      = {};
+    cudaEvent_t phaseEvents[7]      = {};
 
     struct Buffer
     {
@@ -79,6 +80,8 @@ struct ryo_ctx
 
     void releaseAll()
     {
+        for (auto& e : phaseEvents)
+            if (e) cudaEventDestroy(e);
         for (auto& kv : buffers)
             if (kv.second.ptr) cudaFree(kv.second.ptr);
         buffers.clear();
@@ -219,6 +222,9 @@ EwaldHost ewaldSetup(const double* mroot, const double* center, int replicaShell
 void launchEwaldGroups(const EwaldHost& e, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
                        const float* x, const float* y, const float* z, const float* m, float G, float* ugrav,
                        float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- probe.cu
+void measurePeaks(int smCount, double* fp32, double* fp32x2, double* copyGBs, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- direct.cu
 template<class T>

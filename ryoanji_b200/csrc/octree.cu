@@ -126,14 +126,15 @@ __global__ void leafWrite(const uint64_t* __restrict__ leafStart, const uint8_t*
     }
     if (q < numNE)
     {
-        uint32_t last          = q + 1 < numNE ? leafFirst[q + 1] : n;
-        counts[o + gap]        = last - first;
+        uint32_t last   = q + 1 < numNE ? leafFirst[q + 1] : n;
+        leaves[o + gap] = start;
+        counts[o + gap] = last - first;
         if (layout) layout[o + gap] = first;
     }
     else
     {
-        leaves[o] = kKeyEnd;
-        if (layout) layout[o] = n;
+        leaves[o + gap] = kKeyEnd;
+        if (layout) layout[o + gap] = n;
     }
 }
 
