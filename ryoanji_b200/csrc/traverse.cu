@@ -15,6 +15,10 @@
  *   - approximated cells and direct leaves are appended to per-warp lists in shared memory with ballot/popc
  *     compaction and evaluated in dense batches of 32 cells or 32 bodies whose data is staged in shared memory and
  *     read with broadcast loads, so the inner loops are FP32 arithmetic plus one rsqrt per interaction;
+ *   - the two targets of a lane are processed together with the packed f32x2 FMA/ADD/MUL of sm_100a, and the
+ *     staged sources are stored pre-duplicated (s, s) so every source operand is a ready register pair: one
+ *     instruction issues the work of two targets and the freed issue slots carry the rsqrt, shared-memory and
+ *     traversal instructions (the kernel is issue-bound with scalar FP32);
  *   - each batch accumulates into fresh registers and is added to the per-target sums with Kahan compensation;
  *   - the MAC test uses explicitly rounded single operations so that every decision is reproducible bit for bit.
  */
@@ -35,23 +39,51 @@ struct WarpSmem
     int m2p[kM2PCap + kWarp];
     int2 leaves[kLeafCap + kWarp];
     int leafScan[kLeafCap + kWarp];
-    float4 stage[3 * kWarp];
-    float stageH[kWarp];
+    // staged sources, every value duplicated: M2P 5 x 16 bytes per cell, P2P 2 x 16 + 8 bytes per body
+    float4 stage[5 * kWarp];
 };
+
+// ------------------------------------------------------------------------------------------------ packed f32x2
+
+using f2 = unsigned long long; // two floats: low half target 0, high half target 1
+
+__device__ __forceinline__ f2 pk(float lo, float hi)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk(f2 v, float& lo, float& hi) { asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v)); }
+__device__ __forceinline__ f2 add2(f2 a, f2 b)
+{
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b)
+{
+    f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b)
+{
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
+{
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
 
 __device__ __forceinline__ float rsqrtApprox(float x)
 {
     float y;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
-}
-
-__device__ __forceinline__ void kahanAdd(float& sum, float& comp, float v)
-{
-    float y = __fsub_rn(v, comp);
-    float t = __fadd_rn(sum, y);
-    comp    = __fsub_rn(__fsub_rn(t, sum), y);
-    sum     = t;
 }
 
 //! the reference's applyMAC (traversal_gpu.cu:77-84) with every operation rounded once
@@ -66,48 +98,83 @@ __device__ __forceinline__ bool macFails(float4 c, const float tc[3], const floa
     return norm2Exact(dx, dy, dz) < c.w;
 }
 
-//! M2P of one quadrupole (cartesian_qpole.hpp:152-176) into acc = (pot, ax, ay, az)
-__device__ __forceinline__ void m2p(float4& acc, float tx, float ty, float tz, float4 c, float4 q0, float4 q1)
+__device__ __forceinline__ f2 rsqrt2(f2 v)
 {
-    float rx = tx - c.x, ry = ty - c.y, rz = tz - c.z;
-    float r2  = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-    float rm1 = rsqrtApprox(r2);
-    float rm2 = rm1 * rm1;
-    float rm5 = rm2 * rm2 * rm1;
-    // q0 = (m, qxx, qxy, qxz), q1 = (qyy, qyz, qzz, trace)
-    float Qrx = fmaf(rx, q0.y, fmaf(ry, q0.z, rz * q0.w));
-    float Qry = fmaf(rx, q0.z, fmaf(ry, q1.x, rz * q1.y));
-    float Qrz = fmaf(rx, q0.w, fmaf(ry, q1.y, rz * q1.z));
-    float rQr = fmaf(rx, Qrx, fmaf(ry, Qry, rz * Qrz));
-    float mr1 = q0.x * rm1;
-    float f   = fmaf(-2.5f * rQr, rm5, -mr1) * rm2;
-    acc.x -= fmaf(0.5f * rm5, rQr, mr1);
-    acc.y = fmaf(rm5, Qrx, fmaf(f, rx, acc.y));
-    acc.z = fmaf(rm5, Qry, fmaf(f, ry, acc.z));
-    acc.w = fmaf(rm5, Qrz, fmaf(f, rz, acc.w));
+    float a, b;
+    upk(v, a, b);
+    return pk(rsqrtApprox(a), rsqrtApprox(b));
 }
 
-//! P2P (kernel.hpp:99-120) into acc = (pot, ax, ay, az)
-__device__ __forceinline__ void p2p(float4& acc, float4 ti, float4 sj, float hj)
+//! packed accumulators of a lane's two targets: P = -phi, X, Y, Z = acceleration
+struct Acc2
 {
-    float dx   = sj.x - ti.x, dy = sj.y - ti.y, dz = sj.z - ti.z;
-    float r2   = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    float hij  = ti.w + hj;
-    float r2e  = fmaxf(r2, hij * hij);
-    float invR = rsqrtApprox(r2e);
-    float m3   = sj.w * invR * (invR * invR);
-    acc.x      = fmaf(-m3, r2, acc.x);
-    acc.y      = fmaf(dx, m3, acc.y);
-    acc.z      = fmaf(dy, m3, acc.z);
-    acc.w      = fmaf(dz, m3, acc.w);
+    f2 p, x, y, z;
+};
+
+/*! M2P of one quadrupole (cartesian_qpole.hpp:152-176) for both targets; c* and q* are duplicated pairs.
+ *  q = (qxx, qxy, qxz, qyy, qyz, qzz) traceless x3, m the mass. */
+__device__ __forceinline__ void m2p2(Acc2& A, f2 tx, f2 ty, f2 tz, f2 cx, f2 cy, f2 cz, f2 m, f2 qxx, f2 qxy,
+                                     f2 qxz, f2 qyy, f2 qyz, f2 qzz)
+{
+    const f2 kM25  = 0xC0200000C0200000ull; // (-2.5f, -2.5f)
+    const f2 kHalf = 0x3F0000003F000000ull; // (0.5f, 0.5f)
+    f2 rx  = sub2(tx, cx), ry = sub2(ty, cy), rz = sub2(tz, cz);
+    f2 r2  = fma2(rx, rx, fma2(ry, ry, mul2(rz, rz)));
+    f2 rm1 = rsqrt2(r2);
+    f2 rm2 = mul2(rm1, rm1);
+    f2 rm5 = mul2(mul2(rm2, rm2), rm1);
+    f2 Qrx = fma2(rx, qxx, fma2(ry, qxy, mul2(rz, qxz)));
+    f2 Qry = fma2(rx, qxy, fma2(ry, qyy, mul2(rz, qyz)));
+    f2 Qrz = fma2(rx, qxz, fma2(ry, qyz, mul2(rz, qzz)));
+    f2 rQr = fma2(rx, Qrx, fma2(ry, Qry, mul2(rz, Qrz)));
+    f2 mr1 = mul2(m, rm1);
+    f2 t   = mul2(rQr, rm5);
+    f2 f   = mul2(sub2(mul2(t, kM25), mr1), rm2);
+    A.p    = add2(A.p, fma2(t, kHalf, mr1));
+    A.x    = fma2(rm5, Qrx, fma2(f, rx, A.x));
+    A.y    = fma2(rm5, Qry, fma2(f, ry, A.y));
+    A.z    = fma2(rm5, Qrz, fma2(f, rz, A.z));
+}
+
+/*! P2P (kernel.hpp:99-120) for both targets against one source; s* are duplicated pairs, th the targets' h */
+__device__ __forceinline__ void p2p2(Acc2& A, f2 tx, f2 ty, f2 tz, f2 th, f2 sx, f2 sy, f2 sz, f2 sm, f2 sh)
+{
+    f2 dx  = sub2(sx, tx), dy = sub2(sy, ty), dz = sub2(sz, tz);
+    f2 r2  = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    f2 hij = add2(th, sh);
+    f2 hh  = mul2(hij, hij);
+    float r0, r1, h0, h1;
+    upk(r2, r0, r1);
+    upk(hh, h0, h1);
+    f2 ir  = pk(rsqrtApprox(fmaxf(r0, h0)), rsqrtApprox(fmaxf(r1, h1)));
+    f2 m3  = mul2(mul2(sm, ir), mul2(ir, ir));
+    A.p    = fma2(m3, r2, A.p);
+    A.x    = fma2(dx, m3, A.x);
+    A.y    = fma2(dy, m3, A.y);
+    A.z    = fma2(dz, m3, A.z);
 }
 
 struct TargetState
 {
-    float4 ti[2];   // x, y, z, h of the two targets of this lane (shifted by the current replica)
-    float4 acc[2];  // pot, ax, ay, az
-    float4 comp[2]; // Kahan compensation
+    f2 tx, ty, tz, th; // the lane's two targets (shifted by the current replica)
+    Acc2 acc;          // -phi, a
+    Acc2 comp;         // Kahan compensation of acc
 };
+
+__device__ __forceinline__ void kahan2(f2& sum, f2& comp, f2 v)
+{
+    f2 y = sub2(v, comp);
+    f2 t = add2(sum, y);
+    comp = sub2(sub2(t, sum), y);
+    sum  = t;
+}
+
+__device__ __forceinline__ Acc2 zero2()
+{
+    Acc2 a;
+    a.p = a.x = a.y = a.z = 0ull;
+    return a;
+}
 
 //! node data from the packed 64-byte records of the solver path
 struct RecordNodes
@@ -179,16 +246,12 @@ struct SoABodies
     __device__ __forceinline__ float scalar(int i) const { return __ldg(s + i); }
 };
 
-__device__ __forceinline__ void addBatch(TargetState& T, const float4 part[2])
+__device__ __forceinline__ void addBatch(TargetState& T, const Acc2& part)
 {
-#pragma unroll
-    for (int k = 0; k < 2; ++k)
-    {
-        kahanAdd(T.acc[k].x, T.comp[k].x, part[k].x);
-        kahanAdd(T.acc[k].y, T.comp[k].y, part[k].y);
-        kahanAdd(T.acc[k].z, T.comp[k].z, part[k].z);
-        kahanAdd(T.acc[k].w, T.comp[k].w, part[k].w);
-    }
+    kahan2(T.acc.p, T.comp.p, part.p);
+    kahan2(T.acc.x, T.comp.x, part.x);
+    kahan2(T.acc.y, T.comp.y, part.y);
+    kahan2(T.acc.z, T.comp.z, part.z);
 }
 
 //! evaluate the first @p count (<= 32) pending cells
@@ -200,30 +263,31 @@ __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState&
     {
         float4 c, q0, q1;
         nodes.multipole(S.m2p[lane], c, q0, q1);
-        S.stage[3 * lane]     = c;
-        S.stage[3 * lane + 1] = q0;
-        S.stage[3 * lane + 2] = q1;
+        float4* st = S.stage + 5 * lane;
+        st[0]      = make_float4(c.x, c.x, c.y, c.y);
+        st[1]      = make_float4(c.z, c.z, q0.x, q0.x);
+        st[2]      = make_float4(q0.y, q0.y, q0.z, q0.z);
+        st[3]      = make_float4(q0.w, q0.w, q1.x, q1.x);
+        st[4]      = make_float4(q1.y, q1.y, q1.z, q1.z);
     }
     __syncwarp();
-    float4 part[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+    const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
+    Acc2 part            = zero2();
+    auto one = [&](int j)
+    {
+        ulonglong2 a = st[5 * j], b = st[5 * j + 1], c = st[5 * j + 2], d = st[5 * j + 3], e = st[5 * j + 4];
+        m2p2(part, T.tx, T.ty, T.tz, a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y);
+    };
     if (count == kWarp)
     {
 #pragma unroll 4
         for (int j = 0; j < kWarp; ++j)
-        {
-            float4 c = S.stage[3 * j], q0 = S.stage[3 * j + 1], q1 = S.stage[3 * j + 2];
-            m2p(part[0], T.ti[0].x, T.ti[0].y, T.ti[0].z, c, q0, q1);
-            m2p(part[1], T.ti[1].x, T.ti[1].y, T.ti[1].z, c, q0, q1);
-        }
+            one(j);
     }
     else
     {
         for (int j = 0; j < count; ++j)
-        {
-            float4 c = S.stage[3 * j], q0 = S.stage[3 * j + 1], q1 = S.stage[3 * j + 2];
-            m2p(part[0], T.ti[0].x, T.ti[0].y, T.ti[0].z, c, q0, q1);
-            m2p(part[1], T.ti[1].x, T.ti[1].y, T.ti[1].z, c, q0, q1);
-        }
+            one(j);
     }
     addBatch(T, part);
     __syncwarp();
@@ -260,34 +324,34 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
                 if (S.leafScan[mid] > r) hi = mid;
                 else lo = mid + 1;
             }
-            int2 lf    = S.leaves[lo];
-            int body   = lf.x + (r - (S.leafScan[lo] - lf.y));
-            S.stage[lane]  = src.vec(body);
-            S.stageH[lane] = src.scalar(body);
+            int2 lf   = S.leaves[lo];
+            int body  = lf.x + (r - (S.leafScan[lo] - lf.y));
+            float4 sj = src.vec(body);
+            float hj  = src.scalar(body);
+            S.stage[2 * lane]     = make_float4(sj.x, sj.x, sj.y, sj.y);
+            S.stage[2 * lane + 1] = make_float4(sj.z, sj.z, sj.w, sj.w);
+            reinterpret_cast<float2*>(S.stage + 2 * kWarp)[lane] = make_float2(hj, hj);
         }
         __syncwarp();
-        int nvalid     = min(kWarp, total - b * kWarp);
-        float4 part[2] = {make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f)};
+        int nvalid           = min(kWarp, total - b * kWarp);
+        const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
+        const f2* sth        = reinterpret_cast<const f2*>(S.stage + 2 * kWarp);
+        Acc2 part            = zero2();
+        auto one = [&](int j)
+        {
+            ulonglong2 a = st[2 * j], c = st[2 * j + 1];
+            p2p2(part, T.tx, T.ty, T.tz, T.th, a.x, a.y, c.x, c.y, sth[j]);
+        };
         if (nvalid == kWarp)
         {
 #pragma unroll 8
             for (int j = 0; j < kWarp; ++j)
-            {
-                float4 sj = S.stage[j];
-                float hj  = S.stageH[j];
-                p2p(part[0], T.ti[0], sj, hj);
-                p2p(part[1], T.ti[1], sj, hj);
-            }
+                one(j);
         }
         else
         {
             for (int j = 0; j < nvalid; ++j)
-            {
-                float4 sj = S.stage[j];
-                float hj  = S.stageH[j];
-                p2p(part[0], T.ti[0], sj, hj);
-                p2p(part[1], T.ti[1], sj, hj);
-            }
+                one(j);
         }
         addBatch(T, part);
         __syncwarp();
@@ -374,21 +438,16 @@ __global__ void __launch_bounds__(kTravThreads)
 
         const int b = int(P.groupStart[g]), e = int(P.groupEnd[g]);
         TargetState T;
-        float lo[3], hi[3];
-#pragma unroll
-        for (int k = 0; k < 2; ++k)
-        {
-            int idx  = min(b + k * kWarp + lane, e - 1);
-            T.ti[k]  = tgt.vec(idx);
-            T.acc[k]  = make_float4(0.f, 0.f, 0.f, 0.f);
-            T.comp[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        lo[0] = fminf(T.ti[0].x, T.ti[1].x);
-        lo[1] = fminf(T.ti[0].y, T.ti[1].y);
-        lo[2] = fminf(T.ti[0].z, T.ti[1].z);
-        hi[0] = fmaxf(T.ti[0].x, T.ti[1].x);
-        hi[1] = fmaxf(T.ti[0].y, T.ti[1].y);
-        hi[2] = fmaxf(T.ti[0].z, T.ti[1].z);
+        float4 t0 = tgt.vec(min(b + lane, e - 1));
+        float4 t1 = tgt.vec(min(b + kWarp + lane, e - 1));
+        T.tx      = pk(t0.x, t1.x);
+        T.ty      = pk(t0.y, t1.y);
+        T.tz      = pk(t0.z, t1.z);
+        T.th      = pk(t0.w, t1.w);
+        T.acc     = zero2();
+        T.comp    = zero2();
+        float lo[3] = {fminf(t0.x, t1.x), fminf(t0.y, t1.y), fminf(t0.z, t1.z)};
+        float hi[3] = {fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y), fmaxf(t0.z, t1.z)};
         float tc[3], ts[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d)
@@ -411,13 +470,9 @@ __global__ void __launch_bounds__(kTravThreads)
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
                         tc[d] = __fadd_rn(tc[d], sh[d]);
-#pragma unroll
-                    for (int k = 0; k < 2; ++k)
-                    {
-                        T.ti[k].x = __fadd_rn(T.ti[k].x, sh[0]);
-                        T.ti[k].y = __fadd_rn(T.ti[k].y, sh[1]);
-                        T.ti[k].z = __fadd_rn(T.ti[k].z, sh[2]);
-                    }
+                    T.tx = add2(T.tx, pk(sh[0], sh[0]));
+                    T.ty = add2(T.ty, pk(sh[1], sh[1]));
+                    T.tz = add2(T.tz, pk(sh[2], sh[2]));
 
                     int sp = 1, nM = 0, nL = 0;
                     if (lane == 0) stack[0] = P.numNodes == 1 ? kRootOnly : P.initNode;
@@ -485,13 +540,9 @@ __global__ void __launch_bounds__(kTravThreads)
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
                         tc[d] = __fsub_rn(tc[d], sh[d]);
-#pragma unroll
-                    for (int k = 0; k < 2; ++k)
-                    {
-                        T.ti[k].x = __fsub_rn(T.ti[k].x, sh[0]);
-                        T.ti[k].y = __fsub_rn(T.ti[k].y, sh[1]);
-                        T.ti[k].z = __fsub_rn(T.ti[k].z, sh[2]);
-                    }
+                    T.tx = sub2(T.tx, pk(sh[0], sh[0]));
+                    T.ty = sub2(T.ty, pk(sh[1], sh[1]));
+                    T.tz = sub2(T.tz, pk(sh[2], sh[2]));
                 }
 
         if (overflow)
@@ -506,6 +557,12 @@ __global__ void __launch_bounds__(kTravThreads)
             continue;
         }
 
+        // Kahan: the compensated sum is acc - comp; acc.p holds -phi
+        float phi[2], gx[2], gy[2], gz[2];
+        upk(sub2(T.comp.p, T.acc.p), phi[0], phi[1]);
+        upk(sub2(T.acc.x, T.comp.x), gx[0], gx[1]);
+        upk(sub2(T.acc.y, T.comp.y), gy[0], gy[1]);
+        upk(sub2(T.acc.z, T.comp.z), gz[0], gz[1]);
         double pot = 0.0;
 #pragma unroll
         for (int k = 0; k < 2; ++k)
@@ -513,14 +570,12 @@ __global__ void __launch_bounds__(kTravThreads)
             int idx = b + k * kWarp + lane;
             if (idx < e)
             {
-                // Kahan: the compensated sum is acc - comp
-                float mi  = tgt.scalar(idx);
-                float phi = __fsub_rn(T.acc[k].x, T.comp[k].x);
-                pot += double(mi) * double(phi);
-                if (P.p) P.p[idx] += P.G * mi * phi;
-                P.ax[idx] += P.G * __fsub_rn(T.acc[k].y, T.comp[k].y);
-                P.ay[idx] += P.G * __fsub_rn(T.acc[k].z, T.comp[k].z);
-                P.az[idx] += P.G * __fsub_rn(T.acc[k].w, T.comp[k].w);
+                float mi = tgt.scalar(idx);
+                pot += double(mi) * double(phi[k]);
+                if (P.p) P.p[idx] += P.G * mi * phi[k];
+                P.ax[idx] += P.G * gx[k];
+                P.ay[idx] += P.G * gy[k];
+                P.az[idx] += P.G * gz[k];
             }
         }
         pot = warpSum(pot);
