@@ -118,6 +118,16 @@ extern "C"
     RYO_API ryo_status ryo_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf,
                                        uint32_t* valueBuf, void* tmp, size_t tmpBytes, ryo_stream_t stream);
 
+    /* The sort of ryo_sort_by_key for callers that cannot allocate device memory (a host whose pool allocator holds
+     * the free HBM, or a loop that cannot afford the device-wide wait of cudaFree). It has no counterpart in the
+     * reference. Its scratch is one fixed device array per device, so it takes no tmp argument and allocates
+     * nothing; n is at most RYO_SORT_STATIC_MAX_KEYS, a larger n returns RYO_ERR_CAPACITY and sorts nothing.
+     * The first call on a device looks up that array's address (which may load the module): make it before any
+     * stream capture. Calls on one device share the array: calls that overlap in time race, so serialise them. */
+#define RYO_SORT_STATIC_MAX_KEYS (1u << 24)
+    RYO_API ryo_status ryo_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf,
+                                              uint32_t* valueBuf, ryo_stream_t stream);
+
     /* cstone::computeOctree / updateOctreeGpu to convergence (cstone/include/cstone/tree/csarray.hpp:409-440,
      * update_gpu.cuh:43-68): the cornerstone leaf array of sorted keys with at most @p bucketSize particles per
      * leaf. Built in one pass (no host-synchronised rebalance loop); identical to the reference's fixed point.

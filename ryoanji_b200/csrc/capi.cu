@@ -4,6 +4,7 @@
  * Every entry point catches CUDA failures and turns them into a ryo_status with a message (the reference exits
  * the process instead, cstone/include/cstone/cuda/errorcheck.cuh:15-27). Scratch memory is owned by the context
  * (or the TreeBuilder) and grows on demand; nothing is kept in global device symbols, so contexts are independent.
+ * The one exception is ryo_sort_by_key_static, whose scratch is a fixed device array shared by all its callers.
  */
 #include <algorithm>
 #include <cstdio>
@@ -242,6 +243,22 @@ extern "C" ryo_status ryo_sort_by_key(uint64_t* keys, uint32_t* values, size_t n
                        RYO_CUDA(cudaMemcpyAsync(&err, flag, sizeof(err), cudaMemcpyDeviceToHost, stream));
                        RYO_CUDA(cudaStreamSynchronize(stream));
                        if (err) throw ApiError{RYO_ERR_TIMEOUT, "sort_by_key: look-back wait timed out"};
+                   });
+}
+
+extern "C" ryo_status ryo_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf,
+                                             uint32_t* valueBuf, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       if (n == 0) return;
+                       REQUIRE(keys && values && keyBuf && valueBuf, "sort_by_key_static: null argument");
+                       if (n > staticSortMaxKeys())
+                           throw ApiError{RYO_ERR_CAPACITY, "sort_by_key_static: more than RYO_SORT_STATIC_MAX_KEYS "
+                                                            "keys; use ryo_sort_by_key with caller storage"};
+                       if (sortPairsStaticScratch(keys, values, keyBuf, valueBuf, n, stream))
+                           throw ApiError{RYO_ERR_TIMEOUT, "sort_by_key_static: look-back wait timed out"};
                    });
 }
 

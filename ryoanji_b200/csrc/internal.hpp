@@ -106,6 +106,10 @@ void launchGatherT(const uint32_t* order, const T* in, T* out, size_t n, cudaStr
 //! out[i] = sum(in[0:i]) for i in [0, n]; out has n + 1 entries (out[n] = total); in-place allowed
 void exclusiveScanU32(ryo_ctx* ctx, const uint32_t* in, uint32_t* out, size_t n, cudaStream_t s);
 
+size_t staticSortMaxKeys();
+//! sort of bits [0, 64) whose scratch is a fixed device array (no allocation); true if a look-back wait timed out
+bool sortPairsStaticScratch(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_t* valuesAlt, size_t n,
+                            cudaStream_t s);
 size_t sortTempBytes(size_t n);
 /*! stable LSD sort of (keys, values) on bits [beginBit, endBit). Ping-pongs between (keys, values) and
  *  (keysAlt, valuesAlt), all four buffers of n elements; returns true if the result is in the Alt buffers.

@@ -7,6 +7,8 @@
  * with decoupled look-back (bounded waits), stage the tile in shared memory in digit order and write coalesced runs.
  * The sort is stable (keys and payload indices keep their input order within equal keys), as the reference needs.
  */
+#include <mutex>
+
 #include "internal.hpp"
 
 namespace ryo
@@ -384,6 +386,67 @@ bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_
         inAlt = !inAlt;
     }
     return inAlt;
+}
+
+
+// ------------------------------------------------------------------------------------------------ fixed scratch
+
+/*
+ * Scratch for the sort entry point that takes no temporary-storage argument. Some callers cannot allocate device
+ * memory for a sort: a host whose pool allocator has already reserved the free HBM has nothing left for cudaMalloc,
+ * and cudaFree waits for the whole device, which a caller sorting inside a latency-bound loop cannot afford. For them
+ * the digit histograms, tile tickets, look-back status words and the wait-timeout flag live in this one array,
+ * sized for kStaticSortMaxKeys keys. Its storage is created with the module on each device; no call allocates.
+ * Every call clears what must start at zero (histograms, tickets, status words, flag) on its stream before the
+ * first pass reads it. All calls on a device share the array, so calls that overlap in time race and corrupt each
+ * other's results: callers serialise them (one stream, or their own ordering between streams and threads).
+ */
+constexpr size_t kStaticSortMaxKeys = size_t(1) << 24;
+constexpr size_t kStaticSortBytes   = size_t(12) << 20;
+
+static __device__ __align__(256) unsigned char staticSortScratch[kStaticSortBytes];
+
+size_t staticSortMaxKeys() { return kStaticSortMaxKeys; }
+
+//! the array's device address on the current device, looked up on the first call for that device
+static void* staticSortScratchAddress()
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex lock;
+    static void* address[kMaxDevices] = {};
+    int dev = 0;
+    RYO_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw CudaError{cudaErrorInvalidDevice, "static sort: device ordinal"};
+    std::lock_guard<std::mutex> guard(lock);
+    if (!address[dev])
+    {
+        void* p = nullptr;
+        RYO_CUDA(cudaGetSymbolAddress(&p, staticSortScratch));
+        if (!p) throw CudaError{cudaErrorInvalidSymbol, "static sort: scratch symbol has no address"};
+        address[dev] = p;
+    }
+    return address[dev];
+}
+
+bool sortPairsStaticScratch(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_t* valuesAlt, size_t n,
+                            cudaStream_t s)
+{
+    if (n > kStaticSortMaxKeys) throw CudaError{cudaErrorInvalidValue, "static sort: too many keys"};
+    size_t need = sortTempBytes(n);
+    if (need + 64 > kStaticSortBytes) throw CudaError{cudaErrorInvalidValue, "static sort: scratch too small"};
+    char* base         = static_cast<char*>(staticSortScratchAddress());
+    unsigned int* flag = reinterpret_cast<unsigned int*>(base + kStaticSortBytes - 64);
+    RYO_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned int), s));
+    bool alt = radixSortPairs(keys, values, keysAlt, valuesAlt, n, 0, 64, base, need, flag, s, false);
+    if (alt)
+    {
+        RYO_CUDA(cudaMemcpyAsync(keys, keysAlt, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        RYO_CUDA(cudaMemcpyAsync(values, valuesAlt, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    }
+    unsigned int err = 0;
+    RYO_CUDA(cudaMemcpyAsync(&err, flag, sizeof(err), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaStreamSynchronize(s));
+    return err != 0;
 }
 
 } // namespace ryo
