@@ -1,0 +1,354 @@
+/*
+ * ryoanji-b200 — C++ drop-in surface over the C ABI (header only, C++17).
+ *
+ * Re-creates the template signatures that the reference's callers use (ryoanji/src/ryoanji/interface/
+ * treebuilder.cuh:34-125, ryoanji/src/ryoanji/nbody/traversal_gpu.h:51-70, upsweep_gpu.h:24-41,
+ * interface/ewald.cuh:24-27, and the cstone execution::Gpu functions) for the instantiations that the B200 library
+ * implements: 64-bit keys, float coordinates, CartesianQuadrupole<float> multipoles (8 floats per node) and
+ * Vec4<float> source centres (4 floats per node). Device arrays are device pointers, as in the reference.
+ *
+ * Differences a caller sees:
+ *   - everything lives in namespace ryo (a caller switches with `namespace ryoanji = ryo;` or by renaming);
+ *   - failures throw ryo::Error (status + message) instead of exiting the process;
+ *   - each function takes an optional stream (last argument) and an optional ryo::Context; the default context
+ *     is the current device's;
+ *   - traverse ignores gmPool: the traversal stack lives in shared memory. stackSize() returns 0 so a caller that
+ *     sizes gmPool from it allocates nothing.
+ */
+#ifndef RYOANJI_B200_RYOANJI_HPP
+#define RYOANJI_B200_RYOANJI_HPP
+
+#include <array>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+
+#include "../ryoanji_b200.h"
+
+namespace ryo
+{
+
+using TreeNodeIndex = int;
+using LocalIndex    = uint32_t;
+
+class Error : public std::runtime_error
+{
+public:
+    Error(ryo_status s, const std::string& what)
+        : std::runtime_error(what)
+        , status(s)
+    {
+    }
+    ryo_status status;
+};
+
+inline void check(ryo_status s, const ryo_ctx_t* ctx = nullptr)
+{
+    if (s != RYO_OK)
+    {
+        std::string msg = ryo_status_string(s);
+        const char* detail = ryo_ctx_last_error(ctx);
+        if (detail && *detail) msg += std::string(": ") + detail;
+        throw Error(s, msg);
+    }
+}
+
+//! owning handle of a ryo_ctx (per-device counters, statistics, scratch)
+class Context
+{
+public:
+    explicit Context(int device = 0)
+    {
+        ryo_ctx_t* h = nullptr;
+        check(ryo_ctx_create(device, &h));
+        h_.reset(h);
+    }
+    ryo_ctx_t* get() const { return h_.get(); }
+
+private:
+    struct Del
+    {
+        void operator()(ryo_ctx_t* c) const { ryo_ctx_destroy(c); }
+    };
+    std::unique_ptr<ryo_ctx_t, Del> h_;
+};
+
+inline Context& defaultContext()
+{
+    static Context ctx(0);
+    return ctx;
+}
+
+//! the subset of cstone::Box<T> (cstone/include/cstone/sfc/box.hpp:99-213) that the gravity path reads
+enum class BoundaryType : int
+{
+    open     = RYO_BOUNDARY_OPEN,
+    periodic = RYO_BOUNDARY_PERIODIC,
+    fixed    = RYO_BOUNDARY_FIXED,
+};
+
+template<class T>
+class Box
+{
+public:
+    Box(T xmin, T xmax, T ymin, T ymax, T zmin, T zmax, BoundaryType bx = BoundaryType::open,
+        BoundaryType by = BoundaryType::open, BoundaryType bz = BoundaryType::open)
+        : lim_{xmin, xmax, ymin, ymax, zmin, zmax}
+        , bnd_{int(bx), int(by), int(bz)}
+    {
+    }
+    Box(T lo, T hi, BoundaryType b = BoundaryType::open)
+        : Box(lo, hi, lo, hi, lo, hi, b, b, b)
+    {
+    }
+    T xmin() const { return lim_[0]; }
+    T xmax() const { return lim_[1]; }
+    T ymin() const { return lim_[2]; }
+    T ymax() const { return lim_[3]; }
+    T zmin() const { return lim_[4]; }
+    T zmax() const { return lim_[5]; }
+    T lx() const { return lim_[1] - lim_[0]; }
+    T ly() const { return lim_[3] - lim_[2]; }
+    T lz() const { return lim_[5] - lim_[4]; }
+    BoundaryType boundaryX() const { return BoundaryType(bnd_[0]); }
+    BoundaryType boundaryY() const { return BoundaryType(bnd_[1]); }
+    BoundaryType boundaryZ() const { return BoundaryType(bnd_[2]); }
+
+    ryo_box_f32 abiF32() const
+    {
+        ryo_box_f32 b{};
+        for (int i = 0; i < 6; ++i)
+            b.limits[i] = float(lim_[i]);
+        for (int i = 0; i < 3; ++i)
+            b.boundary[i] = bnd_[i];
+        return b;
+    }
+    ryo_box_f64 abiF64() const
+    {
+        ryo_box_f64 b{};
+        for (int i = 0; i < 6; ++i)
+            b.limits[i] = double(lim_[i]);
+        for (int i = 0; i < 3; ++i)
+            b.boundary[i] = bnd_[i];
+        return b;
+    }
+
+private:
+    std::array<T, 6> lim_;
+    std::array<int, 3> bnd_;
+};
+
+//! cstone::GroupView (cstone/include/cstone/traversal/groups.hpp:28-35)
+struct GroupView
+{
+    LocalIndex firstBody, lastBody, numGroups;
+    const LocalIndex* groupStart;
+    const LocalIndex* groupEnd;
+
+    ryo_group_view abi() const { return ryo_group_view{firstBody, lastBody, numGroups, groupStart, groupEnd}; }
+};
+
+template<class T>
+struct Vec3
+{
+    T x, y, z;
+};
+
+//! ryoanji::TreeBuilder (ryoanji/src/ryoanji/interface/treebuilder.cuh:34-125); the returned pointers stay valid
+//! until the next update
+template<class KeyType>
+class TreeBuilder
+{
+    static_assert(std::is_same_v<KeyType, uint64_t>, "the B200 library builds 64-bit key trees");
+
+public:
+    explicit TreeBuilder(unsigned ncrit, Context& ctx = defaultContext())
+        : ctx_(&ctx)
+    {
+        ryo_treebuilder_t* h = nullptr;
+        check(ryo_treebuilder_create(ctx.get(), ncrit, &h), ctx.get());
+        h_.reset(h);
+    }
+
+    //! sorts x, y, z in place along the SFC, builds the tree, returns the total node count
+    template<class T>
+    int update(T* x, T* y, T* z, size_t numBodies, const Box<T>& box, ryo_stream_t stream = nullptr)
+    {
+        static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "float or double coordinates");
+        int numNodes = 0;
+        if constexpr (std::is_same_v<T, float>)
+        {
+            ryo_box_f32 b = box.abiF32();
+            check(ryo_treebuilder_update_f32(h_.get(), x, y, z, numBodies, &b, &numNodes, stream), ctx_->get());
+        }
+        else
+        {
+            ryo_box_f64 b = box.abiF64();
+            check(ryo_treebuilder_update_f64(h_.get(), x, y, z, numBodies, &b, &numNodes, stream), ctx_->get());
+        }
+        check(ryo_treebuilder_view(h_.get(), &view_), ctx_->get());
+        return numNodes;
+    }
+
+    const LocalIndex* layout() const { return view_.layout; }
+    const KeyType* nodeKeys() const { return view_.nodeKeys; }
+    const TreeNodeIndex* childOffsets() const { return view_.childOffsets; }
+    const TreeNodeIndex* leafToInternal() const { return view_.leafToInternal; }
+    const TreeNodeIndex* internalToLeaf() const { return view_.internalToLeaf; }
+    const TreeNodeIndex* levelRange() const { return view_.levelRange; } // host pointer, as in the reference
+    TreeNodeIndex numLeafNodes() const { return view_.numLeafNodes; }
+    unsigned maxTreeLevel() const { return view_.maxTreeLevel; }
+    //! not in the reference: the SFC permutation applied to x, y, z by the last update
+    const LocalIndex* order() const { return view_.order; }
+
+private:
+    struct Del
+    {
+        void operator()(ryo_treebuilder_t* t) const { ryo_treebuilder_destroy(t); }
+    };
+    Context* ctx_;
+    std::unique_ptr<ryo_treebuilder_t, Del> h_;
+    ryo_tree_view view_{};
+};
+
+//! cstone::computeSfcKeys for the GPU (cstone/include/cstone/sfc/sfc_gpu.h)
+template<class T>
+void computeSfcKeys(const T* x, const T* y, const T* z, uint64_t* keys, size_t numKeys, const Box<T>& box,
+                    ryo_stream_t stream = nullptr)
+{
+    if constexpr (std::is_same_v<T, float>)
+    {
+        ryo_box_f32 b = box.abiF32();
+        check(ryo_compute_sfc_keys_f32(x, y, z, keys, numKeys, &b, stream));
+    }
+    else
+    {
+        ryo_box_f64 b = box.abiF64();
+        check(ryo_compute_sfc_keys_f64(x, y, z, keys, numKeys, &b, stream));
+    }
+}
+
+//! cstone::computeFixedGroups (cstone/include/cstone/traversal/groups_gpu.cuh): groups[0..] hold the starts and
+//! the final end; ceil((last - first) / groupSize) + 1 entries
+inline void computeFixedGroups(LocalIndex first, LocalIndex last, unsigned groupSize, LocalIndex* groups,
+                               ryo_stream_t stream = nullptr)
+{
+    check(ryo_compute_fixed_groups(first, last, groupSize, groups, stream));
+}
+
+//! cstone::computeLeafSourceCenterGpu (cstone/include/cstone/focus/source_center_gpu.h)
+inline void computeLeafSourceCenterGpu(const float* x, const float* y, const float* z, const float* m,
+                                       const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
+                                       const LocalIndex* layout, float* centers /* Vec4<float> */,
+                                       ryo_stream_t stream = nullptr)
+{
+    check(ryo_compute_leaf_source_center_f32(x, y, z, m, leafToInternal, numLeaves, layout, centers, stream));
+}
+
+//! cstone::upsweepCentersGpu; levelRange is a host pointer as in the reference
+inline void upsweepCentersGpu(int numLevels, const TreeNodeIndex* levelRange, const TreeNodeIndex* childOffsets,
+                              float* centers, ryo_stream_t stream = nullptr)
+{
+    check(ryo_upsweep_centers_f32(numLevels, levelRange, childOffsets, centers, stream));
+}
+
+//! cstone::setMacGpu with the vector MAC
+inline void setMacGpu(const uint64_t* prefixes, TreeNodeIndex numNodes, float* centers, float invTheta,
+                      const Box<float>& box, ryo_stream_t stream = nullptr)
+{
+    ryo_box_f32 b = box.abiF32();
+    check(ryo_set_mac_f32(prefixes, numNodes, centers, invTheta, &b, stream));
+}
+
+//! ryoanji::computeLeafMultipoles (upsweep_gpu.h:24-28), CartesianQuadrupole<float>
+inline void computeLeafMultipoles(const float* x, const float* y, const float* z, const float* m,
+                                  const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
+                                  const LocalIndex* layout, const float* centers, float* multipoles,
+                                  ryo_stream_t stream = nullptr)
+{
+    check(ryo_compute_leaf_multipoles_f32(x, y, z, m, leafToInternal, numLeaves, layout, centers, multipoles,
+                                          stream));
+}
+
+//! ryoanji::upsweepMultipoles (upsweep_gpu.h:39-41) for cells [firstCell, lastCell) of one level
+inline void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
+                              const float* centers, float* multipoles, ryo_stream_t stream = nullptr)
+{
+    check(ryo_upsweep_multipoles_f32(firstCell, lastCell, childOffsets, centers, multipoles, stream));
+}
+
+inline int bhMaxTargetSize() { return ryo_bh_max_target_size(); }
+inline LocalIndex stackSize(LocalIndex numGroups) { return ryo_stack_size(numGroups); }
+
+/*! ryoanji::traverse (traversal_gpu.h:51-56) for Tc = Th = Tm = Ta = Tf = float, MType = CartesianQuadrupole<float>.
+ *  Accumulates into p (may be null), ax, ay, az and returns the total potential 0.5 G sum m phi. */
+inline double traverse(GroupView grp, int initNodeIdx, const float* xt, const float* yt, const float* zt,
+                       const float* mt, const float* ht, const float* xs, const float* ys, const float* zs,
+                       const float* ms, const float* hs, const TreeNodeIndex* childOffsets,
+                       const TreeNodeIndex* internalToLeaf, const LocalIndex* layout, const float* sourceCenter,
+                       const float* multipoles, float G, int numShells, Vec3<float> boxL, float* p, float* ax,
+                       float* ay, float* az, int* /* gmPool: unused */, Context& ctx = defaultContext(),
+                       ryo_stream_t stream = nullptr)
+{
+    ryo_group_view g = grp.abi();
+    float L[3]       = {boxL.x, boxL.y, boxL.z};
+    double total     = 0;
+    check(ryo_traverse_f32(ctx.get(), &g, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
+                           internalToLeaf, layout, sourceCenter, multipoles, G, numShells, L, p, ax, ay, az, &total,
+                           stream),
+          ctx.get());
+    return total;
+}
+
+//! ryoanji::readBhStats (traversal_gpu.h:64-65): sumP2P, maxP2P, sumM2P, maxM2P, maxStack
+inline std::array<uint64_t, 5> readBhStats(Context& ctx = defaultContext())
+{
+    std::array<uint64_t, 5> s{};
+    check(ryo_read_bh_stats(ctx.get(), s.data()), ctx.get());
+    return s;
+}
+
+inline uint64_t readTraversalRetries(Context& ctx = defaultContext()) { return ryo_read_traversal_retries(ctx.get()); }
+
+//! ryoanji::EwaldSettings (ryoanji/src/ryoanji/nbody/ewald.h:23-31) with the reference defaults
+inline ryo_ewald_settings defaultEwaldSettings()
+{
+    ryo_ewald_settings e{};
+    e.numReplicaShells     = 1;
+    e.lCut                 = 2.6;
+    e.hCut                 = 2.8;
+    e.alpha_scale          = 2.0;
+    e.small_R_scale_factor = 3.0e-3;
+    return e;
+}
+
+/*! ryoanji::computeGravityEwaldGpu (interface/ewald.cuh:24-27) for MType = CartesianQuadrupole<float>; Mroot is
+ *  the root's 8 multipole floats (host). Adds the Ewald correction to ugrav, ax, ay, az and to *ugravTot. */
+inline void computeGravityEwaldGpu(const Vec3<float>& rootCenter, const float* Mroot, GroupView grp, const float* x,
+                                   const float* y, const float* z, const float* m, const Box<float>& box, float G,
+                                   float* ugrav, float* ax, float* ay, float* az, double* ugravTot,
+                                   const ryo_ewald_settings& settings, Context& ctx = defaultContext(),
+                                   ryo_stream_t stream = nullptr)
+{
+    ryo_group_view g = grp.abi();
+    ryo_box_f32 b    = box.abiF32();
+    float rc[3]      = {rootCenter.x, rootCenter.y, rootCenter.z};
+    check(ryo_compute_gravity_ewald_f32(ctx.get(), rc, Mroot, &g, x, y, z, m, &b, G, ugrav, ax, ay, az, ugravTot,
+                                        &settings, stream),
+          ctx.get());
+}
+
+//! ryoanji::directSum (interface/multipole_holder.cuh:91-93): exact sums for targets [first, last)
+inline void directSum(size_t first, size_t last, size_t numBodies, Vec3<float> boxL, int numShells, const float* x,
+                      const float* y, const float* z, const float* m, const float* h, float* p, float* ax, float* ay,
+                      float* az, ryo_stream_t stream = nullptr)
+{
+    float L[3] = {boxL.x, boxL.y, boxL.z};
+    check(ryo_direct_sum_f32(first, last, numBodies, L, numShells, x, y, z, m, h, p, ax, ay, az, stream));
+}
+
+} // namespace ryo
+
+#endif

@@ -76,3 +76,29 @@ def test_cpp_shim_headers_compile():
     r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-x",
                         "c++", "-"], input=src, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-device path")
+def test_cpp_shim_links_and_reports_errors(tmp_path):
+    """a C++ caller of the drop-in header links against the library; without a device, creating a context throws
+    ryo::Error with the no-device status instead of exiting"""
+    from ryoanji_b200._abi import LIB_PATH
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include "ryoanji_b200/ryoanji.hpp"
+#include <cstdio>
+int main() {
+    if (ryo::bhMaxTargetSize() != 64 || ryo::stackSize(1000) != 0) return 2;
+    ryo::Box<float> box(-1.f, 1.f);
+    if (box.lx() != 2.f || box.boundaryX() != ryo::BoundaryType::open) return 3;
+    try { ryo::Context ctx(0); return 4; }
+    catch (const ryo::Error& e) { std::printf("%d %s\n", int(e.status), e.what()); return e.status == RYO_ERR_NO_DEVICE || e.status == RYO_ERR_CUDA ? 0 : 5; }
+}
+''')
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(LIB_PATH)
+    r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                        "-L", libdir, "-lryoanji_b200", f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert run.returncode == 0, (run.returncode, run.stdout, run.stderr)
