@@ -318,6 +318,34 @@ extern "C"
                                      float* ax, float* ay, float* az, uint32_t* order, ryo_solve_stats* stats,
                                      ryo_stream_t stream);
 
+    /* ------------------------------------------------------------------------------------------ batched solve
+     * Many independent systems solved together, one launch per phase (not in the reference, which solves one system
+     * per call). The body arrays are the systems' bodies concatenated: system s owns [firstBody, firstBody +
+     * numBodies), in order and without gaps. Each system gets its own box (given, or the cube enclosing its bodies),
+     * tree, groups, traversal and, for a periodic cubic box, Ewald correction; the results equal per-system calls of
+     * ryo_solve_f32 with the same box and parameters wherever the system's tree stops above level 21 - L, where
+     * L = ceil(log8(numSystems)) (at least 1) octree levels hold the system index. */
+#define RYO_BATCH_MAX_SYSTEMS 4096
+    typedef struct ryo_system
+    {
+        uint64_t firstBody;
+        uint32_t numBodies; /* >= 1 */
+        int useBox;         /* 0: the cube enclosing the system's bodies, open boundaries; 1: box below */
+        ryo_box_f32 box;    /* with useBox; periodic boxes must be cubic */
+        int numShells;      /* periodic replica shells of the traversal (periodic boxes only) */
+    } ryo_system;
+
+    /* params: bucketSize, groupSize, theta, G, ewald, stackCapacity and timing apply to every system (useBox, box and
+     * numShells of params are ignored). Bodies are SFC-sorted within their system on return, vx, vy, vz (may be
+     * NULL) permuted along; p, ax, ay, az overwritten; order (may be NULL) receives the original index of each
+     * sorted body. energies (host, numSystems, may be NULL): 0.5 G sum(m phi) per system; boxes (host, 6 floats per
+     * system, may be NULL): the box each system used. stats: totals over all systems. */
+    RYO_API ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params* params, const ryo_system* systems,
+                                           int numSystems, float* x, float* y, float* z, float* m, float* h, float* vx,
+                                           float* vy, float* vz, size_t n, float* p, float* ax, float* ay, float* az,
+                                           uint32_t* order, double* energies, float* boxes, ryo_solve_stats* stats,
+                                           ryo_stream_t stream);
+
     /* device arrays of the last ryo_solve_f32 on this context (valid until the next solve on it): the sorted keys,
      * permutation, tree and the packed node records the traversal read (16 floats per node: centre x, y, z, squared
      * MAC radius; multipole mass, qxx, qxy, qxz, qyy, qyz, qzz, trace; then 4 ints: first child, first body, body

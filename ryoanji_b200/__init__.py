@@ -21,7 +21,8 @@ __all__ = [
     "Box", "Context", "RyoError", "TreeBuilder", "SolveParams", "SolveResult", "EwaldSettings", "lib",
     "compute_sfc_keys", "compute_bounding_box", "sequence", "sort_by_key", "compute_octree", "build_octree",
     "compute_fixed_groups", "compute_leaf_source_center", "upsweep_centers", "compute_leaf_multipoles",
-    "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries",
+    "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch",
+    "BatchSystem", "BatchResult",
     "compute_gravity_ewald", "direct_sum", "direct_targets_f64", "solve", "solve_arrays", "bh_max_target_size",
     "kernel_launches", "measure_peaks",
     "stack_size",
@@ -518,6 +519,55 @@ def solve(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, v=Non
     ms = dict(zip(("sort", "tree", "upsweep", "traverse", "ewald", "total"), list(st.ms)))
     return SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
                        st.maxStack, st.retries, st.potentialEnergy, list(st.box), ms)
+
+
+@dataclass
+class BatchSystem:
+    """one system of a batched solve: @p num_bodies consecutive bodies; box None means the enclosing cube"""
+    num_bodies: int
+    box: Box | None = None
+    num_shells: int = 1
+
+
+@dataclass
+class BatchResult:
+    stats: SolveResult
+    energies: list
+    boxes: list
+
+
+MAX_BATCH_SYSTEMS = 4096
+
+
+def solve_batch(systems, x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, v=None, order=None,
+                ctx: Context | None = None, stream=None) -> BatchResult:
+    """Solve many independent systems in one launch per phase. The arrays hold the systems' bodies concatenated in
+    the order of @p systems (a list of BatchSystem); each system is sorted in place within its own range."""
+    ctx = ctx or default_context()
+    params = params or SolveParams()
+    pc = params.c()
+    ns = len(systems)
+    arr = (_abi.System * max(ns, 1))()
+    first = 0
+    for i, sy in enumerate(systems):
+        arr[i].firstBody = first
+        arr[i].numBodies = int(sy.num_bodies)
+        arr[i].useBox = 1 if sy.box is not None else 0
+        if sy.box is not None:
+            arr[i].box = sy.box.f32()
+        arr[i].numShells = int(sy.num_shells)
+        first += int(sy.num_bodies)
+    energies = (C.c_double * max(ns, 1))()
+    boxes = (C.c_float * (6 * max(ns, 1)))()
+    st = _abi.SolveStats()
+    vx, vy, vz = v if v is not None else (None, None, None)
+    _check(lib.ryo_solve_batch_f32(ctx.handle, C.byref(pc), arr, ns, _ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(h),
+                                   _ptr(vx), _ptr(vy), _ptr(vz), C.c_size_t(x.numel()), _ptr(p), _ptr(ax), _ptr(ay),
+                                   _ptr(az), _ptr(order), energies, boxes, C.byref(st), _stream(stream)), ctx)
+    ms = dict(zip(("sort", "tree", "upsweep", "traverse", "ewald", "total"), list(st.ms)))
+    res = SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
+                      st.maxStack, st.retries, st.potentialEnergy, [], ms)
+    return BatchResult(res, list(energies)[:ns], [list(boxes[6 * i:6 * i + 6]) for i in range(ns)])
 
 
 _solve_n: dict = {}

@@ -77,6 +77,11 @@ class SolveArrays(C.Structure):
                 ("rootCenter", C.c_double * 3), ("rootMultipole", C.c_double * 8)]
 
 
+class System(C.Structure):
+    _fields_ = [("firstBody", C.c_uint64), ("numBodies", C.c_uint32), ("useBox", C.c_int), ("box", BoxF32),
+                ("numShells", C.c_int)]
+
+
 _p = C.c_void_p
 _sz = C.c_size_t
 _i = C.c_int
@@ -130,6 +135,8 @@ SIGNATURES = {
     "ryo_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "ryo_solve_f32": (_i, [_p, C.POINTER(SolveParams)] + [_p] * 8 + [_sz] + [_p] * 5 + [C.POINTER(SolveStats), _p]),
     "ryo_solve_arrays_get": (_i, [_p, C.POINTER(SolveArrays)]),
+    "ryo_solve_batch_f32": (_i, [_p, C.POINTER(SolveParams), C.POINTER(System), _i] + [_p] * 8 + [_sz] + [_p] * 7
+                            + [C.POINTER(SolveStats), _p]),
     "ryo_kernel_launches": (C.c_uint64, []),
     "ryo_measure_peaks": (_i, [_p, C.POINTER(_d), _p]),
 }

@@ -1,0 +1,241 @@
+/*
+ * ryoanji-b200: kernels of the batched solve (many independent systems, one launch per phase).
+ *
+ * The systems are concatenated: system s owns the bodies [first[s], first[s + 1]). Each body's key is its system
+ * index in the top 3L bits (L = sysLevel octree levels) followed by the top 63 - 3L bits of its Hilbert key in the
+ * system's own box. Sorting these keys sorts every system along its own curve and keeps the systems in place; the
+ * cornerstone tree over them holds each system's tree below the level-L node of its prefix (leaves holding bodies
+ * are forced to level >= L so no leaf spans two systems). A system's tree equals its stand-alone tree wherever
+ * the stand-alone tree stops above level 21 - L.
+ *
+ * The reference solves one system per call (ryoanji/test/demo.cu:82-104); there is no batched counterpart.
+ */
+#include "internal.hpp"
+
+namespace ryo
+{
+
+//! order-preserving map of floats to unsigned integers (min/max by integer atomics)
+__device__ __forceinline__ uint32_t orderedBits(float f)
+{
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float orderedFloat(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+//! system of body i: the last s with first[s] <= i
+__device__ __forceinline__ uint32_t systemOf(const uint64_t* __restrict__ first, uint32_t numSystems, uint64_t i)
+{
+    uint32_t lo = 0, hi = numSystems - 1;
+    while (lo < hi)
+    {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(first + mid) <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+constexpr int kMinMaxChunk = 64;
+
+//! per-system coordinate min/max: each thread scans a chunk of consecutive bodies and flushes at system changes
+__global__ void batchMinMaxKernel(const float* __restrict__ x, const float* __restrict__ y,
+                                  const float* __restrict__ z, size_t n, const uint64_t* __restrict__ first,
+                                  uint32_t numSystems, uint32_t* __restrict__ mm)
+{
+    size_t c0 = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * kMinMaxChunk;
+    if (c0 >= n) return;
+    size_t c1    = c0 + kMinMaxChunk < n ? c0 + kMinMaxChunk : n;
+    uint32_t sys = systemOf(first, numSystems, c0);
+    uint64_t end = __ldg(first + sys + 1);
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    auto flush = [&]()
+    {
+        uint32_t* m = mm + 6 * size_t(sys);
+        for (int d = 0; d < 3; ++d)
+        {
+            atomicMin(m + 2 * d, orderedBits(lo[d]));
+            atomicMax(m + 2 * d + 1, orderedBits(hi[d]));
+            lo[d] = INFINITY;
+            hi[d] = -INFINITY;
+        }
+    };
+    for (size_t i = c0; i < c1; ++i)
+    {
+        if (i >= end)
+        {
+            flush();
+            while (i >= end)
+            {
+                ++sys;
+                end = __ldg(first + sys + 1);
+            }
+        }
+        float v[3] = {x[i], y[i], z[i]};
+        for (int d = 0; d < 3; ++d)
+        {
+            lo[d] = fminf(lo[d], v[d]);
+            hi[d] = fmaxf(hi[d], v[d]);
+        }
+    }
+    flush();
+}
+
+__global__ void batchMinMaxInit(uint32_t* mm, uint32_t numSystems)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 6 * numSystems) mm[i] = (i & 1) ? 0u : 0xffffffffu;
+}
+
+/*! the cube enclosing each system whose box is not given, as the single-system solve derives it: lower corner at the
+ *  minimum, edge = largest extent (FP64), upper limit rounded up to cover the maximum */
+__global__ void batchAutoBoxes(const uint32_t* __restrict__ mm, const int* __restrict__ useGiven, uint32_t numSystems,
+                               DevBox<float>* __restrict__ boxes, float* __restrict__ limits)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= numSystems || useGiven[s]) return;
+    float mn[3], mx[3];
+    double ext = 0.0;
+    for (int d = 0; d < 3; ++d)
+    {
+        mn[d] = orderedFloat(mm[6 * s + 2 * d]);
+        mx[d] = orderedFloat(mm[6 * s + 2 * d + 1]);
+        ext   = fmax(ext, double(mx[d]) - double(mn[d]));
+    }
+    if (!(ext > 0)) ext = 1.0;
+    DevBox<float> b;
+    for (int d = 0; d < 3; ++d)
+    {
+        float lo = mn[d];
+        float hi = float(double(mn[d]) + ext);
+        if (!(hi >= mx[d])) hi = nextafterf(mx[d], 3.4e38f);
+        limits[6 * s + 2 * d]     = lo;
+        limits[6 * s + 2 * d + 1] = hi;
+        b.lo[d]                   = lo;
+        b.len[d]                  = hi - lo;
+        b.inv[d]                  = 1.f / (hi - lo);
+        b.bits[d]                 = kMaxLevel; // a cube: no axis is reduced
+    }
+    b.periodic = 0;
+    boxes[s]   = b;
+}
+
+__global__ void batchKeysKernel(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                                size_t n, const uint64_t* __restrict__ first, uint32_t numSystems,
+                                const DevBox<float>* __restrict__ boxes, int sysBits, uint64_t* __restrict__ keys)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        uint32_t s = systemOf(first, numSystems, i);
+        uint64_t k = pointKey(x[i], y[i], z[i], boxes[s]);
+        keys[i]    = (uint64_t(s) << (63 - sysBits)) | (k >> sysBits);
+    }
+}
+
+/*! each system's root node (the level-L node of its prefix) and its first stack entry; flags a missing root */
+__global__ void batchRootsKernel(uint32_t numSystems, const uint64_t* __restrict__ prefixes, int levelBegin,
+                                 int levelEnd, const int* __restrict__ childOffsets, int sysLevel,
+                                 const DevBox<float>* __restrict__ boxes, const int* __restrict__ numShells,
+                                 SysTrav* __restrict__ out, int* __restrict__ rootNode, unsigned int* __restrict__ err)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= numSystems) return;
+    int sysBits     = 3 * sysLevel;
+    uint64_t target = encodePrefix(uint64_t(s) << (63 - sysBits), sysBits);
+    int lo = levelBegin, hi = levelEnd;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (prefixes[mid] < target) lo = mid + 1;
+        else hi = mid;
+    }
+    SysTrav t;
+    if (lo < levelEnd && prefixes[lo] == target)
+    {
+        int fc  = childOffsets[lo];
+        t.entry = fc != 0 ? fc : -(lo + 2);
+        if (rootNode) rootNode[s] = lo;
+    }
+    else
+    {
+        t.entry = -1; // nothing to traverse; reported as an error
+        if (rootNode) rootNode[s] = -1;
+        atomicExch(err, 1u);
+    }
+    t.numShells = numShells[s];
+    t.boxL[0]   = boxes[s].len[0];
+    t.boxL[1]   = boxes[s].len[1];
+    t.boxL[2]   = boxes[s].len[2];
+    t.pad       = 0;
+    out[s]      = t;
+}
+
+//! fixed groups of at most @p groupSize bodies inside every system
+__global__ void batchGroupsKernel(uint32_t numGroups, const uint64_t* __restrict__ first,
+                                  const uint32_t* __restrict__ groupOffset, uint32_t numSystems, uint32_t groupSize,
+                                  uint32_t* __restrict__ start, uint32_t* __restrict__ end, uint32_t* __restrict__ sys)
+{
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= numGroups) return;
+    uint32_t lo = 0, hi = numSystems - 1;
+    while (lo < hi)
+    {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (groupOffset[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    uint64_t b  = first[lo] + uint64_t(g - groupOffset[lo]) * groupSize;
+    uint64_t e  = b + groupSize;
+    uint64_t se = first[lo + 1];
+    start[g]    = uint32_t(b);
+    end[g]      = uint32_t(e < se ? e : se);
+    sys[g]      = lo;
+}
+
+void launchBatchBoxes(const float* x, const float* y, const float* z, size_t n, const uint64_t* first,
+                      uint32_t numSystems, const int* useGiven, uint32_t* mm, DevBox<float>* boxes, float* limits,
+                      cudaStream_t s)
+{
+    batchMinMaxInit<<<ceilDiv(6 * numSystems, 256), 256, 0, s>>>(mm, numSystems);
+    RYO_LAUNCH_CHECK();
+    size_t threads = (n + kMinMaxChunk - 1) / kMinMaxChunk;
+    batchMinMaxKernel<<<ceilDiv(threads, 256), 256, 0, s>>>(x, y, z, n, first, numSystems, mm);
+    RYO_LAUNCH_CHECK();
+    batchAutoBoxes<<<ceilDiv(numSystems, 128), 128, 0, s>>>(mm, useGiven, numSystems, boxes, limits);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchBatchKeys(const float* x, const float* y, const float* z, size_t n, const uint64_t* first,
+                     uint32_t numSystems, const DevBox<float>* boxes, int sysLevel, uint64_t* keys, int smCount,
+                     cudaStream_t s)
+{
+    size_t want = ceilDiv(n, 256);
+    size_t cap  = size_t(smCount) * 16;
+    batchKeysKernel<<<unsigned(want < cap ? want : cap), 256, 0, s>>>(x, y, z, n, first, numSystems, boxes,
+                                                                      3 * sysLevel, keys);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchBatchRoots(uint32_t numSystems, const uint64_t* prefixes, int levelBegin, int levelEnd,
+                      const int* childOffsets, int sysLevel, const DevBox<float>* boxes, const int* numShells,
+                      SysTrav* out, int* rootNode, unsigned int* err, cudaStream_t s)
+{
+    batchRootsKernel<<<ceilDiv(numSystems, 128), 128, 0, s>>>(numSystems, prefixes, levelBegin, levelEnd, childOffsets,
+                                                               sysLevel, boxes, numShells, out, rootNode, err);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchBatchGroups(uint32_t numGroups, const uint64_t* first, const uint32_t* groupOffset, uint32_t numSystems,
+                       uint32_t groupSize, uint32_t* start, uint32_t* end, uint32_t* sys, cudaStream_t s)
+{
+    if (numGroups == 0) return;
+    batchGroupsKernel<<<ceilDiv(numGroups, 256), 256, 0, s>>>(numGroups, first, groupOffset, numSystems, groupSize,
+                                                              start, end, sys);
+    RYO_LAUNCH_CHECK();
+}
+
+} // namespace ryo

@@ -380,8 +380,8 @@ namespace
 {
 
 __global__ void splitGroupsKernel(const uint32_t* failed, uint32_t numFailed, const uint32_t* starts,
-                                  const uint32_t* ends, uint32_t* newStart, uint32_t* newEnd, unsigned int* unsplit,
-                                  unsigned int* numNew)
+                                  const uint32_t* ends, const uint32_t* sys, uint32_t* newStart, uint32_t* newEnd,
+                                  uint32_t* newSys, unsigned int* unsplit, unsigned int* numNew)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= numFailed) return;
@@ -398,6 +398,7 @@ __global__ void splitGroupsKernel(const uint32_t* failed, uint32_t numFailed, co
     newEnd[slot]       = mid;
     newStart[slot + 1] = mid;
     newEnd[slot + 1]   = b;
+    if (sys) newSys[slot] = newSys[slot + 1] = sys[g];
 }
 
 /*! run a traversal to completion: groups that overflow the stack are split in two along the SFC and traversed
@@ -429,10 +430,12 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
         uint32_t cap      = 2 * numFailed;
         uint32_t* nStart  = ctx->scratch<uint32_t>(flip ? "trav.splitB" : "trav.splitA", cap, s);
         uint32_t* nEnd    = ctx->scratch<uint32_t>(flip ? "trav.splitEndB" : "trav.splitEndA", cap, s);
+        uint32_t* nSys    = t.groupSys ? ctx->scratch<uint32_t>(flip ? "trav.splitSysB" : "trav.splitSysA", cap, s)
+                                       : nullptr;
         unsigned int* cnt = ctx->ctl->counters;
         RYO_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned int), s));
-        splitGroupsKernel<<<ceilDiv(numFailed, 256), 256, 0, s>>>(failed, numFailed, t.groupStart, t.groupEnd, nStart,
-                                                                   nEnd, cnt + 1, cnt);
+        splitGroupsKernel<<<ceilDiv(numFailed, 256), 256, 0, s>>>(failed, numFailed, t.groupStart, t.groupEnd,
+                                                                   t.groupSys, nStart, nEnd, nSys, cnt + 1, cnt);
         RYO_LAUNCH_CHECK();
         unsigned int h[2];
         RYO_CUDA(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -443,6 +446,12 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
         uint32_t* keepEnd   = ctx->scratch<uint32_t>(flip ? "trav.curEndB" : "trav.curEndA", std::max(h[0], 1u), s);
         RYO_CUDA(cudaMemcpyAsync(keepStart, nStart, h[0] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         RYO_CUDA(cudaMemcpyAsync(keepEnd, nEnd, h[0] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        if (t.groupSys)
+        {
+            uint32_t* keepSys = ctx->scratch<uint32_t>(flip ? "trav.curSysB" : "trav.curSysA", std::max(h[0], 1u), s);
+            RYO_CUDA(cudaMemcpyAsync(keepSys, nSys, h[0] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+            t.groupSys = keepSys;
+        }
         t.groupStart = keepStart;
         t.groupEnd   = keepEnd;
         t.numGroups  = int(h[0]);
@@ -1032,6 +1041,268 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                                stats->box[i] = box.limits[i];
                                stats->ms[i]  = ms[i];
                            }
+                       }
+                   });
+}
+
+//! octree levels taken by the system index in batched keys: the smallest L >= 1 with 8^L >= numSystems
+static int batchSystemLevel(int numSystems)
+{
+    int L = 1;
+    while ((size_t(1) << (3 * L)) < size_t(numSystems))
+        ++L;
+    return L;
+}
+
+extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, const ryo_system* systems,
+                                          int numSystems, float* x, float* y, float* z, float* m, float* h, float* vx,
+                                          float* vy, float* vz, size_t n, float* p, float* ax, float* ay, float* az,
+                                          uint32_t* orderOut, double* energies, float* boxesOut,
+                                          ryo_solve_stats* stats, ryo_stream_t stream)
+{
+    if (!ctx || !P) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(systems && numSystems >= 1 && numSystems <= RYO_BATCH_MAX_SYSTEMS,
+                               "solve_batch: numSystems must be in [1, RYO_BATCH_MAX_SYSTEMS]");
+                       REQUIRE(x && y && z && m && h && p && ax && ay && az, "solve_batch: null argument");
+                       REQUIRE(n > 0 && n < (size_t(1) << 32), "solve_batch: body count must be in [1, 2^32)");
+                       REQUIRE(P->groupSize >= 1 && P->groupSize <= 64, "solve_batch: groupSize must be in [1, 64]");
+                       REQUIRE(P->bucketSize >= 1 && P->theta > 0.f, "solve_batch: bad bucketSize or theta");
+                       cudaStream_t s      = stream;
+                       const uint32_t ns   = uint32_t(numSystems);
+                       const int sysLevel  = batchSystemLevel(numSystems);
+                       std::vector<uint64_t> first(ns + 1);
+                       std::vector<int> useGiven(ns), shells(ns);
+                       std::vector<DevBox<float>> hbox(ns);
+                       std::vector<uint32_t> groupOffset(ns + 1);
+                       uint64_t expect = 0, groups = 0;
+                       for (uint32_t k = 0; k < ns; ++k)
+                       {
+                           const ryo_system& sy = systems[k];
+                           REQUIRE(sy.firstBody == expect && sy.numBodies >= 1,
+                                   "solve_batch: systems must tile the body arrays in order, none empty");
+                           first[k]       = expect;
+                           groupOffset[k] = uint32_t(groups);
+                           expect += sy.numBodies;
+                           groups += (sy.numBodies + P->groupSize - 1) / P->groupSize;
+                           useGiven[k] = sy.useBox ? 1 : 0;
+                           shells[k]   = 0;
+                           if (sy.useBox)
+                           {
+                               checkBox(sy.box.limits);
+                               hbox[k] = boxOf(&sy.box);
+                               if (hbox[k].periodic)
+                               {
+                                   if (!(hbox[k].len[0] == hbox[k].len[1] && hbox[k].len[1] == hbox[k].len[2]))
+                                       throw ApiError{RYO_ERR_NOT_CUBIC,
+                                                      "solve_batch: Ewald needs a cubic periodic box"};
+                                   REQUIRE(sy.numShells >= 0 && sy.numShells <= 4, "solve_batch: numShells in [0, 4]");
+                                   shells[k] = sy.numShells;
+                               }
+                           }
+                       }
+                       REQUIRE(expect == n, "solve_batch: the systems' bodies must add up to n");
+                       first[ns]       = expect;
+                       groupOffset[ns] = uint32_t(groups);
+                       const uint32_t numGroups = uint32_t(groups);
+                       mark(ctx, P, 0, s);
+
+                       // per-system tables
+                       uint64_t* dFirst   = ctx->scratch<uint64_t>("batch.first", ns + 1, s);
+                       int* dUseGiven     = ctx->scratch<int>("batch.useGiven", ns, s);
+                       int* dShells       = ctx->scratch<int>("batch.shells", ns, s);
+                       DevBox<float>* dBx = ctx->scratch<DevBox<float>>("batch.boxes", ns, s);
+                       uint32_t* dGOff    = ctx->scratch<uint32_t>("batch.groupOffset", ns + 1, s);
+                       uint32_t* dMM      = ctx->scratch<uint32_t>("batch.minmax", 6 * size_t(ns), s);
+                       float* dLimits     = ctx->scratch<float>("batch.limits", 6 * size_t(ns), s);
+                       RYO_CUDA(cudaMemcpyAsync(dFirst, first.data(), sizeof(uint64_t) * (ns + 1),
+                                                cudaMemcpyHostToDevice, s));
+                       RYO_CUDA(cudaMemcpyAsync(dUseGiven, useGiven.data(), sizeof(int) * ns, cudaMemcpyHostToDevice,
+                                                s));
+                       RYO_CUDA(cudaMemcpyAsync(dShells, shells.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+                       RYO_CUDA(cudaMemcpyAsync(dBx, hbox.data(), sizeof(DevBox<float>) * ns, cudaMemcpyHostToDevice,
+                                                s));
+                       RYO_CUDA(cudaMemcpyAsync(dGOff, groupOffset.data(), sizeof(uint32_t) * (ns + 1),
+                                                cudaMemcpyHostToDevice, s));
+                       launchBatchBoxes(x, y, z, n, dFirst, ns, dUseGiven, dMM, dBx, dLimits, s);
+
+                       // system-prefixed keys, one sort for all systems, permute every per-body array
+                       uint64_t* keys    = ctx->scratch<uint64_t>("solve.keys", n, s);
+                       uint64_t* keysAlt = ctx->scratch<uint64_t>("solve.keysAlt", n, s);
+                       uint32_t* ord     = ctx->scratch<uint32_t>("solve.order", n, s);
+                       uint32_t* ordAlt  = ctx->scratch<uint32_t>("solve.orderAlt", n, s);
+                       size_t tmpBytes   = sortTempBytes(n);
+                       void* tmp         = ctx->scratch<char>("solve.sorttmp", tmpBytes, s);
+                       launchBatchKeys(x, y, z, n, dFirst, ns, dBx, sysLevel, keys, ctx->smCount, s);
+                       bool alt = radixSortPairs(keys, ord, keysAlt, ordAlt, n, 0, 64, tmp, tmpBytes, &ctx->ctl->error,
+                                                 s, true);
+                       const uint64_t* sorted = alt ? keysAlt : keys;
+                       const uint32_t* order  = alt ? ordAlt : ord;
+                       float* tmpF            = ctx->scratch<float>("solve.tmpf", n, s);
+                       for (float* a : {x, y, z, m, h, vx, vy, vz})
+                       {
+                           if (!a) continue;
+                           launchGather(order, a, tmpF, n, s);
+                           RYO_CUDA(cudaMemcpyAsync(a, tmpF, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+                       }
+                       if (orderOut)
+                           RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+                       mark(ctx, P, 1, s);
+                       float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
+                       float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
+                       packSolveBodies<<<ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
+                                                                                        : unsigned(ctx->smCount * 16),
+                                         256, 0, s>>>(x, y, z, m, h, n, xyzm, xyzh);
+                       RYO_LAUNCH_CHECK();
+
+                       // one tree over all systems: leaves holding bodies lie at or below the system level
+                       int cap          = int(std::min<size_t>(n / 2 + 64 + 8 * size_t(ns), size_t(1) << 30));
+                       uint64_t* leaves = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
+                       uint32_t* counts = ctx->scratch<uint32_t>("solve.counts", cap, s);
+                       uint32_t* layout = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
+                       int nl = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s,
+                                            unsigned(sysLevel));
+                       if (nl > cap)
+                       {
+                           cap    = nl;
+                           leaves = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
+                           counts = ctx->scratch<uint32_t>("solve.counts", cap, s);
+                           layout = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
+                           nl     = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s,
+                                                unsigned(sysLevel));
+                       }
+                       int ni = (nl - 1) / 7, nn = nl + ni;
+                       OctreeArrays oct;
+                       oct.prefixes       = ctx->scratch<uint64_t>("solve.prefixes", nn, s);
+                       oct.childOffsets   = ctx->scratch<int>("solve.childOffsets", size_t(nn) + 1, s);
+                       oct.parents        = ctx->scratch<int>("solve.parents", std::max(1, (nn - 1) / 8), s);
+                       oct.internalToLeaf = ctx->scratch<int>("solve.internalToLeaf", nn, s);
+                       oct.leafToInternal = ctx->scratch<int>("solve.leafToInternal", nn, s);
+                       oct.d_levelRange   = ctx->scratch<int>("solve.levelRange", kMaxLevel + 2, s);
+                       int levelRange[kMaxLevel + 2];
+                       linkOctree(ctx, leaves, nl, oct, levelRange, s);
+                       mark(ctx, P, 2, s);
+
+                       // fused upsweep with each system's box; FP64 expansions of the system roots
+                       NodeRecord* records = ctx->scratch<NodeRecord>("solve.records", nn, s);
+                       double* sysRoots    = ctx->scratch<double>("batch.roots", 11 * size_t(ns), s);
+                       DevBox<float> unused = hbox[0];
+                       launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
+                                          oct.parents, oct.prefixes, 1.0f / P->theta, unused, records, nullptr, nullptr,
+                                          nullptr, s, dBx, sysLevel, sysRoots);
+                       mark(ctx, P, 3, s);
+
+                       // groups inside systems, system roots, traversal
+                       uint32_t* gStart = ctx->scratch<uint32_t>("batch.gstart", std::max(numGroups, 1u), s);
+                       uint32_t* gEnd   = ctx->scratch<uint32_t>("batch.gend", std::max(numGroups, 1u), s);
+                       uint32_t* gSys   = ctx->scratch<uint32_t>("batch.gsys", std::max(numGroups, 1u), s);
+                       launchBatchGroups(numGroups, dFirst, dGOff, ns, P->groupSize, gStart, gEnd, gSys, s);
+                       SysTrav* dTrav   = ctx->scratch<SysTrav>("batch.trav", ns, s);
+                       int* dRootNode   = ctx->scratch<int>("batch.rootNode", ns, s);
+                       unsigned int* rootErr = ctx->ctl->counters + 4;
+                       RYO_CUDA(cudaMemsetAsync(rootErr, 0, sizeof(unsigned int), s));
+                       launchBatchRoots(ns, oct.prefixes, levelRange[sysLevel], levelRange[sysLevel + 1],
+                                        oct.childOffsets, sysLevel, dBx, dShells, dTrav, dRootNode, rootErr, s);
+                       double* sysPot = ctx->scratch<double>("batch.pot", 2 * size_t(ns), s); // tree, Ewald
+                       RYO_CUDA(cudaMemsetAsync(sysPot, 0, sizeof(double) * 2 * ns, s));
+                       for (float* a : {p, ax, ay, az})
+                           RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
+                       TraverseLaunch t{};
+                       t.groupStart    = gStart;
+                       t.groupEnd      = gEnd;
+                       t.numGroups     = int(numGroups);
+                       t.initNode      = 1;
+                       t.numNodes      = nn;
+                       t.nodes         = records;
+                       t.tgtXYZH       = xyzh;
+                       t.tgtM          = m;
+                       t.srcXYZM       = xyzm;
+                       t.srcH          = h;
+                       t.G             = P->G;
+                       t.p             = p;
+                       t.ax            = ax;
+                       t.ay            = ay;
+                       t.az            = az;
+                       t.stackCapacity = P->stackCapacity;
+                       t.groupSys      = gSys;
+                       t.systems       = dTrav;
+                       t.sysPotential  = sysPot;
+                       double pot      = 0;
+                       runTraversal(ctx, t, s, &pot);
+                       mark(ctx, P, 4, s);
+
+                       // Ewald for the periodic systems, one launch per periodic system
+                       std::vector<double> hroots;
+                       for (uint32_t k = 0; k < ns; ++k)
+                       {
+                           if (!(useGiven[k] && hbox[k].periodic)) continue;
+                           if (hroots.empty())
+                           {
+                               hroots.resize(11 * size_t(ns));
+                               RYO_CUDA(cudaMemcpyAsync(hroots.data(), sysRoots, sizeof(double) * 11 * ns,
+                                                        cudaMemcpyDeviceToHost, s));
+                               RYO_CUDA(cudaStreamSynchronize(s));
+                           }
+                           const double* r = hroots.data() + 11 * size_t(k);
+                           EwaldHost e = ewaldSetup(r + 3, r, P->ewald.numReplicaShells, double(hbox[k].len[0]),
+                                                    P->ewald.lCut, P->ewald.hCut, P->ewald.alpha_scale,
+                                                    P->ewald.small_R_scale_factor);
+                           uint32_t g0 = groupOffset[k], g1 = groupOffset[k + 1];
+                           launchEwaldGroups(e, gStart + g0, gEnd + g0, g1 - g0, x, y, z, m, P->G, p, ax, ay, az,
+                                             sysPot + ns + k, s);
+                       }
+                       mark(ctx, P, 5, s);
+                       mark(ctx, P, 6, s);
+
+                       std::vector<double> hp(2 * size_t(ns));
+                       RYO_CUDA(cudaMemcpyAsync(hp.data(), sysPot, sizeof(double) * 2 * ns, cudaMemcpyDeviceToHost, s));
+                       unsigned int herr = 0;
+                       RYO_CUDA(cudaMemcpyAsync(&herr, rootErr, sizeof(herr), cudaMemcpyDeviceToHost, s));
+                       std::vector<float> hl;
+                       if (boxesOut)
+                       {
+                           hl.resize(6 * size_t(ns));
+                           RYO_CUDA(cudaMemcpyAsync(hl.data(), dLimits, sizeof(float) * 6 * ns, cudaMemcpyDeviceToHost,
+                                                    s));
+                       }
+                       RYO_CUDA(cudaStreamSynchronize(s));
+                       if (herr) throw ApiError{RYO_ERR_CUDA, "solve_batch: a system root is missing from the tree"};
+                       double total = 0;
+                       for (uint32_t k = 0; k < ns; ++k)
+                       {
+                           double e = 0.5 * double(P->G) * (hp[k] + hp[ns + k]);
+                           total += e;
+                           if (energies) energies[k] = e;
+                           if (boxesOut)
+                               for (int d = 0; d < 6; ++d)
+                                   boxesOut[6 * k + d] = useGiven[k] ? systems[k].box.limits[d] : hl[6 * k + d];
+                       }
+                       float ms[6] = {0, 0, 0, 0, 0, 0};
+                       if (P->timing)
+                       {
+                           RYO_CUDA(cudaEventSynchronize(ctx->phaseEvents[6]));
+                           for (int i = 0; i < 5; ++i)
+                               RYO_CUDA(cudaEventElapsedTime(&ms[i], ctx->phaseEvents[i], ctx->phaseEvents[i + 1]));
+                           RYO_CUDA(cudaEventElapsedTime(&ms[5], ctx->phaseEvents[0], ctx->phaseEvents[6]));
+                       }
+                       if (stats)
+                       {
+                           stats->numLeaves       = nl;
+                           stats->numNodes        = nn;
+                           stats->numGroups       = int(numGroups);
+                           stats->sumP2P          = ctx->hostStats[kSumP2P];
+                           stats->maxP2P          = ctx->hostStats[kMaxP2P];
+                           stats->sumM2P          = ctx->hostStats[kSumM2P];
+                           stats->maxM2P          = ctx->hostStats[kMaxM2P];
+                           stats->maxStack        = ctx->hostStats[kMaxStack];
+                           stats->retries         = ctx->retries;
+                           stats->potentialEnergy = total;
+                           for (int d = 0; d < 6; ++d)
+                               stats->box[d] = 0.f;
+                           for (int i = 0; i < 6; ++i)
+                               stats->ms[i] = ms[i];
                        }
                    });
 }

@@ -120,8 +120,10 @@ bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_
 
 // ---------------------------------------------------------------------------------------------------- octree.cu
 //! cornerstone leaves of sorted keys; returns numLeaves (host), writes only if numLeaves <= capacity
+//! cornerstone leaves of sorted keys; every leaf holding particles lies on level >= minLevel (0: the reference's
+//! leaves; a batched solve uses the level of its system prefix so that no leaf spans two systems)
 int buildLeaves(ryo_ctx* ctx, const uint64_t* sortedKeys, size_t n, unsigned bucket, uint64_t* leaves,
-                uint32_t* counts, uint32_t* layout, int capacity, cudaStream_t s);
+                uint32_t* counts, uint32_t* layout, int capacity, cudaStream_t s, unsigned minLevel = 0);
 
 struct OctreeArrays
 {
@@ -164,7 +166,8 @@ struct alignas(16) NodeRecord
 void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
                         const int* leafToInternal, const int* childOffsets, const int* parents,
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
-                        float4* centers, float* multipoles, double* rootCenterMultipole, cudaStream_t s);
+                        float4* centers, float* multipoles, double* rootCenterMultipole, cudaStream_t s,
+                        const DevBox<float>* sysBoxes = nullptr, int sysLevel = 0, double* sysRoots = nullptr);
 
 //! pack reference-layout tree arrays into node records (for the reference-signature traverse)
 void launchPackNodes(int numNodes, const float4* centers, const float* multipoles, const int* childOffsets,
@@ -207,9 +210,35 @@ struct TraverseLaunch
     uint32_t failedCapacity;
     int stackCapacity;
     Control* ctl;
+    // batched systems (all optional): the system of every group, per-system traversal parameters and potentials
+    const uint32_t* groupSys;
+    const struct SysTrav* systems;
+    double* sysPotential;
+};
+
+//! per-system traversal parameters of a batched solve
+struct SysTrav
+{
+    int entry;     // first stack entry: first child of the system's root, or -(root + 2) for a single-cell tree
+    int numShells; // periodic replicas per dimension
+    float boxL[3];
+    int pad;
 };
 void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s);
 void launchTraversalReset(Control* ctl, bool resetStats, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------------- batch.cu
+void launchBatchBoxes(const float* x, const float* y, const float* z, size_t n, const uint64_t* first,
+                      uint32_t numSystems, const int* useGiven, uint32_t* mm, DevBox<float>* boxes, float* limits,
+                      cudaStream_t s);
+void launchBatchKeys(const float* x, const float* y, const float* z, size_t n, const uint64_t* first,
+                     uint32_t numSystems, const DevBox<float>* boxes, int sysLevel, uint64_t* keys, int smCount,
+                     cudaStream_t s);
+void launchBatchRoots(uint32_t numSystems, const uint64_t* prefixes, int levelBegin, int levelEnd,
+                      const int* childOffsets, int sysLevel, const DevBox<float>* boxes, const int* numShells,
+                      SysTrav* out, int* rootNode, unsigned int* err, cudaStream_t s);
+void launchBatchGroups(uint32_t numGroups, const uint64_t* first, const uint32_t* groupOffset, uint32_t numSystems,
+                       uint32_t groupSize, uint32_t* start, uint32_t* end, uint32_t* sys, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- ewald.cu
 struct EwaldHost

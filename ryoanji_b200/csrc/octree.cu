@@ -29,7 +29,8 @@ constexpr int kLeafBlock = 256;
  * particle's leaf is one level below the deepest window level among the windows that contain it.
  */
 __global__ void __launch_bounds__(kLeafBlock) leafLevels(const uint64_t* __restrict__ keys, uint32_t n,
-                                                         uint32_t bucket, uint8_t* __restrict__ level)
+                                                         uint32_t bucket, uint32_t minLevel,
+                                                         uint8_t* __restrict__ level)
 {
     extern __shared__ unsigned char smem[];
     uint8_t* w = smem; // window levels for j in [i0 - B, i0 + blockDim)
@@ -62,7 +63,8 @@ __global__ void __launch_bounds__(kLeafBlock) leafLevels(const uint64_t* __restr
         uint8_t v = w[j - jFirst];
         mx        = v > mx ? v : mx;
     }
-    level[i] = uint8_t(mx + 1);
+    uint32_t lv = uint32_t(mx) + 1;
+    level[i]    = uint8_t(lv > minLevel ? lv : minLevel);
 }
 
 //! 1 where a particle starts a new non-empty leaf
@@ -151,10 +153,12 @@ __global__ void singleLeaf(uint64_t* leaves, uint32_t* counts, uint32_t* layout,
 }
 
 int buildLeaves(ryo_ctx* ctx, const uint64_t* keys, size_t n64, unsigned bucket, uint64_t* leaves, uint32_t* counts,
-                uint32_t* layout, int capacity, cudaStream_t s)
+                uint32_t* layout, int capacity, cudaStream_t s, unsigned minLevel)
 {
     uint32_t n = uint32_t(n64);
-    if (n <= bucket)
+    if (minLevel > 0 && (n == 0 || minLevel > unsigned(kMaxLevel)))
+        throw CudaError{cudaErrorInvalidValue, "leaf construction: no keys, or minimum level above 21"};
+    if (n <= bucket && minLevel == 0)
     {
         if (capacity >= 1)
         {
@@ -170,7 +174,7 @@ int buildLeaves(ryo_ctx* ctx, const uint64_t* keys, size_t n64, unsigned bucket,
     size_t smemBytes = kLeafBlock + bucket;
     if (smemBytes > 48 * 1024)
         RYO_CUDA(cudaFuncSetAttribute(leafLevels, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemBytes)));
-    leafLevels<<<ceilDiv(n, kLeafBlock), kLeafBlock, smemBytes, s>>>(keys, n, bucket, level);
+    leafLevels<<<ceilDiv(n, kLeafBlock), kLeafBlock, smemBytes, s>>>(keys, n, bucket, minLevel, level);
     RYO_LAUNCH_CHECK();
     leafHeads<<<ceilDiv(n, 256), 256, 0, s>>>(keys, level, n, head);
     RYO_LAUNCH_CHECK();

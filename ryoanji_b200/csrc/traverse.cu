@@ -32,7 +32,8 @@ constexpr int kTravThreads  = kTravWarps * kWarp;
 constexpr int kStackDefault = 1024;
 constexpr int kM2PCap       = 64;  // pending approximated cells (flushed at 32)
 constexpr int kLeafCap      = 64;  // pending direct leaves (flushed when more than 32 are pending)
-constexpr int kRootOnly     = -2;  // stack marker: the root itself is the only cell (single-leaf tree)
+constexpr int kRootOnly     = -2;  // stack marker: the root itself is the only cell (single-leaf tree); a marker
+                                   // -(r + 2) stands for the single cell r
 
 struct WarpSmem
 {
@@ -457,16 +458,32 @@ __global__ void __launch_bounds__(kTravThreads)
             ts[d]   = __fmul_rn(__fsub_rn(h, l), 0.5f);
         }
 
+        // the group's tree root and periodic images: the launch's, or its system's in a batched solve
+        int rootEntry = P.numNodes == 1 ? kRootOnly : P.initNode;
+        int shells    = P.numShells;
+        float boxL[3] = {P.boxL[0], P.boxL[1], P.boxL[2]};
+        uint32_t sys  = 0;
+        if (P.groupSys)
+        {
+            sys               = P.groupSys[g];
+            const SysTrav& st = P.systems[sys];
+            rootEntry         = st.entry;
+            shells            = st.numShells;
+            boxL[0]           = st.boxL[0];
+            boxL[1]           = st.boxL[1];
+            boxL[2]           = st.boxL[2];
+        }
+
         unsigned nM2P = 0, nP2P = 0;
         int maxStack  = 0;
         bool overflow = false;
-        for (int iz = -P.numShells; iz <= P.numShells && !overflow; ++iz)
-            for (int iy = -P.numShells; iy <= P.numShells && !overflow; ++iy)
-                for (int ix = -P.numShells; ix <= P.numShells && !overflow; ++ix)
+        for (int iz = -shells; iz <= shells && !overflow; ++iz)
+            for (int iy = -shells; iy <= shells && !overflow; ++iy)
+                for (int ix = -shells; ix <= shells && !overflow; ++ix)
                 {
                     // the replica shift is added to and later subtracted from centre and targets (as in the reference)
-                    float sh[3] = {__fmul_rn(float(ix), P.boxL[0]), __fmul_rn(float(iy), P.boxL[1]),
-                                   __fmul_rn(float(iz), P.boxL[2])};
+                    float sh[3] = {__fmul_rn(float(ix), boxL[0]), __fmul_rn(float(iy), boxL[1]),
+                                   __fmul_rn(float(iz), boxL[2])};
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
                         tc[d] = __fadd_rn(tc[d], sh[d]);
@@ -475,7 +492,7 @@ __global__ void __launch_bounds__(kTravThreads)
                     T.tz = add2(T.tz, pk(sh[2], sh[2]));
 
                     int sp = 1, nM = 0, nL = 0;
-                    if (lane == 0) stack[0] = P.numNodes == 1 ? kRootOnly : P.initNode;
+                    if (lane == 0) stack[0] = rootEntry;
                     __syncwarp();
                     while (sp > 0)
                     {
@@ -485,7 +502,7 @@ __global__ void __launch_bounds__(kTravThreads)
                         int entry = slot < k ? stack[sp + slot] : -1;
                         __syncwarp();
                         int cell = -1;
-                        if (entry == kRootOnly) cell = (lane & 7) == 0 ? 0 : -1;
+                        if (entry <= kRootOnly) cell = (lane & 7) == 0 ? kRootOnly - entry : -1;
                         else if (entry >= 0) cell = entry + (lane & 7);
 
                         bool valid = cell >= 0;
@@ -588,6 +605,7 @@ __global__ void __launch_bounds__(kTravThreads)
             atomicAdd(&P.ctl->stats[kSumM2P], (unsigned long long)nM2P * size);
             atomicMax(&P.ctl->stats[kMaxStack], (unsigned long long)maxStack);
             atomicAdd(&P.ctl->potential, pot);
+            if (P.sysPotential) atomicAdd(P.sysPotential + sys, pot);
             if (P.groupM2P) P.groupM2P[g] = nM2P;
             if (P.groupP2P) P.groupP2P[g] = nP2P;
         }

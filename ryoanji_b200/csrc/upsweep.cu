@@ -271,15 +271,56 @@ struct FusedArgs
     float4* centers;
     float* multipoles;
     double* root; // 11 doubles: centre (3) + finalized multipole (8)
+    // batched systems: node keys carry a system prefix of sysLevel octree levels; sysBoxes[s] is the box of system
+    // s, and sysRoots (11 doubles per system) receives the FP64 expansion of every system's root node
+    const DevBox<float>* sysBoxes;
+    int sysLevel;
+    double* sysRoots;
 };
+
+//! FP64 centre and finalized quadrupole (11 doubles) of a node, as the Ewald setup reads them
+__device__ inline void writeRootExpansion(double* out, const double c[3], const double raw[7])
+{
+    out[0]    = c[0];
+    out[1]    = c[1];
+    out[2]    = c[2];
+    double tr = raw[1] + raw[4] + raw[6];
+    out[3]    = raw[0];
+    out[4]    = 3 * raw[1] - tr;
+    out[5]    = 3 * raw[2];
+    out[6]    = 3 * raw[3];
+    out[7]    = 3 * raw[4] - tr;
+    out[8]    = 3 * raw[5];
+    out[9]    = 3 * raw[6] - tr;
+    out[10]   = tr;
+}
 
 //! write the float outputs of a finished node
 __device__ void emitNode(const FusedArgs& A, int node, const double c[3], double w, double m, const double q[6],
                          int child, uint32_t firstBody, uint32_t count)
 {
     float com[3] = {float(c[0]), float(c[1]), float(c[2])};
-    float mac    = w != 0.0 && float(w) != 0.f ? vecMacR2(A.prefixes[node], com, A.invTheta, A.box) : 0.f;
     double raw[7] = {m, q[0], q[1], q[2], q[3], q[4], q[5]};
+    float mac     = 0.f;
+    if (!A.sysBoxes)
+        mac = w != 0.0 && float(w) != 0.f ? vecMacR2(A.prefixes[node], com, A.invTheta, A.box) : 0.f;
+    else
+    {
+        // a node inside a system: its geometry is the system-local node (prefix without the system bits) in the
+        // system's box; nodes above the system level mix systems and are never traversed
+        uint64_t prefix = A.prefixes[node];
+        int lvl         = prefixLength(prefix) / 3;
+        if (lvl >= A.sysLevel)
+        {
+            uint64_t start    = prefixStart(prefix);
+            int sysBits       = 3 * A.sysLevel;
+            uint32_t sys      = uint32_t(start >> (63 - sysBits));
+            uint64_t local    = (start << sysBits) & (kKeyEnd - 1);
+            uint64_t localPre = encodePrefix(local, 3 * (lvl - A.sysLevel));
+            if (w != 0.0 && float(w) != 0.f) mac = vecMacR2(localPre, com, A.invTheta, A.sysBoxes[sys]);
+            if (lvl == A.sysLevel && A.sysRoots) writeRootExpansion(A.sysRoots + 11 * size_t(sys), c, raw);
+        }
+    }
     float qf[8];
     finalizeQuad(raw, qf);
     float4 cen = make_float4(com[0], com[1], com[2], mac);
@@ -296,21 +337,7 @@ __device__ void emitNode(const FusedArgs& A, int node, const double c[3], double
         mp[0]      = r.q0;
         mp[1]      = r.q1;
     }
-    if (node == 0 && A.root)
-    {
-        A.root[0] = c[0];
-        A.root[1] = c[1];
-        A.root[2] = c[2];
-        double tr = raw[1] + raw[4] + raw[6];
-        A.root[3] = raw[0];
-        A.root[4] = 3 * raw[1] - tr;
-        A.root[5] = 3 * raw[2];
-        A.root[6] = 3 * raw[3];
-        A.root[7] = 3 * raw[4] - tr;
-        A.root[8] = 3 * raw[5];
-        A.root[9] = 3 * raw[6] - tr;
-        A.root[10] = tr;
-    }
+    if (node == 0 && A.root) writeRootExpansion(A.root, c, raw);
 }
 
 //! combine the eight children of @p node (parallel-axis theorem, double)
@@ -441,9 +468,13 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
 void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
                         const int* leafToInternal, const int* childOffsets, const int* parents,
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
-                        float4* centers, float* multipoles, double* root, cudaStream_t s)
+                        float4* centers, float* multipoles, double* root, cudaStream_t s,
+                        const DevBox<float>* sysBoxes, int sysLevel, double* sysRoots)
 {
     FusedArgs A;
+    A.sysBoxes       = sysBoxes;
+    A.sysLevel       = sysLevel;
+    A.sysRoots       = sysRoots;
     A.xyzm           = xyzm;
     A.layout         = layout;
     A.leafToInternal = leafToInternal;
