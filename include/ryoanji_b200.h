@@ -346,6 +346,63 @@ extern "C"
                                            uint32_t* order, double* energies, float* boxes, ryo_solve_stats* stats,
                                            ryo_stream_t stream);
 
+    /* ------------------------------------------------------------------------------------------ served stream
+     * A request loop over the batched solve (not in the reference): requests (a particle set and K kick-drift-kick
+     * leapfrog steps) are admitted in arrival order while the HBM budget and the system slots allow, stay resident
+     * across their steps, and every ryo_engine_step advances all resident requests with one batched solve. A
+     * request's first step evaluates its initial forces; it then takes numSteps steps of
+     *     v += a dt/2;  x += v dt;  a = F(x);  v += a dt/2
+     * (periodic systems wrap x into their box) and retires. Its host inputs must stay valid until it is admitted,
+     * its host output until it retires. One engine belongs to one host thread; it uses its context's scratch. */
+    typedef struct ryo_engine ryo_engine_t;
+    typedef struct ryo_engine_params
+    {
+        ryo_solve_params solve; /* bucketSize, groupSize, theta, G, ewald, stackCapacity, timing */
+        double hbmBudgetBytes;  /* admission budget (default 120e9) */
+        double bytesPerBody;    /* device bytes charged per resident body (default 256) */
+        int maxSystems;         /* resident requests at most (default and upper limit RYO_BATCH_MAX_SYSTEMS) */
+    } ryo_engine_params;
+    typedef struct ryo_engine_request
+    {
+        uint64_t tag;
+        uint32_t numBodies;
+        const float *x, *y, *z, *m, *h; /* host */
+        const float *vx, *vy, *vz;      /* host, may be NULL (zero velocities) */
+        int useBox;                     /* 0: the cube enclosing the bodies, recomputed every step */
+        ryo_box_f32 box;
+        int numShells;
+        int numSteps; /* leapfrog steps after the initial force evaluation */
+        float dt;
+        float* out; /* host, may be NULL: on retirement 10 * numBodies floats, arrays of x, y, z, vx, vy, vz, ax,
+                       ay, az, p in submission order (ax..p: G a and G m phi at the final positions) */
+    } ryo_engine_request;
+    typedef struct ryo_engine_step_info
+    {
+        int admitted, retired, resident, queued, solved, retries;
+        uint64_t residentBodies;
+        float ms[6]; /* phase times of the batched solve when params.solve.timing */
+    } ryo_engine_step_info;
+    typedef struct ryo_engine_result
+    {
+        uint64_t tag;
+        uint32_t numBodies;
+        int stepsDone;
+        double kineticEnergy, potentialEnergy; /* at retirement */
+        double initialEnergy;                  /* kinetic + potential after the initial force evaluation */
+    } ryo_engine_result;
+
+    RYO_API void ryo_engine_params_default(ryo_engine_params* p);
+    RYO_API ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params* params, ryo_engine_t** out);
+    RYO_API void ryo_engine_destroy(ryo_engine_t* engine);
+    RYO_API const char* ryo_engine_last_error(const ryo_engine_t* engine);
+    /* queue a request; RYO_ERR_CAPACITY if it alone exceeds the budget */
+    RYO_API ryo_status ryo_engine_submit(ryo_engine_t* engine, const ryo_engine_request* request);
+    /* admit, kick-drift, one batched solve of every resident request, kick, retire the finished ones */
+    RYO_API ryo_status ryo_engine_step(ryo_engine_t* engine, ryo_engine_step_info* info, ryo_stream_t stream);
+    /* take up to capacity results of retired requests (oldest first); *count receives how many */
+    RYO_API ryo_status ryo_engine_poll(ryo_engine_t* engine, ryo_engine_result* out, int capacity, int* count);
+    RYO_API ryo_status ryo_engine_status(const ryo_engine_t* engine, int* queued, int* resident, double* bytesInUse);
+
     /* device arrays of the last ryo_solve_f32 on this context (valid until the next solve on it): the sorted keys,
      * permutation, tree and the packed node records the traversal read (16 floats per node: centre x, y, z, squared
      * MAC radius; multipole mass, qxx, qxy, qxz, qyy, qyz, qzz, trace; then 4 ints: first child, first body, body

@@ -12,6 +12,7 @@ import ctypes as C
 import os
 from dataclasses import dataclass
 
+import numpy as np
 import torch
 
 from . import _abi
@@ -22,7 +23,7 @@ __all__ = [
     "compute_sfc_keys", "compute_bounding_box", "sequence", "sort_by_key", "compute_octree", "build_octree",
     "compute_fixed_groups", "compute_leaf_source_center", "upsweep_centers", "compute_leaf_multipoles",
     "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch",
-    "BatchSystem", "BatchResult",
+    "BatchSystem", "BatchResult", "Engine",
     "compute_gravity_ewald", "direct_sum", "direct_targets_f64", "solve", "solve_arrays", "bh_max_target_size",
     "kernel_launches", "measure_peaks",
     "stack_size",
@@ -568,6 +569,104 @@ def solve_batch(systems, x, y, z, m, h, p, ax, ay, az, params: SolveParams | Non
     res = SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
                       st.maxStack, st.retries, st.potentialEnergy, [], ms)
     return BatchResult(res, list(energies)[:ns], [list(boxes[6 * i:6 * i + 6]) for i in range(ns)])
+
+
+class Engine:
+    """The served stream (ryo_engine_*): requests of a particle set and K leapfrog steps, admitted under an HBM
+    budget and advanced together, one batched solve per step. Host inputs are kept referenced until admission and
+    output buffers until retirement."""
+
+    def __init__(self, params: SolveParams | None = None, hbm_budget_bytes: float = 120e9,
+                 bytes_per_body: float = 256.0, max_systems: int = MAX_BATCH_SYSTEMS, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        ep = _abi.EngineParams()
+        lib.ryo_engine_params_default(C.byref(ep))
+        ep.solve = (params or SolveParams()).c()
+        ep.hbmBudgetBytes = hbm_budget_bytes
+        ep.bytesPerBody = bytes_per_body
+        ep.maxSystems = max_systems
+        h = C.c_void_p()
+        _check(lib.ryo_engine_create(self.ctx.handle, C.byref(ep), C.byref(h)), self.ctx)
+        self.handle = h
+        self._keep = {}
+        self._outputs = {}
+
+    def _err(self, st):
+        if st != 0:
+            raise RyoError(st, (lib.ryo_engine_last_error(self.handle) or b"").decode(errors="replace"))
+
+    def submit(self, tag: int, x, y, z, m, h, vx=None, vy=None, vz=None, box: Box | None = None, num_shells: int = 1,
+               steps: int = 1, dt: float = 1e-3, want_output: bool = False):
+        """queue one request; arrays are host float32 (numpy or CPU tensors, pinned memory copies fastest)"""
+        def host(a):
+            if a is None:
+                return None
+            if isinstance(a, torch.Tensor):
+                assert a.device.type == "cpu" and a.dtype == torch.float32 and a.is_contiguous()
+                return a
+            return np.ascontiguousarray(a, dtype=np.float32)
+
+        arrs = [host(a) for a in (x, y, z, m, h, vx, vy, vz)]
+        ptr = lambda a: None if a is None else (a.data_ptr() if isinstance(a, torch.Tensor)  # noqa: E731
+                                                  else a.ctypes.data)
+        r = _abi.EngineRequest()
+        r.tag = tag
+        r.numBodies = len(arrs[0])
+        for k, a in zip(("x", "y", "z", "m", "h", "vx", "vy", "vz"), arrs):
+            setattr(r, k, ptr(a))
+        r.useBox = 1 if box is not None else 0
+        if box is not None:
+            r.box = box.f32()
+        r.numShells = num_shells
+        r.numSteps = steps
+        r.dt = dt
+        out = np.empty((10, r.numBodies), np.float32) if want_output else None
+        r.out = None if out is None else out.ctypes.data
+        self._err(lib.ryo_engine_submit(self.handle, C.byref(r)))
+        self._keep[tag] = arrs
+        if out is not None:
+            self._outputs[tag] = out
+
+    def step(self, stream=None) -> dict:
+        info = _abi.EngineStepInfo()
+        self._err(lib.ryo_engine_step(self.handle, C.byref(info), _stream(stream)))
+        d = {k: getattr(info, k) for k in ("admitted", "retired", "resident", "queued", "solved", "retries",
+                                           "residentBodies")}
+        d["ms"] = list(info.ms)
+        return d
+
+    def poll(self) -> list:
+        """results of retired requests: dicts with tag, bodies, steps, energies and (if requested) the final state
+        (x, y, z, vx, vy, vz, ax, ay, az, p as rows of a 10 x n array, submission order)"""
+        out = []
+        buf = (_abi.EngineResult * 64)()
+        while True:
+            cnt = C.c_int(0)
+            self._err(lib.ryo_engine_poll(self.handle, buf, 64, C.byref(cnt)))
+            for i in range(cnt.value):
+                r = buf[i]
+                self._keep.pop(r.tag, None)
+                out.append(dict(tag=r.tag, bodies=r.numBodies, steps=r.stepsDone, kinetic=r.kineticEnergy,
+                                potential=r.potentialEnergy, initial=r.initialEnergy,
+                                state=self._outputs.pop(r.tag, None)))
+            if cnt.value < 64:
+                return out
+
+    def status(self) -> dict:
+        q, r, b = C.c_int(0), C.c_int(0), C.c_double(0)
+        self._err(lib.ryo_engine_status(self.handle, C.byref(q), C.byref(r), C.byref(b)))
+        return dict(queued=q.value, resident=r.value, bytes_in_use=b.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.ryo_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 _solve_n: dict = {}

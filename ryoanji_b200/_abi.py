@@ -82,6 +82,28 @@ class System(C.Structure):
                 ("numShells", C.c_int)]
 
 
+class EngineParams(C.Structure):
+    _fields_ = [("solve", SolveParams), ("hbmBudgetBytes", C.c_double), ("bytesPerBody", C.c_double),
+                ("maxSystems", C.c_int)]
+
+
+class EngineRequest(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("numBodies", C.c_uint32)] + [(k, C.c_void_p) for k in
+                                                                     ("x", "y", "z", "m", "h", "vx", "vy", "vz")] + \
+               [("useBox", C.c_int), ("box", BoxF32), ("numShells", C.c_int), ("numSteps", C.c_int),
+                ("dt", C.c_float), ("out", C.c_void_p)]
+
+
+class EngineStepInfo(C.Structure):
+    _fields_ = [(k, C.c_int) for k in ("admitted", "retired", "resident", "queued", "solved", "retries")] + \
+               [("residentBodies", C.c_uint64), ("ms", C.c_float * 6)]
+
+
+class EngineResult(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("numBodies", C.c_uint32), ("stepsDone", C.c_int),
+                ("kineticEnergy", C.c_double), ("potentialEnergy", C.c_double), ("initialEnergy", C.c_double)]
+
+
 _p = C.c_void_p
 _sz = C.c_size_t
 _i = C.c_int
@@ -135,6 +157,14 @@ SIGNATURES = {
     "ryo_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "ryo_solve_f32": (_i, [_p, C.POINTER(SolveParams)] + [_p] * 8 + [_sz] + [_p] * 5 + [C.POINTER(SolveStats), _p]),
     "ryo_solve_arrays_get": (_i, [_p, C.POINTER(SolveArrays)]),
+    "ryo_engine_params_default": (None, [C.POINTER(EngineParams)]),
+    "ryo_engine_create": (_i, [_p, C.POINTER(EngineParams), C.POINTER(C.c_void_p)]),
+    "ryo_engine_destroy": (None, [_p]),
+    "ryo_engine_last_error": (C.c_char_p, [_p]),
+    "ryo_engine_submit": (_i, [_p, C.POINTER(EngineRequest)]),
+    "ryo_engine_step": (_i, [_p, C.POINTER(EngineStepInfo), _p]),
+    "ryo_engine_poll": (_i, [_p, C.POINTER(EngineResult), _i, C.POINTER(C.c_int)]),
+    "ryo_engine_status": (_i, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "ryo_solve_batch_f32": (_i, [_p, C.POINTER(SolveParams), C.POINTER(System), _i] + [_p] * 8 + [_sz] + [_p] * 7
                             + [C.POINTER(SolveStats), _p]),
     "ryo_kernel_launches": (C.c_uint64, []),

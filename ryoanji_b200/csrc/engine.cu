@@ -1,0 +1,573 @@
+/*
+ * ryoanji-b200: the served stream. Requests (a particle set plus K kick-drift-kick leapfrog steps) are admitted
+ * under an HBM budget, stay resident on the device across their steps, and every engine step advances all resident
+ * requests together with one batched solve. Requests that arrive while others are being stepped join at the next
+ * step; finished ones leave and free their share of the budget (continuous batching).
+ *
+ * The reference has no serving layer; each step's physics is the reference path (one force evaluation per system
+ * with the single-system solve's semantics, see batch.cu), and the leapfrog is the standard KDK scheme:
+ *   v += a dt/2;  x += v dt;  a = F(x);  v += a dt/2.
+ * A request's first engine step only evaluates its initial forces.
+ *
+ * Resident layout: one arena of per-body arrays (x, y, z, m, h, vx, vy, vz, ax, ay, az, p, id) with the requests
+ * in consecutive ranges; id is the body's index in its request so results go back in submission order. When the
+ * set of resident requests changes, one kernel compacts the survivors into the second arena and the admitted
+ * requests are copied in behind them.
+ */
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <functional>
+
+#include "internal.hpp"
+
+namespace ryo
+{
+
+constexpr int kArenaArrays = 12; // x y z m h vx vy vz ax ay az p (floats); ids are separate
+
+struct Arena
+{
+    float* a[kArenaArrays] = {};
+    uint32_t* id           = nullptr;
+    size_t capacity        = 0;
+
+    void ensure(size_t n)
+    {
+        if (n <= capacity) return;
+        release();
+        size_t cap = std::max<size_t>(n, capacity + capacity / 2);
+        for (int k = 0; k < kArenaArrays; ++k)
+            RYO_CUDA(cudaMalloc(&a[k], cap * sizeof(float)));
+        RYO_CUDA(cudaMalloc(&id, cap * sizeof(uint32_t)));
+        capacity = cap;
+    }
+    void release()
+    {
+        for (int k = 0; k < kArenaArrays; ++k)
+        {
+            if (a[k]) cudaFree(a[k]);
+            a[k] = nullptr;
+        }
+        if (id) cudaFree(id);
+        id       = nullptr;
+        capacity = 0;
+    }
+};
+
+struct ArenaPtrs
+{
+    float* a[kArenaArrays];
+    uint32_t* id;
+};
+
+//! copy the bodies of the surviving requests: destination range r starts at dstFirst[r], source at srcFirst[r]
+__global__ void engineCompact(ArenaPtrs src, ArenaPtrs dst, const uint64_t* __restrict__ dstFirst,
+                              const uint64_t* __restrict__ srcFirst, uint32_t numReq, uint64_t total)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += stride)
+    {
+        uint32_t lo = 0, hi = numReq - 1;
+        while (lo < hi)
+        {
+            uint32_t mid = (lo + hi + 1) >> 1;
+            if (dstFirst[mid] <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        size_t j = srcFirst[lo] + (i - dstFirst[lo]);
+#pragma unroll
+        for (int k = 0; k < kArenaArrays; ++k)
+            dst.a[k][i] = src.a[k][j];
+        dst.id[i] = src.id[j];
+    }
+}
+
+__global__ void engineIota(uint32_t* id, uint64_t first, uint32_t n)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) id[first + i] = i;
+}
+
+struct EngineSys
+{
+    float halfDt, dt;
+    int stepping; // 1: this step kicks and drifts the system
+    int periodic;
+    float lo[3], len[3];
+};
+
+__device__ __forceinline__ uint32_t engineSystemOf(const uint64_t* __restrict__ first, uint32_t numSystems, uint64_t i)
+{
+    uint32_t lo = 0, hi = numSystems - 1;
+    while (lo < hi)
+    {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(first + mid) <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+//! first half kick and drift of the stepping systems; periodic systems wrap back into their box
+__global__ void engineKickDrift(ArenaPtrs A, uint64_t n, const uint64_t* __restrict__ first, uint32_t numSystems,
+                                const EngineSys* __restrict__ sys)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        const EngineSys& S = sys[engineSystemOf(first, numSystems, i)];
+        if (!S.stepping) continue;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            float v  = A.a[5 + d][i] + S.halfDt * A.a[8 + d][i];
+            float x  = A.a[d][i] + S.dt * v;
+            if (S.periodic)
+            {
+                float r = x - S.lo[d];
+                r -= S.len[d] * floorf(r / S.len[d]);
+                if (!(r < S.len[d])) r = 0.f; // rounding can land exactly on the upper face
+                x = S.lo[d] + r;
+            }
+            A.a[5 + d][i] = v;
+            A.a[d][i]     = x;
+        }
+    }
+}
+
+//! second half kick of the stepping systems, then per-system kinetic energy (FP64)
+__global__ void engineKick(ArenaPtrs A, uint64_t n, const uint64_t* __restrict__ first, uint32_t numSystems,
+                           const EngineSys* __restrict__ sys, double* __restrict__ kinetic)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        uint32_t s         = engineSystemOf(first, numSystems, i);
+        const EngineSys& S = sys[s];
+        double v2          = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            float v = A.a[5 + d][i];
+            if (S.stepping) v += S.halfDt * A.a[8 + d][i];
+            A.a[5 + d][i] = v;
+            v2 += double(v) * v;
+        }
+        double ke = 0.5 * double(A.a[3][i]) * v2;
+        // neighbouring threads usually share the system: reduce over the warp's runs of equal s
+        unsigned peers = __match_any_sync(__activemask(), s);
+        int leader     = __ffs(peers) - 1;
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            double other = __shfl_down_sync(__activemask(), ke, o);
+            int src      = int(threadIdx.x & 31) + o;
+            if (src < 32 && ((peers >> src) & 1u)) ke += other;
+        }
+        if (int(threadIdx.x & 31) == leader) atomicAdd(kinetic + s, ke);
+    }
+}
+
+//! gather ids by the permutation of the solve (order[i] = previous index of body i)
+__global__ void engineGatherIds(const uint32_t* __restrict__ order, const uint32_t* __restrict__ in,
+                                uint32_t* __restrict__ out, uint64_t n)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        out[i] = in[order[i]];
+}
+
+//! final state of one request in submission order: out[k][id[i]] = arena[k][first + i] for x y z vx vy vz ax ay az p
+__global__ void engineScatterResult(ArenaPtrs A, uint64_t first, uint32_t n, float* __restrict__ out)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t j      = A.id[first + i];
+    const int k[10] = {0, 1, 2, 5, 6, 7, 8, 9, 10, 11};
+#pragma unroll
+    for (int c = 0; c < 10; ++c)
+        out[size_t(c) * n + j] = A.a[k[c]][first + i];
+}
+
+} // namespace ryo
+
+using namespace ryo;
+
+namespace
+{
+
+struct Request
+{
+    uint64_t tag;
+    uint32_t n;
+    ryo_system sys;
+    int stepsLeft, stepsDone;
+    float dt;
+    bool haveForces;
+    const float* in[8]; // host x y z m h vx vy vz (vx..vz may be null)
+    float* out;         // host, 10 * n floats (may be null)
+    double bytes;
+    double e0;          // total energy after the initial forces
+    uint64_t arenaFirst;
+};
+
+struct Arenas
+{
+    Arena buf[2];
+    int cur = 0;
+};
+
+} // namespace
+
+struct ryo_engine
+{
+    ryo_ctx* ctx;
+    ryo_solve_params solve;
+    double budget;
+    double bytesPerBody;
+    int maxSystems;
+    double used = 0;
+    std::deque<Request> queue;
+    std::vector<Request> resident;
+    std::vector<ryo_engine_result> done;
+    Arenas arenas;
+    uint64_t residentBodies = 0;
+    bool changed            = false;
+    uint64_t solves         = 0;
+    std::string lastError;
+
+    ~ryo_engine()
+    {
+        arenas.buf[0].release();
+        arenas.buf[1].release();
+    }
+};
+
+namespace
+{
+ArenaPtrs ptrsOf(const Arena& a)
+{
+    ArenaPtrs p;
+    for (int k = 0; k < kArenaArrays; ++k)
+        p.a[k] = a.a[k];
+    p.id = a.id;
+    return p;
+}
+
+unsigned gridFor(size_t n, int sms)
+{
+    size_t want = (n + 255) / 256;
+    size_t cap  = size_t(sms) * 16;
+    return unsigned(std::max<size_t>(1, std::min(want, cap)));
+}
+
+//! rebuild the arena: survivors compacted to the front, newly admitted requests copied in behind them
+void rebuildArena(ryo_engine* E, std::vector<Request>& admitted, cudaStream_t s)
+{
+    Arena& src = E->arenas.buf[E->arenas.cur];
+    Arena& dst = E->arenas.buf[1 - E->arenas.cur];
+    uint64_t total = 0;
+    for (auto& r : E->resident)
+        total += r.n;
+    uint64_t survivors = total;
+    for (auto& r : admitted)
+        total += r.n;
+    dst.ensure(std::max<uint64_t>(total, 1));
+    if (!E->resident.empty())
+    {
+        std::vector<uint64_t> df(E->resident.size()), sf(E->resident.size());
+        uint64_t o = 0;
+        for (size_t k = 0; k < E->resident.size(); ++k)
+        {
+            df[k] = o;
+            sf[k] = E->resident[k].arenaFirst;
+            o += E->resident[k].n;
+        }
+        uint64_t* d = E->ctx->scratch<uint64_t>("eng.compact", 2 * df.size(), s);
+        RYO_CUDA(cudaMemcpyAsync(d, df.data(), df.size() * 8, cudaMemcpyHostToDevice, s));
+        RYO_CUDA(cudaMemcpyAsync(d + df.size(), sf.data(), sf.size() * 8, cudaMemcpyHostToDevice, s));
+        engineCompact<<<gridFor(survivors, E->ctx->smCount), 256, 0, s>>>(ptrsOf(src), ptrsOf(dst), d, d + df.size(),
+                                                                         uint32_t(df.size()), survivors);
+        RYO_LAUNCH_CHECK();
+        for (size_t k = 0; k < E->resident.size(); ++k)
+            E->resident[k].arenaFirst = df[k];
+    }
+    uint64_t o = survivors;
+    for (auto& r : admitted)
+    {
+        r.arenaFirst = o;
+        for (int k = 0; k < 8; ++k)
+        {
+            if (r.in[k])
+                RYO_CUDA(cudaMemcpyAsync(dst.a[k] + o, r.in[k], r.n * sizeof(float), cudaMemcpyHostToDevice, s));
+            else
+                RYO_CUDA(cudaMemsetAsync(dst.a[k] + o, 0, r.n * sizeof(float), s));
+        }
+        engineIota<<<ceilDiv(r.n, 256), 256, 0, s>>>(dst.id, o, r.n);
+        RYO_LAUNCH_CHECK();
+        o += r.n;
+        E->resident.push_back(r);
+    }
+    E->arenas.cur     = 1 - E->arenas.cur;
+    E->residentBodies = total;
+}
+
+ryo_status engineGuard(ryo_engine* E, const std::function<void()>& f)
+{
+    try
+    {
+        f();
+        return RYO_OK;
+    }
+    catch (const CudaError& e)
+    {
+        E->lastError = std::string(e.what) + ": " + cudaGetErrorString(e.err);
+        return e.err == cudaErrorMemoryAllocation ? RYO_ERR_OOM : RYO_ERR_CUDA;
+    }
+    catch (const std::bad_alloc&)
+    {
+        E->lastError = "host allocation failed";
+        return RYO_ERR_OOM;
+    }
+}
+} // namespace
+
+extern "C" void ryo_engine_params_default(ryo_engine_params* p)
+{
+    if (!p) return;
+    *p = ryo_engine_params{};
+    ryo_solve_params_default(&p->solve);
+    p->hbmBudgetBytes = 120e9;
+    p->bytesPerBody   = 256.0;
+    p->maxSystems     = RYO_BATCH_MAX_SYSTEMS;
+}
+
+extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params* p, ryo_engine_t** out)
+{
+    if (!ctx || !p || !out) return RYO_ERR_BAD_ARG;
+    if (!(p->hbmBudgetBytes > 0) || !(p->bytesPerBody > 0) || p->maxSystems < 1 ||
+        p->maxSystems > RYO_BATCH_MAX_SYSTEMS)
+        return RYO_ERR_BAD_ARG;
+    try
+    {
+        auto* E         = new ryo_engine();
+        E->ctx          = ctx;
+        E->solve        = p->solve;
+        E->budget       = p->hbmBudgetBytes;
+        E->bytesPerBody = p->bytesPerBody;
+        E->maxSystems   = p->maxSystems;
+        *out            = E;
+        return RYO_OK;
+    }
+    catch (const std::bad_alloc&)
+    {
+        return RYO_ERR_OOM;
+    }
+}
+
+extern "C" void ryo_engine_destroy(ryo_engine_t* E)
+{
+    if (E) cudaDeviceSynchronize();
+    delete E;
+}
+
+extern "C" const char* ryo_engine_last_error(const ryo_engine_t* E) { return E ? E->lastError.c_str() : ""; }
+
+extern "C" ryo_status ryo_engine_submit(ryo_engine_t* E, const ryo_engine_request* r)
+{
+    if (!E || !r) return RYO_ERR_BAD_ARG;
+    if (!r->x || !r->y || !r->z || !r->m || !r->h || r->numBodies < 1 || r->numSteps < 0 || !(r->dt >= 0.f))
+    {
+        E->lastError = "engine_submit: bad request";
+        return RYO_ERR_BAD_ARG;
+    }
+    if (r->useBox)
+    {
+        const float* l = r->box.limits;
+        for (int d = 0; d < 3; ++d)
+            if (!(l[2 * d + 1] > l[2 * d]))
+            {
+                E->lastError = "engine_submit: every box axis needs max > min";
+                return RYO_ERR_BAD_ARG;
+            }
+    }
+    Request q{};
+    q.tag                = r->tag;
+    q.n                  = r->numBodies;
+    q.sys.numBodies      = r->numBodies;
+    q.sys.useBox         = r->useBox;
+    q.sys.box            = r->box;
+    q.sys.numShells      = r->numShells;
+    q.stepsLeft          = r->numSteps;
+    q.dt                 = r->dt;
+    const float* in[8]   = {r->x, r->y, r->z, r->m, r->h, r->vx, r->vy, r->vz};
+    for (int k = 0; k < 8; ++k)
+        q.in[k] = in[k];
+    q.out   = r->out;
+    q.bytes = E->bytesPerBody * double(r->numBodies);
+    if (q.bytes > E->budget)
+    {
+        E->lastError = "engine_submit: the request alone exceeds the HBM budget";
+        return RYO_ERR_CAPACITY;
+    }
+    E->queue.push_back(q);
+    return RYO_OK;
+}
+
+extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* info, ryo_stream_t stream)
+{
+    if (!E) return RYO_ERR_BAD_ARG;
+    return engineGuard(E,
+                       [&]
+                       {
+                           cudaStream_t s = stream;
+                           ryo_engine_step_info st{};
+                           // admission: arrival order, while the budget and the system slots allow
+                           std::vector<Request> admitted;
+                           while (!E->queue.empty() &&
+                                  int(E->resident.size() + admitted.size()) < E->maxSystems &&
+                                  E->used + E->queue.front().bytes <= E->budget)
+                           {
+                               E->used += E->queue.front().bytes;
+                               admitted.push_back(E->queue.front());
+                               E->queue.pop_front();
+                           }
+                           st.admitted = int(admitted.size());
+                           if (!admitted.empty() || E->changed) rebuildArena(E, admitted, s);
+                           E->changed = false;
+                           st.resident       = int(E->resident.size());
+                           st.residentBodies = E->residentBodies;
+                           st.queued         = int(E->queue.size());
+                           if (E->resident.empty())
+                           {
+                               if (info) *info = st;
+                               return;
+                           }
+                           const uint32_t ns = uint32_t(E->resident.size());
+                           Arena& A          = E->arenas.buf[E->arenas.cur];
+                           ArenaPtrs P       = ptrsOf(A);
+                           const uint64_t n  = E->residentBodies;
+
+                           std::vector<ryo_system> sys(ns);
+                           std::vector<EngineSys> es(ns);
+                           std::vector<uint64_t> first(ns + 1);
+                           for (uint32_t k = 0; k < ns; ++k)
+                           {
+                               Request& q          = E->resident[k];
+                               sys[k]              = q.sys;
+                               sys[k].firstBody    = q.arenaFirst;
+                               first[k]            = q.arenaFirst;
+                               EngineSys& e        = es[k];
+                               e.dt                = q.dt;
+                               e.halfDt            = 0.5f * q.dt;
+                               e.stepping          = q.haveForces ? 1 : 0;
+                               bool periodic       = q.sys.useBox && q.sys.box.boundary[0] == RYO_BOUNDARY_PERIODIC &&
+                                               q.sys.box.boundary[1] == RYO_BOUNDARY_PERIODIC &&
+                                               q.sys.box.boundary[2] == RYO_BOUNDARY_PERIODIC;
+                               e.periodic          = periodic ? 1 : 0;
+                               for (int d = 0; d < 3; ++d)
+                               {
+                                   e.lo[d]  = q.sys.box.limits[2 * d];
+                                   e.len[d] = q.sys.box.limits[2 * d + 1] - q.sys.box.limits[2 * d];
+                               }
+                           }
+                           first[ns]          = n;
+                           uint64_t* dFirst   = E->ctx->scratch<uint64_t>("eng.first", ns + 1, s);
+                           EngineSys* dSys    = E->ctx->scratch<EngineSys>("eng.sys", ns, s);
+                           double* dKin       = E->ctx->scratch<double>("eng.kinetic", ns, s);
+                           RYO_CUDA(cudaMemcpyAsync(dFirst, first.data(), 8 * (ns + 1), cudaMemcpyHostToDevice, s));
+                           RYO_CUDA(cudaMemcpyAsync(dSys, es.data(), sizeof(EngineSys) * ns, cudaMemcpyHostToDevice,
+                                                    s));
+                           RYO_CUDA(cudaMemsetAsync(dKin, 0, sizeof(double) * ns, s));
+                           engineKickDrift<<<gridFor(n, E->ctx->smCount), 256, 0, s>>>(P, n, dFirst, ns, dSys);
+                           RYO_LAUNCH_CHECK();
+
+                           uint32_t* order = E->ctx->scratch<uint32_t>("eng.order", n, s);
+                           std::vector<double> pe(ns);
+                           ryo_solve_stats ss{};
+                           ryo_status rs = ryo_solve_batch_f32(E->ctx, &E->solve, sys.data(), int(ns), P.a[0], P.a[1],
+                                                               P.a[2], P.a[3], P.a[4], P.a[5], P.a[6], P.a[7], n,
+                                                               P.a[11], P.a[8], P.a[9], P.a[10], order, pe.data(),
+                                                               nullptr, &ss, s);
+                           if (rs != RYO_OK)
+                               throw CudaError{cudaErrorUnknown, "engine_step: batched solve failed"};
+                           E->solves += ns;
+                           uint32_t* idTmp = E->ctx->scratch<uint32_t>("eng.idtmp", n, s);
+                           engineGatherIds<<<gridFor(n, E->ctx->smCount), 256, 0, s>>>(order, A.id, idTmp, n);
+                           RYO_LAUNCH_CHECK();
+                           RYO_CUDA(cudaMemcpyAsync(A.id, idTmp, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+                           engineKick<<<gridFor(n, E->ctx->smCount), 256, 0, s>>>(P, n, dFirst, ns, dSys, dKin);
+                           RYO_LAUNCH_CHECK();
+                           std::vector<double> ke(ns);
+                           RYO_CUDA(cudaMemcpyAsync(ke.data(), dKin, sizeof(double) * ns, cudaMemcpyDeviceToHost, s));
+                           RYO_CUDA(cudaStreamSynchronize(s));
+
+                           // advance the requests; retire the finished ones
+                           std::vector<Request> keep;
+                           for (uint32_t k = 0; k < ns; ++k)
+                           {
+                               Request& q = E->resident[k];
+                               if (!q.haveForces)
+                               {
+                                   q.haveForces = true;
+                                   q.e0         = ke[k] + pe[k];
+                               }
+                               else
+                               {
+                                   --q.stepsLeft;
+                                   ++q.stepsDone;
+                               }
+                               if (q.stepsLeft > 0)
+                               {
+                                   keep.push_back(q);
+                                   continue;
+                               }
+                               if (q.out)
+                               {
+                                   float* tmp = E->ctx->scratch<float>("eng.result", 10 * size_t(q.n), s);
+                                   engineScatterResult<<<ceilDiv(q.n, 256), 256, 0, s>>>(P, q.arenaFirst, q.n, tmp);
+                                   RYO_LAUNCH_CHECK();
+                                   RYO_CUDA(cudaMemcpyAsync(q.out, tmp, 10 * size_t(q.n) * sizeof(float),
+                                                            cudaMemcpyDeviceToHost, s));
+                                   RYO_CUDA(cudaStreamSynchronize(s));
+                               }
+                               ryo_engine_result res{};
+                               res.tag             = q.tag;
+                               res.numBodies       = q.n;
+                               res.stepsDone       = q.stepsDone;
+                               res.kineticEnergy   = ke[k];
+                               res.potentialEnergy = pe[k];
+                               res.initialEnergy   = q.e0;
+                               E->done.push_back(res);
+                               E->used -= q.bytes;
+                               ++st.retired;
+                               E->changed = true;
+                           }
+                           E->resident.swap(keep);
+                           st.solved    = int(ns);
+                           st.retries   = int(ss.retries);
+                           for (int i = 0; i < 6; ++i)
+                               st.ms[i] = ss.ms[i];
+                           if (info) *info = st;
+                       });
+}
+
+extern "C" ryo_status ryo_engine_poll(ryo_engine_t* E, ryo_engine_result* out, int capacity, int* count)
+{
+    if (!E || !count || capacity < 0 || (capacity > 0 && !out)) return RYO_ERR_BAD_ARG;
+    int c = std::min<int>(capacity, int(E->done.size()));
+    for (int i = 0; i < c; ++i)
+        out[i] = E->done[i];
+    E->done.erase(E->done.begin(), E->done.begin() + c);
+    *count = c;
+    return RYO_OK;
+}
+
+extern "C" ryo_status ryo_engine_status(const ryo_engine_t* E, int* queued, int* resident, double* bytesInUse)
+{
+    if (!E) return RYO_ERR_BAD_ARG;
+    if (queued) *queued = int(E->queue.size());
+    if (resident) *resident = int(E->resident.size());
+    if (bytesInUse) *bytesInUse = E->used;
+    return RYO_OK;
+}

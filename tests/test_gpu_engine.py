@@ -1,0 +1,140 @@
+"""Served stream (ryo_engine_*): continuous batching must not change any request's result.
+
+Each request is run alone and in a mix of requests that arrive at different engine steps; the final states
+must agree within 1e-5 relative. Forces in a batch equal the single-system solve's, so the trajectories
+agree to rounding. The leapfrog itself is checked against a float64 numpy KDK integrator on a system the tree
+evaluates exactly (one leaf, all P2P). Energy drift, admission under the budget and error statuses are checked too.
+"""
+import numpy as np
+import pytest
+import torch
+
+from ryoanji_b200 import datasets as ds
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests():
+    import ryoanji_b200 as ryo
+    pb = ds.periodic_box(2000, seed=4, eps=0.002)
+    pb.vx, pb.vy, pb.vz = (np.random.default_rng(k).normal(0, 0.05, pb.n).astype(np.float32) for k in range(3))
+    return [
+        dict(tag=1, p=ds.plummer(3000, seed=1), steps=5, box=None),
+        dict(tag=2, p=ds.uniform_cube(5000, seed=2, eps=0.004), steps=3, box=None),
+        dict(tag=3, p=pb, steps=4, box=ryo.Box(*pb.box, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)),
+        dict(tag=4, p=ds.plummer(10000, seed=3), steps=0, box=None),
+        dict(tag=5, p=ds.uniform_cube(1500, seed=5, eps=0.01), steps=7, box=None),
+        dict(tag=6, p=ds.plummer(800, seed=6, a=0.3), steps=2, box=None),
+    ] + [dict(tag=10 + k, p=ds.plummer(300 + 50 * k, seed=20 + k), steps=1 + k % 3, box=None) for k in range(6)]
+
+
+def _submit(eng, r, dt=1e-3):
+    p = r["p"]
+    eng.submit(r["tag"], p.x, p.y, p.z, p.m, p.h, p.vx, p.vy, p.vz, box=r["box"], steps=r["steps"], dt=dt,
+               want_output=True)
+
+
+def _drain(eng, max_steps=200):
+    res = {}
+    for _ in range(max_steps):
+        info = eng.step()
+        for d in eng.poll():
+            res[d["tag"]] = d
+        if info["resident"] == 0 and info["queued"] == 0 and info["retired"] == 0:
+            break
+    return res
+
+
+def test_each_request_same_alone_and_in_the_mix():
+    import ryoanji_b200 as ryo
+    reqs = _requests()
+    params = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32)
+    mix = ryo.Engine(params)
+    # staggered arrivals: two at once, then one per step
+    _submit(mix, reqs[0])
+    _submit(mix, reqs[1])
+    mixed = {}
+    for r in reqs[2:]:
+        mix.step()
+        for d in mix.poll():
+            mixed[d["tag"]] = d
+        _submit(mix, r)
+    mixed.update(_drain(mix))
+    assert sorted(mixed) == sorted(r["tag"] for r in reqs)
+    for r in reqs:
+        alone = ryo.Engine(params)
+        _submit(alone, r)
+        a = _drain(alone)[r["tag"]]
+        b = mixed[r["tag"]]
+        assert a["steps"] == b["steps"] == r["steps"]
+        sa, sb = a["state"], b["state"]
+        scale = np.abs(sa).max(axis=1, keepdims=True) + 1e-30
+        rel = float((np.abs(sa - sb) / scale).max())
+        assert rel <= 1e-5, (r["tag"], rel)
+        assert b["potential"] == pytest.approx(a["potential"], rel=1e-6)
+        alone.close()
+    mix.close()
+
+
+def test_leapfrog_matches_float64_reference():
+    """50 bodies in one leaf: the tree force is the exact softened sum, so the engine's KDK can be compared with
+    a float64 numpy KDK of the same scheme"""
+    import ryoanji_b200 as ryo
+    p = ds.plummer(50, seed=9)
+    K, dt = 20, 2e-3
+    eng = ryo.Engine(ryo.SolveParams(theta=0.5, bucket_size=64, group_size=64))
+    eng.submit(7, p.x, p.y, p.z, p.m, p.h, p.vx, p.vy, p.vz, steps=K, dt=dt, want_output=True)
+    got = _drain(eng)[7]["state"]
+
+    x = np.stack([p.x, p.y, p.z], 1).astype(np.float64)
+    v = np.stack([p.vx, p.vy, p.vz], 1).astype(np.float64)
+    m = p.m.astype(np.float64)
+    h = p.h.astype(np.float64)
+
+    def acc(x):
+        d = x[None, :, :] - x[:, None, :]
+        r2 = (d * d).sum(-1)
+        hh = (h[:, None] + h[None, :]) ** 2
+        r2e = np.maximum(r2, hh)
+        w = m[None, :] / (r2e * np.sqrt(r2e))
+        np.fill_diagonal(w, 0.0)
+        return (d * w[:, :, None]).sum(1)
+
+    a = acc(x)
+    for _ in range(K):
+        v += 0.5 * dt * a
+        x += dt * v
+        a = acc(x)
+        v += 0.5 * dt * a
+    ref = np.concatenate([x.T, v.T, a.T], 0)
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    rel = np.abs(got[:9] - ref) / scale
+    assert float(rel.max()) < 2e-4, float(rel.max())
+
+
+def test_energy_drift_small():
+    import ryoanji_b200 as ryo
+    p = ds.plummer(4000, seed=12)
+    eng = ryo.Engine(ryo.SolveParams(theta=0.4))
+    eng.submit(1, p.x, p.y, p.z, p.m, p.h, p.vx, p.vy, p.vz, steps=30, dt=1e-3)
+    d = _drain(eng)[1]
+    e1 = d["kinetic"] + d["potential"]
+    assert abs(e1 - d["initial"]) / abs(d["initial"]) < 2e-3, (e1, d["initial"])
+
+
+def test_admission_respects_budget():
+    import ryoanji_b200 as ryo
+    reqs = [ds.plummer(1000, seed=30 + k) for k in range(6)]
+    # 256 B per body: 2.5 requests fit in 640 kB
+    eng = ryo.Engine(ryo.SolveParams(), hbm_budget_bytes=640e3, bytes_per_body=256.0)
+    for k, p in enumerate(reqs):
+        eng.submit(k, p.x, p.y, p.z, p.m, p.h, p.vx, p.vy, p.vz, steps=2, dt=1e-3)
+    first = eng.step()
+    assert first["resident"] == 2 and first["queued"] == 4
+    assert eng.status()["bytes_in_use"] <= 640e3
+    done = _drain(eng)
+    assert sorted(done) == list(range(6))
+    big = ds.plummer(3000, seed=40)
+    with pytest.raises(ryo.RyoError):
+        eng.submit(99, big.x, big.y, big.z, big.m, big.h, steps=1)
+    eng.close()
