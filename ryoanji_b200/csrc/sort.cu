@@ -165,32 +165,43 @@ size_t sortTempBytes(size_t n)
     return 2 * kMaxPasses * kDigits * sizeof(uint32_t) + 256 + (tiles + 1) * kDigits * sizeof(unsigned long long);
 }
 
-//! all digit histograms in one read of the keys; warp-aggregated shared-memory counts
+//! all digit histograms in one read of the keys: two shared-memory copies per block (each shared by four warps),
+//! plain shared atomics, and one aggregated add when a whole warp holds the same digit (top digits of clustered or
+//! presorted keys)
 __global__ void __launch_bounds__(256) digitHistogram(const uint64_t* __restrict__ keys, size_t n, int beginBit,
                                                       int numPasses, uint32_t* hist)
 {
-    __shared__ uint32_t sh[kMaxPasses][kDigits];
-    for (int i = threadIdx.x; i < kMaxPasses * kDigits; i += blockDim.x)
-        (&sh[0][0])[i] = 0;
+    __shared__ uint32_t sh[2][kMaxPasses][kDigits];
+    for (int i = threadIdx.x; i < 2 * kMaxPasses * kDigits; i += blockDim.x)
+        (&sh[0][0][0])[i] = 0;
     __syncthreads();
-    size_t stride = size_t(gridDim.x) * blockDim.x;
+    uint32_t(*mine)[kDigits] = sh[(threadIdx.x >> 7) & 1];
+    const unsigned lane      = laneId();
+    size_t stride            = size_t(gridDim.x) * blockDim.x;
     for (size_t i0 = size_t(blockIdx.x) * blockDim.x; i0 < n; i0 += stride)
     {
         size_t i       = i0 + threadIdx.x;
         bool valid     = i < n;
         uint64_t key   = valid ? keys[i] : 0;
         unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        if (vmask == 0) continue;
+        int lead = __ffs(vmask) - 1;
         for (int p = 0; p < numPasses; ++p)
         {
-            unsigned d     = valid ? unsigned(key >> (beginBit + 8 * p)) & 255u : 256u;
-            unsigned peers = __match_any_sync(0xffffffffu, d) & vmask;
-            if (valid && (peers & lanemaskLt()) == 0) atomicAdd(&sh[p][d], __popc(peers));
+            unsigned d  = unsigned(key >> (beginBit + 8 * p)) & 255u;
+            unsigned d0 = __shfl_sync(0xffffffffu, d, lead);
+            if (__all_sync(0xffffffffu, !valid || d == d0))
+            {
+                if (lane == unsigned(lead)) atomicAdd(&mine[p][d0], __popc(vmask));
+            }
+            else if (valid)
+                atomicAdd(&mine[p][d], 1u);
         }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < numPasses * kDigits; i += blockDim.x)
     {
-        uint32_t c = (&sh[0][0])[i];
+        uint32_t c = (&sh[0][0][0])[i] + (&sh[1][0][0])[i];
         if (c) atomicAdd(hist + i, c);
     }
 }

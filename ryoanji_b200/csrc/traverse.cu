@@ -137,6 +137,22 @@ __device__ __forceinline__ void m2p2(Acc2& A, f2 tx, f2 ty, f2 tz, f2 cx, f2 cy,
     A.z    = fma2(rm5, Qrz, fma2(f, rz, A.z));
 }
 
+/*! P2P with a softening floor hh = (h_i + h_j)^2 common to both targets and the source: the same arithmetic as
+ *  p2p2 when every h is equal, without the two packed operations that form hh */
+__device__ __forceinline__ void p2p2u(Acc2& A, f2 tx, f2 ty, f2 tz, float hh, f2 sx, f2 sy, f2 sz, f2 sm)
+{
+    f2 dx  = sub2(sx, tx), dy = sub2(sy, ty), dz = sub2(sz, tz);
+    f2 r2  = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    float r0, r1;
+    upk(r2, r0, r1);
+    f2 ir  = pk(rsqrtApprox(fmaxf(r0, hh)), rsqrtApprox(fmaxf(r1, hh)));
+    f2 m3  = mul2(mul2(sm, ir), mul2(ir, ir));
+    A.p    = fma2(m3, r2, A.p);
+    A.x    = fma2(dx, m3, A.x);
+    A.y    = fma2(dy, m3, A.y);
+    A.z    = fma2(dz, m3, A.z);
+}
+
 /*! P2P (kernel.hpp:99-120) for both targets against one source; s* are duplicated pairs, th the targets' h */
 __device__ __forceinline__ void p2p2(Acc2& A, f2 tx, f2 ty, f2 tz, f2 th, f2 sx, f2 sy, f2 sz, f2 sm, f2 sh)
 {
@@ -160,6 +176,8 @@ struct TargetState
     f2 tx, ty, tz, th; // the lane's two targets (shifted by the current replica)
     Acc2 acc;          // -phi, a
     Acc2 comp;         // Kahan compensation of acc
+    float h0;          // the common smoothing length of the group's targets, if uniformH
+    bool uniformH;
 };
 
 __device__ __forceinline__ void kahan2(f2& sum, f2& comp, f2 v)
@@ -338,6 +356,37 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
         const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
         const f2* sth        = reinterpret_cast<const f2*>(S.stage + 2 * kWarp);
         Acc2 part            = zero2();
+        // equal smoothing lengths for the targets and this batch's sources: hh is one constant
+        if (T.uniformH)
+        {
+            float hj0, hjl, dup;
+            upk(sth[0], hj0, dup);
+            upk(sth[lane < nvalid ? lane : 0], hjl, dup);
+            if (__all_sync(0xffffffffu, hjl == hj0))
+            {
+                float hij = __fadd_rn(T.h0, hj0);
+                float hh  = __fmul_rn(hij, hij);
+                auto oneU = [&](int j)
+                {
+                    ulonglong2 a = st[2 * j], c = st[2 * j + 1];
+                    p2p2u(part, T.tx, T.ty, T.tz, hh, a.x, a.y, c.x, c.y);
+                };
+                if (nvalid == kWarp)
+                {
+#pragma unroll 8
+                    for (int j = 0; j < kWarp; ++j)
+                        oneU(j);
+                }
+                else
+                {
+                    for (int j = 0; j < nvalid; ++j)
+                        oneU(j);
+                }
+                addBatch(T, part);
+                __syncwarp();
+                continue;
+            }
+        }
         auto one = [&](int j)
         {
             ulonglong2 a = st[2 * j], c = st[2 * j + 1];
@@ -421,7 +470,7 @@ void launchTraversalReset(Control* ctl, bool resetStats, cudaStream_t s)
 }
 
 template<class Nodes, class Targets, class Sources>
-__global__ void __launch_bounds__(kTravThreads)
+__global__ void __launch_bounds__(kTravThreads, 5)
     traverseKernel(TraverseLaunch P, Nodes nodes, Targets tgt, Sources src)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
@@ -445,6 +494,8 @@ __global__ void __launch_bounds__(kTravThreads)
         T.ty      = pk(t0.y, t1.y);
         T.tz      = pk(t0.z, t1.z);
         T.th      = pk(t0.w, t1.w);
+        T.h0       = __shfl_sync(0xffffffffu, t0.w, 0);
+        T.uniformH = __all_sync(0xffffffffu, t0.w == T.h0 && t1.w == T.h0);
         T.acc     = zero2();
         T.comp    = zero2();
         float lo[3] = {fminf(t0.x, t1.x), fminf(t0.y, t1.y), fminf(t0.z, t1.z)};

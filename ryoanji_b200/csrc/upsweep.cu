@@ -340,44 +340,48 @@ __device__ void emitNode(const FusedArgs& A, int node, const double c[3], double
     if (node == 0 && A.root) writeRootExpansion(A.root, c, raw);
 }
 
-//! combine the eight children of @p node (parallel-axis theorem, double)
-__device__ void combineChildren(const FusedArgs& A, int node, int fc)
+//! sum over the eight lanes of a leaf group
+__device__ __forceinline__ double groupSum8(double v, unsigned gmask)
 {
-    double cc[8][3], cw[8], cm[8], cq[8][6];
-    double W = 0, M = 0, sx = 0, sy = 0, sz = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
-    {
-        loadDNode(A.dn + fc + k, cc[k], cw[k], cm[k], cq[k]);
-        double w = fabs(cw[k]);
-        W += w;
-        M += cm[k];
-        sx += w * cc[k][0];
-        sy += w * cc[k][1];
-        sz += w * cc[k][2];
-    }
+    for (int o = 1; o < kTpl; o <<= 1)
+        v += __shfl_xor_sync(gmask, v, o, kTpl);
+    return v;
+}
+
+//! combine the eight children of @p node (parallel-axis theorem, double): lane @p sub of the group holds child sub
+__device__ void combineChildren(const FusedArgs& A, int node, int fc, int sub, unsigned gmask)
+{
+    double cc[3], cw, cm, cq[6];
+    loadDNode(A.dn + fc + sub, cc, cw, cm, cq);
+    double w  = fabs(cw);
+    double W  = groupSum8(w, gmask);
+    double M  = groupSum8(cm, gmask);
+    double sx = groupSum8(w * cc[0], gmask);
+    double sy = groupSum8(w * cc[1], gmask);
+    double sz = groupSum8(w * cc[2], gmask);
     double c[3];
     double inv = W != 0.0 ? 1.0 / W : 1.0;
     c[0]       = sx * inv;
     c[1]       = sy * inv;
     c[2]       = sz * inv;
-    double q[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
+    double dx = cc[0] - c[0], dy = cc[1] - c[1], dz = cc[2] - c[2];
+    double q[6];
+    q[0] = groupSum8(cq[0] + cm * dx * dx, gmask);
+    q[1] = groupSum8(cq[1] + cm * dx * dy, gmask);
+    q[2] = groupSum8(cq[2] + cm * dx * dz, gmask);
+    q[3] = groupSum8(cq[3] + cm * dy * dy, gmask);
+    q[4] = groupSum8(cq[4] + cm * dy * dz, gmask);
+    q[5] = groupSum8(cq[5] + cm * dz * dz, gmask);
+    if (sub == 0)
     {
-        double dx = cc[k][0] - c[0], dy = cc[k][1] - c[1], dz = cc[k][2] - c[2];
-        q[0] += cq[k][0] + cm[k] * dx * dx;
-        q[1] += cq[k][1] + cm[k] * dx * dy;
-        q[2] += cq[k][2] + cm[k] * dx * dz;
-        q[3] += cq[k][3] + cm[k] * dy * dy;
-        q[4] += cq[k][4] + cm[k] * dy * dz;
-        q[5] += cq[k][5] + cm[k] * dz * dz;
+        storeDNode(A.dn + node, c, W, M, q);
+        emitNode(A, node, c, W, M, q, fc, 0, 0);
     }
-    storeDNode(A.dn + node, c, W, M, q);
-    emitNode(A, node, c, W, M, q, fc, 0, 0);
 }
 
-/*! eight lanes per leaf: one pass over the bodies, then the last-arriving sibling climbs to combine parents */
+/*! eight lanes per leaf: one pass over the bodies, then the group of the last-arriving sibling climbs and combines
+ *  each parent with one child per lane (small register footprint, so many leaf groups stay resident per SM) */
 __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
 {
     int tid     = blockIdx.x * blockDim.x + threadIdx.x;
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
 #pragma unroll
     for (int k = 0; k < 14; ++k)
         s[k] = groupSum8(s[k]);
-    if (!active || sub != 0) return;
+    if (!active) return; // the eight lanes of a leaf group leave together
 
     int node = A.leafToInternal[leaf];
     double W = s[0], M = s[4];
@@ -449,18 +453,27 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
         q[4] = s[12] + oy * s[7] + oz * s[6] + M * oy * oz;
         q[5] = s[13] + 2 * oz * s[7] + M * oz * oz;
     }
-    storeDNode(A.dn + node, c, W, M, q);
-    emitNode(A, node, c, W, M, q, 0, b0, b1 - b0);
+    if (sub == 0)
+    {
+        storeDNode(A.dn + node, c, W, M, q);
+        emitNode(A, node, c, W, M, q, 0, b0, b1 - b0);
+    }
 
-    // climb: the eighth sibling to arrive combines the parent
+    // climb: the group of the eighth sibling to arrive combines the parent, one child per lane
+    const unsigned gmask = 0xFFu << (threadIdx.x & 24u);
     while (node > 0)
     {
         int parent = A.parents[(node - 1) / 8];
+        int last   = 0;
+        if (sub == 0)
+        {
+            __threadfence();
+            last = atomicAdd(A.arrivals + parent, 1u) == 7u;
+        }
+        last = __shfl_sync(gmask, last, 0, kTpl);
+        if (!last) break;
         __threadfence();
-        unsigned prev = atomicAdd(A.arrivals + parent, 1u);
-        if (prev != 7) break;
-        __threadfence();
-        combineChildren(A, parent, A.childOffsets[parent]);
+        combineChildren(A, parent, A.childOffsets[parent], sub, gmask);
         node = parent;
     }
 }

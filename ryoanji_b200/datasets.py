@@ -159,3 +159,108 @@ def cube_box(p: Particles, pad: float = 0.0):
     hi = np.array([p.x.max(), p.y.max(), p.z.max()], np.float64)
     ext = float((hi - lo).max()) * (1 + pad)
     return (lo[0], lo[0] + ext, lo[1], lo[1] + ext, lo[2], lo[2] + ext)
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# device-side generators for the batched ensemble and the served stream (torch, seeded generator on the device)
+
+def _t_directions(n, gen, device):
+    import torch
+    cos_t = torch.rand(n, generator=gen, device=device, dtype=torch.float64) * 2 - 1
+    phi = torch.rand(n, generator=gen, device=device, dtype=torch.float64) * (2 * np.pi)
+    sin_t = torch.sqrt(1 - cos_t * cos_t)
+    return sin_t * torch.cos(phi), sin_t * torch.sin(phi), cos_t
+
+
+def plummer_device(a, gen, G: float = 1.0, total_mass=None, rmax: float = 50.0, velocities: bool = True):
+    """Plummer bodies with per-body scale radius a (torch float64 tensor on the device; systems are runs of equal
+    a): r = a / sqrt(U^(-2/3) - 1) resampled above rmax a, isotropic directions, Aarseth-Henon-Wielen velocities
+    for a system of mass total_mass (per body, default 1). Returns float64 tensors (x, y, z, vx, vy, vz)."""
+    import torch
+    n, device = a.numel(), a.device
+    M = torch.ones_like(a) if total_mass is None else total_mass
+    r = torch.empty(n, dtype=torch.float64, device=device)
+    todo = torch.arange(n, device=device)
+    while todo.numel():
+        u = torch.rand(todo.numel(), generator=gen, device=device, dtype=torch.float64).clamp_min(1e-300)
+        rr = a[todo] / torch.sqrt(u ** (-2.0 / 3.0) - 1.0)
+        ok = rr <= rmax * a[todo]
+        r[todo[ok]] = rr[ok]
+        todo = todo[~ok]
+    dx, dy, dz = _t_directions(n, gen, device)
+    if not velocities:
+        z = torch.zeros_like(r)
+        return r * dx, r * dy, r * dz, z, z.clone(), z.clone()
+    q = torch.empty(n, dtype=torch.float64, device=device)
+    todo = torch.arange(n, device=device)
+    while todo.numel():
+        xq = torch.rand(todo.numel(), generator=gen, device=device, dtype=torch.float64)
+        yq = torch.rand(todo.numel(), generator=gen, device=device, dtype=torch.float64) * 0.1
+        ok = yq < xq * xq * (1 - xq * xq) ** 3.5
+        q[todo[ok]] = xq[ok]
+        todo = todo[~ok]
+    vesc = torch.sqrt(2 * G * M / a) * (1 + (r / a) ** 2) ** -0.25
+    v = q * vesc
+    ux, uy, uz = _t_directions(n, gen, device)
+    return r * dx, r * dy, r * dz, v * ux, v * uy, v * uz
+
+
+def ensemble_sizes(num_systems: int = 1024, seed: int = 0, lo_log2: float = 10.0, hi_log2: float = 18.0):
+    """system sizes round(2^U[lo, hi]) and Plummer scale radii U[0.5, 2] of the batched ensemble"""
+    rng = np.random.default_rng(seed)
+    sizes = np.rint(2.0 ** rng.uniform(lo_log2, hi_log2, num_systems)).astype(np.int64)
+    radii = rng.uniform(0.5, 2.0, num_systems)
+    return sizes, radii
+
+
+def plummer_ensemble(sizes, radii, seed: int = 0, device="cuda"):
+    """the concatenated bodies of independent Plummer systems (mass 1, softening eps = 0.01 a, h = eps / 2):
+    float32 device tensors x, y, z, m, h, vx, vy, vz"""
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    sizes_t = torch.as_tensor(np.asarray(sizes), device=device)
+    a = torch.repeat_interleave(torch.as_tensor(np.asarray(radii), dtype=torch.float64, device=device), sizes_t)
+    x, y, z, vx, vy, vz = plummer_device(a, gen)
+    m = torch.repeat_interleave(1.0 / sizes_t.double(), sizes_t)
+    h = 0.005 * a
+    return [t.float().contiguous() for t in (x, y, z, m, h, vx, vy, vz)]
+
+
+def served_requests(num_requests: int, seed: int = 0, rate_per_s: float = 24.0, lo_log2: float = 12.0,
+                    hi_log2: float = 22.0):
+    """the served-stream request mix: open-loop Poisson arrivals, N = round(2^U[lo, hi]); 45% Plummer (a = 1,
+    eps = 0.01, AHW velocities), 45% uniform cube [-1, 1]^3 at rest (h = 1e-6), 10% periodic unit box at rest with
+    Ewald (h = 1e-6); K ~ U{1..64} leapfrog steps, dt = 1e-3. Returns descriptions without bodies."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_per_s, num_requests))
+    out = []
+    for k in range(num_requests):
+        u = rng.uniform()
+        kind = "plummer" if u < 0.45 else ("cube" if u < 0.90 else "periodic")
+        out.append(dict(tag=k, n=int(np.rint(2.0 ** rng.uniform(lo_log2, hi_log2))), kind=kind,
+                        steps=int(rng.integers(1, 65)), dt=1e-3, arrival=float(t[k]) - float(t[0]),
+                        seed=int(rng.integers(1 << 31))))
+    return out
+
+
+def request_bodies(req: dict, device="cuda"):
+    """float32 device tensors x, y, z, m, h, vx, vy, vz of one served request"""
+    import torch
+    n = req["n"]
+    gen = torch.Generator(device=device)
+    gen.manual_seed(req["seed"])
+    if req["kind"] == "plummer":
+        x, y, z, vx, vy, vz = plummer_device(torch.ones(n, dtype=torch.float64, device=device), gen)
+        h = torch.full((n,), 0.005, dtype=torch.float64, device=device)
+    else:
+        lo, hi = (-1.0, 1.0) if req["kind"] == "cube" else (0.0, 1.0)
+        x, y, z = (torch.rand(n, generator=gen, device=device, dtype=torch.float64) * (hi - lo) + lo
+                   for _ in range(3))
+        if req["kind"] == "periodic":
+            top = float(np.nextafter(np.float32(hi), np.float32(0)))
+            x, y, z = (v.clamp_max(top) for v in (x, y, z))
+        vx = vy = vz = torch.zeros(n, dtype=torch.float64, device=device)
+        h = torch.full((n,), 1e-6, dtype=torch.float64, device=device)
+    m = torch.full((n,), 1.0 / n, dtype=torch.float64, device=device)
+    return [t.float().contiguous() for t in (x, y, z, m, h, vx, vy, vz)]
