@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--served-requests", type=int, default=48)
     ap.add_argument("--served-rate", type=float, default=24.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--no-accuracy-matched", action="store_true")
+    ap.add_argument("--precision", action="store_true",
+                    help="run the precision study (clustered halos and periodic box at theta 0.3/0.5/0.7) instead")
     return ap.parse_args()
 
 
@@ -513,6 +515,72 @@ def run_accuracy_matched(args, ctx, dev, work, out, pristine, n) -> dict:
     return {"theta": None, "note": "no theta in the list met 5e-4"}
 
 
+def run_precision(args) -> dict:
+    """precision study: 64 Hernquist halos (N = 2^24) against FP64 direct sums on 16384 targets, and a periodic unit
+    box (N = 2^22, Ewald defaults, one replica shell) against the FP64 particle-level Ewald sum on 1024 targets, at
+    theta 0.3, 0.5 and 0.7; reports the 1st-percentile and maximum relative acceleration error and the relative error
+    of the targets' summed potential"""
+    import torch
+    import ryoanji_b200 as ryo
+    from ryoanji_b200 import datasets as ds
+    dev = torch.device("cuda", 0)
+    ctx = ryo.Context(0)
+    out = {}
+
+    def errors(ax, ay, az, pot, tgt, ref, periodic):
+        rp, rx, ry, rz = ref
+        a = torch.stack([ax[tgt], ay[tgt], az[tgt]], 1).double()
+        r = torch.stack([rx, ry, rz], 1)
+        err = (torch.linalg.norm(a - r, dim=1) / torch.linalg.norm(r, dim=1)).cpu().numpy()
+        out = {"err_p99_1st_pct": float(np.percentile(err, 99)), "err_max": float(err.max()),
+               "err_median": float(np.median(err))}
+        pt = pot[tgt].double()
+        if periodic:
+            # periodic potentials are defined up to a constant, and the two Ewald forms place it differently
+            # (the particle-level form includes every body's own image terms): compare after removing the mean
+            off = float((pt - rp).mean())
+            out["potential_offset_rel"] = off / float(rp.abs().mean())
+            out["potential_rms_rel_after_offset"] = float(torch.sqrt(((pt - rp - off) ** 2).mean()) /
+                                                          rp.abs().mean())
+        else:
+            out["potential_rel"] = abs(float(pt.sum()) - float(rp.sum())) / abs(float(rp.sum()))
+        return out
+
+    cases = [("hernquist_halos_2^24", ds.hernquist_halos(1 << 24, num_halos=64, seed=21), None, 16384),
+             ("periodic_box_2^22", ds.periodic_box(1 << 22, seed=22), 1.0, 1024)]
+    for name, p, L, nt in cases:
+        base = [torch.from_numpy(a).to(dev) for a in (p.x, p.y, p.z, p.m, p.h)]
+        n = p.n
+        tgt_idx = None
+        res = {}
+        for theta in (0.3, 0.5, 0.7):
+            work = [b.clone() for b in base]
+            pot, ax, ay, az = (torch.empty(n, device=dev) for _ in range(4))
+            box = ryo.Box(*p.box, boundary=(ryo.BOUNDARY_PERIODIC,) * 3) if L else None
+            params = ryo.SolveParams(theta=theta, box=box, num_shells=1, timing=True)
+            r = ryo.solve(*work, pot, ax, ay, az, params=params, ctx=ctx)
+            if tgt_idx is None:
+                # the sorted order is the same for every theta: pick targets and the FP64 reference once
+                tgt_idx = torch.from_numpy(np.random.default_rng(5).choice(n, nt, replace=False)).to(dev)
+                t0 = time.perf_counter()
+                if L:
+                    ref = ryo.ewald_targets_f64(tgt_idx, *work, L=L, ctx=ctx)
+                else:
+                    ref = ryo.direct_targets_f64(tgt_idx, *work)
+                torch.cuda.synchronize()
+                ref_s = time.perf_counter() - t0
+            e = errors(ax, ay, az, pot, tgt_idx, ref, bool(L))
+            e["solve_ms"] = r.ms["total"]
+            e["p2p_per_body"] = r.sum_p2p / n
+            e["m2p_per_body"] = r.sum_m2p / n
+            res[f"theta_{theta}"] = e
+        res["reference"] = ("FP64 particle-level Ewald sum (replica shells + every source's monopole correction)"
+                            if L else "FP64 direct sum") + f" on {nt} targets, {ref_s:.1f} s"
+        out[name] = res
+    return {"precision_study": out, "dtype": "f32 bulk, FP64 upsweep/Ewald k-space/potential",
+            "data": "synthetic, seeded"}
+
+
 def _measured_hbm(peaks):
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -528,6 +596,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.precision:
+        if rank == 0:
+            print(json.dumps(run_precision(args)), flush=True)
         return
     run_ours(args, rank, world, local_rank)
 

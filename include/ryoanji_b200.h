@@ -248,6 +248,15 @@ extern "C"
                                               size_t numBodies, double G, const double* boxL, int numShells,
                                               double* pot, double* ax, double* ay, double* az, ryo_stream_t stream);
 
+    /* The periodic check (not in the reference): ADDS the FP64 particle-level Ewald correction to pot (G m phi), ax,
+     * ay, az of the chosen targets, i.e. the reference's Ewald formulas (ryoanji/src/ryoanji/nbody/ewald.hpp:200-327)
+     * with every source's monopole in place of the root multipole. After ryo_direct_targets_f64 with numShells =
+     * settings->numReplicaShells over the same cubic box of edge L this gives the targets' periodic sum. */
+    RYO_API ryo_status ryo_ewald_targets_f64(ryo_ctx_t* ctx, const int64_t* targets, size_t numTargets, const float* x,
+                                             const float* y, const float* z, const float* m, size_t numBodies,
+                                             double L, const ryo_ewald_settings* settings, double G, double* pot,
+                                             double* ax, double* ay, double* az, ryo_stream_t stream);
+
     /* ------------------------------------------------------------------------------------------ TreeBuilder
      * ryoanji::TreeBuilder<uint64_t> (ryoanji/src/ryoanji/interface/treebuilder.cuh:34-125) */
 

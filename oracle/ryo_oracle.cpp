@@ -1009,6 +1009,8 @@ extern "C"
                 pos[k][1] = yt[i];
                 pos[k][2] = zt[i];
             }
+            float pos0[kTargets][3];
+            std::memcpy(pos0, pos, sizeof(pos));
             float lo[3] = {pos[0][0], pos[0][1], pos[0][2]}, hi[3] = {lo[0], lo[1], lo[2]};
             for (int k = 1; k < kTargets; ++k)
                 for (int d = 0; d < 3; ++d)
@@ -1030,13 +1032,17 @@ extern "C"
                 for (int iy = -numShells; iy <= numShells; ++iy)
                     for (int ix = -numShells; ix <= numShells; ++ix)
                     {
-                        // the shift is added to and later subtracted from the float centre and positions
+                        // the shift is added to and later subtracted from the float group centre, as in the
+                        // reference (traversal_gpu.cu:484-505), so the MAC decisions are the reference's; the target
+                        // positions are the original ones plus the shift. The reference shifts them back and forth
+                        // too, which leaves rounding residues: a target then meets itself at a distance of about one
+                        // float ulp of the box coordinates and, with a softening below that, gets a spurious force.
                         float sh[3] = {float(ix) * boxL3[0], float(iy) * boxL3[1], float(iz) * boxL3[2]};
                         for (int d = 0; d < 3; ++d)
                         {
                             tc[d] += sh[d];
                             for (int k = 0; k < kTargets; ++k)
-                                pos[k][d] += sh[d];
+                                pos[k][d] = pos0[k][d] + sh[d];
                         }
 
                         // interaction rule of traverseWarp (traversal_gpu.cu:210-237); order does not matter
@@ -1100,11 +1106,7 @@ extern "C"
                         }
 
                         for (int d = 0; d < 3; ++d)
-                        {
                             tc[d] -= sh[d];
-                            for (int k = 0; k < kTargets; ++k)
-                                pos[k][d] -= sh[d];
-                        }
                     }
             m2pCount[g] = nM2P;
             p2pCount[g] = nP2P;

@@ -23,7 +23,7 @@ __all__ = [
     "compute_sfc_keys", "compute_bounding_box", "sequence", "sort_by_key", "compute_octree", "build_octree",
     "compute_fixed_groups", "compute_leaf_source_center", "upsweep_centers", "compute_leaf_multipoles",
     "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch",
-    "BatchSystem", "BatchResult", "Engine",
+    "BatchSystem", "BatchResult", "Engine", "ewald_targets_f64",
     "compute_gravity_ewald", "direct_sum", "direct_targets_f64", "solve", "solve_arrays", "bh_max_target_size",
     "kernel_launches", "measure_peaks",
     "stack_size",
@@ -368,6 +368,20 @@ def direct_targets_f64(targets: torch.Tensor, x, y, z, m, h, G: float = 1.0, box
     _check(lib.ryo_direct_targets_f64(_ptr(targets), C.c_size_t(nt), _ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(h),
                                       C.c_size_t(x.numel()), C.c_double(G), bl, num_shells, *[_ptr(o) for o in out],
                                       _stream(stream)))
+    return out
+
+
+def ewald_targets_f64(targets: torch.Tensor, x, y, z, m, h, L: float, G: float = 1.0,
+                      ewald: "EwaldSettings | None" = None, ctx: Context | None = None, stream=None):
+    """FP64 periodic sum for chosen targets of a cubic box [x0, x0 + L)^3: direct sum over the replica shells plus
+    the particle-level Ewald correction; (pot = G m phi, ax, ay, az) float64 tensors"""
+    ctx = ctx or default_context()
+    e = (ewald or EwaldSettings()).c()
+    out = direct_targets_f64(targets, x, y, z, m, h, G=G, box_l=(L, L, L), num_shells=e.numReplicaShells,
+                             stream=stream)
+    _check(lib.ryo_ewald_targets_f64(ctx.handle, _ptr(targets), C.c_size_t(targets.numel()), _ptr(x), _ptr(y),
+                                     _ptr(z), _ptr(m), C.c_size_t(x.numel()), C.c_double(L), C.byref(e),
+                                     C.c_double(G), *[_ptr(o) for o in out], _stream(stream)), ctx)
     return out
 
 

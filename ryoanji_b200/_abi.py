@@ -165,6 +165,8 @@ SIGNATURES = {
     "ryo_engine_step": (_i, [_p, C.POINTER(EngineStepInfo), _p]),
     "ryo_engine_poll": (_i, [_p, C.POINTER(EngineResult), _i, C.POINTER(C.c_int)]),
     "ryo_engine_status": (_i, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "ryo_ewald_targets_f64": (_i, [_p, _p, _sz] + [_p] * 4 + [_sz, C.c_double, C.POINTER(EwaldSettings), C.c_double]
+                              + [_p] * 5),
     "ryo_solve_batch_f32": (_i, [_p, C.POINTER(SolveParams), C.POINTER(System), _i] + [_p] * 8 + [_sz] + [_p] * 7
                             + [C.POINTER(SolveStats), _p]),
     "ryo_kernel_launches": (C.c_uint64, []),

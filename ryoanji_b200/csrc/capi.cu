@@ -1307,6 +1307,25 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                    });
 }
 
+extern "C" ryo_status ryo_ewald_targets_f64(ryo_ctx_t* ctx, const int64_t* targets, size_t numTargets,
+                                            const float* x, const float* y, const float* z, const float* m,
+                                            size_t numBodies, double L, const ryo_ewald_settings* settings, double G,
+                                            double* pot, double* ax, double* ay, double* az, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(settings && L > 0, "ewald_targets: bad settings or box");
+                       REQUIRE(numTargets == 0 || (targets && x && y && z && m && pot && ax && ay && az),
+                               "ewald_targets: null argument");
+                       launchEwaldTargetsF64(ctx, targets, numTargets, x, y, z, m, numBodies, L,
+                                             settings->numReplicaShells, settings->lCut, settings->hCut,
+                                             settings->alpha_scale, settings->small_R_scale_factor, G, pot, ax, ay, az,
+                                             stream);
+                   });
+}
+
 extern "C" ryo_status ryo_solve_arrays_get(ryo_ctx_t* ctx, ryo_solve_arrays* out)
 {
     if (!ctx || !out) return RYO_ERR_BAD_ARG;

@@ -245,4 +245,208 @@ void launchEwaldGroups(const EwaldHost& h, const uint32_t* groupStart, const uin
     RYO_LAUNCH_CHECK();
 }
 
+// ------------------------------------------------------------------------------------------------ FP64 oracle
+
+/*
+ * Particle-level Ewald sum in FP64 for chosen targets, the check of the periodic solve: the same real-space and
+ * reciprocal-space formulas as the correction above with every source's own monopole in place of the root
+ * multipole. Added to the FP64 direct sum over the (2 numReplicaShells + 1)^3 replica boxes it gives each target's
+ * periodic potential and acceleration without the tree's multipole approximation of the far replicas.
+ */
+struct EwaldParticleParams
+{
+    double L, lCut2, alpha, alpha2, ka, k1, smallR2;
+    int replicaShells, ewaldShells;
+};
+
+constexpr int kEwaldOracleThreads = 256;
+
+__device__ inline double blockSumD(double v, double* sh)
+{
+    v = warpSum(v);
+    if (laneId() == 0) sh[threadIdx.x / kWarp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < kWarp)
+    {
+        t = threadIdx.x < blockDim.x / kWarp ? sh[threadIdx.x] : 0.0;
+        t = warpSum(t);
+    }
+    __syncthreads();
+    return t;
+}
+
+//! real-space images of every source's monopole for one target per block; adds G m_i phi and G a
+__global__ void __launch_bounds__(kEwaldOracleThreads)
+    ewaldRealTargetsKernel(const int64_t* __restrict__ targets, const float* __restrict__ x,
+                           const float* __restrict__ y, const float* __restrict__ z, const float* __restrict__ m,
+                           size_t numBodies, EwaldParticleParams P, double G, double* pot, double* ax, double* ay,
+                           double* az)
+{
+    __shared__ double sh[kEwaldOracleThreads / kWarp];
+    int64_t i      = targets[blockIdx.x];
+    double xi[3]   = {x[i], y[i], z[i]};
+    double acc[4]  = {0, 0, 0, 0};
+    const int S = P.ewaldShells, Rs = P.replicaShells;
+    for (size_t j = threadIdx.x; j < numBodies; j += blockDim.x)
+    {
+        double mj   = m[j];
+        double r[3] = {xi[0] - double(x[j]), xi[1] - double(y[j]), xi[2] - double(z[j])};
+        for (int ix = -S; ix <= S; ++ix)
+            for (int iy = -S; iy <= S; ++iy)
+                for (int iz = -S; iz <= S; ++iz)
+                {
+                    bool pre    = (-Rs <= ix && ix <= Rs) && (-Rs <= iy && iy <= Rs) && (-Rs <= iz && iz <= Rs);
+                    double R[3] = {r[0] + ix * P.L, r[1] + iy * P.L, r[2] + iz * P.L};
+                    double R2   = R[0] * R[0] + (R[1] * R[1] + R[2] * R[2]);
+                    if (R2 > P.lCut2 && !pre) continue;
+                    double g0, g1;
+                    if (R2 < P.smallR2 && P.ka > 0.0)
+                    {
+                        double a2 = R2 * P.alpha2;
+                        g0        = P.ka * (a2 / 3.0 - 1.0);
+                        g1        = P.ka * 2 * P.alpha2 * (a2 / 5.0 - 1.0 / 3.0);
+                    }
+                    else
+                    {
+                        double Rm = sqrt(R2), iR = 1.0 / Rm, iR2 = iR * iR;
+                        double a  = exp(-R2 * P.alpha2) * P.ka * iR2;
+                        double fn = pre ? -erf(P.alpha * Rm) : erfc(P.alpha * Rm);
+                        g0        = fn * iR;
+                        g1        = g0 * iR2 + a;
+                    }
+                    acc[0] -= g0 * mj;
+                    double f = g1 * mj;
+                    acc[1] -= R[0] * f;
+                    acc[2] -= R[1] * f;
+                    acc[3] -= R[2] * f;
+                }
+    }
+    for (int k = 0; k < 4; ++k)
+        acc[k] = blockSumD(acc[k], sh);
+    if (threadIdx.x == 0)
+    {
+        pot[blockIdx.x] += G * double(m[i]) * acc[0];
+        ax[blockIdx.x] += G * acc[1];
+        ay[blockIdx.x] += G * acc[2];
+        az[blockIdx.x] += G * acc[3];
+    }
+}
+
+//! structure factors S(k) = sum_j m_j exp(i k . x_j), one block per wave vector
+__global__ void __launch_bounds__(kEwaldOracleThreads)
+    structureFactorKernel(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                          const float* __restrict__ m, size_t numBodies, const int* __restrict__ hvec,
+                          double twoPiOverL, double* S)
+{
+    __shared__ double sh[kEwaldOracleThreads / kWarp];
+    int hx = hvec[3 * blockIdx.x], hy = hvec[3 * blockIdx.x + 1], hz = hvec[3 * blockIdx.x + 2];
+    double re = 0.0, im = 0.0;
+    for (size_t j = threadIdx.x; j < numBodies; j += blockDim.x)
+    {
+        double ph = twoPiOverL * (hx * double(x[j]) + hy * double(y[j]) + hz * double(z[j]));
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        re += double(m[j]) * cs;
+        im += double(m[j]) * sn;
+    }
+    re = blockSumD(re, sh);
+    im = blockSumD(im, sh);
+    if (threadIdx.x == 0)
+    {
+        S[2 * blockIdx.x]     = re;
+        S[2 * blockIdx.x + 1] = im;
+    }
+}
+
+//! reciprocal-space sum and the neutralising constant for each target
+__global__ void ewaldKspaceTargetsKernel(const int64_t* __restrict__ targets, size_t numTargets,
+                                         const float* __restrict__ x, const float* __restrict__ y,
+                                         const float* __restrict__ z, const float* __restrict__ m,
+                                         const int* __restrict__ hvec, const double* __restrict__ g0,
+                                         const double* __restrict__ S, int numK, double twoPiOverL, double k1M,
+                                         double G, double* pot, double* ax, double* ay, double* az)
+{
+    size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= numTargets) return;
+    int64_t i = targets[t];
+    double xi[3] = {x[i], y[i], z[i]};
+    double phi = k1M, a[3] = {0, 0, 0};
+    for (int q = 0; q < numK; ++q)
+    {
+        int h[3]  = {hvec[3 * q], hvec[3 * q + 1], hvec[3 * q + 2]};
+        double ph = twoPiOverL * (h[0] * xi[0] + h[1] * xi[1] + h[2] * xi[2]);
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        double c = cs * S[2 * q] + sn * S[2 * q + 1]; // sum_j m_j cos(k.(x_i - x_j))
+        double s = sn * S[2 * q] - cs * S[2 * q + 1]; // sum_j m_j sin(k.(x_i - x_j))
+        phi += g0[q] * c;
+        for (int d = 0; d < 3; ++d)
+            a[d] -= g0[q] * s * (twoPiOverL * h[d]);
+    }
+    pot[t] += G * double(m[i]) * phi;
+    ax[t] += G * a[0];
+    ay[t] += G * a[1];
+    az[t] += G * a[2];
+}
+
+void launchEwaldTargetsF64(ryo_ctx* ctx, const int64_t* targets, size_t numTargets, const float* x, const float* y,
+                           const float* z, const float* m, size_t numBodies, double L, int replicaShells, double lCut,
+                           double hCut, double alphaScale, double smallR, double G, double* pot, double* ax,
+                           double* ay, double* az, cudaStream_t s)
+{
+    if (numTargets == 0 || numBodies == 0) return;
+    EwaldParticleParams P{};
+    double alpha    = alphaScale / L;
+    P.L             = L;
+    P.lCut2         = lCut * lCut * L * L;
+    P.alpha         = alpha;
+    P.alpha2        = alpha * alpha;
+    P.ka            = 2.0 * alpha / std::sqrt(M_PI);
+    P.k1            = M_PI / (alpha * alpha * L * L * L);
+    P.smallR2       = smallR * L * L;
+    P.replicaShells = replicaShells;
+    P.ewaldShells   = std::max(int(std::ceil(lCut)), replicaShells);
+    ewaldRealTargetsKernel<<<unsigned(numTargets), kEwaldOracleThreads, 0, s>>>(targets, x, y, z, m, numBodies, P, G,
+                                                                               pot, ax, ay, az);
+    RYO_LAUNCH_CHECK();
+    // wave vectors and their coefficients as in ewaldSetup, for a unit monopole
+    std::vector<int> hv;
+    std::vector<double> g0;
+    int hReps = int(std::ceil(hCut));
+    double k4 = M_PI * M_PI / (alpha * alpha * L * L);
+    for (int hx = -hReps; hx <= hReps; ++hx)
+        for (int hy = -hReps; hy <= hReps; ++hy)
+            for (int hz = -hReps; hz <= hReps; ++hz)
+            {
+                double h2 = double(hx) * hx + (double(hy) * hy + double(hz) * hz);
+                if (h2 == 0 || h2 > hCut * hCut) continue;
+                hv.insert(hv.end(), {hx, hy, hz});
+                g0.push_back(std::exp(-k4 * h2) / (M_PI * h2 * L));
+            }
+    int numK = int(g0.size());
+    // total mass for the neutralising constant
+    std::vector<float> hm(numBodies);
+    RYO_CUDA(cudaMemcpyAsync(hm.data(), m, numBodies * sizeof(float), cudaMemcpyDeviceToHost, s));
+    int* dh    = ctx->scratch<int>("ew.hvec", std::max<size_t>(3 * size_t(numK), 1), s);
+    double* dg = ctx->scratch<double>("ew.g0", std::max(numK, 1), s);
+    double* dS = ctx->scratch<double>("ew.S", std::max<size_t>(2 * size_t(numK), 1), s);
+    if (numK > 0)
+    {
+        RYO_CUDA(cudaMemcpyAsync(dh, hv.data(), sizeof(int) * hv.size(), cudaMemcpyHostToDevice, s));
+        RYO_CUDA(cudaMemcpyAsync(dg, g0.data(), sizeof(double) * g0.size(), cudaMemcpyHostToDevice, s));
+        structureFactorKernel<<<unsigned(numK), kEwaldOracleThreads, 0, s>>>(x, y, z, m, numBodies, dh,
+                                                                            2 * M_PI / L, dS);
+        RYO_LAUNCH_CHECK();
+    }
+    RYO_CUDA(cudaStreamSynchronize(s));
+    double M = 0;
+    for (float v : hm)
+        M += v;
+    ewaldKspaceTargetsKernel<<<ceilDiv(numTargets, 128), 128, 0, s>>>(targets, numTargets, x, y, z, m, dh, dg, dS,
+                                                                       numK, 2 * M_PI / L, P.k1 * M, G, pot, ax, ay,
+                                                                       az);
+    RYO_LAUNCH_CHECK();
+}
+
 } // namespace ryo

@@ -252,6 +252,11 @@ struct EwaldHost
 };
 EwaldHost ewaldSetup(const double* mroot, const double* center, int replicaShells, double L, double lCut,
                      double hCut, double alphaScale, double smallR);
+//! adds the FP64 particle-level Ewald correction (every source's monopole) to pot (G m phi), ax, ay, az of targets
+void launchEwaldTargetsF64(ryo_ctx* ctx, const int64_t* targets, size_t numTargets, const float* x, const float* y,
+                           const float* z, const float* m, size_t numBodies, double L, int replicaShells, double lCut,
+                           double hCut, double alphaScale, double smallR, double G, double* pot, double* ax,
+                           double* ay, double* az, cudaStream_t s);
 void launchEwaldGroups(const EwaldHost& e, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
                        const float* x, const float* y, const float* z, const float* m, float G, float* ugrav,
                        float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s);

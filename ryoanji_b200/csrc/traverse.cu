@@ -532,15 +532,24 @@ __global__ void __launch_bounds__(kTravThreads, 5)
             for (int iy = -shells; iy <= shells && !overflow; ++iy)
                 for (int ix = -shells; ix <= shells && !overflow; ++ix)
                 {
-                    // the replica shift is added to and later subtracted from centre and targets (as in the reference)
+                    // the replica shift is added to and later subtracted from the group centre, as in the
+                    // reference (traversal_gpu.cu:484-505), so the MAC decisions are the reference's. The targets
+                    // are the original positions plus the shift: shifting them back and forth as the reference
+                    // does leaves rounding residues, and a target then meets itself at about one float ulp of the
+                    // box coordinates, which a softening below that turns into a large spurious force.
                     float sh[3] = {__fmul_rn(float(ix), boxL[0]), __fmul_rn(float(iy), boxL[1]),
                                    __fmul_rn(float(iz), boxL[2])};
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
                         tc[d] = __fadd_rn(tc[d], sh[d]);
-                    T.tx = add2(T.tx, pk(sh[0], sh[0]));
-                    T.ty = add2(T.ty, pk(sh[1], sh[1]));
-                    T.tz = add2(T.tz, pk(sh[2], sh[2]));
+                    if (shells > 0)
+                    {
+                        float4 u0 = tgt.vec(min(b + lane, e - 1));
+                        float4 u1 = tgt.vec(min(b + kWarp + lane, e - 1));
+                        T.tx      = add2(pk(u0.x, u1.x), pk(sh[0], sh[0]));
+                        T.ty      = add2(pk(u0.y, u1.y), pk(sh[1], sh[1]));
+                        T.tz      = add2(pk(u0.z, u1.z), pk(sh[2], sh[2]));
+                    }
 
                     int sp = 1, nM = 0, nL = 0;
                     if (lane == 0) stack[0] = rootEntry;
@@ -608,9 +617,6 @@ __global__ void __launch_bounds__(kTravThreads, 5)
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
                         tc[d] = __fsub_rn(tc[d], sh[d]);
-                    T.tx = sub2(T.tx, pk(sh[0], sh[0]));
-                    T.ty = sub2(T.ty, pk(sh[1], sh[1]));
-                    T.tz = sub2(T.tz, pk(sh[2], sh[2]));
                 }
 
         if (overflow)
