@@ -300,10 +300,10 @@ def run_ours(args, rank, world, local_rank):
 
     if world == 1 and not args.no_accuracy_matched and args.accuracy_targets > 0:
         line["accuracy_matched"] = run_accuracy_matched(args, ctx, dev, work, out, pristine, n)
-    if world == 1 and not args.no_ensemble:
-        line["ensemble"] = run_ensemble(args, ctx, dev)
-    if world == 1 and not args.no_served:
-        line["served"] = run_served(args, ctx, dev)
+    if not args.no_ensemble:
+        line["ensemble"] = run_ensemble(args, ctx, dev, rank, world, max_over_ranks)
+    if not args.no_served:
+        line["served"] = run_served(args, ctx, dev, rank, world, dist)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, dt, sec = cpu_reference_solve(args.cpu_log2n, args.theta, seed=3)
@@ -326,15 +326,24 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def run_ensemble(args, ctx, dev) -> dict:
+def run_ensemble(args, ctx, dev, rank=0, world=1, max_over_ranks=lambda v: v) -> dict:
     """batched ensemble: independent Plummer systems (N = round(2^U[10, 18]), a ~ U[0.5, 2], eps = 0.01 a) solved in
-    one launch per phase with autotuned bucket/group/stack, against a loop of the single-system solve"""
+    one launch per phase with autotuned bucket/group/stack, against a loop of the single-system solve. With several
+    ranks each solves its LPT share of the systems; times are the maximum over ranks."""
     import torch
     import ryoanji_b200 as ryo
     from ryoanji_b200 import autotune
     from ryoanji_b200 import datasets as ds
-    sizes, radii = ds.ensemble_sizes(args.ensemble_systems, seed=5)
-    bodies = ds.plummer_ensemble(sizes, radii, seed=5, device=dev)
+    from ryoanji_b200.shard import lpt_partition, solve_cost
+    all_sizes, all_radii = ds.ensemble_sizes(args.ensemble_systems, seed=5)
+    total_systems, total_bodies = len(all_sizes), int(all_sizes.sum())
+    all_bodies = ds.plummer_ensemble(all_sizes, all_radii, seed=5, device=dev)
+    mine = lpt_partition([solve_cost(int(k)) for k in all_sizes], world)[rank]
+    offs_all = np.concatenate([[0], np.cumsum(all_sizes)])
+    idx = torch.cat([torch.arange(int(offs_all[i]), int(offs_all[i + 1]), device=dev) for i in mine])
+    bodies = [b[idx].contiguous() for b in all_bodies]
+    del all_bodies
+    sizes = all_sizes[mine]
     n = int(sizes.sum())
     systems = [ryo.BatchSystem(int(k)) for k in sizes]
     base = ryo.SolveParams(theta=0.5)
@@ -359,7 +368,7 @@ def run_ensemble(args, ctx, dev) -> dict:
         e1.record()
         e1.synchronize()
         ms += e0.elapsed_time(e1)
-    batched_ms = ms / steps
+    batched_ms = max_over_ranks(ms / steps)
 
     # the plain path: one single-system solve per system, same parameters
     offs = np.concatenate([[0], np.cumsum(sizes)])
@@ -377,10 +386,11 @@ def run_ensemble(args, ctx, dev) -> dict:
     plain_loop()
     e1.record()
     e1.synchronize()
-    plain_ms = e0.elapsed_time(e1)
-    ns = len(sizes)
+    plain_ms = max_over_ranks(e0.elapsed_time(e1))
+    ns, n = total_systems, total_bodies
     return {"workload": f"{ns} Plummer systems, N=round(2^U[10,18]) ({n} bodies), a~U[0.5,2], eps=0.01a, theta 0.5, "
-                        "quadrupole; one solve of every system per step",
+                        "quadrupole; one solve of every system per step"
+                        + (f"; LPT shares over {world} GPUs, times = max over ranks" if world > 1 else ""),
             "autotuned": {"bucket": tuned.bucket_size, "group": tuned.group_size, "stack": tuned.stack_capacity,
                           "candidates_ms": [list(t) for t in table]},
             "batched": {"ms_per_step": batched_ms, "solves_per_s": ns / (batched_ms * 1e-3),
@@ -390,7 +400,7 @@ def run_ensemble(args, ctx, dev) -> dict:
             "speedup_solves_per_s": plain_ms / batched_ms}
 
 
-def run_served(args, ctx, dev) -> dict:
+def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
     """served stream: open-loop Poisson arrivals of solve requests (N = round(2^U[12, 22]); 45% Plummer, 45% cube,
     10% periodic with Ewald; K ~ U{1..64} leapfrog steps, dt = 1e-3) through the engine, against the plain path
     taking the same requests one at a time in arrival order. Inputs come from pinned host memory and every request's
@@ -398,18 +408,34 @@ def run_served(args, ctx, dev) -> dict:
     import torch
     import ryoanji_b200 as ryo
     from ryoanji_b200 import datasets as ds
-    reqs = ds.served_requests(args.served_requests, seed=11, rate_per_s=args.served_rate)
+    from ryoanji_b200.shard import route_requests
+    all_reqs = ds.served_requests(args.served_requests, seed=11, rate_per_s=args.served_rate)
+    route = route_requests(all_reqs, world)
+    reqs = [q for q, r in zip(all_reqs, route) if r == rank]
     host = {}
     for q in reqs:
         host[q["tag"]] = [t.cpu().pin_memory() for t in ds.request_bodies(q, device=dev)]
     torch.cuda.synchronize()
     params = ryo.SolveParams(theta=0.5)
     periodic = ryo.Box(0.0, 1.0, 0.0, 1.0, 0.0, 1.0, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
-    arrival = {q["tag"]: q["arrival"] for q in reqs}
-    solves = sum(q["steps"] + 1 for q in reqs)
-    body_solves = sum(q["n"] * (q["steps"] + 1) for q in reqs)
+    arrival = {q["tag"]: q["arrival"] for q in all_reqs}
+    solves = sum(q["steps"] + 1 for q in all_reqs)
+    body_solves = sum(q["n"] * (q["steps"] + 1) for q in all_reqs)
+
+    def gather(done):
+        # latencies of every rank's requests; the makespan is the latest completion on any rank
+        if dist is None:
+            return done
+        parts = [None] * world
+        dist.all_gather_object(parts, done)
+        merged = {}
+        for p in parts:
+            merged.update(p)
+        return merged
 
     def summary(done, t_end):
+        done = gather(done)
+        t_end = max(done.values())
         lat = np.array([done[k] - arrival[k] for k in arrival])
         return {"makespan_s": t_end, "solves_per_s": solves / t_end, "mparticles_per_s": body_solves / t_end / 1e6,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
@@ -421,6 +447,8 @@ def run_served(args, ctx, dev) -> dict:
     done = {}
     i = 0
     steps = 0
+    if dist is not None:
+        dist.barrier()
     t0 = time.perf_counter()
     while len(done) < len(reqs):
         now = time.perf_counter() - t0
@@ -439,15 +467,17 @@ def run_served(args, ctx, dev) -> dict:
         for d in eng.poll():
             done[d["tag"]] = time.perf_counter() - t0
             outs[d["tag"]] = d
-    served = summary(done, max(done.values()))
+    served = summary(done, max(done.values(), default=0.0))
     served["engine_steps"] = steps
     drift = [abs(d["kinetic"] + d["potential"] - d["initial"]) / abs(d["initial"]) for d in outs.values()
              if d["initial"] != 0]
-    served["energy_drift_median"] = float(np.median(drift))
+    served["energy_drift_median"] = float(np.median(drift)) if drift else None
     eng.close()
 
     # plain: one request at a time, single-system solve and leapfrog on the device
     done = {}
+    if dist is not None:
+        dist.barrier()
     t0 = time.perf_counter()
     for q in reqs:
         wait = q["arrival"] - (time.perf_counter() - t0)
@@ -472,10 +502,11 @@ def run_served(args, ctx, dev) -> dict:
         result = torch.stack([x, y, z, vx, vy, vz, ax, ay, az, p]).cpu()
         done[q["tag"]] = time.perf_counter() - t0
         del result
-    plain = summary(done, max(done.values()))
-    return {"workload": f"{len(reqs)} requests, Poisson arrivals at {args.served_rate}/s, N=round(2^U[12,22]), "
+    plain = summary(done, max(done.values(), default=0.0))
+    return {"workload": f"{len(all_reqs)} requests, Poisson arrivals at {args.served_rate}/s, N=round(2^U[12,22]), "
                         "45% Plummer / 45% cube / 10% periodic+Ewald, K~U{1..64} KDK steps, dt=1e-3, theta 0.5, "
-                        "120 GB admission budget",
+                        "120 GB admission budget"
+                        + (f"; requests routed over {world} GPUs by estimated backlog" if world > 1 else ""),
             "solves": solves, "body_solves": body_solves, "served": served, "plain": plain,
             "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"],
             "h2d": "pinned host inputs copied per request", "d2h": "final state of every request copied back"}
