@@ -19,7 +19,9 @@
  *     staged sources are stored pre-duplicated (s, s) so every source operand is a ready register pair: one
  *     instruction issues the work of two targets and the freed issue slots carry the rsqrt, shared-memory and
  *     traversal instructions (the kernel is issue-bound with scalar FP32);
- *   - each batch accumulates into fresh registers and is added to the per-target sums with Kahan compensation;
+ *   - a batch accumulates even and odd sources into two sets of fresh registers (two independent dependency
+ *     chains per lane), and their sum is added to the per-target running sums with Kahan compensation; the running
+ *     sums and compensations live in shared memory, which keeps the kernel at 96 registers (five blocks per SM);
  *   - the MAC test uses explicitly rounded single operations so that every decision is reproducible bit for bit.
  */
 #include "internal.hpp"
@@ -42,6 +44,8 @@ struct WarpSmem
     int leafScan[kLeafCap + kWarp];
     // staged sources, every value duplicated: M2P 5 x 16 bytes per cell, P2P 2 x 16 + 8 bytes per body
     float4 stage[5 * kWarp];
+    // per lane: Kahan running sums [0] and compensations [1] of (-phi, ax, ay, az), both targets packed
+    unsigned long long sums[2][4][kWarp];
 };
 
 // ------------------------------------------------------------------------------------------------ packed f32x2
@@ -174,8 +178,6 @@ __device__ __forceinline__ void p2p2(Acc2& A, f2 tx, f2 ty, f2 tz, f2 th, f2 sx,
 struct TargetState
 {
     f2 tx, ty, tz, th; // the lane's two targets (shifted by the current replica)
-    Acc2 acc;          // -phi, a
-    Acc2 comp;         // Kahan compensation of acc
     float h0;          // the common smoothing length of the group's targets, if uniformH
     bool uniformH;
 };
@@ -265,12 +267,28 @@ struct SoABodies
     __device__ __forceinline__ float scalar(int i) const { return __ldg(s + i); }
 };
 
-__device__ __forceinline__ void addBatch(TargetState& T, const Acc2& part)
+__device__ __forceinline__ Acc2 sum2(const Acc2& a, const Acc2& b)
 {
-    kahan2(T.acc.p, T.comp.p, part.p);
-    kahan2(T.acc.x, T.comp.x, part.x);
-    kahan2(T.acc.y, T.comp.y, part.y);
-    kahan2(T.acc.z, T.comp.z, part.z);
+    Acc2 r;
+    r.p = add2(a.p, b.p);
+    r.x = add2(a.x, b.x);
+    r.y = add2(a.y, b.y);
+    r.z = add2(a.z, b.z);
+    return r;
+}
+//! add one batch's partial sums to the lane's Kahan-compensated running sums in shared memory
+__device__ __forceinline__ void addBatchS(WarpSmem& S, const Acc2& part)
+{
+    int lane = laneId();
+    f2 v[4] = {part.p, part.x, part.y, part.z};
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+        f2 sum = S.sums[0][c][lane], comp = S.sums[1][c][lane];
+        kahan2(sum, comp, v[c]);
+        S.sums[0][c][lane] = sum;
+        S.sums[1][c][lane] = comp;
+    }
 }
 
 //! evaluate the first @p count (<= 32) pending cells
@@ -291,24 +309,32 @@ __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState&
     }
     __syncwarp();
     const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
-    Acc2 part            = zero2();
-    auto one = [&](int j)
+    Acc2 pa = zero2(), pb = zero2();
+    auto one = [&](Acc2& part, int j)
     {
         ulonglong2 a = st[5 * j], b = st[5 * j + 1], c = st[5 * j + 2], d = st[5 * j + 3], e = st[5 * j + 4];
         m2p2(part, T.tx, T.ty, T.tz, a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y);
     };
     if (count == kWarp)
     {
-#pragma unroll 4
-        for (int j = 0; j < kWarp; ++j)
-            one(j);
+#pragma unroll 2
+        for (int j = 0; j < kWarp; j += 2)
+        {
+            one(pa, j);
+            one(pb, j + 1);
+        }
     }
     else
     {
-        for (int j = 0; j < count; ++j)
-            one(j);
+        int j = 0;
+        for (; j + 1 < count; j += 2)
+        {
+            one(pa, j);
+            one(pb, j + 1);
+        }
+        if (j < count) one(pa, j);
     }
-    addBatch(T, part);
+    addBatchS(S, sum2(pa, pb));
     __syncwarp();
 }
 
@@ -366,23 +392,32 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
             {
                 float hij = __fadd_rn(T.h0, hj0);
                 float hh  = __fmul_rn(hij, hij);
-                auto oneU = [&](int j)
+                Acc2 pb   = zero2();
+                auto oneU = [&](Acc2& pp, int j)
                 {
                     ulonglong2 a = st[2 * j], c = st[2 * j + 1];
-                    p2p2u(part, T.tx, T.ty, T.tz, hh, a.x, a.y, c.x, c.y);
+                    p2p2u(pp, T.tx, T.ty, T.tz, hh, a.x, a.y, c.x, c.y);
                 };
                 if (nvalid == kWarp)
                 {
-#pragma unroll 8
-                    for (int j = 0; j < kWarp; ++j)
-                        oneU(j);
+#pragma unroll 4
+                    for (int j = 0; j < kWarp; j += 2)
+                    {
+                        oneU(part, j);
+                        oneU(pb, j + 1);
+                    }
                 }
                 else
                 {
-                    for (int j = 0; j < nvalid; ++j)
-                        oneU(j);
+                    int j = 0;
+                    for (; j + 1 < nvalid; j += 2)
+                    {
+                        oneU(part, j);
+                        oneU(pb, j + 1);
+                    }
+                    if (j < nvalid) oneU(part, j);
                 }
-                addBatch(T, part);
+                addBatchS(S, sum2(part, pb));
                 __syncwarp();
                 continue;
             }
@@ -403,7 +438,7 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
             for (int j = 0; j < nvalid; ++j)
                 one(j);
         }
-        addBatch(T, part);
+        addBatchS(S, part);
         __syncwarp();
     }
     if (all) return 0;
@@ -496,8 +531,9 @@ __global__ void __launch_bounds__(kTravThreads, 5)
         T.th      = pk(t0.w, t1.w);
         T.h0       = __shfl_sync(0xffffffffu, t0.w, 0);
         T.uniformH = __all_sync(0xffffffffu, t0.w == T.h0 && t1.w == T.h0);
-        T.acc     = zero2();
-        T.comp    = zero2();
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            S.sums[0][c][lane] = S.sums[1][c][lane] = 0ull;
         float lo[3] = {fminf(t0.x, t1.x), fminf(t0.y, t1.y), fminf(t0.z, t1.z)};
         float hi[3] = {fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y), fmaxf(t0.z, t1.z)};
         float tc[3], ts[3];
@@ -633,10 +669,10 @@ __global__ void __launch_bounds__(kTravThreads, 5)
 
         // Kahan: the compensated sum is acc - comp; acc.p holds -phi
         float phi[2], gx[2], gy[2], gz[2];
-        upk(sub2(T.comp.p, T.acc.p), phi[0], phi[1]);
-        upk(sub2(T.acc.x, T.comp.x), gx[0], gx[1]);
-        upk(sub2(T.acc.y, T.comp.y), gy[0], gy[1]);
-        upk(sub2(T.acc.z, T.comp.z), gz[0], gz[1]);
+        upk(sub2(S.sums[1][0][lane], S.sums[0][0][lane]), phi[0], phi[1]);
+        upk(sub2(S.sums[0][1][lane], S.sums[1][1][lane]), gx[0], gx[1]);
+        upk(sub2(S.sums[0][2][lane], S.sums[1][2][lane]), gy[0], gy[1]);
+        upk(sub2(S.sums[0][3][lane], S.sums[1][3][lane]), gz[0], gz[1]);
         double pot = 0.0;
 #pragma unroll
         for (int k = 0; k < 2; ++k)
