@@ -148,6 +148,20 @@ extern "C"
     RYO_API ryo_status ryo_compute_fixed_groups(uint32_t first, uint32_t last, unsigned groupSize, uint32_t* groups,
                                                 ryo_stream_t stream);
 
+    /* cstone::computeGroupSplits (cstone/include/cstone/traversal/groups_gpu.cu:60-151, groups_gpu.cuh:39-265):
+     * spatially compact target groups of at most groupSize (32 or 64) SFC-sorted bodies [first, last): fixed windows
+     * split where consecutive bodies are farther apart than min(tolFactor * cbrt(smallest leaf volume), 2 h) and, when
+     * a window is longer than extentRatio * tolFactor * its smallest leaf edge, into equal chunks. h may be NULL.
+     * leaves/layout: the cornerstone leaf array and body layout of the same tree; box: the key box. extentRatio < 0
+     * selects the reference default (8, or the environment variable CSTONE_GROUP_EXTENT_SPLIT). *numGroups (host)
+     * always receives the count; groups[0:*numGroups + 1] are written if capacity allows (else RYO_ERR_CAPACITY). */
+    RYO_API ryo_status ryo_compute_group_splits_f32(ryo_ctx_t* ctx, uint32_t first, uint32_t last, const float* x,
+                                                    const float* y, const float* z, const float* h,
+                                                    const uint64_t* leaves, int numLeaves, const uint32_t* layout,
+                                                    const ryo_box_f32* box, unsigned groupSize, float tolFactor,
+                                                    float extentRatio, uint32_t* groups, uint32_t capacity,
+                                                    uint32_t* numGroups, ryo_stream_t stream);
+
     /* ------------------------------------------------------------------------------------------ upsweep
      * The individual steps of the reference's upward pass. Sums run in double precision on the device; stored
      * values are float. centers: 4 floats per node, multipoles: 8 floats per node. */
@@ -304,6 +318,10 @@ extern "C"
         ryo_ewald_settings ewald;    /* Ewald settings when periodic */
         int stackCapacity;           /* 0 = default */
         int timing;                  /* 1: record per-phase device times into ryo_solve_stats.ms */
+        float groupTolerance;        /* > 0: spatial target groups (ryo_compute_group_splits_f32) with this
+                                        tolFactor, groupSize 32 or 64; 0: fixed groups, the reference demo's (0).
+                                        The batched solve and the engine always use fixed groups. */
+        float groupExtentRatio;      /* window-extent ratio of the spatial groups; < 0: the reference default (-1) */
     } ryo_solve_params;
 
     typedef struct ryo_solve_stats

@@ -213,6 +213,38 @@ class Oracle:
                                                  C.c_double(alpha_scale), C.c_double(small_r))
         return u, pot, ax, ay, az
 
+    # ---- spatial target groups (restatement only: the reference's version is device code)
+    def find_splits(self, pos4, dist_crit_sq):
+        """split bits of one window of targets (rows x, y, z, w)"""
+        assert not self.reference
+        pos = np.ascontiguousarray(pos4, np.float64)
+        return int(self._f("find_splits_f64", C.c_uint64)(_ptr(pos), C.c_int(len(pos)), C.c_double(dist_crit_sq)))
+
+    def make_splits(self, mask, group_size=64):
+        assert not self.reference
+        out = np.zeros(group_size + 1, np.uint32)
+        k = self._f("make_splits", C.c_int)(C.c_uint64(mask), C.c_int(group_size), _ptr(out))
+        return out[:k]
+
+    def group_splits(self, first, last, x, y, z, h, leaves, layout, box6, group_size=64, tol_factor=2.0,
+                     extent_ratio=8.0):
+        """(groups[numGroups + 1], counts per fixed window)"""
+        assert not self.reference
+        dt = x.dtype
+        name = "group_splits_f32" if dt == np.float32 else "group_splits_f64"
+        nl = len(leaves) - 1
+        nw = (last - first + group_size - 1) // group_size
+        counts = np.zeros(max(nw, 1), np.uint32)
+        cap = last - first + 2
+        groups = np.zeros(cap, np.uint32)
+        hp = _ptr(np.ascontiguousarray(h, dt)) if h is not None else None
+        ng = self._f(name, C.c_long)(C.c_uint32(first), C.c_uint32(last), _ptr(x), _ptr(y), _ptr(z), hp,
+                                     _ptr(np.ascontiguousarray(leaves, np.uint64)), C.c_int(nl),
+                                     _ptr(np.ascontiguousarray(layout, np.uint32)), _ptr(np.asarray(box6, dt)),
+                                     C.c_int(group_size), C.c_float(tol_factor), C.c_float(extent_ratio),
+                                     _ptr(counts), _ptr(groups), C.c_long(cap))
+        return groups[:ng + 1].copy(), counts[:nw].copy()
+
     def ewald_single_particle_energy(self, m, N, L, G=1.0, alpha_scale=2.0):
         return self._f("ewald_single_particle_energy", C.c_double)(C.c_double(m), C.c_uint(N), C.c_double(L),
                                                                     C.c_double(G), C.c_double(alpha_scale))

@@ -733,6 +733,125 @@ void ewaldTarget(const double pos[3], const EwaldParams& p, double acc[4])
 
 // ==================================================================================================== C ABI
 
+// ------------------------------------------------------------------------------------------------ target groups
+
+/*! split bits of one window of G consecutive targets (findSplits, cstone/traversal/groups_gpu.cuh:39-73): bit i is
+ *  set when the squared distance from target i to target i + 1 exceeds min(distCritSq, w_i^2); the last target of
+ *  the window has no successor */
+template<class T>
+uint64_t findSplitsWindow(const T* pos4, int G, T distCritSq)
+{
+    uint64_t mask = 0;
+    for (int i = 0; i + 1 < G; ++i)
+    {
+        const T* a = pos4 + 4 * i;
+        const T* b = pos4 + 4 * (i + 1);
+        T dx = b[0] - a[0], dy = b[1] - a[1], dz = b[2] - a[2];
+        T d2 = norm2(dx, dy, dz);
+        if (d2 > std::min(distCritSq, a[3] * a[3])) mask |= uint64_t(1) << i;
+    }
+    return mask;
+}
+
+/*! groupSplitsKernel (cstone/traversal/groups_gpu.cuh:148-265) for window w of G targets starting at first + w G:
+ *  returns its split bits. Coordinates are in units of the longest box edge, leaf sizes in the unit box of the same
+ *  aspect ratio; windows whose extent along an axis exceeds extentRatio * tolFactor * smallest leaf edge are also cut
+ *  into equal power-of-two chunks. */
+template<class Tc, class T>
+uint64_t groupSplitsWindow(uint32_t first, uint32_t last, const Tc* x, const Tc* y, const Tc* z, const T* h,
+                           const uint64_t* leaves, int numLeaves, const uint32_t* layout, const Tc* box6, int G,
+                           float tolFactor, float extentRatio, uint32_t w)
+{
+    BoxT<Tc> box = makeBox(box6);
+    unsigned bits[3] = {box.bits[0], box.bits[1], box.bits[2]};
+    T unit6[6]       = {0, T(1) / T(1u << (kMaxLevel - bits[0])), 0, T(1) / T(1u << (kMaxLevel - bits[1])), 0,
+                        T(1) / T(1u << (kMaxLevel - bits[2]))};
+    BoxT<T> unitBox  = makeBox(unit6);
+    std::vector<uint32_t> body(G);
+    T nodeVolume = 1, leafEdge[3] = {1, 1, 1};
+    for (int i = 0; i < G; ++i)
+    {
+        body[i]  = std::min<uint32_t>(first + w * uint32_t(G) + uint32_t(i), last - 1);
+        int leaf = int(std::upper_bound(layout, layout + numLeaves, body[i]) - layout) - 1;
+        uint64_t k0 = leaves[leaf], k1 = leaves[leaf + 1];
+        auto ib     = nodeIBox(k0, rangeLevel(k1 - k0), unitBox.bits);
+        T c[3], sz[3];
+        geoCenterSize(ib, unitBox, c, sz);
+        T vol      = 8 * sz[0] * sz[1] * sz[2];
+        nodeVolume = vol > 0 ? std::min(vol, nodeVolume) : nodeVolume;
+        for (int d = 0; d < 3; ++d)
+            leafEdge[d] = std::min(leafEdge[d], T(2) * sz[d]);
+    }
+    Tc distCrit     = Tc(std::cbrt(nodeVolume) * tolFactor);
+    Tc maxExtent    = std::max(std::max(box.len[0], box.len[1]), box.len[2]);
+    Tc invMaxExtent = Tc(1) / maxExtent;
+    std::vector<Tc> pos(4 * size_t(G));
+    for (int i = 0; i < G; ++i)
+    {
+        uint32_t j     = body[i];
+        pos[4 * i]     = x[j] * invMaxExtent;
+        pos[4 * i + 1] = y[j] * invMaxExtent;
+        pos[4 * i + 2] = z[j] * invMaxExtent;
+        pos[4 * i + 3] = h ? Tc(2) * Tc(h[j]) * invMaxExtent : Tc(1);
+    }
+    uint64_t mask = findSplitsWindow<Tc>(pos.data(), G, distCrit * distCrit);
+
+    Tc lo[3] = {pos[0], pos[1], pos[2]}, hi[3] = {lo[0], lo[1], lo[2]};
+    for (int i = 0; i < G; ++i)
+        for (int d = 0; d < 3; ++d)
+        {
+            lo[d] = std::min(lo[d], pos[4 * i + d]);
+            hi[d] = std::max(hi[d], pos[4 * i + d]);
+        }
+    Tc ratio = 0;
+    for (int d = 0; d < 3; ++d)
+    {
+        Tc allowed = Tc(tolFactor) * Tc(leafEdge[d]);
+        Tc extent  = hi[d] - lo[d];
+        if (allowed > 0) ratio = std::max(ratio, extent / allowed);
+    }
+    if (extentRatio > 0 && ratio > Tc(extentRatio))
+    {
+        unsigned chunk = unsigned(G);
+        while (chunk > 1 && Tc(chunk) * ratio > Tc(G) * Tc(extentRatio))
+            chunk /= 2;
+        uint32_t inWindow = std::min<uint32_t>(uint32_t(G), last - (first + w * uint32_t(G)));
+        for (int i = 0; i < G; ++i)
+        {
+            uint32_t next = uint32_t(i) + 1;
+            if (next < inWindow && next % chunk == 0) mask |= uint64_t(1) << i;
+        }
+    }
+    return mask;
+}
+
+template<class Tc, class T>
+long groupSplits(uint32_t first, uint32_t last, const Tc* x, const Tc* y, const Tc* z, const T* h,
+                 const uint64_t* leaves, int numLeaves, const uint32_t* layout, const Tc* box6, int G,
+                 float tolFactor, float extentRatio, uint32_t* counts, uint32_t* groups, long capacity)
+{
+    uint32_t numWindows = (last - first + uint32_t(G) - 1) / uint32_t(G);
+    std::vector<uint32_t> starts;
+    for (uint32_t w = 0; w < numWindows; ++w)
+    {
+        uint64_t mask = groupSplitsWindow<Tc, T>(first, last, x, y, z, h, leaves, numLeaves, layout, box6, G,
+                                                 tolFactor, extentRatio, w);
+        if (counts) counts[w] = 1u + uint32_t(__builtin_popcountll(mask));
+        uint32_t base = first + w * uint32_t(G);
+        starts.push_back(base);
+        for (int b = 0; b < G; ++b)
+            if ((mask >> b) & 1u) starts.push_back(base + uint32_t(b) + 1);
+    }
+    long numGroups = long(starts.size());
+    if (groups && numGroups + 1 <= capacity)
+    {
+        for (long i = 0; i < numGroups; ++i)
+            groups[i] = starts[size_t(i)];
+        groups[numGroups] = last;
+    }
+    return numGroups;
+}
+
 extern "C"
 {
 
@@ -1392,4 +1511,44 @@ extern "C"
         return u;
     }
 
+    uint64_t orc_find_splits_f64(const double* pos4, int G, double distCritSq)
+    {
+        return findSplitsWindow<double>(pos4, G, distCritSq);
+    }
+
+    int orc_make_splits(uint64_t mask, int G, uint32_t* lengths)
+    {
+        // lengths of the runs ended by the 1-bits of a G-bit stream, then the remainder (makeSplits,
+        // cstone/traversal/groups_gpu.cuh:86-110)
+        int n = 0, run = 0;
+        for (int b = 0; b < G; ++b)
+        {
+            ++run;
+            if ((mask >> b) & 1u)
+            {
+                lengths[n++] = uint32_t(run);
+                run          = 0;
+            }
+        }
+        lengths[n++] = uint32_t(run);
+        return n;
+    }
+
+    long orc_group_splits_f32(uint32_t first, uint32_t last, const float* x, const float* y, const float* z,
+                              const float* h, const uint64_t* leaves, int numLeaves, const uint32_t* layout,
+                              const float* box6, int groupSize, float tolFactor, float extentRatio, uint32_t* counts,
+                              uint32_t* groups, long capacity)
+    {
+        return groupSplits<float, float>(first, last, x, y, z, h, leaves, numLeaves, layout, box6, groupSize,
+                                         tolFactor, extentRatio, counts, groups, capacity);
+    }
+
+    long orc_group_splits_f64(uint32_t first, uint32_t last, const double* x, const double* y, const double* z,
+                              const double* h, const uint64_t* leaves, int numLeaves, const uint32_t* layout,
+                              const double* box6, int groupSize, float tolFactor, float extentRatio,
+                              uint32_t* counts, uint32_t* groups, long capacity)
+    {
+        return groupSplits<double, double>(first, last, x, y, z, h, leaves, numLeaves, layout, box6, groupSize,
+                                           tolFactor, extentRatio, counts, groups, capacity);
+    }
 } // extern "C"

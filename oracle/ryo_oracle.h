@@ -100,6 +100,19 @@ extern "C"
                          unsigned bucket, float theta, float G, float* pot, float* ax, float* ay, float* az,
                          double* seconds);
 
+    /* ---- spatial target groups (cstone/traversal/groups_gpu.cuh:39-265, groups_gpu.cu:60-118) */
+    uint64_t orc_find_splits_f64(const double* pos4, int G, double distCritSq);
+    int orc_make_splits(uint64_t mask, int G, uint32_t* lengths);
+    /* writes counts[window] (1 + splits) and, if capacity allows, groups[numGroups + 1]; returns numGroups */
+    long orc_group_splits_f32(uint32_t first, uint32_t last, const float* x, const float* y, const float* z,
+                              const float* h, const uint64_t* leaves, int numLeaves, const uint32_t* layout,
+                              const float* box6, int groupSize, float tolFactor, float extentRatio, uint32_t* counts,
+                              uint32_t* groups, long capacity);
+    long orc_group_splits_f64(uint32_t first, uint32_t last, const double* x, const double* y, const double* z,
+                              const double* h, const uint64_t* leaves, int numLeaves, const uint32_t* layout,
+                              const double* box6, int groupSize, float tolFactor, float extentRatio,
+                              uint32_t* counts, uint32_t* groups, long capacity);
+
 #ifdef __cplusplus
 }
 #endif

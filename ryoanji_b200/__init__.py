@@ -22,7 +22,7 @@ __all__ = [
     "Box", "Context", "RyoError", "TreeBuilder", "SolveParams", "SolveResult", "EwaldSettings", "lib",
     "compute_sfc_keys", "compute_bounding_box", "sequence", "sort_by_key", "compute_octree", "build_octree",
     "compute_fixed_groups", "compute_leaf_source_center", "upsweep_centers", "compute_leaf_multipoles",
-    "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch",
+    "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch", "compute_group_splits",
     "BatchSystem", "BatchResult", "Engine", "ewald_targets_f64",
     "compute_gravity_ewald", "direct_sum", "direct_targets_f64", "solve", "solve_arrays", "bh_max_target_size",
     "kernel_launches", "measure_peaks",
@@ -238,6 +238,25 @@ def compute_fixed_groups(first: int, last: int, group_size: int, device=None, st
     _check(lib.ryo_compute_fixed_groups(C.c_uint32(first), C.c_uint32(last), C.c_uint(group_size), _ptr(g),
                                         _stream(stream)))
     return g
+
+
+def compute_group_splits(x, y, z, h, leaves, layout, box: Box, group_size: int = 64, tol_factor: float = 2.0,
+                         extent_ratio: float = -1.0, first: int = 0, last: int | None = None,
+                         ctx: Context | None = None, stream=None) -> torch.Tensor:
+    """cstone::computeGroupSplits: spatial target groups of SFC-sorted bodies (int32 tensor of numGroups + 1
+    entries: group starts, then last); leaves/layout are the cornerstone leaf array and body layout"""
+    ctx = ctx or default_context()
+    last = x.numel() if last is None else last
+    cap = (last - first) + 2
+    groups = torch.empty(cap, dtype=torch.int32, device=x.device)
+    num = C.c_uint32(0)
+    bx = box.f32()
+    _check(lib.ryo_compute_group_splits_f32(ctx.handle, C.c_uint32(first), C.c_uint32(last), _ptr(x), _ptr(y),
+                                            _ptr(z), _ptr(h), _ptr(leaves), C.c_int(leaves.numel() - 1),
+                                            _ptr(layout), C.byref(bx), C.c_uint(group_size), C.c_float(tol_factor),
+                                            C.c_float(extent_ratio), _ptr(groups), C.c_uint32(cap), C.byref(num),
+                                            _stream(stream)), ctx)
+    return groups[:num.value + 1]
 
 
 # ---------------------------------------------------------------------------------------------------- upsweep
@@ -483,6 +502,8 @@ class SolveParams:
     ewald: EwaldSettings | None = None
     stack_capacity: int = 0
     timing: bool = False
+    group_tolerance: float = 0.0  # > 0: spatial target groups with this tolFactor (the reference's production uses 2)
+    group_extent_ratio: float = -1.0  # < 0: the reference default
 
     def c(self) -> _abi.SolveParams:
         p = _abi.SolveParams()
@@ -499,6 +520,8 @@ class SolveParams:
             p.ewald = self.ewald.c()
         p.stackCapacity = self.stack_capacity
         p.timing = int(self.timing)
+        p.groupTolerance = self.group_tolerance
+        p.groupExtentRatio = self.group_extent_ratio
         return p
 
 

@@ -58,7 +58,8 @@ class TreeView(C.Structure):
 class SolveParams(C.Structure):
     _fields_ = [("bucketSize", C.c_uint), ("groupSize", C.c_uint), ("theta", C.c_float), ("G", C.c_float),
                 ("useBox", C.c_int), ("box", BoxF32), ("numShells", C.c_int), ("ewald", EwaldSettings),
-                ("stackCapacity", C.c_int), ("timing", C.c_int)]
+                ("stackCapacity", C.c_int), ("timing", C.c_int), ("groupTolerance", C.c_float),
+                ("groupExtentRatio", C.c_float)]
 
 
 class SolveStats(C.Structure):
@@ -167,6 +168,8 @@ SIGNATURES = {
     "ryo_engine_status": (_i, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "ryo_ewald_targets_f64": (_i, [_p, _p, _sz] + [_p] * 4 + [_sz, C.c_double, C.POINTER(EwaldSettings), C.c_double]
                               + [_p] * 5),
+    "ryo_compute_group_splits_f32": (_i, [_p, _u32, _u32] + [_p] * 5 + [_i, _p, C.POINTER(BoxF32), _u, C.c_float,
+                                                                      C.c_float, _p, _u32, C.POINTER(C.c_uint32), _p]),
     "ryo_solve_batch_f32": (_i, [_p, C.POINTER(SolveParams), C.POINTER(System), _i] + [_p] * 8 + [_sz] + [_p] * 7
                             + [C.POINTER(SolveStats), _p]),
     "ryo_kernel_launches": (C.c_uint64, []),

@@ -307,6 +307,34 @@ extern "C" ryo_status ryo_compute_fixed_groups(uint32_t first, uint32_t last, un
                    });
 }
 
+extern "C" ryo_status ryo_compute_group_splits_f32(ryo_ctx_t* ctx, uint32_t first, uint32_t last, const float* x,
+                                                   const float* y, const float* z, const float* h,
+                                                   const uint64_t* leaves, int numLeaves, const uint32_t* layout,
+                                                   const ryo_box_f32* box, unsigned groupSize, float tolFactor,
+                                                   float extentRatio, uint32_t* groups, uint32_t capacity,
+                                                   uint32_t* numGroups, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       REQUIRE(numGroups && box && last >= first, "compute_group_splits: bad argument");
+                       REQUIRE(groupSize == 32 || groupSize == 64, "compute_group_splits: groupSize must be 32 or 64");
+                       REQUIRE(tolFactor > 0.f, "compute_group_splits: tolFactor must be positive");
+                       REQUIRE(last == first || (x && y && z && leaves && layout && numLeaves >= 1),
+                               "compute_group_splits: null argument");
+                       checkBox(box->limits);
+                       float ratio = extentRatio < 0.f ? defaultExtentRatio() : extentRatio;
+                       uint32_t ng = computeGroupSplits(ctx, first, last, x, y, z, h, leaves, numLeaves, layout,
+                                                        boxOf(box), groupSize, tolFactor, ratio, groups, capacity,
+                                                        stream);
+                       *numGroups = ng;
+                       if (last > first && (!groups || ng + 1 > capacity))
+                           throw ApiError{RYO_ERR_CAPACITY, "compute_group_splits: groups needs numGroups + 1 entries"};
+                       RYO_CUDA(cudaStreamSynchronize(stream));
+                   });
+}
+
 // ==================================================================================================== upsweep
 
 extern "C" ryo_status ryo_compute_leaf_source_center_f32(const float* x, const float* y, const float* z,
@@ -793,6 +821,8 @@ extern "C" void ryo_solve_params_default(ryo_solve_params* p)
     p->ewald.alpha_scale          = 2.0;
     p->ewald.small_R_scale_factor = 3.0e-3;
     p->stackCapacity              = 0;
+    p->groupTolerance             = 0.f;
+    p->groupExtentRatio           = -1.f;
 }
 
 namespace
@@ -930,8 +960,23 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                        mark(ctx, P, 3, s);
                        // groups and traversal
                        uint32_t numGroups = uint32_t((n + P->groupSize - 1) / P->groupSize);
-                       uint32_t* groups   = ctx->scratch<uint32_t>("solve.groups", size_t(numGroups) + 1, s);
-                       launchFixedGroups(0, uint32_t(n), P->groupSize, groups, s);
+                       uint32_t* groups   = nullptr;
+                       if (P->groupTolerance > 0.f)
+                       {
+                           // spatial groups (the reference's production grouping); at most one group per body
+                           REQUIRE(P->groupSize == 32 || P->groupSize == 64,
+                                   "solve: spatial groups need groupSize 32 or 64");
+                           groups      = ctx->scratch<uint32_t>("solve.groups", n + 2, s);
+                           float ratio = P->groupExtentRatio < 0.f ? defaultExtentRatio() : P->groupExtentRatio;
+                           numGroups   = computeGroupSplits(ctx, 0, uint32_t(n), x, y, z, h, leaves, nl, layout, dbox,
+                                                            P->groupSize, P->groupTolerance, ratio, groups,
+                                                            uint32_t(n + 2), s);
+                       }
+                       else
+                       {
+                           groups = ctx->scratch<uint32_t>("solve.groups", size_t(numGroups) + 1, s);
+                           launchFixedGroups(0, uint32_t(n), P->groupSize, groups, s);
+                       }
                        for (float* a : {p, ax, ay, az})
                            RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
                        TraverseLaunch t{};

@@ -227,6 +227,16 @@ struct SysTrav
 void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s);
 void launchTraversalReset(Control* ctl, bool resetStats, cudaStream_t s);
 
+// ---------------------------------------------------------------------------------------------------- groups.cu
+//! the reference's default window-extent ratio (8, or CSTONE_GROUP_EXTENT_SPLIT)
+float defaultExtentRatio();
+/*! spatial target groups of the sorted targets [first, last): returns the group count; writes groups[count + 1]
+ *  (starts, then last) when capacity >= count + 1 */
+uint32_t computeGroupSplits(ryo_ctx* ctx, uint32_t first, uint32_t last, const float* x, const float* y,
+                            const float* z, const float* h, const uint64_t* leaves, int numLeaves,
+                            const uint32_t* layout, const DevBox<float>& box, unsigned groupSize, float tolFactor,
+                            float extentRatio, uint32_t* groups, uint32_t capacity, cudaStream_t s);
+
 // ---------------------------------------------------------------------------------------------------- batch.cu
 void launchBatchBoxes(const float* x, const float* y, const float* z, size_t n, const uint64_t* first,
                       uint32_t numSystems, const int* useGiven, uint32_t* mm, DevBox<float>* boxes, float* limits,
