@@ -319,7 +319,8 @@ extern "C"
         int stackCapacity;           /* 0 = default */
         int timing;                  /* 1: record per-phase device times into ryo_solve_stats.ms */
         float groupTolerance;        /* > 0: spatial target groups (ryo_compute_group_splits_f32) with this
-                                        tolFactor, groupSize 32 or 64; 0: fixed groups, the reference demo's (0).
+                                        tolFactor and no interaction radius (h is the softening here), groupSize
+                                        32 or 64; 0: fixed groups, the reference demo's (0).
                                         The batched solve and the engine always use fixed groups. */
         float groupExtentRatio;      /* window-extent ratio of the spatial groups; < 0: the reference default (-1) */
     } ryo_solve_params;

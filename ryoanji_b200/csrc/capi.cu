@@ -963,12 +963,15 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                        uint32_t* groups   = nullptr;
                        if (P->groupTolerance > 0.f)
                        {
-                           // spatial groups (the reference's production grouping); at most one group per body
+                           // spatial groups (the reference's production grouping); at most one group per body.
+                           // No interaction radius: h here is the gravitational softening, not the SPH smoothing
+                           // length the grouping's radius criterion was made for, and a tiny softening would split
+                           // every pair of bodies.
                            REQUIRE(P->groupSize == 32 || P->groupSize == 64,
                                    "solve: spatial groups need groupSize 32 or 64");
                            groups      = ctx->scratch<uint32_t>("solve.groups", n + 2, s);
                            float ratio = P->groupExtentRatio < 0.f ? defaultExtentRatio() : P->groupExtentRatio;
-                           numGroups   = computeGroupSplits(ctx, 0, uint32_t(n), x, y, z, h, leaves, nl, layout, dbox,
+                           numGroups   = computeGroupSplits(ctx, 0, uint32_t(n), x, y, z, nullptr, leaves, nl, layout, dbox,
                                                             P->groupSize, P->groupTolerance, ratio, groups,
                                                             uint32_t(n + 2), s);
                        }

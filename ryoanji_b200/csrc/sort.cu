@@ -264,12 +264,23 @@ __global__ void __launch_bounds__(kSortBlock) onesweepPass(const uint64_t* __res
         }
     }
 
-    // rank within the warp: items in (item, lane) order, which is this warp's input order
+    // rank within the warp: items in (item, lane) order, which is this warp's input order. The lanes holding the
+    // same digit are found with one ballot per digit bit (plus one for the padding items past n).
     const unsigned lt = lanemaskLt();
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i)
     {
-        unsigned peers = __match_any_sync(0xffffffffu, d[i]);
+        const bool valid = d[i] < kDigits;
+        const unsigned vm = __ballot_sync(0xffffffffu, valid);
+        unsigned peers    = valid ? vm : ~vm;
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+        {
+            if (b >= nbits) break; // uniform across the warp
+            const bool bit    = (d[i] >> b) & 1u;
+            const unsigned bv = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bv : ~bv;
+        }
         int leader     = __ffs(peers) - 1;
         uint32_t before = 0;
         if (lane == leader && d[i] < kDigits)
