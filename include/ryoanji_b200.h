@@ -431,6 +431,17 @@ extern "C"
     RYO_API ryo_status ryo_engine_poll(ryo_engine_t* engine, ryo_engine_result* out, int capacity, int* count);
     RYO_API ryo_status ryo_engine_status(const ryo_engine_t* engine, int* queued, int* resident, double* bytesInUse);
 
+    /* Field of the last ryo_solve_f32 on this context at separate targets: the reference's MultipoleHolder::compute
+     * with distinct target and source arrays (ryoanji/src/ryoanji/interface/multipole_holder.cuh:64-77). The targets
+     * (any order, any positions) are SFC-sorted internally and grouped in fixed groups of the solve's groupSize;
+     * mt (may be NULL: unit masses) scales the potential, ht (may be NULL: 0) is the targets' softening. p (may be
+     * NULL), ax, ay, az are OVERWRITTEN in the caller's order with G m phi and G a, Ewald included for a periodic
+     * solve. The solve's tree and its source arrays (its x, y, z, m, h) must be unchanged since that solve; a
+     * batched solve on the same context invalidates it. stats (may be NULL): interaction counts, energy. */
+    RYO_API ryo_status ryo_solve_targets_f32(ryo_ctx_t* ctx, const float* xt, const float* yt, const float* zt,
+                                             const float* mt, const float* ht, size_t n, float* p, float* ax,
+                                             float* ay, float* az, ryo_solve_stats* stats, ryo_stream_t stream);
+
     /* device arrays of the last ryo_solve_f32 on this context (valid until the next solve on it): the sorted keys,
      * permutation, tree and the packed node records the traversal read (16 floats per node: centre x, y, z, squared
      * MAC radius; multipole mass, qxx, qxy, qxz, qyy, qyz, qzz, trace; then 4 ints: first child, first body, body

@@ -22,7 +22,7 @@ __all__ = [
     "Box", "Context", "RyoError", "TreeBuilder", "SolveParams", "SolveResult", "EwaldSettings", "lib",
     "compute_sfc_keys", "compute_bounding_box", "sequence", "sort_by_key", "compute_octree", "build_octree",
     "compute_fixed_groups", "compute_leaf_source_center", "upsweep_centers", "compute_leaf_multipoles",
-    "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch", "compute_group_splits",
+    "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch", "compute_group_splits", "solve_targets",
     "BatchSystem", "BatchResult", "Engine", "ewald_targets_f64",
     "compute_gravity_ewald", "direct_sum", "direct_targets_f64", "solve", "solve_arrays", "bh_max_target_size",
     "kernel_launches", "measure_peaks",
@@ -704,6 +704,20 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def solve_targets(xt, yt, zt, mt=None, ht=None, ctx: Context | None = None, stream=None):
+    """field of the last solve() on @p ctx at separate targets (MultipoleHolder::compute with distinct targets):
+    (p = G m phi, ax, ay, az) in the targets' order, and the interaction statistics"""
+    ctx = ctx or default_context()
+    n = xt.numel()
+    p, ax, ay, az = (torch.empty(n, device=xt.device) for _ in range(4))
+    st = _abi.SolveStats()
+    _check(lib.ryo_solve_targets_f32(ctx.handle, _ptr(xt), _ptr(yt), _ptr(zt), _ptr(mt), _ptr(ht), C.c_size_t(n),
+                                     _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), C.byref(st), _stream(stream)), ctx)
+    res = SolveResult(0, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P, st.maxStack,
+                      st.retries, st.potentialEnergy, list(st.box), {})
+    return (p, ax, ay, az), res
 
 
 _solve_n: dict = {}

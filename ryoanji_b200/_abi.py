@@ -170,6 +170,7 @@ SIGNATURES = {
                               + [_p] * 5),
     "ryo_compute_group_splits_f32": (_i, [_p, _u32, _u32] + [_p] * 5 + [_i, _p, C.POINTER(BoxF32), _u, C.c_float,
                                                                       C.c_float, _p, _u32, C.POINTER(C.c_uint32), _p]),
+    "ryo_solve_targets_f32": (_i, [_p] * 6 + [_sz] + [_p] * 4 + [C.POINTER(SolveStats), _p]),
     "ryo_solve_batch_f32": (_i, [_p, C.POINTER(SolveParams), C.POINTER(System), _i] + [_p] * 8 + [_sz] + [_p] * 7
                             + [C.POINTER(SolveStats), _p]),
     "ryo_kernel_launches": (C.c_uint64, []),

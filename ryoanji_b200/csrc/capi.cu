@@ -1042,6 +1042,18 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                            RYO_CUDA(cudaEventElapsedTime(&ms[5], ctx->phaseEvents[0], ctx->phaseEvents[6]));
                        }
                        {
+                           auto& st      = ctx->solveState;
+                           st.valid      = true;
+                           st.nodes      = records;
+                           st.xyzm       = xyzm;
+                           st.srcH       = h;
+                           st.numNodes   = nn;
+                           st.groupSize  = P->groupSize;
+                           st.G          = P->G;
+                           st.periodic   = periodic ? 1 : 0;
+                           st.numShells  = periodic ? P->numShells : 0;
+                           st.box        = box;
+                           st.ewald      = P->ewald;
                            ryo_solve_arrays& a = ctx->lastSolve;
                            a.numLeaves         = nl;
                            a.numNodes          = nn;
@@ -1068,6 +1080,8 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                                a.rootCenter[i] = hr[i];
                            for (int i = 0; i < 8; ++i)
                                a.rootMultipole[i] = hr[3 + i];
+                           for (int i = 0; i < 11; ++i)
+                               st.root[i] = hr[i];
                        }
                        if (ctx->hostStats[kMaxP2P] == 0xFFFFFFFFull)
                            throw ApiError{RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE, "solve: a single target overflowed"};
@@ -1121,6 +1135,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        cudaStream_t s      = stream;
                        const uint32_t ns   = uint32_t(numSystems);
                        const int sysLevel  = batchSystemLevel(numSystems);
+                       ctx->solveState.valid = false; // the solve buffers are about to be reused
                        std::vector<uint64_t> first(ns + 1);
                        std::vector<int> useGiven(ns), shells(ns);
                        std::vector<DevBox<float>> hbox(ns);
@@ -1371,6 +1386,143 @@ extern "C" ryo_status ryo_ewald_targets_f64(ryo_ctx_t* ctx, const int64_t* targe
                                              settings->numReplicaShells, settings->lCut, settings->hCut,
                                              settings->alpha_scale, settings->small_R_scale_factor, G, pot, ax, ay, az,
                                              stream);
+                   });
+}
+
+namespace
+{
+//! sorted target copies: packed (x, y, z, h), mass, and x, y, z, m again as separate arrays for the Ewald kernel
+__global__ void packTargets(const uint32_t* __restrict__ order, const float* __restrict__ x,
+                            const float* __restrict__ y, const float* __restrict__ z, const float* __restrict__ m,
+                            const float* __restrict__ h, size_t n, float4* __restrict__ xyzh, float* __restrict__ sx,
+                            float* __restrict__ sy, float* __restrict__ sz, float* __restrict__ sm)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        uint32_t j = order[i];
+        float vx = x[j], vy = y[j], vz = z[j];
+        float vm = m ? m[j] : 1.f;
+        float vh = h ? h[j] : 0.f;
+        xyzh[i]  = make_float4(vx, vy, vz, vh);
+        sx[i]    = vx;
+        sy[i]    = vy;
+        sz[i]    = vz;
+        sm[i]    = vm;
+    }
+}
+
+//! results back to the caller's order: out[order[i]] = in[i] for the four arrays
+__global__ void scatterTargets(const uint32_t* __restrict__ order, const float* __restrict__ in, size_t n,
+                               float* __restrict__ p, float* __restrict__ ax, float* __restrict__ ay,
+                               float* __restrict__ az)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        uint32_t j = order[i];
+        if (p) p[j] = in[i];
+        ax[j] = in[n + i];
+        ay[j] = in[2 * n + i];
+        az[j] = in[3 * n + i];
+    }
+}
+} // namespace
+
+extern "C" ryo_status ryo_solve_targets_f32(ryo_ctx_t* ctx, const float* xt, const float* yt, const float* zt,
+                                           const float* mt, const float* ht, size_t n, float* p, float* ax,
+                                           float* ay, float* az, ryo_solve_stats* stats, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       const auto& S = ctx->solveState;
+                       REQUIRE(S.valid, "solve_targets: needs a preceding ryo_solve_f32 on this context");
+                       REQUIRE(n > 0 && n < (size_t(1) << 32) && xt && yt && zt && ax && ay && az,
+                               "solve_targets: bad argument");
+                       cudaStream_t s      = stream;
+                       DevBox<float> dbox  = boxOf(&S.box);
+                       uint64_t* keys      = ctx->scratch<uint64_t>("tgt.keys", n, s);
+                       uint64_t* keysAlt   = ctx->scratch<uint64_t>("tgt.keysAlt", n, s);
+                       uint32_t* ord       = ctx->scratch<uint32_t>("tgt.order", n, s);
+                       uint32_t* ordAlt    = ctx->scratch<uint32_t>("tgt.orderAlt", n, s);
+                       size_t tmpBytes     = sortTempBytes(n);
+                       void* tmp           = ctx->scratch<char>("tgt.sorttmp", tmpBytes, s);
+                       // targets in SFC order of the solve's box, so that fixed groups are compact
+                       launchKeys<float>(xt, yt, zt, keys, n, dbox, false, s);
+                       bool alt = radixSortPairs(keys, ord, keysAlt, ordAlt, n, 0, 64, tmp, tmpBytes,
+                                                 &ctx->ctl->error, s, true);
+                       const uint32_t* order = alt ? ordAlt : ord;
+                       float4* xyzh = ctx->scratch<float4>("tgt.xyzh", n, s);
+                       float* sorted = ctx->scratch<float>("tgt.sorted", 8 * n, s); // x y z m | p ax ay az
+                       unsigned grid = ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
+                                                                                    : unsigned(ctx->smCount * 16);
+                       packTargets<<<grid, 256, 0, s>>>(order, xt, yt, zt, mt, ht, n, xyzh, sorted, sorted + n,
+                                                        sorted + 2 * n, sorted + 3 * n);
+                       RYO_LAUNCH_CHECK();
+                       float* out = sorted + 4 * n;
+                       RYO_CUDA(cudaMemsetAsync(out, 0, 4 * n * sizeof(float), s));
+                       uint32_t numGroups = uint32_t((n + S.groupSize - 1) / S.groupSize);
+                       uint32_t* groups   = ctx->scratch<uint32_t>("tgt.groups", size_t(numGroups) + 1, s);
+                       launchFixedGroups(0, uint32_t(n), S.groupSize, groups, s);
+
+                       TraverseLaunch t{};
+                       t.groupStart    = groups;
+                       t.groupEnd      = groups + 1;
+                       t.numGroups     = int(numGroups);
+                       t.initNode      = S.numNodes == 1 ? 0 : 1;
+                       t.numNodes      = S.numNodes;
+                       t.nodes         = static_cast<const NodeRecord*>(S.nodes);
+                       t.tgtXYZH       = xyzh;
+                       t.tgtM          = sorted + 3 * n;
+                       t.srcXYZM       = static_cast<const float4*>(S.xyzm);
+                       t.srcH          = S.srcH;
+                       t.G             = S.G;
+                       t.numShells     = S.numShells;
+                       for (int d = 0; d < 3; ++d)
+                           t.boxL[d] = dbox.len[d];
+                       t.p             = out;
+                       t.ax            = out + n;
+                       t.ay            = out + 2 * n;
+                       t.az            = out + 3 * n;
+                       double pot      = 0;
+                       runTraversal(ctx, t, s, &pot);
+                       double energy = 0.5 * double(S.G) * pot;
+                       if (S.periodic)
+                       {
+                           EwaldHost e = ewaldSetup(S.root + 3, S.root, S.ewald.numReplicaShells, double(dbox.len[0]),
+                                                    S.ewald.lCut, S.ewald.hCut, S.ewald.alpha_scale,
+                                                    S.ewald.small_R_scale_factor);
+                           double* ep = &ctx->ctl->ewaldPotential;
+                           RYO_CUDA(cudaMemsetAsync(ep, 0, sizeof(double), s));
+                           launchEwaldGroups(e, groups, groups + 1, numGroups, sorted, sorted + n, sorted + 2 * n,
+                                             sorted + 3 * n, S.G, out, out + n, out + 2 * n, out + 3 * n, ep, s);
+                           double he = 0;
+                           RYO_CUDA(cudaMemcpyAsync(&he, ep, sizeof(double), cudaMemcpyDeviceToHost, s));
+                           RYO_CUDA(cudaStreamSynchronize(s));
+                           energy += 0.5 * double(S.G) * he;
+                       }
+                       scatterTargets<<<grid, 256, 0, s>>>(order, out, n, p, ax, ay, az);
+                       RYO_LAUNCH_CHECK();
+                       if (ctx->hostStats[kMaxP2P] == 0xFFFFFFFFull)
+                           throw ApiError{RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE, "solve_targets: a target overflowed"};
+                       checkDeviceError(ctx, s);
+                       if (stats)
+                       {
+                           *stats                 = ryo_solve_stats{};
+                           stats->numGroups       = int(numGroups);
+                           stats->numNodes        = S.numNodes;
+                           stats->sumP2P          = ctx->hostStats[kSumP2P];
+                           stats->maxP2P          = ctx->hostStats[kMaxP2P];
+                           stats->sumM2P          = ctx->hostStats[kSumM2P];
+                           stats->maxM2P          = ctx->hostStats[kMaxM2P];
+                           stats->maxStack        = ctx->hostStats[kMaxStack];
+                           stats->retries         = ctx->retries;
+                           stats->potentialEnergy = energy;
+                           for (int i = 0; i < 6; ++i)
+                               stats->box[i] = S.box.limits[i];
+                       }
                    });
 }
 

@@ -45,6 +45,23 @@ struct ryo_ctx
     unsigned long long hostStats[5] = {0, 0, 0, 0, 0};
     uint64_t retries                = 0;
     ryo_solve_arrays lastSolve      = {};
+    //! what ryo_solve_targets_f32 needs of the last single-system solve (cleared by a batched solve, which reuses
+    //! the same scratch buffers)
+    struct SolveState
+    {
+        bool valid         = false;
+        const void* nodes  = nullptr; // NodeRecord per node
+        const void* xyzm   = nullptr; // float4 per source body
+        const float* srcH  = nullptr; // the caller's h array of the solve (sorted)
+        int numNodes       = 0;
+        unsigned groupSize = 64;
+        float G            = 1.f;
+        int periodic       = 0;
+        int numShells      = 0;
+        ryo_box_f32 box    = {};
+        ryo_ewald_settings ewald = {};
+        double root[11]    = {};
+    } solveState;
     cudaEvent_t phaseEvents[7]      = {};
 
     struct Buffer
