@@ -306,6 +306,13 @@ extern "C"
      * The B200 plain path for one system: keys, sort, gather, leaves, links, fused FP64 upsweep with MAC radii,
      * fixed groups, traversal, Ewald if periodic. Not in the reference; it composes the functions above with the
      * reference's semantics except that it permutes every per-particle array (TreeBuilder permutes only x, y, z). */
+    /* multipole types of the reference (ryoanji/src/ryoanji/nbody/cartesian_qpole.hpp) */
+    enum
+    {
+        RYO_MULTIPOLE_QUADRUPOLE = 0, /* CartesianQuadrupole: mass + traceless quadrupole (8 values) */
+        RYO_MULTIPOLE_MDQ        = 1  /* CartesianMDQpole: mass + traceless quadrupole + dipole (12 values) */
+    };
+
     typedef struct ryo_solve_params
     {
         unsigned bucketSize;         /* leaf capacity, reference ncrit (64) */
@@ -323,6 +330,8 @@ extern "C"
                                         32 or 64; 0: fixed groups, the reference demo's (0).
                                         The batched solve and the engine always use fixed groups. */
         float groupExtentRatio;      /* window-extent ratio of the spatial groups; < 0: the reference default (-1) */
+        int multipole;               /* RYO_MULTIPOLE_QUADRUPOLE (CartesianQuadrupole, default) or
+                                        RYO_MULTIPOLE_MDQ (CartesianMDQpole: adds the dipole, for signed masses) */
     } ryo_solve_params;
 
     typedef struct ryo_solve_stats
@@ -465,6 +474,7 @@ extern "C"
         int levelRange[23];
         double rootCenter[3];
         double rootMultipole[8];
+        const float* dipoles; /* RYO_MULTIPOLE_MDQ: 4 floats per node (px, py, pz, 0); NULL otherwise */
     } ryo_solve_arrays;
     RYO_API ryo_status ryo_solve_arrays_get(ryo_ctx_t* ctx, ryo_solve_arrays* out);
 

@@ -213,6 +213,28 @@ class Oracle:
                                                  C.c_double(alpha_scale), C.c_double(small_r))
         return u, pot, ax, ay, az
 
+    # ---- monopole + dipole + quadrupole (same names for the restatement and the reference wrapper)
+    def mdq_p2m(self, x, y, z, m):
+        c = np.zeros(4)
+        q = np.zeros(12)
+        self._f("mdq_p2m_f64")(*(_ptr(np.ascontiguousarray(a, np.float64)) for a in (x, y, z, m)),
+                               C.c_uint(len(x)), _ptr(c), _ptr(q))
+        return c, q
+
+    def mdq_m2m(self, centers, mdqs, out_center):
+        out = np.zeros(12)
+        self._f("mdq_m2m_f64")(C.c_int(len(centers)), _ptr(np.ascontiguousarray(centers, np.float64)),
+                               _ptr(np.ascontiguousarray(mdqs, np.float64)),
+                               _ptr(np.ascontiguousarray(out_center, np.float64)), _ptr(out))
+        return out
+
+    def mdq_m2p(self, target, center, mdq):
+        acc = np.zeros(4)
+        self._f("mdq_m2p_f64")(_ptr(np.ascontiguousarray(target, np.float64)),
+                               _ptr(np.ascontiguousarray(center, np.float64)),
+                               _ptr(np.ascontiguousarray(mdq, np.float64)), _ptr(acc))
+        return acc
+
     # ---- spatial target groups (restatement only: the reference's version is device code)
     def find_splits(self, pos4, dist_crit_sq):
         """split bits of one window of targets (rows x, y, z, w)"""

@@ -43,6 +43,7 @@ cstone::Box<T> makeBox(const T* b, int periodic)
 }
 
 using Quad = ryoanji::CartesianQuadrupole<float>;
+using MDQ  = ryoanji::CartesianMDQpole<float>;
 using Center = cstone::SourceCenterType<float>;
 } // namespace
 
@@ -289,6 +290,88 @@ extern "C"
             seconds[2] = std::chrono::duration<double>(t3 - t2).count();
         }
         return u;
+    }
+
+    // ---- monopole + dipole + quadrupole (CartesianMDQpole, ryoanji/src/ryoanji/nbody/cartesian_qpole.hpp:237-423)
+
+    //! ryoanji::P2M for CartesianMDQpole about the |m|-weighted centre (cstone::massCenter), double
+    void ref_mdq_p2m_f64(const double* x, const double* y, const double* z, const double* m, unsigned n,
+                         double* center4, double* mdq12)
+    {
+        auto c = cstone::massCenter<double>(x, y, z, m, 0, n);
+        ryoanji::CartesianMDQpole<double> q;
+        ryoanji::P2M(x, y, z, m, 0, n, c, q);
+        for (int i = 0; i < 4; ++i)
+            center4[i] = c[i];
+        for (int i = 0; i < 12; ++i)
+            mdq12[i] = q[i];
+    }
+
+    //! ryoanji::M2M for CartesianMDQpole, double: children centres (4 each) and multipoles (12 each)
+    void ref_mdq_m2m_f64(int numChildren, const double* centers4, const double* mdq12, const double* outCenter4,
+                         double* out12)
+    {
+        std::vector<cstone::Vec4<double>> c(numChildren);
+        std::vector<ryoanji::CartesianMDQpole<double>> q(numChildren);
+        for (int k = 0; k < numChildren; ++k)
+        {
+            for (int i = 0; i < 4; ++i)
+                c[k][i] = centers4[4 * k + i];
+            for (int i = 0; i < 12; ++i)
+                q[k][i] = mdq12[12 * k + i];
+        }
+        cstone::Vec4<double> oc{outCenter4[0], outCenter4[1], outCenter4[2], outCenter4[3]};
+        ryoanji::CartesianMDQpole<double> out;
+        ryoanji::M2M(0, numChildren, oc, c.data(), q.data(), out);
+        for (int i = 0; i < 12; ++i)
+            out12[i] = out[i];
+    }
+
+    //! ryoanji::M2P for CartesianMDQpole, double, accumulating into acc4
+    void ref_mdq_m2p_f64(const double* target, const double* center, const double* mdq12, double* acc4)
+    {
+        ryoanji::CartesianMDQpole<double> q;
+        for (int i = 0; i < 12; ++i)
+            q[i] = mdq12[i];
+        cstone::Vec4<double> acc{acc4[0], acc4[1], acc4[2], acc4[3]};
+        acc = ryoanji::M2P(acc, cstone::Vec3<double>{target[0], target[1], target[2]},
+                           cstone::Vec3<double>{center[0], center[1], center[2]}, q);
+        for (int i = 0; i < 4; ++i)
+            acc4[i] = acc[i];
+    }
+
+    //! the reference CPU upsweep (as ref_upsweep_f32) with CartesianMDQpole multipoles (12 floats per node)
+    void ref_upsweep_mdq_f32(const float* x, const float* y, const float* z, const float* m, size_t n, int numLeaves,
+                             const uint32_t* layout, const int* leafToInternalLeaves, const int* childOffsets,
+                             const int* levelRange, const uint64_t* prefixes, int numNodes, float theta,
+                             const float* box, float* centers, float* multipoles)
+    {
+        auto* c  = reinterpret_cast<Center*>(centers);
+        auto* mp = reinterpret_cast<MDQ*>(multipoles);
+        std::fill(centers, centers + 4 * numNodes, 0.f);
+        std::fill(multipoles, multipoles + 12 * numNodes, 0.f);
+        std::span<const TreeNodeIndex> l2i(leafToInternalLeaves, numLeaves);
+        cstone::computeLeafMassCenter<float, float, float>({x, n}, {y, n}, {z, n}, {m, n}, l2i, layout, c);
+        std::span<const TreeNodeIndex> lr(levelRange, 23);
+        cstone::upsweep(lr, childOffsets, c, cstone::CombineSourceCenter<float>{});
+        ryoanji::computeLeafMultipoles(x, y, z, m, l2i, layout, c, mp);
+        ryoanji::upsweepMultipoles(lr, childOffsets, c, mp);
+        cstone::setMac<float, uint64_t>({prefixes, size_t(numNodes)}, {c, size_t(numNodes)}, 1.0f / theta,
+                                        makeBox(box));
+    }
+
+    //! ryoanji::computeGravity with CartesianMDQpole multipoles
+    double ref_gravity_cpu_mdq_f32(const int* childOffsets, const int* parents, const int* internalToLeaf,
+                                   const float* centers, const float* multipoles, const uint32_t* layout,
+                                   int numLeaves, const float* x, const float* y, const float* z, const float* h,
+                                   const float* m, const float* box, int periodic, float G, int numShells,
+                                   float* pot, float* ax, float* ay, float* az)
+    {
+        float utot = 0;
+        ryoanji::computeGravity(childOffsets, parents, internalToLeaf, reinterpret_cast<const Center*>(centers),
+                                reinterpret_cast<const MDQ*>(multipoles), layout, 0, numLeaves, x, y, z, h, m,
+                                makeBox(box, periodic), G, pot, ax, ay, az, &utot, numShells);
+        return utot;
     }
 
 } // extern "C"

@@ -852,6 +852,86 @@ long groupSplits(uint32_t first, uint32_t last, const Tc* x, const Tc* y, const 
     return numGroups;
 }
 
+// ------------------------------------------------------------------------------------------------ MDQpole
+
+/*! monopole + dipole + traceless quadrupole (12 values: mass, qxx, qxy, qxz, qyy, qyz, qzz, trace, px, py, pz, 0)
+ *  about centre c (P2M_add / P2M_finalize, cartesian_qpole.hpp:237-303) */
+template<class T>
+void mdqP2M(const T* x, const T* y, const T* z, const T* m, size_t a, size_t b, const T c[3], T out[12])
+{
+    T g[12] = {};
+    for (size_t i = a; i < b; ++i)
+    {
+        T rx = x[i] - c[0], ry = y[i] - c[1], rz = z[i] - c[2], mi = m[i];
+        g[0] += mi;
+        g[8] += mi * rx;
+        g[9] += mi * ry;
+        g[10] += mi * rz;
+        g[1] += rx * rx * mi;
+        g[2] += rx * ry * mi;
+        g[3] += rx * rz * mi;
+        g[4] += ry * ry * mi;
+        g[5] += ry * rz * mi;
+        g[6] += rz * rz * mi;
+    }
+    T tr = g[1] + g[4] + g[6];
+    g[7] = tr;
+    g[1] = 3 * g[1] - tr;
+    g[4] = 3 * g[4] - tr;
+    g[6] = 3 * g[6] - tr;
+    g[2] *= 3;
+    g[3] *= 3;
+    g[5] *= 3;
+    std::copy(g, g + 12, out);
+}
+
+//! add a child expansion at centre offset dX = parentCentre - childCentre (addQuadrupole, cartesian_qpole.hpp:352-398)
+template<class T>
+void mdqAdd(T out[12], const T dX[3], const T* a)
+{
+    T rx = dX[0], ry = dX[1], rz = dX[2];
+    T rx2 = rx * rx, ry2 = ry * ry, rz2 = rz * rz;
+    T r2  = (rx2 + ry2 + rz2) * (1.0 / 3.0);
+    T ml  = a[0] * 3;
+    T px = a[8], py = a[9], pz = a[10];
+    T dip = rx * px + ry * py + rz * pz;
+    out[7] = out[7] + a[7] + ml * r2 - 2.0 * dip;
+    out[0] += a[0];
+    out[8] += a[8] - a[0] * rx;
+    out[9] += a[9] - a[0] * ry;
+    out[10] += a[10] - a[0] * rz;
+    out[1] += a[1] + ml * (rx2 - r2) - 6.0 * rx * px + 2.0 * dip;
+    out[2] += a[2] + ml * rx * ry - 3.0 * (rx * py + ry * px);
+    out[3] += a[3] + ml * rx * rz - 3.0 * (rx * pz + rz * px);
+    out[4] += a[4] + ml * (ry2 - r2) - 6.0 * ry * py + 2.0 * dip;
+    out[5] += a[5] + ml * ry * rz - 3.0 * (ry * pz + rz * py);
+    out[6] += a[6] + ml * (rz2 - r2) - 6.0 * rz * pz + 2.0 * dip;
+}
+
+//! M2P of a CartesianMDQpole (cartesian_qpole.hpp:305-343), accumulating (u, ax, ay, az)
+template<class T, class R>
+void mdqM2P(T acc[4], const T t[3], const T c[3], const T* q, R rsq)
+{
+    T r[3] = {t[0] - c[0], t[1] - c[1], t[2] - c[2]};
+    T r2   = norm2(r[0], r[1], r[2]);
+    T rm1  = rsq(r2);
+    T rm2  = rm1 * rm1;
+    T rm5  = rm2 * rm2 * rm1;
+    T Qrx  = r[0] * q[1] + r[1] * q[2] + r[2] * q[3];
+    T Qry  = r[0] * q[2] + r[1] * q[4] + r[2] * q[5];
+    T Qrz  = r[0] * q[3] + r[1] * q[5] + r[2] * q[6];
+    T rQr  = r[0] * Qrx + r[1] * Qry + r[2] * Qrz;
+    T qm   = (T(-2.5) * rQr * rm5 - q[0] * rm1) * rm2;
+    T PR   = r[0] * q[8] + r[1] * q[9] + r[2] * q[10];
+    T Px   = rm5 * (q[8] * r2 - T(3) * PR * r[0]);
+    T Py   = rm5 * (q[9] * r2 - T(3) * PR * r[1]);
+    T Pz   = rm5 * (q[10] * r2 - T(3) * PR * r[2]);
+    acc[0] += (-q[0] - PR * rm2) * rm1 + T(-0.5) * rm5 * rQr;
+    acc[1] += rm5 * Qrx + qm * r[0] + Px;
+    acc[2] += rm5 * Qry + qm * r[1] + Py;
+    acc[3] += rm5 * Qrz + qm * r[2] + Pz;
+}
+
 extern "C"
 {
 
@@ -1550,5 +1630,41 @@ extern "C"
     {
         return groupSplits<double, double>(first, last, x, y, z, h, leaves, numLeaves, layout, box6, groupSize,
                                            tolFactor, extentRatio, counts, groups, capacity);
+    }
+    void orc_mdq_p2m_f64(const double* x, const double* y, const double* z, const double* m, unsigned n,
+                         double* center4, double* mdq12)
+    {
+        double c[4] = {0, 0, 0, 0};
+        for (unsigned i = 0; i < n; ++i)
+        {
+            double w = std::abs(m[i]);
+            c[0] += w * x[i];
+            c[1] += w * y[i];
+            c[2] += w * z[i];
+            c[3] += w;
+        }
+        double inv = c[3] != 0 ? 1.0 / c[3] : 1.0;
+        for (int d = 0; d < 3; ++d)
+            c[d] *= inv;
+        mdqP2M<double>(x, y, z, m, 0, n, c, mdq12);
+        std::copy(c, c + 4, center4);
+    }
+
+    void orc_mdq_m2m_f64(int numChildren, const double* centers4, const double* mdq12, const double* outCenter4,
+                         double* out12)
+    {
+        std::fill(out12, out12 + 12, 0.0);
+        for (int k = 0; k < numChildren; ++k)
+        {
+            double dX[3] = {outCenter4[0] - centers4[4 * k], outCenter4[1] - centers4[4 * k + 1],
+                            outCenter4[2] - centers4[4 * k + 2]};
+            mdqAdd<double>(out12, dX, mdq12 + 12 * k);
+        }
+    }
+
+    void orc_mdq_m2p_f64(const double* target, const double* center, const double* mdq12, double* acc4)
+    {
+        // the reference's double inverseSquareRoot evaluates in single precision (kernel.hpp:38-52)
+        mdqM2P<double>(acc4, target, center, mdq12, [](double v) { return double(1.0f / std::sqrt(float(v))); });
     }
 } // extern "C"

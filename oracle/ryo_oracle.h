@@ -113,6 +113,13 @@ extern "C"
                               const double* box6, int groupSize, float tolFactor, float extentRatio,
                               uint32_t* counts, uint32_t* groups, long capacity);
 
+    /* ---- monopole + dipole + quadrupole expansions (cartesian_qpole.hpp:237-423), double; 12 values per expansion */
+    void orc_mdq_p2m_f64(const double* x, const double* y, const double* z, const double* m, unsigned n,
+                         double* center4, double* mdq12);
+    void orc_mdq_m2m_f64(int numChildren, const double* centers4, const double* mdq12, const double* outCenter4,
+                         double* out12);
+    void orc_mdq_m2p_f64(const double* target, const double* center, const double* mdq12, double* acc4);
+
 #ifdef __cplusplus
 }
 #endif

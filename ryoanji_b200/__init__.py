@@ -504,6 +504,7 @@ class SolveParams:
     timing: bool = False
     group_tolerance: float = 0.0  # > 0: spatial target groups with this tolFactor (the reference's production uses 2)
     group_extent_ratio: float = -1.0  # < 0: the reference default
+    multipole: str = "quadrupole"  # or "mdq": monopole + dipole + quadrupole (CartesianMDQpole), for signed masses
 
     def c(self) -> _abi.SolveParams:
         p = _abi.SolveParams()
@@ -522,6 +523,7 @@ class SolveParams:
         p.timing = int(self.timing)
         p.groupTolerance = self.group_tolerance
         p.groupExtentRatio = self.group_extent_ratio
+        p.multipole = {"quadrupole": _abi.MULTIPOLE_QUADRUPOLE, "mdq": _abi.MULTIPOLE_MDQ}[self.multipole]
         return p
 
 
@@ -757,4 +759,5 @@ def solve_arrays(ctx: Context | None = None, device=None) -> dict:
                 multipoles=nd[:, 4:12], links=nd[:, 12:16].view(torch.int32), groups=w(a.groups, ng + 1, torch.int32),
                 groupM2P=w(a.groupM2P, ng, torch.int32), groupP2P=w(a.groupP2P, ng, torch.int32),
                 sortedKeys=w(a.sortedKeys, 0 if not a.sortedKeys else _last_n(ctx), torch.int64),
-                levelRange=list(a.levelRange), rootCenter=list(a.rootCenter), rootMultipole=list(a.rootMultipole))
+                levelRange=list(a.levelRange), rootCenter=list(a.rootCenter), rootMultipole=list(a.rootMultipole),
+                dipoles=w(a.dipoles, 4 * nn, torch.float32).view(nn, 4) if a.dipoles else None)

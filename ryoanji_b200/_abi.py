@@ -59,7 +59,7 @@ class SolveParams(C.Structure):
     _fields_ = [("bucketSize", C.c_uint), ("groupSize", C.c_uint), ("theta", C.c_float), ("G", C.c_float),
                 ("useBox", C.c_int), ("box", BoxF32), ("numShells", C.c_int), ("ewald", EwaldSettings),
                 ("stackCapacity", C.c_int), ("timing", C.c_int), ("groupTolerance", C.c_float),
-                ("groupExtentRatio", C.c_float)]
+                ("groupExtentRatio", C.c_float), ("multipole", C.c_int)]
 
 
 class SolveStats(C.Structure):
@@ -75,7 +75,7 @@ class SolveArrays(C.Structure):
                 ("childOffsets", C.c_void_p), ("internalToLeaf", C.c_void_p), ("leafToInternal", C.c_void_p),
                 ("parents", C.c_void_p), ("nodeData", C.c_void_p), ("groups", C.c_void_p),
                 ("groupM2P", C.c_void_p), ("groupP2P", C.c_void_p), ("levelRange", C.c_int * 23),
-                ("rootCenter", C.c_double * 3), ("rootMultipole", C.c_double * 8)]
+                ("rootCenter", C.c_double * 3), ("rootMultipole", C.c_double * 8), ("dipoles", C.c_void_p)]
 
 
 class System(C.Structure):
@@ -104,6 +104,8 @@ class EngineResult(C.Structure):
     _fields_ = [("tag", C.c_uint64), ("numBodies", C.c_uint32), ("stepsDone", C.c_int),
                 ("kineticEnergy", C.c_double), ("potentialEnergy", C.c_double), ("initialEnergy", C.c_double)]
 
+
+MULTIPOLE_QUADRUPOLE, MULTIPOLE_MDQ = 0, 1
 
 _p = C.c_void_p
 _sz = C.c_size_t

@@ -823,6 +823,7 @@ extern "C" void ryo_solve_params_default(ryo_solve_params* p)
     p->stackCapacity              = 0;
     p->groupTolerance             = 0.f;
     p->groupExtentRatio           = -1.f;
+    p->multipole                  = RYO_MULTIPOLE_QUADRUPOLE;
 }
 
 namespace
@@ -951,11 +952,16 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
 
                        mark(ctx, P, 2, s);
                        // fused upsweep: node records + FP64 root expansion
+                       REQUIRE(P->multipole == RYO_MULTIPOLE_QUADRUPOLE || P->multipole == RYO_MULTIPOLE_MDQ,
+                               "solve: unknown multipole type");
                        NodeRecord* records = ctx->scratch<NodeRecord>("solve.records", nn, s);
                        double* root        = ctx->scratch<double>("solve.root", 16, s);
+                       float4* dipoles     = P->multipole == RYO_MULTIPOLE_MDQ
+                                                 ? ctx->scratch<float4>("solve.dipoles", nn, s)
+                                                 : nullptr;
                        launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
                                           oct.parents, oct.prefixes, 1.0f / P->theta, dbox, records, nullptr, nullptr,
-                                          root, s);
+                                          root, s, nullptr, 0, nullptr, dipoles);
 
                        mark(ctx, P, 3, s);
                        // groups and traversal
@@ -1002,6 +1008,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                        t.ay = ay;
                        t.az = az;
                        t.stackCapacity = P->stackCapacity;
+                       t.dipoles       = dipoles;
                        uint32_t* gm2p  = ctx->scratch<uint32_t>("solve.groupM2P", numGroups, s);
                        uint32_t* gp2p  = ctx->scratch<uint32_t>("solve.groupP2P", numGroups, s);
                        RYO_CUDA(cudaMemsetAsync(gm2p, 0, sizeof(uint32_t) * numGroups, s));
@@ -1054,6 +1061,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                            st.numShells  = periodic ? P->numShells : 0;
                            st.box        = box;
                            st.ewald      = P->ewald;
+                           st.dipoles    = dipoles;
                            ryo_solve_arrays& a = ctx->lastSolve;
                            a.numLeaves         = nl;
                            a.numNodes          = nn;
@@ -1071,6 +1079,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                            a.groups            = groups;
                            a.groupM2P          = gm2p;
                            a.groupP2P          = gp2p;
+                           a.dipoles           = reinterpret_cast<const float*>(dipoles);
                            for (int i = 0; i < kMaxLevel + 2; ++i)
                                a.levelRange[i] = levelRange[i];
                            double hr[11];
@@ -1249,12 +1258,17 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        mark(ctx, P, 2, s);
 
                        // fused upsweep with each system's box; FP64 expansions of the system roots
+                       REQUIRE(P->multipole == RYO_MULTIPOLE_QUADRUPOLE || P->multipole == RYO_MULTIPOLE_MDQ,
+                               "solve_batch: unknown multipole type");
                        NodeRecord* records = ctx->scratch<NodeRecord>("solve.records", nn, s);
                        double* sysRoots    = ctx->scratch<double>("batch.roots", 11 * size_t(ns), s);
+                       float4* dipoles     = P->multipole == RYO_MULTIPOLE_MDQ
+                                                 ? ctx->scratch<float4>("solve.dipoles", nn, s)
+                                                 : nullptr;
                        DevBox<float> unused = hbox[0];
                        launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
                                           oct.parents, oct.prefixes, 1.0f / P->theta, unused, records, nullptr, nullptr,
-                                          nullptr, s, dBx, sysLevel, sysRoots);
+                                          nullptr, s, dBx, sysLevel, sysRoots, dipoles);
                        mark(ctx, P, 3, s);
 
                        // groups inside systems, system roots, traversal
@@ -1290,6 +1304,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        t.az            = az;
                        t.stackCapacity = P->stackCapacity;
                        t.groupSys      = gSys;
+                       t.dipoles       = dipoles;
                        t.systems       = dTrav;
                        t.sysPotential  = sysPot;
                        double pot      = 0;
@@ -1474,6 +1489,7 @@ extern "C" ryo_status ryo_solve_targets_f32(ryo_ctx_t* ctx, const float* xt, con
                        t.initNode      = S.numNodes == 1 ? 0 : 1;
                        t.numNodes      = S.numNodes;
                        t.nodes         = static_cast<const NodeRecord*>(S.nodes);
+                       t.dipoles       = static_cast<const float4*>(S.dipoles);
                        t.tgtXYZH       = xyzh;
                        t.tgtM          = sorted + 3 * n;
                        t.srcXYZM       = static_cast<const float4*>(S.xyzm);

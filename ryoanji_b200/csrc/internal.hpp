@@ -53,6 +53,7 @@ struct ryo_ctx
         const void* nodes  = nullptr; // NodeRecord per node
         const void* xyzm   = nullptr; // float4 per source body
         const float* srcH  = nullptr; // the caller's h array of the solve (sorted)
+        const void* dipoles = nullptr; // float4 per node for dipole expansions, else null
         int numNodes       = 0;
         unsigned groupSize = 64;
         float G            = 1.f;
@@ -184,7 +185,8 @@ void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int num
                         const int* leafToInternal, const int* childOffsets, const int* parents,
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
                         float4* centers, float* multipoles, double* rootCenterMultipole, cudaStream_t s,
-                        const DevBox<float>* sysBoxes = nullptr, int sysLevel = 0, double* sysRoots = nullptr);
+                        const DevBox<float>* sysBoxes = nullptr, int sysLevel = 0, double* sysRoots = nullptr,
+                        float4* dipoles = nullptr);
 
 //! pack reference-layout tree arrays into node records (for the reference-signature traverse)
 void launchPackNodes(int numNodes, const float4* centers, const float* multipoles, const int* childOffsets,
@@ -227,6 +229,10 @@ struct TraverseLaunch
     uint32_t failedCapacity;
     int stackCapacity;
     Control* ctl;
+    // monopole + dipole + quadrupole expansions: node dipoles beside the records (packed form), or 12-float
+    // multipoles in the reference form
+    const float4* dipoles;
+    int mdqArrays;
     // batched systems (all optional): the system of every group, per-system traversal parameters and potentials
     const uint32_t* groupSys;
     const struct SysTrav* systems;

@@ -43,7 +43,7 @@ struct WarpSmem
     int2 leaves[kLeafCap + kWarp];
     int leafScan[kLeafCap + kWarp];
     // staged sources, every value duplicated: M2P 5 x 16 bytes per cell, P2P 2 x 16 + 8 bytes per body
-    float4 stage[5 * kWarp];
+    float4 stage[7 * kWarp]; // M2P of dipole expansions stages 7 float4 per cell
     // per lane: Kahan running sums [0] and compensations [1] of (-phi, ax, ay, az), both targets packed
     unsigned long long sums[2][4][kWarp];
 };
@@ -141,6 +141,34 @@ __device__ __forceinline__ void m2p2(Acc2& A, f2 tx, f2 ty, f2 tz, f2 cx, f2 cy,
     A.z    = fma2(rm5, Qrz, fma2(f, rz, A.z));
 }
 
+/*! M2P of a monopole + dipole + quadrupole expansion (cartesian_qpole.hpp:305-343) for both targets: the
+ *  quadrupole terms of m2p2 plus the dipole p: -phi += (p.r) / r^3, a += p / r^3 - 3 (p.r) r / r^5 */
+__device__ __forceinline__ void m2p2mdq(Acc2& A, f2 tx, f2 ty, f2 tz, f2 cx, f2 cy, f2 cz, f2 m, f2 qxx, f2 qxy,
+                                        f2 qxz, f2 qyy, f2 qyz, f2 qzz, f2 px, f2 py, f2 pz)
+{
+    const f2 kM25  = 0xC0200000C0200000ull; // (-2.5f, -2.5f)
+    const f2 kHalf = 0x3F0000003F000000ull; // (0.5f, 0.5f)
+    const f2 kM3   = 0xC0400000C0400000ull; // (-3f, -3f)
+    f2 rx  = sub2(tx, cx), ry = sub2(ty, cy), rz = sub2(tz, cz);
+    f2 r2  = fma2(rx, rx, fma2(ry, ry, mul2(rz, rz)));
+    f2 rm1 = rsqrt2(r2);
+    f2 rm2 = mul2(rm1, rm1);
+    f2 rm3 = mul2(rm2, rm1);
+    f2 rm5 = mul2(rm3, rm2);
+    f2 Qrx = fma2(rx, qxx, fma2(ry, qxy, mul2(rz, qxz)));
+    f2 Qry = fma2(rx, qxy, fma2(ry, qyy, mul2(rz, qyz)));
+    f2 Qrz = fma2(rx, qxz, fma2(ry, qyz, mul2(rz, qzz)));
+    f2 rQr = fma2(rx, Qrx, fma2(ry, Qry, mul2(rz, Qrz)));
+    f2 PR  = fma2(rx, px, fma2(ry, py, mul2(rz, pz)));
+    f2 mr1 = mul2(m, rm1);
+    f2 t   = mul2(rQr, rm5);
+    f2 f   = fma2(mul2(kM3, PR), rm5, mul2(sub2(mul2(t, kM25), mr1), rm2));
+    A.p    = add2(A.p, fma2(PR, rm3, fma2(t, kHalf, mr1)));
+    A.x    = fma2(rm5, Qrx, fma2(f, rx, fma2(px, rm3, A.x)));
+    A.y    = fma2(rm5, Qry, fma2(f, ry, fma2(py, rm3, A.y)));
+    A.z    = fma2(rm5, Qrz, fma2(f, rz, fma2(pz, rm3, A.z)));
+}
+
 /*! P2P with a softening floor hh = (h_i + h_j)^2 common to both targets and the source: the same arithmetic as
  *  p2p2 when every h is equal, without the two packed operations that form hh */
 __device__ __forceinline__ void p2p2u(Acc2& A, f2 tx, f2 ty, f2 tz, float hh, f2 sx, f2 sy, f2 sz, f2 sm)
@@ -200,13 +228,14 @@ __device__ __forceinline__ Acc2 zero2()
 //! node data from the packed 64-byte records of the solver path
 struct RecordNodes
 {
+    static constexpr bool kDipole = false;
     const NodeRecord* __restrict__ r;
     __device__ __forceinline__ void load(int cell, float4& c, int4& link) const
     {
         c    = __ldg(&r[cell].center);
         link = __ldg(&r[cell].link);
     }
-    __device__ __forceinline__ void multipole(int cell, float4& c, float4& q0, float4& q1) const
+    __device__ __forceinline__ void multipole(int cell, float4& c, float4& q0, float4& q1, float4& dp) const
     {
         c  = __ldg(&r[cell].center);
         q0 = __ldg(&r[cell].q0);
@@ -214,11 +243,24 @@ struct RecordNodes
     }
 };
 
+//! the records plus node dipoles: monopole + dipole + quadrupole expansions (CartesianMDQpole)
+struct RecordNodesMDQ : RecordNodes
+{
+    static constexpr bool kDipole = true;
+    const float4* __restrict__ dip;
+    __device__ __forceinline__ void multipole(int cell, float4& c, float4& q0, float4& q1, float4& dp) const
+    {
+        RecordNodes::multipole(cell, c, q0, q1, dp);
+        dp = __ldg(dip + cell);
+    }
+};
+
 //! node data from the reference's separate arrays (centres, multipoles, childOffsets, internalToLeaf, layout)
 struct ArrayNodes
 {
+    static constexpr bool kDipole = false;
     const float4* __restrict__ centers;
-    const float4* __restrict__ mpoles; // two float4 per node
+    const float4* __restrict__ mpoles; // two float4 per node (three for CartesianMDQpole)
     const int* __restrict__ childOffsets;
     const int* __restrict__ internalToLeaf;
     const uint32_t* __restrict__ layout;
@@ -235,11 +277,24 @@ struct ArrayNodes
             link.z     = int(b - a);
         }
     }
-    __device__ __forceinline__ void multipole(int cell, float4& c, float4& q0, float4& q1) const
+    __device__ __forceinline__ void multipole(int cell, float4& c, float4& q0, float4& q1, float4& dp) const
     {
         c  = __ldg(centers + cell);
         q0 = __ldg(mpoles + 2 * cell);
         q1 = __ldg(mpoles + 2 * cell + 1);
+    }
+};
+
+//! the reference's CartesianMDQpole arrays: 12 floats per node (mass, q x6, trace, px, py, pz, unused)
+struct ArrayNodesMDQ : ArrayNodes
+{
+    static constexpr bool kDipole = true;
+    __device__ __forceinline__ void multipole(int cell, float4& c, float4& q0, float4& q1, float4& dp) const
+    {
+        c  = __ldg(centers + cell);
+        q0 = __ldg(mpoles + 3 * cell);
+        q1 = __ldg(mpoles + 3 * cell + 1);
+        dp = __ldg(mpoles + 3 * cell + 2);
     }
 };
 
@@ -295,25 +350,38 @@ __device__ __forceinline__ void addBatchS(WarpSmem& S, const Acc2& part)
 template<class Nodes>
 __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState& T)
 {
+    constexpr int kStride = Nodes::kDipole ? 7 : 5; // staged float4 per cell
     int lane = laneId();
     if (lane < count)
     {
-        float4 c, q0, q1;
-        nodes.multipole(S.m2p[lane], c, q0, q1);
-        float4* st = S.stage + 5 * lane;
+        float4 c, q0, q1, dp = make_float4(0.f, 0.f, 0.f, 0.f);
+        nodes.multipole(S.m2p[lane], c, q0, q1, dp);
+        float4* st = S.stage + kStride * lane;
         st[0]      = make_float4(c.x, c.x, c.y, c.y);
         st[1]      = make_float4(c.z, c.z, q0.x, q0.x);
         st[2]      = make_float4(q0.y, q0.y, q0.z, q0.z);
         st[3]      = make_float4(q0.w, q0.w, q1.x, q1.x);
         st[4]      = make_float4(q1.y, q1.y, q1.z, q1.z);
+        if (Nodes::kDipole)
+        {
+            st[5 % kStride] = make_float4(dp.x, dp.x, dp.y, dp.y);
+            st[6 % kStride] = make_float4(dp.z, dp.z, 0.f, 0.f);
+        }
     }
     __syncwarp();
     const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
     Acc2 pa = zero2(), pb = zero2();
     auto one = [&](Acc2& part, int j)
     {
-        ulonglong2 a = st[5 * j], b = st[5 * j + 1], c = st[5 * j + 2], d = st[5 * j + 3], e = st[5 * j + 4];
-        m2p2(part, T.tx, T.ty, T.tz, a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y);
+        const ulonglong2* sj = st + kStride * j;
+        ulonglong2 a = sj[0], b = sj[1], c = sj[2], d = sj[3], e = sj[4];
+        if constexpr (Nodes::kDipole)
+        {
+            ulonglong2 f = sj[5 % kStride], g = sj[6 % kStride];
+            m2p2mdq(part, T.tx, T.ty, T.tz, a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y, f.x, f.y, g.x);
+        }
+        else
+            m2p2(part, T.tx, T.ty, T.tz, a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y);
     };
     if (count == kWarp)
     {
@@ -726,16 +794,30 @@ void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s)
     if (t.numGroups <= 0) return;
     if (t.nodes)
     {
-        RecordNodes nodes{t.nodes};
         PackedBodies tgt{t.tgtXYZH, t.tgtM}, src{t.srcXYZM, t.srcH};
-        launchTyped(t, nodes, tgt, src, smCount, s);
+        if (t.dipoles)
+        {
+            RecordNodesMDQ nodes;
+            nodes.r   = t.nodes;
+            nodes.dip = t.dipoles;
+            launchTyped(t, nodes, tgt, src, smCount, s);
+        }
+        else
+            launchTyped(t, RecordNodes{t.nodes}, tgt, src, smCount, s);
     }
     else
     {
         ArrayNodes nodes{t.centers, reinterpret_cast<const float4*>(t.multipoles), t.childOffsets, t.internalToLeaf,
                          t.layout};
         SoABodies tgt{t.xt, t.yt, t.zt, t.ht, t.mt}, src{t.xs, t.ys, t.zs, t.ms, t.hs};
-        launchTyped(t, nodes, tgt, src, smCount, s);
+        if (t.mdqArrays)
+        {
+            ArrayNodesMDQ mdq;
+            static_cast<ArrayNodes&>(mdq) = nodes;
+            launchTyped(t, mdq, tgt, src, smCount, s);
+        }
+        else
+            launchTyped(t, nodes, tgt, src, smCount, s);
     }
 }
 

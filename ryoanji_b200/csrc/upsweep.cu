@@ -221,10 +221,12 @@ struct alignas(128) DNode
     double w;    // sum |m|
     double m;    // sum m
     double q[6]; // second moments about c: xx, xy, xz, yy, yz, zz
-    double pad[5];
+    double p[3]; // dipole about c: sum m (x - c) (zero for positive masses; kept for signed ones)
+    double pad[2];
 };
 
-__device__ inline void storeDNode(DNode* d, const double c[3], double w, double m, const double q[6])
+__device__ inline void storeDNode(DNode* d, const double c[3], double w, double m, const double q[6],
+                                  const double dp[3])
 {
     double2* p = reinterpret_cast<double2*>(d);
     __stcg(p + 0, make_double2(c[0], c[1]));
@@ -232,14 +234,18 @@ __device__ inline void storeDNode(DNode* d, const double c[3], double w, double 
     __stcg(p + 2, make_double2(m, q[0]));
     __stcg(p + 3, make_double2(q[1], q[2]));
     __stcg(p + 4, make_double2(q[3], q[4]));
-    __stcg(p + 5, make_double2(q[5], 0.0));
+    __stcg(p + 5, make_double2(q[5], dp[0]));
+    __stcg(p + 6, make_double2(dp[1], dp[2]));
 }
 
-__device__ inline void loadDNode(const DNode* d, double c[3], double& w, double& m, double q[6])
+__device__ inline void loadDNode(const DNode* d, double c[3], double& w, double& m, double q[6], double dp[3])
 {
     const double2* p = reinterpret_cast<const double2*>(d);
     double2 a = __ldcg(p + 0), b = __ldcg(p + 1), e = __ldcg(p + 2), f = __ldcg(p + 3), g = __ldcg(p + 4),
-            k = __ldcg(p + 5);
+            k = __ldcg(p + 5), l = __ldcg(p + 6);
+    dp[0] = k.y;
+    dp[1] = l.x;
+    dp[2] = l.y;
     c[0] = a.x;
     c[1] = a.y;
     c[2] = b.x;
@@ -276,6 +282,9 @@ struct FusedArgs
     const DevBox<float>* sysBoxes;
     int sysLevel;
     double* sysRoots;
+    // monopole + dipole + quadrupole expansions: node dipoles (px, py, pz, 0) are written here when not null, and
+    // the second moments are combined with the dipole terms of the parallel-axis theorem
+    float4* dipoles;
 };
 
 //! FP64 centre and finalized quadrupole (11 doubles) of a node, as the Ewald setup reads them
@@ -297,8 +306,9 @@ __device__ inline void writeRootExpansion(double* out, const double c[3], const 
 
 //! write the float outputs of a finished node
 __device__ void emitNode(const FusedArgs& A, int node, const double c[3], double w, double m, const double q[6],
-                         int child, uint32_t firstBody, uint32_t count)
+                         const double dp[3], int child, uint32_t firstBody, uint32_t count)
 {
+    if (A.dipoles) A.dipoles[node] = make_float4(float(dp[0]), float(dp[1]), float(dp[2]), 0.f);
     float com[3] = {float(c[0]), float(c[1]), float(c[2])};
     double raw[7] = {m, q[0], q[1], q[2], q[3], q[4], q[5]};
     float mac     = 0.f;
@@ -352,8 +362,8 @@ __device__ __forceinline__ double groupSum8(double v, unsigned gmask)
 //! combine the eight children of @p node (parallel-axis theorem, double): lane @p sub of the group holds child sub
 __device__ void combineChildren(const FusedArgs& A, int node, int fc, int sub, unsigned gmask)
 {
-    double cc[3], cw, cm, cq[6];
-    loadDNode(A.dn + fc + sub, cc, cw, cm, cq);
+    double cc[3], cw, cm, cq[6], cp[3];
+    loadDNode(A.dn + fc + sub, cc, cw, cm, cq, cp);
     double w  = fabs(cw);
     double W  = groupSum8(w, gmask);
     double M  = groupSum8(cm, gmask);
@@ -366,17 +376,24 @@ __device__ void combineChildren(const FusedArgs& A, int node, int fc, int sub, u
     c[1]       = sy * inv;
     c[2]       = sz * inv;
     double dx = cc[0] - c[0], dy = cc[1] - c[1], dz = cc[2] - c[2];
-    double q[6];
-    q[0] = groupSum8(cq[0] + cm * dx * dx, gmask);
-    q[1] = groupSum8(cq[1] + cm * dx * dy, gmask);
-    q[2] = groupSum8(cq[2] + cm * dx * dz, gmask);
-    q[3] = groupSum8(cq[3] + cm * dy * dy, gmask);
-    q[4] = groupSum8(cq[4] + cm * dy * dz, gmask);
-    q[5] = groupSum8(cq[5] + cm * dz * dz, gmask);
+    // dipole about the parent centre; the quadrupole-only expansion drops the dipole terms, as the reference's
+    // 8-value M2M does (they vanish for positive masses)
+    double px = cp[0], py = cp[1], pz = cp[2];
+    if (!A.dipoles) px = py = pz = 0.0;
+    double q[6], dp[3];
+    q[0]  = groupSum8(cq[0] + cm * dx * dx + 2 * dx * px, gmask);
+    q[1]  = groupSum8(cq[1] + cm * dx * dy + dx * py + dy * px, gmask);
+    q[2]  = groupSum8(cq[2] + cm * dx * dz + dx * pz + dz * px, gmask);
+    q[3]  = groupSum8(cq[3] + cm * dy * dy + 2 * dy * py, gmask);
+    q[4]  = groupSum8(cq[4] + cm * dy * dz + dy * pz + dz * py, gmask);
+    q[5]  = groupSum8(cq[5] + cm * dz * dz + 2 * dz * pz, gmask);
+    dp[0] = groupSum8(cp[0] + cm * dx, gmask);
+    dp[1] = groupSum8(cp[1] + cm * dy, gmask);
+    dp[2] = groupSum8(cp[2] + cm * dz, gmask);
     if (sub == 0)
     {
-        storeDNode(A.dn + node, c, W, M, q);
-        emitNode(A, node, c, W, M, q, fc, 0, 0);
+        storeDNode(A.dn + node, c, W, M, q, dp);
+        emitNode(A, node, c, W, M, q, dp, fc, 0, 0);
     }
 }
 
@@ -425,7 +442,7 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
 
     int node = A.leafToInternal[leaf];
     double W = s[0], M = s[4];
-    double c[3], q[6];
+    double c[3], q[6], dp[3];
     if (W != 0.0)
     {
         double inv = 1.0 / W;
@@ -440,6 +457,10 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
         q[3] = s[11] - 2 * ey * s[6] + M * ey * ey;
         q[4] = s[12] - ey * s[7] - ez * s[6] + M * ey * ez;
         q[5] = s[13] - 2 * ez * s[7] + M * ez * ez;
+        // sum m (d - e)
+        dp[0] = s[5] - M * ex;
+        dp[1] = s[6] - M * ey;
+        dp[2] = s[7] - M * ez;
     }
     else
     {
@@ -452,11 +473,14 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
         q[3] = s[11] + 2 * oy * s[6] + M * oy * oy;
         q[4] = s[12] + oy * s[7] + oz * s[6] + M * oy * oz;
         q[5] = s[13] + 2 * oz * s[7] + M * oz * oz;
+        dp[0] = s[5] + M * ox;
+        dp[1] = s[6] + M * oy;
+        dp[2] = s[7] + M * oz;
     }
     if (sub == 0)
     {
-        storeDNode(A.dn + node, c, W, M, q);
-        emitNode(A, node, c, W, M, q, 0, b0, b1 - b0);
+        storeDNode(A.dn + node, c, W, M, q, dp);
+        emitNode(A, node, c, W, M, q, dp, 0, b0, b1 - b0);
     }
 
     // climb: the group of the eighth sibling to arrive combines the parent, one child per lane
@@ -482,9 +506,10 @@ void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int num
                         const int* leafToInternal, const int* childOffsets, const int* parents,
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
                         float4* centers, float* multipoles, double* root, cudaStream_t s,
-                        const DevBox<float>* sysBoxes, int sysLevel, double* sysRoots)
+                        const DevBox<float>* sysBoxes, int sysLevel, double* sysRoots, float4* dipoles)
 {
     FusedArgs A;
+    A.dipoles        = dipoles;
     A.sysBoxes       = sysBoxes;
     A.sysLevel       = sysLevel;
     A.sysRoots       = sysRoots;

@@ -254,3 +254,45 @@ def test_group_volumes_known_answers():
     tol = float(np.float32(np.sqrt(3.0) / dist_crit * 1.01))
     groups, _ = orc.group_splits(first, last, x, y, z, h, leaves, layout, box, 64, tol, 0.0)
     assert list(groups) == [4, 6, 68, 75, 128]
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# monopole + dipole + quadrupole expansions: restatement against the reference's own code (signed masses)
+
+@pytest.fixture(scope="module")
+def ref_oracle():
+    import pyoracle
+    if not pyoracle.have_reference():
+        pytest.skip("reference wrapper not built")
+    return pyoracle.Oracle(reference=True)
+
+
+def test_mdq_p2m_m2m_m2p_match_reference(oracle, ref_oracle):
+    rng = np.random.default_rng(21)
+    n = 160
+    x, y, z = (rng.uniform(0, 1, n) for _ in range(3))
+    m = rng.uniform(-0.5, 0.5, n)
+    c_o, q_o = oracle.mdq_p2m(x, y, z, m)
+    c_r, q_r = ref_oracle.mdq_p2m(x, y, z, m)
+    assert np.allclose(c_o, c_r, rtol=1e-13, atol=1e-15) and np.allclose(q_o, q_r, rtol=1e-12, atol=1e-14)
+    assert abs(q_r[8]) + abs(q_r[9]) + abs(q_r[10]) > 1e-3  # signed masses: a real dipole
+    # M2M of eight sub-expansions equals the direct expansion (cartesian_qpole.cpp:180-239)
+    cs, qs = [], []
+    for k in range(8):
+        sl = slice(20 * k, 20 * (k + 1))
+        c, q = ref_oracle.mdq_p2m(x[sl], y[sl], z[sl], m[sl])
+        cs.append(c)
+        qs.append(q)
+    comp_r = ref_oracle.mdq_m2m(np.array(cs), np.array(qs), c_r)
+    comp_o = oracle.mdq_m2m(np.array(cs), np.array(qs), c_r)
+    assert np.allclose(comp_o, comp_r, rtol=1e-12, atol=1e-14)
+    assert np.allclose(comp_r, q_r, rtol=1e-9, atol=1e-10)
+    for t in ([-8.0, 0.0, 0.0], [3.0, 2.5, -4.0]):
+        a_o = oracle.mdq_m2p(t, c_r, q_r)
+        a_r = ref_oracle.mdq_m2p(t, c_r, q_r)
+        assert np.allclose(a_o, a_r, rtol=1e-13, atol=1e-16)
+        # and approximates the direct sum (cartesian_qpole.cpp:130-172)
+        d = np.array([x - t[0], y - t[1], z - t[2]])
+        r = np.sqrt((d * d).sum(0))
+        direct = np.array([-(m / r).sum(), *(m * d / r ** 3).sum(1)])
+        assert np.allclose(a_r, direct, atol=1e-3)
