@@ -183,6 +183,15 @@ extern "C"
     RYO_API ryo_status ryo_upsweep_multipoles_f32(int firstCell, int lastCell, const int* childOffsets,
                                                   const float* centers, float* multipoles, ryo_stream_t stream);
     /* cstone::setMacGpu (source_center_gpu.h:104-116): centers[i][3] = squared vector-MAC radius, 0 if massless */
+    /* the same two steps for CartesianMDQpole (INSTANTIATE_MULTIPOLE(CartesianMDQpole), upsweep_gpu.cu:143):
+     * 12 floats per node (mass, qxx, qxy, qxz, qyy, qyz, qzz, trace, px, py, pz, 0), FP64 sums */
+    RYO_API ryo_status ryo_compute_leaf_multipoles_mdq_f32(const float* x, const float* y, const float* z,
+                                                           const float* m, const int* leafToInternal, int numLeaves,
+                                                           const uint32_t* layout, const float* centers,
+                                                           float* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_upsweep_multipoles_mdq_f32(int firstCell, int lastCell, const int* childOffsets,
+                                                      const float* centers, float* multipoles, ryo_stream_t stream);
+
     RYO_API ryo_status ryo_set_mac_f32(const uint64_t* prefixes, int numNodes, float* centers, float invTheta,
                                        const ryo_box_f32* box, ryo_stream_t stream);
 
@@ -214,6 +223,8 @@ extern "C"
         uint32_t* groupM2P; /* device, numGroups entries (may be NULL): approximated cells per group */
         uint32_t* groupP2P; /* device, numGroups entries (may be NULL): directly summed source bodies per group */
         int stackCapacity;  /* traversal stack entries per warp, 0 = default (1024); small values force splits */
+        int multipole;      /* RYO_MULTIPOLE_QUADRUPOLE: 8 floats per node in multipoles (default);
+                               RYO_MULTIPOLE_MDQ: 12 floats per node (CartesianMDQpole, traversal_gpu.cu:641) */
     } ryo_traverse_options;
 
     RYO_API ryo_status ryo_traverse_ex_f32(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx,

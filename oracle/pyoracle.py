@@ -124,6 +124,19 @@ class Oracle:
                                    _ptr(mp))
         return centers, mp
 
+    def upsweep_mdq(self, x, y, z, m, layout, tree, theta, box6):
+        """the reference CPU upsweep with CartesianMDQpole multipoles (12 floats per node)"""
+        assert self.reference
+        nn = tree["numNodes"]
+        centers = np.zeros((nn, 4), np.float32)
+        mp = np.zeros((nn, 12), np.float32)
+        l2i = np.ascontiguousarray(tree["leafToInternal"][tree["numInternal"]:])
+        self._f("upsweep_mdq_f32")(_ptr(x), _ptr(y), _ptr(z), _ptr(m), _sz(len(x)), C.c_int(tree["numLeaves"]),
+                                   _ptr(layout), _ptr(l2i), _ptr(tree["childOffsets"]), _ptr(tree["levelRange"]),
+                                   _ptr(tree["prefixes"]), C.c_int(nn), C.c_float(theta),
+                                   _ptr(np.asarray(box6, np.float32)), _ptr(centers), _ptr(mp))
+        return centers, mp
+
     # ---- gravity
     def gravity_cpu(self, tree, centers, mp, layout, x, y, z, h, m, box6, G=1.0, numShells=0, periodic=False):
         n = len(x)

@@ -272,15 +272,18 @@ def upsweep_centers(num_levels: int, level_range, child_offsets, centers, stream
     _check(lib.ryo_upsweep_centers_f32(num_levels, lr, _ptr(child_offsets), _ptr(centers), _stream(stream)))
 
 
-def compute_leaf_multipoles(x, y, z, m, leaf_to_internal, layout, centers, multipoles, stream=None):
+def compute_leaf_multipoles(x, y, z, m, leaf_to_internal, layout, centers, multipoles, stream=None, mdq=False):
+    """ryoanji::computeLeafMultipoles: 8 floats per node, or 12 with mdq (CartesianMDQpole)"""
     nl = leaf_to_internal.numel()
-    _check(lib.ryo_compute_leaf_multipoles_f32(_ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(leaf_to_internal), nl,
-                                               _ptr(layout), _ptr(centers), _ptr(multipoles), _stream(stream)))
+    fn = lib.ryo_compute_leaf_multipoles_mdq_f32 if mdq else lib.ryo_compute_leaf_multipoles_f32
+    _check(fn(_ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(leaf_to_internal), nl, _ptr(layout), _ptr(centers),
+              _ptr(multipoles), _stream(stream)))
 
 
-def upsweep_multipoles(first_cell: int, last_cell: int, child_offsets, centers, multipoles, stream=None):
-    _check(lib.ryo_upsweep_multipoles_f32(first_cell, last_cell, _ptr(child_offsets), _ptr(centers),
-                                          _ptr(multipoles), _stream(stream)))
+def upsweep_multipoles(first_cell: int, last_cell: int, child_offsets, centers, multipoles, stream=None, mdq=False):
+    """ryoanji::upsweepMultipoles for the cells [first_cell, last_cell) of one level"""
+    fn = lib.ryo_upsweep_multipoles_mdq_f32 if mdq else lib.ryo_upsweep_multipoles_f32
+    _check(fn(first_cell, last_cell, _ptr(child_offsets), _ptr(centers), _ptr(multipoles), _stream(stream)))
 
 
 def set_mac(prefixes, centers, inv_theta: float, box: Box, stream=None):
@@ -302,7 +305,7 @@ def stack_size(num_groups: int) -> int:
 def traverse(groups: torch.Tensor, init_node: int, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, child_offsets,
              internal_to_leaf, layout, source_center, multipoles, G: float, num_shells: int, box_l, p, ax, ay, az,
              ctx: Context | None = None, stack_capacity: int = 0, group_counts: bool = False, first_body: int = 0,
-             last_body: int | None = None, stream=None):
+             last_body: int | None = None, stream=None, mdq: bool = False):
     """ryoanji::traverse: accumulates G m phi into p (may be None) and G a into ax, ay, az.
 
     ``groups`` holds numGroups + 1 boundaries (computeFixedGroups layout). Returns the total potential
@@ -313,6 +316,7 @@ def traverse(groups: torch.Tensor, init_node: int, xt, yt, zt, mt, ht, xs, ys, z
     gv = _abi.GroupView(first_body, last_body if last_body is not None else xt.numel(), ng,
                         C.c_void_p(groups.data_ptr()), C.c_void_p(groups.data_ptr() + 4))
     opts = _abi.TraverseOptions()
+    opts.multipole = _abi.MULTIPOLE_MDQ if mdq else _abi.MULTIPOLE_QUADRUPOLE
     m2p = p2p = None
     if group_counts:
         m2p = torch.zeros(ng, dtype=torch.int32, device=groups.device)

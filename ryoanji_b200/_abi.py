@@ -44,7 +44,7 @@ class EwaldSettings(C.Structure):
 
 
 class TraverseOptions(C.Structure):
-    _fields_ = [("groupM2P", C.c_void_p), ("groupP2P", C.c_void_p), ("stackCapacity", C.c_int)]
+    _fields_ = [("groupM2P", C.c_void_p), ("groupP2P", C.c_void_p), ("stackCapacity", C.c_int), ("multipole", C.c_int)]
 
 
 class TreeView(C.Structure):
@@ -136,6 +136,8 @@ SIGNATURES = {
     "ryo_upsweep_centers_f32": (_i, [_i, C.POINTER(_i), _p, _p, _p]),
     "ryo_compute_leaf_multipoles_f32": (_i, [_p, _p, _p, _p, _p, _i, _p, _p, _p, _p]),
     "ryo_upsweep_multipoles_f32": (_i, [_i, _i, _p, _p, _p, _p]),
+    "ryo_compute_leaf_multipoles_mdq_f32": (_i, [_p] * 5 + [_i] + [_p] * 4),
+    "ryo_upsweep_multipoles_mdq_f32": (_i, [_i, _i] + [_p] * 4),
     "ryo_set_mac_f32": (_i, [_p, _i, _p, _f, C.POINTER(BoxF32), _p]),
     "ryo_bh_max_target_size": (_i, []),
     "ryo_stack_size": (_u32, [_u32]),

@@ -386,6 +386,30 @@ extern "C" ryo_status ryo_upsweep_multipoles_f32(int firstCell, int lastCell, co
                    });
 }
 
+extern "C" ryo_status ryo_compute_leaf_multipoles_mdq_f32(const float* x, const float* y, const float* z,
+                                                          const float* m, const int* leafToInternal, int numLeaves,
+                                                          const uint32_t* layout, const float* centers,
+                                                          float* multipoles, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       launchLeafMultipolesMDQ(x, y, z, m, leafToInternal, numLeaves, layout,
+                                               reinterpret_cast<const float4*>(centers), multipoles, stream);
+                   });
+}
+
+extern "C" ryo_status ryo_upsweep_multipoles_mdq_f32(int firstCell, int lastCell, const int* childOffsets,
+                                                     const float* centers, float* multipoles, ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       launchUpsweepMultipolesMDQ(firstCell, lastCell, childOffsets,
+                                                  reinterpret_cast<const float4*>(centers), multipoles, stream);
+                   });
+}
+
 extern "C" ryo_status ryo_set_mac_f32(const uint64_t* prefixes, int numNodes, float* centers, float invTheta,
                                       const ryo_box_f32* box, ryo_stream_t stream)
 {
@@ -545,6 +569,7 @@ extern "C" ryo_status ryo_traverse_ex_f32(ryo_ctx_t* ctx, const ryo_group_view* 
                        t.groupM2P      = options ? options->groupM2P : nullptr;
                        t.groupP2P      = options ? options->groupP2P : nullptr;
                        t.stackCapacity = options ? options->stackCapacity : 0;
+                       t.mdqArrays     = options && options->multipole == RYO_MULTIPOLE_MDQ ? 1 : 0;
                        double pot      = 0;
                        runTraversal(ctx, t, stream, &pot);
                        if (totalPotential) *totalPotential = 0.5 * double(G) * pot;

@@ -166,6 +166,11 @@ void launchLeafMultipoles(const float* x, const float* y, const float* z, const 
                           cudaStream_t s);
 void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const float4* centers, float* multipoles,
                              cudaStream_t s);
+void launchLeafMultipolesMDQ(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
+                             int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
+                             cudaStream_t s);
+void launchUpsweepMultipolesMDQ(int first, int last, const int* childOffsets, const float4* centers,
+                                float* multipoles, cudaStream_t s);
 void launchSetMac(const uint64_t* prefixes, int numNodes, float4* centers, float invTheta, const DevBox<float>& box,
                   cudaStream_t s);
 

@@ -157,6 +157,88 @@ __global__ void upsweepMultipolesKernel(int first, int last, const int* __restri
         o[k] = float(acc[k]);
 }
 
+//! leaf CartesianMDQpole expansions (P2M_add / P2M_finalize, cartesian_qpole.hpp:237-303), double sums
+__global__ void leafMultipolesMDQKernel(const float* __restrict__ x, const float* __restrict__ y,
+                                        const float* __restrict__ z, const float* __restrict__ m,
+                                        const int* __restrict__ leafToInternal, int numLeaves,
+                                        const uint32_t* __restrict__ layout, const float4* __restrict__ centers,
+                                        float* __restrict__ multipoles)
+{
+    int tid  = blockIdx.x * blockDim.x + threadIdx.x;
+    int leaf = tid / kTpl;
+    double q[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0}; // mass, xx, xy, xz, yy, yz, zz, px, py, pz
+    int node     = 0;
+    if (leaf < numLeaves)
+    {
+        node     = leafToInternal[leaf];
+        float4 c = centers[node];
+        for (uint32_t i = layout[leaf] + tid % kTpl; i < layout[leaf + 1]; i += kTpl)
+        {
+            double rx = double(x[i]) - c.x, ry = double(y[i]) - c.y, rz = double(z[i]) - c.z, mi = m[i];
+            q[0] += mi;
+            q[1] += rx * rx * mi;
+            q[2] += rx * ry * mi;
+            q[3] += rx * rz * mi;
+            q[4] += ry * ry * mi;
+            q[5] += ry * rz * mi;
+            q[6] += rz * rz * mi;
+            q[7] += mi * rx;
+            q[8] += mi * ry;
+            q[9] += mi * rz;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k)
+        q[k] = groupSum8(q[k]);
+    if (leaf < numLeaves && tid % kTpl == 0)
+    {
+        float* o = multipoles + 12 * size_t(node);
+        finalizeQuad(q, o);
+        o[8]  = float(q[7]);
+        o[9]  = float(q[8]);
+        o[10] = float(q[9]);
+        o[11] = 0.f;
+    }
+}
+
+//! M2M of CartesianMDQpole cells [first, last) from their eight children (addQuadrupole, cartesian_qpole.hpp:352-418)
+__global__ void upsweepMultipolesMDQKernel(int first, int last, const int* __restrict__ childOffsets,
+                                           const float4* __restrict__ centers, float* multipoles)
+{
+    int i = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= last) return;
+    int fc = childOffsets[i];
+    if (!fc) return;
+    float4 cp = centers[i];
+    double acc[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = fc; k < fc + 8; ++k)
+    {
+        float4 ck      = centers[k];
+        const float* a = multipoles + 12 * size_t(k);
+        double rx = double(cp.x) - ck.x, ry = double(cp.y) - ck.y, rz = double(cp.z) - ck.z;
+        double r2  = (rx * rx + ry * ry + rz * rz) * (1.0 / 3.0);
+        double ml  = double(a[0]) * 3;
+        double px = a[8], py = a[9], pz = a[10];
+        double dip = rx * px + ry * py + rz * pz;
+        acc[7] += a[7] + ml * r2 - 2.0 * dip;
+        acc[0] += a[0];
+        acc[8] += px - double(a[0]) * rx;
+        acc[9] += py - double(a[0]) * ry;
+        acc[10] += pz - double(a[0]) * rz;
+        acc[1] += a[1] + ml * (rx * rx - r2) - 6.0 * rx * px + 2.0 * dip;
+        acc[2] += a[2] + ml * rx * ry - 3.0 * (rx * py + ry * px);
+        acc[3] += a[3] + ml * rx * rz - 3.0 * (rx * pz + rz * px);
+        acc[4] += a[4] + ml * (ry * ry - r2) - 6.0 * ry * py + 2.0 * dip;
+        acc[5] += a[5] + ml * ry * rz - 3.0 * (ry * pz + rz * py);
+        acc[6] += a[6] + ml * (rz * rz - r2) - 6.0 * rz * pz + 2.0 * dip;
+    }
+    float* o = multipoles + 12 * size_t(i);
+#pragma unroll
+    for (int k = 0; k < 11; ++k)
+        o[k] = float(acc[k]);
+    o[11] = 0.f;
+}
+
 __global__ void setMacKernel(const uint64_t* __restrict__ prefixes, int numNodes, float4* centers, float invTheta,
                              DevBox<float> box)
 {
@@ -201,6 +283,26 @@ void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const
     if (last <= first) return;
     upsweepMultipolesKernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets, centers,
                                                                        multipoles);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchLeafMultipolesMDQ(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
+                             int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
+                             cudaStream_t s)
+{
+    if (numLeaves <= 0) return;
+    leafMultipolesMDQKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(x, y, z, m, leafToInternal,
+                                                                                  numLeaves, layout, centers,
+                                                                                  multipoles);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchUpsweepMultipolesMDQ(int first, int last, const int* childOffsets, const float4* centers,
+                                float* multipoles, cudaStream_t s)
+{
+    if (last <= first) return;
+    upsweepMultipolesMDQKernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets, centers,
+                                                                          multipoles);
     RYO_LAUNCH_CHECK();
 }
 

@@ -100,3 +100,64 @@ def test_positive_masses_and_interaction_lists():
     a_m = torch.stack(om[1:], 1)
     rel = (torch.linalg.norm(a_q - a_m, dim=1) / torch.linalg.norm(a_q, dim=1)).max()
     assert float(rel) < 2e-5, float(rel)
+
+
+def test_step_flow_matches_reference_cpu_upsweep_and_direct_sums(ref_oracle_or_skip):
+    """TreeBuilder + the individual steps with 12-float multipoles, then traverse(mdq=True): moments against the
+    reference's own CPU upsweep of the same tree, forces against the FP64 direct sum"""
+    import ryoanji_b200 as ryo
+    ref = ref_oracle_or_skip
+    p = _signed_gaussian(40000, 34)
+    box = ryo.Box.cube(-1.0, 1.0)
+    x, y, z, m, h = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (p.x, p.y, p.z, p.m, p.h))
+    tb = ryo.TreeBuilder(64)
+    nn = tb.update(x, y, z, box)
+    order = tb.order().long()
+    m, h = m[order].contiguous(), h[order].contiguous()
+    centers = torch.zeros(nn, 4, device="cuda")
+    mp = torch.zeros(nn, 12, device="cuda")
+    ryo.compute_leaf_source_center(x, y, z, m, tb.leafToInternal(), tb.layout(), centers)
+    ryo.upsweep_centers(tb.maxTreeLevel, tb.levelRange, tb.childOffsets(), centers)
+    ryo.compute_leaf_multipoles(x, y, z, m, tb.leafToInternal(), tb.layout(), centers, mp, mdq=True)
+    lr = tb.levelRange
+    for level in range(tb.maxTreeLevel - 1, -1, -1):
+        ryo.upsweep_multipoles(lr[level], lr[level + 1], tb.childOffsets(), centers, mp, mdq=True)
+    ryo.set_mac(tb.nodeKeys(), centers, 1.0 / 0.2, box)
+
+    host = lambda t: np.ascontiguousarray(t.cpu().numpy())  # noqa: E731
+    nl = tb.numLeafNodes
+    ni = (nl - 1) // 7
+    tree = dict(numNodes=nn, numLeaves=nl, numInternal=ni, childOffsets=host(tb.childOffsets()),
+                levelRange=np.asarray(tb.levelRange, np.int32), prefixes=host(tb.nodeKeys()).view(np.uint64),
+                leafToInternal=np.concatenate([np.zeros(ni, np.int32), host(tb.leafToInternal())]))
+    layout = host(tb.layout()).view(np.uint32)
+    xs, ys, zs, ms = (host(t) for t in (x, y, z, m))
+    c_ref, mp_ref = ref.upsweep_mdq(xs, ys, zs, ms, layout, tree, 0.2, [-1, 1, -1, 1, -1, 1])
+    got = host(mp)
+    w = np.abs(ms).sum()
+    scale = np.array([w] + [3 * w * 4.0] * 7 + [w * 2.0] * 3 + [1.0])
+    # the reference sums in float, the steps in double: compare at float-accumulation level
+    assert np.all(np.abs(got - mp_ref) <= 1e-4 * scale + 1e-9), np.abs(got - mp_ref).max(0)
+
+    groups = ryo.compute_fixed_groups(0, p.n, 64)
+    pot, ax, ay, az = (torch.zeros(p.n, device="cuda") for _ in range(4))
+    ryo.traverse(groups, 1, x, y, z, m, h, x, y, z, m, h, tb.childOffsets(), tb.internalToLeaf(), tb.layout(),
+                 centers, mp, 1.0, 0, (0.0, 0.0, 0.0), pot, ax, ay, az, mdq=True)
+    tgt = torch.from_numpy(np.random.default_rng(4).choice(p.n, 4000, replace=False)).cuda()
+    _, rx, ry, rz = ryo.direct_targets_f64(tgt, x, y, z, m, h)
+    a = torch.stack([ax[tgt], ay[tgt], az[tgt]], 1).double()
+    r = torch.stack([rx, ry, rz], 1)
+    d = (torch.linalg.norm(a - r, dim=1) / torch.linalg.norm(r, dim=1)).cpu().numpy()
+    assert np.percentile(d, 99) < 3e-3 and d.max() < 3e-2, (np.percentile(d, 99), d.max())
+
+
+@pytest.fixture
+def ref_oracle_or_skip():
+    import sys
+    import os
+    from conftest import ROOT
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    if not pyoracle.have_reference():
+        pytest.skip("reference wrapper not built")
+    return pyoracle.Oracle(reference=True)
