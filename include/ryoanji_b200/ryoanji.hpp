@@ -156,6 +156,12 @@ struct Vec3
     T x, y, z;
 };
 
+//! the reference's multipole types (ryoanji/src/ryoanji/nbody/cartesian_qpole.hpp:24-48): float instantiations
+template<class T>
+using CartesianQuadrupole = std::array<T, 8>;
+template<class T>
+using CartesianMDQpole = std::array<T, 12>;
+
 //! ryoanji::TreeBuilder (ryoanji/src/ryoanji/interface/treebuilder.cuh:34-125); the returned pointers stay valid
 //! until the next update
 template<class KeyType>
@@ -272,11 +278,57 @@ inline void computeLeafMultipoles(const float* x, const float* y, const float* z
                                           stream));
 }
 
+//! ryoanji::computeLeafMultipoles with typed expansions (CartesianQuadrupole or CartesianMDQpole)
+inline void computeLeafMultipoles(const float* x, const float* y, const float* z, const float* m,
+                                  const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
+                                  const LocalIndex* layout, const float* centers,
+                                  CartesianQuadrupole<float>* multipoles, ryo_stream_t stream = nullptr)
+{
+    computeLeafMultipoles(x, y, z, m, leafToInternal, numLeaves, layout, centers, multipoles->data(), stream);
+}
+inline void computeLeafMultipoles(const float* x, const float* y, const float* z, const float* m,
+                                  const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
+                                  const LocalIndex* layout, const float* centers, CartesianMDQpole<float>* multipoles,
+                                  ryo_stream_t stream = nullptr)
+{
+    check(ryo_compute_leaf_multipoles_mdq_f32(x, y, z, m, leafToInternal, numLeaves, layout, centers,
+                                              multipoles->data(), stream));
+}
+
 //! ryoanji::upsweepMultipoles (upsweep_gpu.h:39-41) for cells [firstCell, lastCell) of one level
 inline void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
                               const float* centers, float* multipoles, ryo_stream_t stream = nullptr)
 {
     check(ryo_upsweep_multipoles_f32(firstCell, lastCell, childOffsets, centers, multipoles, stream));
+}
+
+inline void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
+                              const float* centers, CartesianQuadrupole<float>* multipoles,
+                              ryo_stream_t stream = nullptr)
+{
+    upsweepMultipoles(firstCell, lastCell, childOffsets, centers, multipoles->data(), stream);
+}
+inline void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
+                              const float* centers, CartesianMDQpole<float>* multipoles, ryo_stream_t stream = nullptr)
+{
+    check(ryo_upsweep_multipoles_mdq_f32(firstCell, lastCell, childOffsets, centers, multipoles->data(), stream));
+}
+
+/*! cstone::computeGroupSplits (groups_gpu.cu:60-151): spatial target groups of SFC-sorted bodies [first, last) into
+ *  @p groups (capacity entries, at least last - first + 1); returns the group count. extentRatio < 0: the default. */
+inline LocalIndex computeGroupSplits(LocalIndex first, LocalIndex last, const float* x, const float* y,
+                                     const float* z, const float* h, const uint64_t* leaves, TreeNodeIndex numLeaves,
+                                     const LocalIndex* layout, const Box<float>& box, unsigned groupSize,
+                                     float tolFactor, LocalIndex* groups, LocalIndex capacity,
+                                     float extentRatio = -1.f, Context& ctx = defaultContext(),
+                                     ryo_stream_t stream = nullptr)
+{
+    ryo_box_f32 b  = box.abiF32();
+    LocalIndex num = 0;
+    check(ryo_compute_group_splits_f32(ctx.get(), first, last, x, y, z, h, leaves, numLeaves, layout, &b, groupSize,
+                                       tolFactor, extentRatio, groups, capacity, &num, stream),
+          ctx.get());
+    return num;
 }
 
 inline int bhMaxTargetSize() { return ryo_bh_max_target_size(); }
@@ -300,6 +352,37 @@ inline double traverse(GroupView grp, int initNodeIdx, const float* xt, const fl
                            stream),
           ctx.get());
     return total;
+}
+
+//! ryoanji::traverse with CartesianMDQpole multipoles (TRAVERSE_MPOLE(CartesianMDQpole), traversal_gpu.cu:641)
+inline double traverse(GroupView grp, int initNodeIdx, const float* xt, const float* yt, const float* zt,
+                       const float* mt, const float* ht, const float* xs, const float* ys, const float* zs,
+                       const float* ms, const float* hs, const TreeNodeIndex* childOffsets,
+                       const TreeNodeIndex* internalToLeaf, const LocalIndex* layout, const float* sourceCenter,
+                       const CartesianMDQpole<float>* multipoles, float G, int numShells, Vec3<float> boxL, float* p,
+                       float* ax, float* ay, float* az, int* /* gmPool: unused */, Context& ctx = defaultContext(),
+                       ryo_stream_t stream = nullptr)
+{
+    ryo_group_view g = grp.abi();
+    float L[3]       = {boxL.x, boxL.y, boxL.z};
+    double total     = 0;
+    ryo_traverse_options opt{};
+    opt.multipole = RYO_MULTIPOLE_MDQ;
+    check(ryo_traverse_ex_f32(ctx.get(), &g, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
+                              internalToLeaf, layout, sourceCenter, multipoles->data(), G, numShells, L, p, ax, ay,
+                              az, &total, &opt, stream),
+          ctx.get());
+    return total;
+}
+
+/*! MultipoleHolder::compute with separate targets (multipole_holder.cuh:64-77) after a ryo_solve_f32 on @p ctx:
+ *  overwrites p (may be null), ax, ay, az in the targets' order */
+inline void computeTargets(const float* xt, const float* yt, const float* zt, const float* mt, const float* ht,
+                           size_t numTargets, float* p, float* ax, float* ay, float* az,
+                           Context& ctx = defaultContext(), ryo_stream_t stream = nullptr)
+{
+    check(ryo_solve_targets_f32(ctx.get(), xt, yt, zt, mt, ht, numTargets, p, ax, ay, az, nullptr, stream),
+          ctx.get());
 }
 
 //! ryoanji::readBhStats (traversal_gpu.h:64-65): sumP2P, maxP2P, sumM2P, maxM2P, maxStack
