@@ -339,7 +339,8 @@ extern "C"
         float groupTolerance;        /* > 0: spatial target groups (ryo_compute_group_splits_f32) with this
                                         tolFactor and no interaction radius (h is the softening here), groupSize
                                         32 or 64; 0: fixed groups, the reference demo's (0).
-                                        The batched solve and the engine always use fixed groups. */
+                                        The batched solve and the engine split each system's fixed windows
+                                        with that system's box. */
         float groupExtentRatio;      /* window-extent ratio of the spatial groups; < 0: the reference default (-1) */
         int multipole;               /* RYO_MULTIPOLE_QUADRUPOLE (CartesianQuadrupole, default) or
                                         RYO_MULTIPOLE_MDQ (CartesianMDQpole: adds the dipole, for signed masses) */
@@ -429,6 +430,8 @@ extern "C"
         int admitted, retired, resident, queued, solved, retries;
         uint64_t residentBodies;
         float ms[6]; /* phase times of the batched solve when params.solve.timing */
+        /* interactions of the step's batched solve: sums over bodies and maxima over target groups */
+        uint64_t sumP2P, maxP2P, sumM2P, maxM2P;
     } ryo_engine_step_info;
     typedef struct ryo_engine_result
     {

@@ -674,7 +674,7 @@ class Engine:
         info = _abi.EngineStepInfo()
         self._err(lib.ryo_engine_step(self.handle, C.byref(info), _stream(stream)))
         d = {k: getattr(info, k) for k in ("admitted", "retired", "resident", "queued", "solved", "retries",
-                                           "residentBodies")}
+                                           "residentBodies", "sumP2P", "maxP2P", "sumM2P", "maxM2P")}
         d["ms"] = list(info.ms)
         return d
 

@@ -97,7 +97,8 @@ class EngineRequest(C.Structure):
 
 class EngineStepInfo(C.Structure):
     _fields_ = [(k, C.c_int) for k in ("admitted", "retired", "resident", "queued", "solved", "retries")] + \
-               [("residentBodies", C.c_uint64), ("ms", C.c_float * 6)]
+               [("residentBodies", C.c_uint64), ("ms", C.c_float * 6)] + \
+               [(k, C.c_uint64) for k in ("sumP2P", "maxP2P", "sumM2P", "maxM2P")]
 
 
 class EngineResult(C.Structure):

@@ -455,6 +455,19 @@ __global__ void splitGroupsKernel(const uint32_t* failed, uint32_t numFailed, co
 
 /*! run a traversal to completion: groups that overflow the stack are split in two along the SFC and traversed
  *  again until none fails (traversal_gpu.cu:572-623); counts per group refer to the groups of @p t */
+/*! the interaction count (direct bodies + 2 x approximated cells) past which a group is taken off its warp and
+ *  split over several in a second pass. Uniform and Plummer groups stay well below it (at most about 17,000 at theta
+ *  0.5); the groups that pass it are sparse outskirts whose bounding box reaches the dense centre, with up to a few
+ *  hundred thousand direct bodies, which one warp would evaluate while the rest of the GPU idles. */
+constexpr unsigned kHeavyCost = 32768;
+
+//! warps per queued group: enough items to fill the GPU, at most 16 (each part repeats the group's walk)
+int heavyParts(uint32_t numHeavy, int smCount)
+{
+    uint32_t want = (uint32_t(smCount) * 20u + numHeavy - 1) / numHeavy;
+    return int(std::max(2u, std::min(16u, want)));
+}
+
 void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potentialOut)
 {
     const uint32_t numGroups = uint32_t(t.numGroups);
@@ -472,10 +485,32 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
     {
         if (pass > 0) launchTraversalReset(ctx->ctl, false, s);
         ++pass;
+        // first pass: groups too costly for one warp are queued; second pass: each queued group split over warps
+        t.heavyGroups   = ctx->scratch<uint32_t>("trav.heavy", std::max(t.numGroups, 1), s);
+        t.heavyCapacity = uint32_t(t.numGroups);
+        t.heavyCost     = kHeavyCost;
+        t.parts         = 0;
+        t.numHeavy      = 0;
         launchTraverse(t, ctx->smCount, s);
-        unsigned int numFailed = 0;
-        RYO_CUDA(cudaMemcpyAsync(&numFailed, &ctx->ctl->failedCount, sizeof(numFailed), cudaMemcpyDeviceToHost, s));
+        unsigned int counts[2] = {0, 0}; // failed, queued
+        RYO_CUDA(cudaMemcpyAsync(&counts[0], &ctx->ctl->failedCount, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        RYO_CUDA(cudaMemcpyAsync(&counts[1], &ctx->ctl->heavyCount, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         RYO_CUDA(cudaStreamSynchronize(s));
+        if (counts[1] > 0)
+        {
+            TraverseLaunch t2 = t;
+            t2.numHeavy       = std::min(counts[1], t.heavyCapacity);
+            t2.parts          = heavyParts(t2.numHeavy, ctx->smCount);
+            size_t items      = size_t(t2.numHeavy) * size_t(t2.parts);
+            t2.partials       = ctx->scratch<float4>("trav.partials", items * 2 * kWarp, s);
+            t2.partStatus     = ctx->scratch<int>("trav.partStatus", items, s);
+            RYO_CUDA(cudaMemsetAsync(&ctx->ctl->workCounter, 0, sizeof(unsigned), s));
+            launchTraverse(t2, ctx->smCount, s);
+            launchCombineHeavy(t2, t.nodes ? t.tgtM : t.mt, s);
+            RYO_CUDA(cudaMemcpyAsync(&counts[0], &ctx->ctl->failedCount, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            RYO_CUDA(cudaStreamSynchronize(s));
+        }
+        unsigned int numFailed = counts[0];
         if (numFailed == 0) break;
         ctx->retries += numFailed;
         // split the failed groups on the device: halves along the SFC
@@ -1301,6 +1336,25 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        uint32_t* gEnd   = ctx->scratch<uint32_t>("batch.gend", std::max(numGroups, 1u), s);
                        uint32_t* gSys   = ctx->scratch<uint32_t>("batch.gsys", std::max(numGroups, 1u), s);
                        launchBatchGroups(numGroups, dFirst, dGOff, ns, P->groupSize, gStart, gEnd, gSys, s);
+                       // traversal groups: the fixed windows, or their spatial splits within each system
+                       uint32_t travGroups = numGroups;
+                       uint32_t* tStart    = gStart;
+                       uint32_t* tEnd      = gEnd;
+                       uint32_t* tSys      = gSys;
+                       if (P->groupTolerance > 0.f)
+                       {
+                           REQUIRE(P->groupSize == 32 || P->groupSize == 64,
+                                   "solve_batch: spatial groups need groupSize 32 or 64");
+                           uint32_t* sg   = ctx->scratch<uint32_t>("batch.sgroups", n + 2, s);
+                           uint32_t* sSys = ctx->scratch<uint32_t>("batch.sgsys", n + 1, s);
+                           float ratio    = P->groupExtentRatio < 0.f ? defaultExtentRatio() : P->groupExtentRatio;
+                           travGroups = computeGroupSplitsBatch(ctx, gStart, gEnd, gSys, numGroups, dBx, sysLevel, x, y,
+                                                                z, leaves, nl, layout, P->groupSize,
+                                                                P->groupTolerance, ratio, sg, sSys, uint32_t(n + 2), s);
+                           tStart = sg;
+                           tEnd   = sg + 1;
+                           tSys   = sSys;
+                       }
                        SysTrav* dTrav   = ctx->scratch<SysTrav>("batch.trav", ns, s);
                        int* dRootNode   = ctx->scratch<int>("batch.rootNode", ns, s);
                        unsigned int* rootErr = ctx->ctl->counters + 4;
@@ -1312,9 +1366,9 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        for (float* a : {p, ax, ay, az})
                            RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
                        TraverseLaunch t{};
-                       t.groupStart    = gStart;
-                       t.groupEnd      = gEnd;
-                       t.numGroups     = int(numGroups);
+                       t.groupStart    = tStart;
+                       t.groupEnd      = tEnd;
+                       t.numGroups     = int(travGroups);
                        t.initNode      = 1;
                        t.numNodes      = nn;
                        t.nodes         = records;
@@ -1328,7 +1382,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        t.ay            = ay;
                        t.az            = az;
                        t.stackCapacity = P->stackCapacity;
-                       t.groupSys      = gSys;
+                       t.groupSys      = tSys;
                        t.dipoles       = dipoles;
                        t.systems       = dTrav;
                        t.sysPotential  = sysPot;
@@ -1394,7 +1448,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        {
                            stats->numLeaves       = nl;
                            stats->numNodes        = nn;
-                           stats->numGroups       = int(numGroups);
+                           stats->numGroups       = int(travGroups);
                            stats->sumP2P          = ctx->hostStats[kSumP2P];
                            stats->maxP2P          = ctx->hostStats[kMaxP2P];
                            stats->sumM2P          = ctx->hostStats[kSumM2P];

@@ -312,12 +312,24 @@ void rebuildArena(ryo_engine* E, std::vector<Request>& admitted, cudaStream_t s)
     E->residentBodies = total;
 }
 
+//! a failed batched solve inside a step: its status and the context's message
+struct SolveFailed
+{
+    ryo_status status;
+    std::string msg;
+};
+
 ryo_status engineGuard(ryo_engine* E, const std::function<void()>& f)
 {
     try
     {
         f();
         return RYO_OK;
+    }
+    catch (const SolveFailed& e)
+    {
+        E->lastError = e.msg;
+        return e.status;
     }
     catch (const CudaError& e)
     {
@@ -490,7 +502,7 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                                                                P.a[11], P.a[8], P.a[9], P.a[10], order, pe.data(),
                                                                nullptr, &ss, s);
                            if (rs != RYO_OK)
-                               throw CudaError{cudaErrorUnknown, "engine_step: batched solve failed"};
+                               throw SolveFailed{rs, "engine_step: batched solve failed: " + E->ctx->lastError};
                            E->solves += ns;
                            uint32_t* idTmp = E->ctx->scratch<uint32_t>("eng.idtmp", n, s);
                            engineGatherIds<<<gridFor(n, E->ctx->smCount), 256, 0, s>>>(order, A.id, idTmp, n);
@@ -546,6 +558,10 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                            E->resident.swap(keep);
                            st.solved    = int(ns);
                            st.retries   = int(ss.retries);
+                           st.sumP2P    = ss.sumP2P;
+                           st.maxP2P    = ss.maxP2P;
+                           st.sumM2P    = ss.sumM2P;
+                           st.maxM2P    = ss.maxM2P;
                            for (int i = 0; i < 6; ++i)
                                st.ms[i] = ss.ms[i];
                            if (info) *info = st;

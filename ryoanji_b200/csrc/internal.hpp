@@ -23,6 +23,7 @@ struct Control
     double potential;          // sum m * phi of the traversal (no G)
     double ewaldPotential;     // sum m * phi of the Ewald correction (no G)
     unsigned int counters[8];  // scratch counters for other kernels
+    unsigned int heavyCount;   // groups queued for the split second traversal pass
 };
 
 enum BhStat
@@ -242,6 +243,17 @@ struct TraverseLaunch
     const uint32_t* groupSys;
     const struct SysTrav* systems;
     double* sysPotential;
+    // groups too costly for one warp. First pass (parts == 0, heavyGroups set): a group whose interaction count
+    // (direct bodies + 2 x approximated cells) passes heavyCost stops and is queued in heavyGroups. Second pass
+    // (parts > 0): item i walks group heavyGroups[i / parts] in full but evaluates only every parts-th batch,
+    // starting at batch i % parts, and writes its compensated partial sums to partials[i][64] for the combine step.
+    uint32_t* heavyGroups;
+    uint32_t heavyCapacity;
+    unsigned heavyCost;
+    int parts;
+    uint32_t numHeavy;  // second pass: queued groups
+    float4* partials;   // second pass: (-phi, ax, ay, az) of the group's 64 targets, per item
+    int* partStatus;    // second pass: per item, 1 if the walk overflowed the stack
 };
 
 //! per-system traversal parameters of a batched solve
@@ -253,6 +265,9 @@ struct SysTrav
     int pad;
 };
 void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s);
+/*! after a second pass: per queued group, the parts' partial sums added in part order into the outputs (and the
+ *  potential); a group whose walk overflowed the stack goes to t.failedGroups instead. @p mass: target masses */
+void launchCombineHeavy(const TraverseLaunch& t, const float* mass, cudaStream_t s);
 void launchTraversalReset(Control* ctl, bool resetStats, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- groups.cu
@@ -264,6 +279,15 @@ uint32_t computeGroupSplits(ryo_ctx* ctx, uint32_t first, uint32_t last, const f
                             const float* z, const float* h, const uint64_t* leaves, int numLeaves,
                             const uint32_t* layout, const DevBox<float>& box, unsigned groupSize, float tolFactor,
                             float extentRatio, uint32_t* groups, uint32_t capacity, cudaStream_t s);
+/*! spatial groups of a batched solve: each fixed window [windowStart[w], windowEnd[w]) of system windowSys[w] is split
+ *  with that system's box (no interaction radius); returns the group count and, when capacity >= count + 1, writes
+ *  groups[count + 1] (starts, then the end of the last window) and groupSys[count] */
+uint32_t computeGroupSplitsBatch(ryo_ctx* ctx, const uint32_t* windowStart, const uint32_t* windowEnd,
+                                 const uint32_t* windowSys, uint32_t numWindows, const DevBox<float>* sysBoxes,
+                                 int sysLevel, const float* x, const float* y, const float* z,
+                                 const uint64_t* leaves, int numLeaves, const uint32_t* layout, unsigned groupSize,
+                                 float tolFactor, float extentRatio, uint32_t* groups, uint32_t* groupSys,
+                                 uint32_t capacity, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- batch.cu
 void launchBatchBoxes(const float* x, const float* y, const float* z, size_t n, const uint64_t* first,

@@ -3,7 +3,7 @@
  *
  * Replaces the CUB DeviceRadixSort::SortPairs call of the reference (cstone/include/cstone/primitives/
  * primitives_gpu.cu:311-356). One upfront pass histograms every digit position; each 8-bit digit pass then reads
- * the keys once and writes them once: tiles rank their keys with warp match/ballot, publish per-digit tile counts
+ * the keys once and writes them once: tiles rank their keys with one warp ballot per digit bit, publish per-digit tile counts
  * with decoupled look-back (bounded waits), stage the tile in shared memory in digit order and write coalesced runs.
  * The sort is stable (keys and payload indices keep their input order within equal keys), as the reference needs.
  */

@@ -46,7 +46,20 @@ struct WarpSmem
     float4 stage[7 * kWarp]; // M2P of dipole expansions stages 7 float4 per cell
     // per lane: Kahan running sums [0] and compensations [1] of (-phi, ax, ay, az), both targets packed
     unsigned long long sums[2][4][kWarp];
+    // evaluation batches of the current walk: the next batch's number, and which of them this warp evaluates
+    // (batch j when j % parts == part; parts is 1 outside the split second pass)
+    int batchNext, part, parts, item;
 };
+
+//! true if the walk's next evaluation batch belongs to this warp; counts the batch either way
+__device__ __forceinline__ bool ownBatch(WarpSmem& S)
+{
+    int j = S.batchNext;
+    __syncwarp();
+    if (laneId() == 0) S.batchNext = j + 1;
+    __syncwarp();
+    return S.parts <= 1 || j % S.parts == S.part;
+}
 
 // ------------------------------------------------------------------------------------------------ packed f32x2
 
@@ -351,6 +364,7 @@ template<class Nodes>
 __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState& T)
 {
     constexpr int kStride = Nodes::kDipole ? 7 : 5; // staged float4 per cell
+    if (!ownBatch(S)) return;
     int lane = laneId();
     if (lane < count)
     {
@@ -426,6 +440,7 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
     int numBatches = all ? (total + kWarp - 1) / kWarp : total / kWarp;
     for (int b = 0; b < numBatches; ++b)
     {
+        if (!ownBatch(S)) continue;
         int r = b * kWarp + lane;
         if (r < total)
         {
@@ -557,6 +572,7 @@ __global__ void resetTraversal(Control* ctl, bool resetStats)
     {
         ctl->workCounter = 0;
         ctl->failedCount = 0;
+        ctl->heavyCount  = 0;
         if (resetStats)
         {
             for (int i = 0; i < 5; ++i)
@@ -572,6 +588,68 @@ void launchTraversalReset(Control* ctl, bool resetStats, cudaStream_t s)
     RYO_LAUNCH_CHECK();
 }
 
+//! one warp per queued group: add the parts' partial sums in part order (FP64) and write the group's results
+__global__ void combineHeavyKernel(TraverseLaunch P, const float* __restrict__ mass)
+{
+    const unsigned w    = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+    const unsigned lane = laneId();
+    if (w >= P.numHeavy) return; // whole warps leave together
+    const unsigned g   = P.heavyGroups[w];
+    const int K        = P.parts;
+    const size_t item0 = size_t(w) * unsigned(K);
+    bool failed        = false;
+    for (int k = int(lane); k < K; k += kWarp)
+        failed |= P.partStatus[item0 + k] != 0;
+    if (__any_sync(0xffffffffu, failed))
+    {
+        if (lane == 0)
+        {
+            unsigned slotF = atomicAdd(&P.ctl->failedCount, 1u);
+            if (slotF < P.failedCapacity) P.failedGroups[slotF] = g;
+        }
+        return;
+    }
+    const int b = int(P.groupStart[g]), e = int(P.groupEnd[g]);
+    double pot  = 0.0;
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+    {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (int k = 0; k < K; ++k)
+        {
+            float4 v = P.partials[(item0 + k) * (2 * kWarp) + t * kWarp + lane];
+            s0 += v.x;
+            s1 += v.y;
+            s2 += v.z;
+            s3 += v.w;
+        }
+        int idx = b + t * kWarp + int(lane);
+        if (idx < e)
+        {
+            float phi = float(s0), gx = float(s1), gy = float(s2), gz = float(s3);
+            float mi  = mass[idx];
+            pot += double(mi) * double(phi);
+            if (P.p) P.p[idx] += P.G * mi * phi;
+            P.ax[idx] += P.G * gx;
+            P.ay[idx] += P.G * gy;
+            P.az[idx] += P.G * gz;
+        }
+    }
+    pot = warpSum(pot);
+    if (lane == 0)
+    {
+        atomicAdd(&P.ctl->potential, pot);
+        if (P.sysPotential) atomicAdd(P.sysPotential + (P.groupSys ? P.groupSys[g] : 0u), pot);
+    }
+}
+
+void launchCombineHeavy(const TraverseLaunch& t, const float* mass, cudaStream_t s)
+{
+    if (t.numHeavy == 0) return;
+    combineHeavyKernel<<<ceilDiv(size_t(t.numHeavy) * kWarp, 256), 256, 0, s>>>(t, mass);
+    RYO_LAUNCH_CHECK();
+}
+
 template<class Nodes, class Targets, class Sources>
 __global__ void __launch_bounds__(kTravThreads, 5)
     traverseKernel(TraverseLaunch P, Nodes nodes, Targets tgt, Sources src)
@@ -582,12 +660,22 @@ __global__ void __launch_bounds__(kTravThreads, 5)
     WarpSmem& S    = reinterpret_cast<WarpSmem*>(smemRaw + sizeof(int) * kTravWarps * P.stackCapacity)[warp];
     const unsigned lt = lanemaskLt();
 
+    const unsigned numItems = P.parts > 0 ? P.numHeavy * unsigned(P.parts) : unsigned(P.numGroups);
     while (true)
     {
-        unsigned g = 0;
-        if (lane == 0) g = atomicAdd(&P.ctl->workCounter, 1u);
-        g = __shfl_sync(0xffffffffu, g, 0);
-        if (g >= unsigned(P.numGroups)) return;
+        unsigned item = 0;
+        if (lane == 0) item = atomicAdd(&P.ctl->workCounter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= numItems) return;
+        unsigned g = item;
+        if (P.parts > 0) g = P.heavyGroups[item / unsigned(P.parts)];
+        if (lane == 0)
+        {
+            S.batchNext = 0;
+            S.part      = P.parts > 0 ? int(item % unsigned(P.parts)) : 0;
+            S.parts     = P.parts > 0 ? P.parts : 1;
+            S.item      = int(item);
+        }
 
         const int b = int(P.groupStart[g]), e = int(P.groupEnd[g]);
         TargetState T;
@@ -631,7 +719,8 @@ __global__ void __launch_bounds__(kTravThreads, 5)
 
         unsigned nM2P = 0, nP2P = 0;
         int maxStack  = 0;
-        bool overflow = false;
+        bool overflow = false, heavy = false;
+        const bool mayQueue = P.parts == 0 && P.heavyGroups != nullptr;
         for (int iz = -shells; iz <= shells && !overflow; ++iz)
             for (int iy = -shells; iy <= shells && !overflow; ++iy)
                 for (int ix = -shells; ix <= shells && !overflow; ++ix)
@@ -703,6 +792,13 @@ __global__ void __launch_bounds__(kTravThreads, 5)
                         nL += __popc(bl);
                         nP2P += __reduce_add_sync(0xffffffffu, hasB ? unsigned(link.z) : 0u);
                         __syncwarp();
+                        if (mayQueue && nP2P + 2u * nM2P > P.heavyCost)
+                        {
+                            // too much for one warp: leave it to the split second pass
+                            heavy    = true;
+                            overflow = true;
+                            break;
+                        }
 
                         while (nM >= kWarp)
                         {
@@ -723,13 +819,31 @@ __global__ void __launch_bounds__(kTravThreads, 5)
                         tc[d] = __fsub_rn(tc[d], sh[d]);
                 }
 
-        if (overflow)
+        if (heavy)
         {
-            // write nothing; the host splits the group and traverses the halves again
             if (lane == 0)
             {
-                unsigned slotF = atomicAdd(&P.ctl->failedCount, 1u);
-                if (slotF < P.failedCapacity) P.failedGroups[slotF] = g;
+                unsigned slotH = atomicAdd(&P.ctl->heavyCount, 1u);
+                if (slotH < P.heavyCapacity) P.heavyGroups[slotH] = g;
+            }
+            continue;
+        }
+        if (overflow)
+        {
+            // write nothing; the host splits the group and traverses the halves again (in the second pass the
+            // combine step reports the group)
+            if (P.parts > 0)
+            {
+                if (lane == 0) P.partStatus[S.item] = 1;
+                if (S.part != 0) continue;
+            }
+            if (lane == 0)
+            {
+                if (P.parts == 0)
+                {
+                    unsigned slotF = atomicAdd(&P.ctl->failedCount, 1u);
+                    if (slotF < P.failedCapacity) P.failedGroups[slotF] = g;
+                }
                 atomicMax(&P.ctl->stats[kMaxStack], (unsigned long long)maxStack);
             }
             continue;
@@ -742,21 +856,34 @@ __global__ void __launch_bounds__(kTravThreads, 5)
         upk(sub2(S.sums[0][2][lane], S.sums[1][2][lane]), gy[0], gy[1]);
         upk(sub2(S.sums[0][3][lane], S.sums[1][3][lane]), gz[0], gz[1]);
         double pot = 0.0;
-#pragma unroll
-        for (int k = 0; k < 2; ++k)
+        if (P.parts > 0)
         {
-            int idx = b + k * kWarp + lane;
-            if (idx < e)
-            {
-                float mi = tgt.scalar(idx);
-                pot += double(mi) * double(phi[k]);
-                if (P.p) P.p[idx] += P.G * mi * phi[k];
-                P.ax[idx] += P.G * gx[k];
-                P.ay[idx] += P.G * gy[k];
-                P.az[idx] += P.G * gz[k];
-            }
+            // this part's share; the combine step adds the parts in order. Every part walked the whole group, so
+            // part 0 reports the group's interaction counts.
+            float4* out       = P.partials + size_t(S.item) * (2 * kWarp);
+            out[lane]         = make_float4(phi[0], gx[0], gy[0], gz[0]);
+            out[kWarp + lane] = make_float4(phi[1], gx[1], gy[1], gz[1]);
+            if (lane == 0) P.partStatus[S.item] = 0;
+            if (S.part != 0) continue;
         }
-        pot = warpSum(pot);
+        else
+        {
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+            {
+                int idx = b + k * kWarp + lane;
+                if (idx < e)
+                {
+                    float mi = tgt.scalar(idx);
+                    pot += double(mi) * double(phi[k]);
+                    if (P.p) P.p[idx] += P.G * mi * phi[k];
+                    P.ax[idx] += P.G * gx[k];
+                    P.ay[idx] += P.G * gy[k];
+                    P.az[idx] += P.G * gz[k];
+                }
+            }
+            pot = warpSum(pot);
+        }
         if (lane == 0)
         {
             unsigned long long size = (unsigned long long)(e - b);
@@ -765,8 +892,11 @@ __global__ void __launch_bounds__(kTravThreads, 5)
             atomicMax(&P.ctl->stats[kMaxM2P], (unsigned long long)nM2P);
             atomicAdd(&P.ctl->stats[kSumM2P], (unsigned long long)nM2P * size);
             atomicMax(&P.ctl->stats[kMaxStack], (unsigned long long)maxStack);
-            atomicAdd(&P.ctl->potential, pot);
-            if (P.sysPotential) atomicAdd(P.sysPotential + sys, pot);
+            if (P.parts == 0)
+            {
+                atomicAdd(&P.ctl->potential, pot);
+                if (P.sysPotential) atomicAdd(P.sysPotential + sys, pot);
+            }
             if (P.groupM2P) P.groupM2P[g] = nM2P;
             if (P.groupP2P) P.groupP2P[g] = nP2P;
         }
@@ -783,7 +913,8 @@ static void launchTyped(const TraverseLaunch& t, const Nodes& nodes, const Targe
     int perSm = 0;
     RYO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kTravThreads, smem));
     if (perSm < 1) perSm = 1;
-    int want   = (t.numGroups + kTravWarps - 1) / kTravWarps;
+    int items  = t.parts > 0 ? int(t.numHeavy) * t.parts : t.numGroups;
+    int want   = (items + kTravWarps - 1) / kTravWarps;
     int blocks = min(want, perSm * smCount);
     kernel<<<blocks, kTravThreads, smem, s>>>(t, nodes, tgt, src);
     RYO_LAUNCH_CHECK();
@@ -791,7 +922,7 @@ static void launchTyped(const TraverseLaunch& t, const Nodes& nodes, const Targe
 
 void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s)
 {
-    if (t.numGroups <= 0) return;
+    if (t.numGroups <= 0 || (t.parts > 0 && t.numHeavy == 0)) return;
     if (t.nodes)
     {
         PackedBodies tgt{t.tgtXYZH, t.tgtM}, src{t.srcXYZM, t.srcH};

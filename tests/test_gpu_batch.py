@@ -24,6 +24,8 @@ def _systems(seed=0):
     out.append(("given-open", g, "open"))
     out.append(("tiny", ds.uniform_cube(40, seed=seed + 6, eps=0.01), None))
     out.append(("single", ds.uniform_cube(1, seed=seed + 7, eps=0.01), None))
+    # sparse outskirts: some groups are split over several warps in a second traversal pass
+    out.append(("outskirts", ds.plummer(100000, seed=1, velocities=True), None))
     return out
 
 
@@ -63,13 +65,16 @@ def _run_batch(systems, params):
     return res, dict(x=x, y=y, z=z, m=m, h=h, vx=vx, p=pot, ax=ax, ay=ay, az=az, order=order)
 
 
-def test_batch_equals_single_solves():
+@pytest.mark.parametrize("tol", [0.0, 2.0], ids=["fixed-groups", "spatial-groups"])
+def test_batch_equals_single_solves(tol):
+    """with spatial groups each system's fixed windows are split with its own box, exactly as its single solve does"""
     import ryoanji_b200 as ryo
     systems = _systems()
-    params = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32)
+    params = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32, group_tolerance=tol)
     res, B = _run_batch(systems, params)
     assert res.stats.retries == 0
     first = 0
+    groups = 0
     for (name, p, kind), e_batch, box in zip(systems, res.energies, res.boxes):
         n = p.n
         sl = slice(first, first + n)
@@ -79,8 +84,9 @@ def test_batch_equals_single_solves():
         pot, ax, ay, az = (torch.empty(n, device="cuda") for _ in range(4))
         order = torch.empty(n, dtype=torch.int32, device="cuda")
         given = _box_for(kind, p)
-        sp = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32, box=given, num_shells=1)
+        sp = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32, box=given, num_shells=1, group_tolerance=tol)
         r = ryo.solve(x, y, z, m, h, pot, ax, ay, az, sp, v=(vx, vy, vz), order=order)
+        groups += r.num_groups
         if given is None:
             assert r.box == pytest.approx(box, rel=0, abs=0), name  # the same enclosing cube, bit for bit
         assert torch.equal(B["order"][sl] - (first - n), order), name
@@ -92,6 +98,7 @@ def test_batch_equals_single_solves():
         dp = (B["p"][sl] - pot).abs() / (pot.abs() + 1e-30)
         assert float(dp.max()) <= 1e-6, (name, float(dp.max()))
         assert e_batch == pytest.approx(r.potential_energy, rel=1e-9, abs=1e-12), name
+    assert res.stats.num_groups == groups
 
 
 def test_batch_many_small_systems_against_direct_sums():

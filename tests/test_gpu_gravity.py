@@ -181,6 +181,49 @@ def test_solve_matches_oracle_path(oracle):
     assert res.sum_m2p == int((m2p.astype(np.int64) * np.diff(g)).sum())
 
 
+SPLIT_COST = 32768  # direct bodies + 2 x approximated cells past which the traversal splits a group over warps
+
+
+def test_heavy_groups_split_over_warps(oracle):
+    """groups whose interaction lists are too long for one warp (sparse outskirts of a Plummer sphere whose bounding
+    box reaches the centre) are evaluated by several warps in a second pass: per-group counts stay bit-exact, forces
+    match the double evaluation of the same lists, and a repeated solve gives identical results"""
+    import ryoanji_b200 as ryo
+    from ryoanji_b200 import datasets as ds
+    pset = ds.plummer(100000, seed=1, velocities=False)
+    ctx = ryo.Context()
+    runs = []
+    for _ in range(2):
+        x, y, z, m, h = (dev(a) for a in (pset.x, pset.y, pset.z, pset.m, pset.h))
+        n = x.numel()
+        out = [torch.empty(n, device="cuda") for _ in range(4)]
+        res = ryo.solve(x, y, z, m, h, *out, ryo.SolveParams(theta=0.5), ctx=ctx)
+        runs.append(out)
+    for a, b in zip(*runs):
+        assert torch.equal(a, b)
+    p, ax, ay, az = runs[-1]
+    arr = ryo.solve_arrays(ctx)
+    g = host(arr["groups"]).view(np.uint32)
+    gm, gp = host(arr["groupM2P"]).view(np.uint32), host(arr["groupP2P"]).view(np.uint32)
+    heavy = gp.astype(np.int64) + 2 * gm.astype(np.int64) > SPLIT_COST
+    assert heavy.sum() >= 1 and res.max_p2p > SPLIT_COST // 2
+    tree = dict(childOffsets=host(arr["childOffsets"]), internalToLeaf=host(arr["internalToLeaf"]))
+    cg = np.ascontiguousarray(host(arr["centers"]))
+    mg = np.ascontiguousarray(host(arr["multipoles"]))
+    hx, hy, hz, hm, hh = host(x), host(y), host(z), host(m), host(h)
+    m2p, p2p, acc = oracle.traverse_rule(g[:-1], g[1:], hx, hy, hz, hh, hm, tree, host(arr["layout"]).view(np.uint32),
+                                         cg, mg, evaluate=True)
+    assert np.array_equal(gm, m2p) and np.array_equal(gp, p2p)
+    sizes = np.diff(g).astype(np.int64)
+    assert res.sum_p2p == int((p2p.astype(np.int64) * sizes).sum()) and res.max_p2p == int(p2p.max())
+    e = rel_err(host(ax), host(ay), host(az), acc[:, 1], acc[:, 2], acc[:, 3])
+    assert np.percentile(e, 99) < 2e-6 and e.max() < 5e-5
+    for k in np.flatnonzero(heavy):  # the split groups themselves
+        assert e[g[k]:g[k + 1]].max() < 5e-6, k
+    assert np.allclose(host(p), hm * acc[:, 0], rtol=1e-5, atol=1e-6 * np.abs(hm * acc[:, 0]).max())
+    assert res.potential_energy == pytest.approx(0.5 * float((hm * acc[:, 0]).sum()), rel=1e-5)
+
+
 @pytest.mark.parametrize("kind", ["plummer", "cube", "halos"])
 def test_solve_accuracy_vs_fp64_direct(kind):
     import ryoanji_b200 as ryo
