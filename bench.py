@@ -280,28 +280,29 @@ def run_ours(args, rank, world, local_rank):
                             "potential_sample_rel_diff": abs(pt - pd) / abs(pd),
                             "potential_energy_tree": res.potential_energy}
 
-    # end to end through the public API: host buffers in, host results out
+    # end to end through the public host-memory call (ryo_solve_host_f32): x, y, z, m, h from pinned host memory;
+    # potential, acceleration and the permutation that maps them back to the input order into pinned host memory.
+    # The call overlaps its copies with the solve and returns when every output is on the host.
     if not args.no_e2e:
         host_in = [t.cpu().pin_memory() for t in pristine]
         host_out = [torch.empty(n).pin_memory() for _ in range(4)]
+        host_order = torch.empty(n, dtype=torch.int32).pin_memory()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def solve_host():
+            return ryo.solve_host(*host_in, *host_out, params=params, order=host_order, ctx=ctx)
+
         for _ in range(2):
-            for w, h in zip(work, host_in):
-                w.copy_(h, non_blocking=True)
-            solve()
+            solve_host()
         barrier()
         e0.record()
         for _ in range(args.steps):
-            for w, h in zip(work, host_in):
-                w.copy_(h, non_blocking=True)
-            solve()
-            for h, o in zip(host_out, out):
-                h.copy_(o, non_blocking=True)
+            solve_host()
         e1.record()
         barrier()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1))
         line["e2e"] = {"value": world * n * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mparticles/s",
-                       "h2d_bytes_per_step": 5 * 4 * n, "d2h_bytes_per_step": 4 * 4 * n}
+                       "h2d_bytes_per_step": 5 * 4 * n, "d2h_bytes_per_step": 5 * 4 * n}
 
     if world == 1 and not args.no_accuracy_matched and args.accuracy_targets > 0:
         line["accuracy_matched"] = run_accuracy_matched(args, ctx, dev, work, out, pristine, n)
@@ -417,9 +418,11 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
     all_reqs = ds.served_requests(args.served_requests, seed=11, rate_per_s=args.served_rate)
     route = route_requests(all_reqs, world)
     reqs = [q for q, r in zip(all_reqs, route) if r == rank]
-    host = {}
+    host, result = {}, {}
     for q in reqs:
         host[q["tag"]] = [t.cpu().pin_memory() for t in ds.request_bodies(q, device=dev)]
+        # the final state (x y z vx vy vz ax ay az p) of every request lands in pinned host memory in both arms
+        result[q["tag"]] = torch.empty((10, q["n"]), dtype=torch.float32).pin_memory()
     torch.cuda.synchronize()
     params = ryo.SolveParams(theta=0.5)
     periodic = ryo.Box(0.0, 1.0, 0.0, 1.0, 0.0, 1.0, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
@@ -446,8 +449,9 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
                 "latency_max_s": float(lat.max())}
 
-    # served: the engine admits what has arrived at every step
-    eng = ryo.Engine(params, hbm_budget_bytes=120e9, ctx=ctx)
+    # served: the engine admits what has arrived at every step. Its two arenas are reserved at creation for 2^25
+    # resident bodies (the stream peaks near 2.5e7), as a server sizes them at start-up.
+    eng = ryo.Engine(params, hbm_budget_bytes=120e9, ctx=ctx, reserve_bodies=1 << 25)
     outs = {}
     done = {}
     i = 0
@@ -461,7 +465,7 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
             q = reqs[i]
             x, y, z, m, h, vx, vy, vz = host[q["tag"]]
             eng.submit(q["tag"], x, y, z, m, h, vx, vy, vz, box=periodic if q["kind"] == "periodic" else None,
-                       steps=q["steps"], dt=q["dt"], want_output=True)
+                       steps=q["steps"], dt=q["dt"], want_output=True, out=result[q["tag"]])
             i += 1
         st = eng.status()
         if st["queued"] == 0 and st["resident"] == 0:
@@ -504,9 +508,8 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
             ryo.solve(x, y, z, m, h, p, ax, ay, az, params=pp, v=(vx, vy, vz), ctx=ctx)
             for v, a in ((vx, ax), (vy, ay), (vz, az)):
                 v.add_(a, alpha=hdt)
-        result = torch.stack([x, y, z, vx, vy, vz, ax, ay, az, p]).cpu()
+        result[q["tag"]].copy_(torch.stack([x, y, z, vx, vy, vz, ax, ay, az, p]))
         done[q["tag"]] = time.perf_counter() - t0
-        del result
     plain = summary(done, max(done.values(), default=0.0))
     return {"workload": f"{len(all_reqs)} requests, Poisson arrivals at {args.served_rate}/s, N=round(2^U[12,22]), "
                         "45% Plummer / 45% cube / 10% periodic+Ewald, K~U{1..64} KDK steps, dt=1e-3, theta 0.5, "
@@ -514,7 +517,8 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
                         + (f"; requests routed over {world} GPUs by estimated backlog" if world > 1 else ""),
             "solves": solves, "body_solves": body_solves, "served": served, "plain": plain,
             "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"],
-            "h2d": "pinned host inputs copied per request", "d2h": "final state of every request copied back"}
+            "h2d": "pinned host inputs copied per request",
+            "d2h": "final state of every request copied back into pinned host memory"}
 
 
 def run_accuracy_matched(args, ctx, dev, work, out, pristine, n) -> dict:

@@ -367,6 +367,17 @@ extern "C"
                                      float* ax, float* ay, float* az, uint32_t* order, ryo_solve_stats* stats,
                                      ryo_stream_t stream);
 
+    /* The same solve from and to HOST memory (pinned memory copies fastest): x, y, z, m, h are read (not changed);
+     * xs, ys, zs (may be NULL) receive the positions in SFC order, p, ax, ay, az the potential and acceleration in
+     * that order, order (may be NULL) the original index of each sorted body. The copies overlap the solve: m and h
+     * upload during the key sort, the order and sorted positions download while the tree is built, and for an open
+     * box with fixed groups the traversal runs in 8 launches whose results download while the next one runs.
+     * Returns when every output is in host memory. Device buffers are context scratch. */
+    RYO_API ryo_status ryo_solve_host_f32(ryo_ctx_t* ctx, const ryo_solve_params* params, const float* x,
+                                          const float* y, const float* z, const float* m, const float* h, size_t n,
+                                          float* xs, float* ys, float* zs, float* p, float* ax, float* ay, float* az,
+                                          uint32_t* order, ryo_solve_stats* stats, ryo_stream_t stream);
+
     /* ------------------------------------------------------------------------------------------ batched solve
      * Many independent systems solved together, one launch per phase (not in the reference, which solves one system
      * per call). The body arrays are the systems' bodies concatenated: system s owns [firstBody, firstBody +
@@ -410,6 +421,8 @@ extern "C"
         double hbmBudgetBytes;  /* admission budget (default 120e9) */
         double bytesPerBody;    /* device bytes charged per resident body (default 256) */
         int maxSystems;         /* resident requests at most (default and upper limit RYO_BATCH_MAX_SYSTEMS) */
+        uint64_t reserveBodies; /* resident bodies the arenas hold from creation on (default 0: grown on demand,
+                                   doubling, which waits for the device at each growth) */
     } ryo_engine_params;
     typedef struct ryo_engine_request
     {
@@ -432,6 +445,9 @@ extern "C"
         float ms[6]; /* phase times of the batched solve when params.solve.timing */
         /* interactions of the step's batched solve: sums over bodies and maxima over target groups */
         uint64_t sumP2P, maxP2P, sumM2P, maxM2P;
+        /* host wall milliseconds of the step's parts: admission and arena rebuild, batched solve, kicks and
+         * energies, retirement (results to the host) */
+        float hostMs[4];
     } ryo_engine_step_info;
     typedef struct ryo_engine_result
     {

@@ -565,6 +565,32 @@ def solve(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, v=Non
                        st.maxStack, st.retries, st.potentialEnergy, list(st.box), ms)
 
 
+def solve_host(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, sorted_xyz=None, order=None,
+               ctx: Context | None = None, stream=None) -> SolveResult:
+    """The fused solve from and to host memory (ryo_solve_host_f32): x, y, z, m, h are contiguous host float32
+    arrays (CPU tensors, pinned for the fastest copies), left unchanged; p, ax, ay, az (host float32) receive G m phi
+    and G a in SFC order, sorted_xyz (three host arrays, optional) the positions in that order and order (host
+    int32, optional) the original index of each sorted body. Host copies overlap the solve; returns when every
+    output is in host memory."""
+    ctx = ctx or default_context()
+    params = params or SolveParams()
+    for a in (x, y, z, m, h, p, ax, ay, az) + tuple(sorted_xyz or ()) + ((order,) if order is not None else ()):
+        if not (isinstance(a, torch.Tensor) and a.device.type == "cpu" and a.is_contiguous() and
+                a.numel() == x.numel() and a.element_size() == 4):
+            raise ValueError("solve_host: every array must be a contiguous 4-byte CPU tensor of n elements")
+    pc = params.c()
+    st = _abi.SolveStats()
+    xs, ys, zs = sorted_xyz if sorted_xyz is not None else (None, None, None)
+    hp = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731  (host pointers, checked above)
+    _check(lib.ryo_solve_host_f32(ctx.handle, C.byref(pc), hp(x), hp(y), hp(z), hp(m), hp(h), C.c_size_t(x.numel()),
+                                  hp(xs), hp(ys), hp(zs), hp(p), hp(ax), hp(ay), hp(az), hp(order), C.byref(st),
+                                  _stream(stream)), ctx)
+    _solve_n[id(ctx)] = x.numel()
+    ms = dict(zip(("sort", "tree", "upsweep", "traverse", "ewald", "total"), list(st.ms)))
+    return SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
+                       st.maxStack, st.retries, st.potentialEnergy, list(st.box), ms)
+
+
 @dataclass
 class BatchSystem:
     """one system of a batched solve: @p num_bodies consecutive bodies; box None means the enclosing cube"""
@@ -620,7 +646,8 @@ class Engine:
     output buffers until retirement."""
 
     def __init__(self, params: SolveParams | None = None, hbm_budget_bytes: float = 120e9,
-                 bytes_per_body: float = 256.0, max_systems: int = MAX_BATCH_SYSTEMS, ctx: Context | None = None):
+                 bytes_per_body: float = 256.0, max_systems: int = MAX_BATCH_SYSTEMS, ctx: Context | None = None,
+                 reserve_bodies: int = 0):
         self.ctx = ctx or default_context()
         ep = _abi.EngineParams()
         lib.ryo_engine_params_default(C.byref(ep))
@@ -628,6 +655,7 @@ class Engine:
         ep.hbmBudgetBytes = hbm_budget_bytes
         ep.bytesPerBody = bytes_per_body
         ep.maxSystems = max_systems
+        ep.reserveBodies = reserve_bodies
         h = C.c_void_p()
         _check(lib.ryo_engine_create(self.ctx.handle, C.byref(ep), C.byref(h)), self.ctx)
         self.handle = h
@@ -639,8 +667,10 @@ class Engine:
             raise RyoError(st, (lib.ryo_engine_last_error(self.handle) or b"").decode(errors="replace"))
 
     def submit(self, tag: int, x, y, z, m, h, vx=None, vy=None, vz=None, box: Box | None = None, num_shells: int = 1,
-               steps: int = 1, dt: float = 1e-3, want_output: bool = False):
-        """queue one request; arrays are host float32 (numpy or CPU tensors, pinned memory copies fastest)"""
+               steps: int = 1, dt: float = 1e-3, want_output: bool = False, out=None):
+        """queue one request; arrays are host float32 (numpy or CPU tensors, pinned memory copies fastest).
+        With want_output, the final state goes to @p out (a contiguous host float32 array or tensor of 10 x n,
+        pinned for the fastest copy) or to a new numpy array."""
         def host(a):
             if a is None:
                 return None
@@ -663,8 +693,17 @@ class Engine:
         r.numShells = num_shells
         r.numSteps = steps
         r.dt = dt
-        out = np.empty((10, r.numBodies), np.float32) if want_output else None
-        r.out = None if out is None else out.ctypes.data
+        if not want_output:
+            out = None
+        elif out is None:
+            out = np.empty((10, r.numBodies), np.float32)
+        else:
+            ok = (out.dtype in (np.float32, torch.float32) and tuple(out.shape) == (10, r.numBodies) and
+                  (out.is_contiguous() and out.device.type == "cpu" if isinstance(out, torch.Tensor)
+                   else out.flags.c_contiguous))
+            if not ok:
+                raise ValueError("out must be a contiguous host float32 array of shape (10, n)")
+        r.out = None if out is None else ptr(out)
         self._err(lib.ryo_engine_submit(self.handle, C.byref(r)))
         self._keep[tag] = arrs
         if out is not None:
@@ -676,6 +715,7 @@ class Engine:
         d = {k: getattr(info, k) for k in ("admitted", "retired", "resident", "queued", "solved", "retries",
                                            "residentBodies", "sumP2P", "maxP2P", "sumM2P", "maxM2P")}
         d["ms"] = list(info.ms)
+        d["host_ms"] = list(info.hostMs)
         return d
 
     def poll(self) -> list:

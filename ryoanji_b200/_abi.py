@@ -85,7 +85,7 @@ class System(C.Structure):
 
 class EngineParams(C.Structure):
     _fields_ = [("solve", SolveParams), ("hbmBudgetBytes", C.c_double), ("bytesPerBody", C.c_double),
-                ("maxSystems", C.c_int)]
+                ("maxSystems", C.c_int), ("reserveBodies", C.c_uint64)]
 
 
 class EngineRequest(C.Structure):
@@ -98,7 +98,7 @@ class EngineRequest(C.Structure):
 class EngineStepInfo(C.Structure):
     _fields_ = [(k, C.c_int) for k in ("admitted", "retired", "resident", "queued", "solved", "retries")] + \
                [("residentBodies", C.c_uint64), ("ms", C.c_float * 6)] + \
-               [(k, C.c_uint64) for k in ("sumP2P", "maxP2P", "sumM2P", "maxM2P")]
+               [(k, C.c_uint64) for k in ("sumP2P", "maxP2P", "sumM2P", "maxM2P")] + [("hostMs", C.c_float * 4)]
 
 
 class EngineResult(C.Structure):
@@ -162,6 +162,8 @@ SIGNATURES = {
     "ryo_treebuilder_view": (_i, [_p, C.POINTER(TreeView)]),
     "ryo_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "ryo_solve_f32": (_i, [_p, C.POINTER(SolveParams)] + [_p] * 8 + [_sz] + [_p] * 5 + [C.POINTER(SolveStats), _p]),
+    "ryo_solve_host_f32": (_i, [_p, C.POINTER(SolveParams)] + [_p] * 5 + [_sz] + [_p] * 8 +
+                           [C.POINTER(SolveStats), _p]),
     "ryo_solve_arrays_get": (_i, [_p, C.POINTER(SolveArrays)]),
     "ryo_engine_params_default": (None, [C.POINTER(EngineParams)]),
     "ryo_engine_create": (_i, [_p, C.POINTER(EngineParams), C.POINTER(C.c_void_p)]),

@@ -913,6 +913,348 @@ void mark(ryo_ctx* ctx, const ryo_solve_params* P, int i, cudaStream_t s)
 }
 } // namespace
 
+namespace
+{
+/*! host-memory pipeline of ryo_solve_host_f32: copies that overlap the solve on a second stream */
+struct HostPipe
+{
+    cudaStream_t copy;       // the copy stream
+    cudaEvent_t massReady;   // m and h on the device (recorded on the copy stream)
+    float *hx, *hy, *hz;     // host: positions in SFC order (each may be null)
+    float *hp, *hax, *hay, *haz;
+    uint32_t* horder;        // host: original index of every sorted body (may be null)
+    int chunks;              // traversal launches whose results are copied while the next one runs
+};
+
+//! record an event on @p from and make @p to wait for it
+void streamAfter(ryo_ctx* ctx, cudaStream_t to, cudaStream_t from, int slot)
+{
+    if (!ctx->pipeEvents[slot]) RYO_CUDA(cudaEventCreateWithFlags(&ctx->pipeEvents[slot], cudaEventDisableTiming));
+    RYO_CUDA(cudaEventRecord(ctx->pipeEvents[slot], from));
+    RYO_CUDA(cudaStreamWaitEvent(to, ctx->pipeEvents[slot], 0));
+}
+
+void d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    if (dst && bytes) RYO_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+}
+
+/*! the fused single-system solve (ryo_solve_f32); with @p pipe, the host copies of ryo_solve_host_f32 are issued on
+ *  its copy stream as soon as their data is final */
+void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, float* z, float* m, float* h, float* vx,
+                 float* vy, float* vz, size_t n, float* p, float* ax, float* ay, float* az, uint32_t* orderOut,
+                 ryo_solve_stats* stats, cudaStream_t stream, const HostPipe* pipe)
+{
+    REQUIRE(x && y && z && m && h && p && ax && ay && az, "solve: null argument");
+    REQUIRE(n > 0 && n < (size_t(1) << 32), "solve: body count must be in [1, 2^32)");
+    REQUIRE(P->groupSize >= 1 && P->groupSize <= 64, "solve: groupSize must be in [1, 64]");
+    REQUIRE(P->bucketSize >= 1 && P->theta > 0.f, "solve: bad bucketSize or theta");
+    cudaStream_t s = stream;
+    mark(ctx, P, 0, s);
+
+    // box: given, or the cube enclosing the data (exact min/max)
+    ryo_box_f32 box{};
+    if (P->useBox) { box = P->box; }
+    else
+    {
+        double* mm = ctx->scratch<double>("solve.bbox", 6, s);
+        launchBoundingBox(x, y, z, n, mm, s);
+        double hb[6];
+        RYO_CUDA(cudaMemcpyAsync(hb, mm, sizeof(hb), cudaMemcpyDeviceToHost, s));
+        RYO_CUDA(cudaStreamSynchronize(s));
+        double ext = std::max({hb[1] - hb[0], hb[3] - hb[2], hb[5] - hb[4]});
+        if (!(ext > 0)) ext = 1.0;
+        for (int d = 0; d < 3; ++d)
+        {
+            box.limits[2 * d]     = float(hb[2 * d]);
+            box.limits[2 * d + 1] = float(hb[2 * d] + ext);
+            if (!(box.limits[2 * d + 1] >= float(hb[2 * d + 1])))
+                box.limits[2 * d + 1] = std::nextafter(float(hb[2 * d + 1]), 3.4e38f);
+            box.boundary[d] = RYO_BOUNDARY_OPEN;
+        }
+    }
+    checkBox(box.limits);
+    DevBox<float> dbox = boxOf(&box);
+    bool periodic      = dbox.periodic;
+
+    // keys and sort
+    uint64_t* keys    = ctx->scratch<uint64_t>("solve.keys", n, s);
+    uint64_t* keysAlt = ctx->scratch<uint64_t>("solve.keysAlt", n, s);
+    uint32_t* ord     = ctx->scratch<uint32_t>("solve.order", n, s);
+    uint32_t* ordAlt  = ctx->scratch<uint32_t>("solve.orderAlt", n, s);
+    size_t tmpBytes   = sortTempBytes(n);
+    void* tmp         = ctx->scratch<char>("solve.sorttmp", tmpBytes, s);
+    launchKeys<float>(x, y, z, keys, n, dbox, false, s);
+    bool alt = radixSortPairs(keys, ord, keysAlt, ordAlt, n, 0, 64, tmp, tmpBytes, &ctx->ctl->error,
+                              s, true);
+    const uint64_t* sorted = alt ? keysAlt : keys;
+    const uint32_t* order  = alt ? ordAlt : ord;
+
+    // permute every per-particle array (a host solve's masses and softenings arrive on the copy stream meanwhile)
+    if (pipe) RYO_CUDA(cudaStreamWaitEvent(s, pipe->massReady, 0));
+    float* tmpF = ctx->scratch<float>("solve.tmpf", n, s);
+    for (float* a : {x, y, z, m, h, vx, vy, vz})
+    {
+        if (!a) continue;
+        launchGather(order, a, tmpF, n, s);
+        RYO_CUDA(cudaMemcpyAsync(a, tmpF, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
+    if (orderOut)
+        RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    if (pipe)
+    {
+        // the permutation and the sorted positions are final: copy them out while the tree is built
+        streamAfter(ctx, pipe->copy, s, 0);
+        d2h(pipe->horder, order, n * sizeof(uint32_t), pipe->copy);
+        d2h(pipe->hx, x, n * sizeof(float), pipe->copy);
+        d2h(pipe->hy, y, n * sizeof(float), pipe->copy);
+        d2h(pipe->hz, z, n * sizeof(float), pipe->copy);
+    }
+    mark(ctx, P, 1, s);
+    float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
+    float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
+    packSolveBodies<<<ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
+                                                                     : unsigned(ctx->smCount * 16),
+                      256, 0, s>>>(x, y, z, m, h, n, xyzm, xyzh);
+    RYO_LAUNCH_CHECK();
+
+    // leaves, links
+    int cap           = int(std::min<size_t>(n / 2 + 64, size_t(1) << 30));
+    uint64_t* leaves  = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
+    uint32_t* counts  = ctx->scratch<uint32_t>("solve.counts", cap, s);
+    uint32_t* layout  = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
+    int nl = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s);
+    if (nl > cap)
+    {
+        cap    = nl;
+        leaves = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
+        counts = ctx->scratch<uint32_t>("solve.counts", cap, s);
+        layout = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
+        nl     = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s);
+    }
+    int ni = (nl - 1) / 7, nn = nl + ni;
+    OctreeArrays oct;
+    oct.prefixes       = ctx->scratch<uint64_t>("solve.prefixes", nn, s);
+    oct.childOffsets   = ctx->scratch<int>("solve.childOffsets", size_t(nn) + 1, s);
+    oct.parents        = ctx->scratch<int>("solve.parents", std::max(1, (nn - 1) / 8), s);
+    oct.internalToLeaf = ctx->scratch<int>("solve.internalToLeaf", nn, s);
+    oct.leafToInternal = ctx->scratch<int>("solve.leafToInternal", nn, s);
+    oct.d_levelRange   = ctx->scratch<int>("solve.levelRange", kMaxLevel + 2, s);
+    int levelRange[kMaxLevel + 2];
+    linkOctree(ctx, leaves, nl, oct, levelRange, s);
+
+    mark(ctx, P, 2, s);
+    // fused upsweep: node records + FP64 root expansion
+    REQUIRE(P->multipole == RYO_MULTIPOLE_QUADRUPOLE || P->multipole == RYO_MULTIPOLE_MDQ,
+            "solve: unknown multipole type");
+    NodeRecord* records = ctx->scratch<NodeRecord>("solve.records", nn, s);
+    double* root        = ctx->scratch<double>("solve.root", 16, s);
+    float4* dipoles     = P->multipole == RYO_MULTIPOLE_MDQ
+                              ? ctx->scratch<float4>("solve.dipoles", nn, s)
+                              : nullptr;
+    launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
+                       oct.parents, oct.prefixes, 1.0f / P->theta, dbox, records, nullptr, nullptr,
+                       root, s, nullptr, 0, nullptr, dipoles);
+
+    mark(ctx, P, 3, s);
+    // groups and traversal
+    uint32_t numGroups = uint32_t((n + P->groupSize - 1) / P->groupSize);
+    uint32_t* groups   = nullptr;
+    if (P->groupTolerance > 0.f)
+    {
+        // spatial groups (the reference's production grouping); at most one group per body.
+        // No interaction radius: h here is the gravitational softening, not the SPH smoothing
+        // length the grouping's radius criterion was made for, and a tiny softening would split
+        // every pair of bodies.
+        REQUIRE(P->groupSize == 32 || P->groupSize == 64,
+                "solve: spatial groups need groupSize 32 or 64");
+        groups      = ctx->scratch<uint32_t>("solve.groups", n + 2, s);
+        float ratio = P->groupExtentRatio < 0.f ? defaultExtentRatio() : P->groupExtentRatio;
+        numGroups   = computeGroupSplits(ctx, 0, uint32_t(n), x, y, z, nullptr, leaves, nl, layout, dbox,
+                                         P->groupSize, P->groupTolerance, ratio, groups,
+                                         uint32_t(n + 2), s);
+    }
+    else
+    {
+        groups = ctx->scratch<uint32_t>("solve.groups", size_t(numGroups) + 1, s);
+        launchFixedGroups(0, uint32_t(n), P->groupSize, groups, s);
+    }
+    for (float* a : {p, ax, ay, az})
+        RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
+    TraverseLaunch t{};
+    t.groupStart    = groups;
+    t.groupEnd      = groups + 1;
+    t.numGroups     = int(numGroups);
+    t.initNode      = nn == 1 ? 0 : 1;
+    t.numNodes      = nn;
+    t.nodes         = records;
+    t.tgtXYZH       = xyzh;
+    t.tgtM          = m;
+    t.srcXYZM       = xyzm;
+    t.srcH          = h;
+    t.G             = P->G;
+    t.numShells     = periodic ? P->numShells : 0;
+    for (int d = 0; d < 3; ++d)
+        t.boxL[d] = dbox.len[d];
+    t.p  = p;
+    t.ax = ax;
+    t.ay = ay;
+    t.az = az;
+    t.stackCapacity = P->stackCapacity;
+    t.dipoles       = dipoles;
+    uint32_t* gm2p  = ctx->scratch<uint32_t>("solve.groupM2P", numGroups, s);
+    uint32_t* gp2p  = ctx->scratch<uint32_t>("solve.groupP2P", numGroups, s);
+    RYO_CUDA(cudaMemsetAsync(gm2p, 0, sizeof(uint32_t) * numGroups, s));
+    RYO_CUDA(cudaMemsetAsync(gp2p, 0, sizeof(uint32_t) * numGroups, s));
+    t.groupM2P      = gm2p;
+    t.groupP2P      = gp2p;
+    double pot = 0;
+    // a host solve of an open system with fixed groups traverses in chunks of groups and copies each chunk's results
+    // to the host while the next chunk runs
+    const bool chunked = pipe && pipe->chunks > 1 && !periodic && !(P->groupTolerance > 0.f) &&
+                         numGroups >= uint32_t(pipe->chunks);
+    if (!chunked) runTraversal(ctx, t, s, &pot);
+    else
+    {
+        unsigned long long acc[5] = {0, 0, 0, 0, 0};
+        uint64_t retries          = 0;
+        for (int c = 0; c < pipe->chunks; ++c)
+        {
+            uint32_t g0 = uint32_t(uint64_t(numGroups) * uint64_t(c) / uint64_t(pipe->chunks));
+            uint32_t g1 = uint32_t(uint64_t(numGroups) * uint64_t(c + 1) / uint64_t(pipe->chunks));
+            TraverseLaunch tc = t;
+            tc.groupStart     = groups + g0;
+            tc.groupEnd       = groups + g0 + 1;
+            tc.numGroups      = int(g1 - g0);
+            tc.groupM2P       = gm2p + g0;
+            tc.groupP2P       = gp2p + g0;
+            double cp         = 0;
+            runTraversal(ctx, tc, s, &cp);
+            pot += cp;
+            acc[kSumP2P] += ctx->hostStats[kSumP2P];
+            acc[kSumM2P] += ctx->hostStats[kSumM2P];
+            for (int k : {int(kMaxP2P), int(kMaxM2P), int(kMaxStack)})
+                acc[k] = std::max(acc[k], ctx->hostStats[k]);
+            retries += ctx->retries;
+            // fixed groups: group k holds bodies [k G, min((k + 1) G, n))
+            size_t b0 = size_t(g0) * P->groupSize, b1 = std::min(size_t(g1) * P->groupSize, n);
+            streamAfter(ctx, pipe->copy, s, 0);
+            d2h(pipe->hp + b0, p + b0, (b1 - b0) * sizeof(float), pipe->copy);
+            d2h(pipe->hax + b0, ax + b0, (b1 - b0) * sizeof(float), pipe->copy);
+            d2h(pipe->hay + b0, ay + b0, (b1 - b0) * sizeof(float), pipe->copy);
+            d2h(pipe->haz + b0, az + b0, (b1 - b0) * sizeof(float), pipe->copy);
+        }
+        for (int k = 0; k < 5; ++k)
+            ctx->hostStats[k] = acc[k];
+        ctx->retries = retries;
+    }
+    double energy = 0.5 * double(P->G) * pot;
+    mark(ctx, P, 4, s);
+
+    if (periodic)
+    {
+        if (!(dbox.len[0] == dbox.len[1] && dbox.len[1] == dbox.len[2]))
+            throw ApiError{RYO_ERR_NOT_CUBIC, "solve: Ewald needs a cubic periodic box"};
+        double hr[16];
+        RYO_CUDA(cudaMemcpyAsync(hr, root, sizeof(double) * 11, cudaMemcpyDeviceToHost, s));
+        RYO_CUDA(cudaStreamSynchronize(s));
+        EwaldHost e = ewaldSetup(hr + 3, hr, P->ewald.numReplicaShells, double(dbox.len[0]),
+                                 P->ewald.lCut, P->ewald.hCut, P->ewald.alpha_scale,
+                                 P->ewald.small_R_scale_factor);
+        double* ep = &ctx->ctl->ewaldPotential;
+        RYO_CUDA(cudaMemsetAsync(ep, 0, sizeof(double), s));
+        launchEwaldGroups(e, groups, groups + 1, numGroups, x, y, z, m, P->G, p, ax, ay, az, ep, s);
+        double he = 0;
+        RYO_CUDA(cudaMemcpyAsync(&he, ep, sizeof(double), cudaMemcpyDeviceToHost, s));
+        RYO_CUDA(cudaStreamSynchronize(s));
+        energy += 0.5 * double(P->G) * he;
+    }
+    if (pipe && !chunked)
+    {
+        streamAfter(ctx, pipe->copy, s, 0);
+        d2h(pipe->hp, p, n * sizeof(float), pipe->copy);
+        d2h(pipe->hax, ax, n * sizeof(float), pipe->copy);
+        d2h(pipe->hay, ay, n * sizeof(float), pipe->copy);
+        d2h(pipe->haz, az, n * sizeof(float), pipe->copy);
+    }
+    mark(ctx, P, 5, s);
+    mark(ctx, P, 6, s);
+    float ms[6] = {0, 0, 0, 0, 0, 0};
+    if (P->timing)
+    {
+        RYO_CUDA(cudaEventSynchronize(ctx->phaseEvents[6]));
+        for (int i = 0; i < 5; ++i)
+            RYO_CUDA(cudaEventElapsedTime(&ms[i], ctx->phaseEvents[i], ctx->phaseEvents[i + 1]));
+        RYO_CUDA(cudaEventElapsedTime(&ms[5], ctx->phaseEvents[0], ctx->phaseEvents[6]));
+    }
+    {
+        auto& st      = ctx->solveState;
+        st.valid      = true;
+        st.nodes      = records;
+        st.xyzm       = xyzm;
+        st.srcH       = h;
+        st.numNodes   = nn;
+        st.groupSize  = P->groupSize;
+        st.G          = P->G;
+        st.periodic   = periodic ? 1 : 0;
+        st.numShells  = periodic ? P->numShells : 0;
+        st.box        = box;
+        st.ewald      = P->ewald;
+        st.dipoles    = dipoles;
+        ryo_solve_arrays& a = ctx->lastSolve;
+        a.numLeaves         = nl;
+        a.numNodes          = nn;
+        a.numGroups         = int(numGroups);
+        a.sortedKeys        = sorted;
+        a.order             = order;
+        a.leaves            = leaves;
+        a.layout            = layout;
+        a.prefixes          = oct.prefixes;
+        a.childOffsets      = oct.childOffsets;
+        a.internalToLeaf    = oct.internalToLeaf;
+        a.leafToInternal    = oct.leafToInternal;
+        a.parents           = oct.parents;
+        a.nodeData          = reinterpret_cast<const float*>(records);
+        a.groups            = groups;
+        a.groupM2P          = gm2p;
+        a.groupP2P          = gp2p;
+        a.dipoles           = reinterpret_cast<const float*>(dipoles);
+        for (int i = 0; i < kMaxLevel + 2; ++i)
+            a.levelRange[i] = levelRange[i];
+        double hr[11];
+        RYO_CUDA(cudaMemcpyAsync(hr, root, sizeof(hr), cudaMemcpyDeviceToHost, s));
+        RYO_CUDA(cudaStreamSynchronize(s));
+        for (int i = 0; i < 3; ++i)
+            a.rootCenter[i] = hr[i];
+        for (int i = 0; i < 8; ++i)
+            a.rootMultipole[i] = hr[3 + i];
+        for (int i = 0; i < 11; ++i)
+            st.root[i] = hr[i];
+    }
+    if (ctx->hostStats[kMaxP2P] == 0xFFFFFFFFull)
+        throw ApiError{RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE, "solve: a single target overflowed"};
+    checkDeviceError(ctx, s);
+    if (stats)
+    {
+        stats->numLeaves       = nl;
+        stats->numNodes        = nn;
+        stats->numGroups       = int(numGroups);
+        stats->sumP2P          = ctx->hostStats[kSumP2P];
+        stats->maxP2P          = ctx->hostStats[kMaxP2P];
+        stats->sumM2P          = ctx->hostStats[kSumM2P];
+        stats->maxM2P          = ctx->hostStats[kMaxM2P];
+        stats->maxStack        = ctx->hostStats[kMaxStack];
+        stats->retries         = ctx->retries;
+        stats->potentialEnergy = energy;
+        for (int i = 0; i < 6; ++i)
+        {
+            stats->box[i] = box.limits[i];
+            stats->ms[i]  = ms[i];
+        }
+    }
+}
+} // namespace
+
 extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, float* x, float* y, float* z, float* m,
                                     float* h, float* vx, float* vy, float* vz, size_t n, float* p, float* ax,
                                     float* ay, float* az, uint32_t* orderOut, ryo_solve_stats* stats,
@@ -920,259 +1262,43 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
 {
     if (!ctx || !P) return RYO_ERR_BAD_ARG;
     return guarded(ctx->lastError,
+                   [&] { solveSingle(ctx, P, x, y, z, m, h, vx, vy, vz, n, p, ax, ay, az, orderOut, stats, stream,
+                                     nullptr); });
+}
+
+extern "C" ryo_status ryo_solve_host_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, const float* x, const float* y,
+                                         const float* z, const float* m, const float* h, size_t n, float* xs,
+                                         float* ys, float* zs, float* p, float* ax, float* ay, float* az,
+                                         uint32_t* order, ryo_solve_stats* stats, ryo_stream_t stream)
+{
+    if (!ctx || !P) return RYO_ERR_BAD_ARG;
+    return guarded(ctx->lastError,
                    [&]
                    {
-                       REQUIRE(x && y && z && m && h && p && ax && ay && az, "solve: null argument");
-                       REQUIRE(n > 0 && n < (size_t(1) << 32), "solve: body count must be in [1, 2^32)");
-                       REQUIRE(P->groupSize >= 1 && P->groupSize <= 64, "solve: groupSize must be in [1, 64]");
-                       REQUIRE(P->bucketSize >= 1 && P->theta > 0.f, "solve: bad bucketSize or theta");
+                       REQUIRE(x && y && z && m && h && p && ax && ay && az, "solve_host: null argument");
+                       REQUIRE(n > 0 && n < (size_t(1) << 32), "solve_host: body count must be in [1, 2^32)");
                        cudaStream_t s = stream;
-                       mark(ctx, P, 0, s);
-
-                       // box: given, or the cube enclosing the data (exact min/max)
-                       ryo_box_f32 box{};
-                       if (P->useBox) { box = P->box; }
-                       else
-                       {
-                           double* mm = ctx->scratch<double>("solve.bbox", 6, s);
-                           launchBoundingBox(x, y, z, n, mm, s);
-                           double hb[6];
-                           RYO_CUDA(cudaMemcpyAsync(hb, mm, sizeof(hb), cudaMemcpyDeviceToHost, s));
-                           RYO_CUDA(cudaStreamSynchronize(s));
-                           double ext = std::max({hb[1] - hb[0], hb[3] - hb[2], hb[5] - hb[4]});
-                           if (!(ext > 0)) ext = 1.0;
-                           for (int d = 0; d < 3; ++d)
-                           {
-                               box.limits[2 * d]     = float(hb[2 * d]);
-                               box.limits[2 * d + 1] = float(hb[2 * d] + ext);
-                               if (!(box.limits[2 * d + 1] >= float(hb[2 * d + 1])))
-                                   box.limits[2 * d + 1] = std::nextafter(float(hb[2 * d + 1]), 3.4e38f);
-                               box.boundary[d] = RYO_BOUNDARY_OPEN;
-                           }
-                       }
-                       checkBox(box.limits);
-                       DevBox<float> dbox = boxOf(&box);
-                       bool periodic      = dbox.periodic;
-
-                       // keys and sort
-                       uint64_t* keys    = ctx->scratch<uint64_t>("solve.keys", n, s);
-                       uint64_t* keysAlt = ctx->scratch<uint64_t>("solve.keysAlt", n, s);
-                       uint32_t* ord     = ctx->scratch<uint32_t>("solve.order", n, s);
-                       uint32_t* ordAlt  = ctx->scratch<uint32_t>("solve.orderAlt", n, s);
-                       size_t tmpBytes   = sortTempBytes(n);
-                       void* tmp         = ctx->scratch<char>("solve.sorttmp", tmpBytes, s);
-                       launchKeys<float>(x, y, z, keys, n, dbox, false, s);
-                       bool alt = radixSortPairs(keys, ord, keysAlt, ordAlt, n, 0, 64, tmp, tmpBytes, &ctx->ctl->error,
-                                                 s, true);
-                       const uint64_t* sorted = alt ? keysAlt : keys;
-                       const uint32_t* order  = alt ? ordAlt : ord;
-
-                       // permute every per-particle array
-                       float* tmpF = ctx->scratch<float>("solve.tmpf", n, s);
-                       for (float* a : {x, y, z, m, h, vx, vy, vz})
-                       {
-                           if (!a) continue;
-                           launchGather(order, a, tmpF, n, s);
-                           RYO_CUDA(cudaMemcpyAsync(a, tmpF, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-                       }
-                       if (orderOut)
-                           RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-                       mark(ctx, P, 1, s);
-                       float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
-                       float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
-                       packSolveBodies<<<ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
-                                                                                        : unsigned(ctx->smCount * 16),
-                                         256, 0, s>>>(x, y, z, m, h, n, xyzm, xyzh);
-                       RYO_LAUNCH_CHECK();
-
-                       // leaves, links
-                       int cap           = int(std::min<size_t>(n / 2 + 64, size_t(1) << 30));
-                       uint64_t* leaves  = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
-                       uint32_t* counts  = ctx->scratch<uint32_t>("solve.counts", cap, s);
-                       uint32_t* layout  = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
-                       int nl = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s);
-                       if (nl > cap)
-                       {
-                           cap    = nl;
-                           leaves = ctx->scratch<uint64_t>("solve.leaves", size_t(cap) + 1, s);
-                           counts = ctx->scratch<uint32_t>("solve.counts", cap, s);
-                           layout = ctx->scratch<uint32_t>("solve.layout", size_t(cap) + 1, s);
-                           nl     = buildLeaves(ctx, sorted, n, P->bucketSize, leaves, counts, layout, cap, s);
-                       }
-                       int ni = (nl - 1) / 7, nn = nl + ni;
-                       OctreeArrays oct;
-                       oct.prefixes       = ctx->scratch<uint64_t>("solve.prefixes", nn, s);
-                       oct.childOffsets   = ctx->scratch<int>("solve.childOffsets", size_t(nn) + 1, s);
-                       oct.parents        = ctx->scratch<int>("solve.parents", std::max(1, (nn - 1) / 8), s);
-                       oct.internalToLeaf = ctx->scratch<int>("solve.internalToLeaf", nn, s);
-                       oct.leafToInternal = ctx->scratch<int>("solve.leafToInternal", nn, s);
-                       oct.d_levelRange   = ctx->scratch<int>("solve.levelRange", kMaxLevel + 2, s);
-                       int levelRange[kMaxLevel + 2];
-                       linkOctree(ctx, leaves, nl, oct, levelRange, s);
-
-                       mark(ctx, P, 2, s);
-                       // fused upsweep: node records + FP64 root expansion
-                       REQUIRE(P->multipole == RYO_MULTIPOLE_QUADRUPOLE || P->multipole == RYO_MULTIPOLE_MDQ,
-                               "solve: unknown multipole type");
-                       NodeRecord* records = ctx->scratch<NodeRecord>("solve.records", nn, s);
-                       double* root        = ctx->scratch<double>("solve.root", 16, s);
-                       float4* dipoles     = P->multipole == RYO_MULTIPOLE_MDQ
-                                                 ? ctx->scratch<float4>("solve.dipoles", nn, s)
-                                                 : nullptr;
-                       launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
-                                          oct.parents, oct.prefixes, 1.0f / P->theta, dbox, records, nullptr, nullptr,
-                                          root, s, nullptr, 0, nullptr, dipoles);
-
-                       mark(ctx, P, 3, s);
-                       // groups and traversal
-                       uint32_t numGroups = uint32_t((n + P->groupSize - 1) / P->groupSize);
-                       uint32_t* groups   = nullptr;
-                       if (P->groupTolerance > 0.f)
-                       {
-                           // spatial groups (the reference's production grouping); at most one group per body.
-                           // No interaction radius: h here is the gravitational softening, not the SPH smoothing
-                           // length the grouping's radius criterion was made for, and a tiny softening would split
-                           // every pair of bodies.
-                           REQUIRE(P->groupSize == 32 || P->groupSize == 64,
-                                   "solve: spatial groups need groupSize 32 or 64");
-                           groups      = ctx->scratch<uint32_t>("solve.groups", n + 2, s);
-                           float ratio = P->groupExtentRatio < 0.f ? defaultExtentRatio() : P->groupExtentRatio;
-                           numGroups   = computeGroupSplits(ctx, 0, uint32_t(n), x, y, z, nullptr, leaves, nl, layout, dbox,
-                                                            P->groupSize, P->groupTolerance, ratio, groups,
-                                                            uint32_t(n + 2), s);
-                       }
-                       else
-                       {
-                           groups = ctx->scratch<uint32_t>("solve.groups", size_t(numGroups) + 1, s);
-                           launchFixedGroups(0, uint32_t(n), P->groupSize, groups, s);
-                       }
-                       for (float* a : {p, ax, ay, az})
-                           RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
-                       TraverseLaunch t{};
-                       t.groupStart    = groups;
-                       t.groupEnd      = groups + 1;
-                       t.numGroups     = int(numGroups);
-                       t.initNode      = nn == 1 ? 0 : 1;
-                       t.numNodes      = nn;
-                       t.nodes         = records;
-                       t.tgtXYZH       = xyzh;
-                       t.tgtM          = m;
-                       t.srcXYZM       = xyzm;
-                       t.srcH          = h;
-                       t.G             = P->G;
-                       t.numShells     = periodic ? P->numShells : 0;
-                       for (int d = 0; d < 3; ++d)
-                           t.boxL[d] = dbox.len[d];
-                       t.p  = p;
-                       t.ax = ax;
-                       t.ay = ay;
-                       t.az = az;
-                       t.stackCapacity = P->stackCapacity;
-                       t.dipoles       = dipoles;
-                       uint32_t* gm2p  = ctx->scratch<uint32_t>("solve.groupM2P", numGroups, s);
-                       uint32_t* gp2p  = ctx->scratch<uint32_t>("solve.groupP2P", numGroups, s);
-                       RYO_CUDA(cudaMemsetAsync(gm2p, 0, sizeof(uint32_t) * numGroups, s));
-                       RYO_CUDA(cudaMemsetAsync(gp2p, 0, sizeof(uint32_t) * numGroups, s));
-                       t.groupM2P      = gm2p;
-                       t.groupP2P      = gp2p;
-                       double pot      = 0;
-                       runTraversal(ctx, t, s, &pot);
-                       double energy = 0.5 * double(P->G) * pot;
-                       mark(ctx, P, 4, s);
-
-                       if (periodic)
-                       {
-                           if (!(dbox.len[0] == dbox.len[1] && dbox.len[1] == dbox.len[2]))
-                               throw ApiError{RYO_ERR_NOT_CUBIC, "solve: Ewald needs a cubic periodic box"};
-                           double hr[16];
-                           RYO_CUDA(cudaMemcpyAsync(hr, root, sizeof(double) * 11, cudaMemcpyDeviceToHost, s));
-                           RYO_CUDA(cudaStreamSynchronize(s));
-                           EwaldHost e = ewaldSetup(hr + 3, hr, P->ewald.numReplicaShells, double(dbox.len[0]),
-                                                    P->ewald.lCut, P->ewald.hCut, P->ewald.alpha_scale,
-                                                    P->ewald.small_R_scale_factor);
-                           double* ep = &ctx->ctl->ewaldPotential;
-                           RYO_CUDA(cudaMemsetAsync(ep, 0, sizeof(double), s));
-                           launchEwaldGroups(e, groups, groups + 1, numGroups, x, y, z, m, P->G, p, ax, ay, az, ep, s);
-                           double he = 0;
-                           RYO_CUDA(cudaMemcpyAsync(&he, ep, sizeof(double), cudaMemcpyDeviceToHost, s));
-                           RYO_CUDA(cudaStreamSynchronize(s));
-                           energy += 0.5 * double(P->G) * he;
-                       }
-                       mark(ctx, P, 5, s);
-                       mark(ctx, P, 6, s);
-                       float ms[6] = {0, 0, 0, 0, 0, 0};
-                       if (P->timing)
-                       {
-                           RYO_CUDA(cudaEventSynchronize(ctx->phaseEvents[6]));
-                           for (int i = 0; i < 5; ++i)
-                               RYO_CUDA(cudaEventElapsedTime(&ms[i], ctx->phaseEvents[i], ctx->phaseEvents[i + 1]));
-                           RYO_CUDA(cudaEventElapsedTime(&ms[5], ctx->phaseEvents[0], ctx->phaseEvents[6]));
-                       }
-                       {
-                           auto& st      = ctx->solveState;
-                           st.valid      = true;
-                           st.nodes      = records;
-                           st.xyzm       = xyzm;
-                           st.srcH       = h;
-                           st.numNodes   = nn;
-                           st.groupSize  = P->groupSize;
-                           st.G          = P->G;
-                           st.periodic   = periodic ? 1 : 0;
-                           st.numShells  = periodic ? P->numShells : 0;
-                           st.box        = box;
-                           st.ewald      = P->ewald;
-                           st.dipoles    = dipoles;
-                           ryo_solve_arrays& a = ctx->lastSolve;
-                           a.numLeaves         = nl;
-                           a.numNodes          = nn;
-                           a.numGroups         = int(numGroups);
-                           a.sortedKeys        = sorted;
-                           a.order             = order;
-                           a.leaves            = leaves;
-                           a.layout            = layout;
-                           a.prefixes          = oct.prefixes;
-                           a.childOffsets      = oct.childOffsets;
-                           a.internalToLeaf    = oct.internalToLeaf;
-                           a.leafToInternal    = oct.leafToInternal;
-                           a.parents           = oct.parents;
-                           a.nodeData          = reinterpret_cast<const float*>(records);
-                           a.groups            = groups;
-                           a.groupM2P          = gm2p;
-                           a.groupP2P          = gp2p;
-                           a.dipoles           = reinterpret_cast<const float*>(dipoles);
-                           for (int i = 0; i < kMaxLevel + 2; ++i)
-                               a.levelRange[i] = levelRange[i];
-                           double hr[11];
-                           RYO_CUDA(cudaMemcpyAsync(hr, root, sizeof(hr), cudaMemcpyDeviceToHost, s));
-                           RYO_CUDA(cudaStreamSynchronize(s));
-                           for (int i = 0; i < 3; ++i)
-                               a.rootCenter[i] = hr[i];
-                           for (int i = 0; i < 8; ++i)
-                               a.rootMultipole[i] = hr[3 + i];
-                           for (int i = 0; i < 11; ++i)
-                               st.root[i] = hr[i];
-                       }
-                       if (ctx->hostStats[kMaxP2P] == 0xFFFFFFFFull)
-                           throw ApiError{RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE, "solve: a single target overflowed"};
-                       checkDeviceError(ctx, s);
-                       if (stats)
-                       {
-                           stats->numLeaves       = nl;
-                           stats->numNodes        = nn;
-                           stats->numGroups       = int(numGroups);
-                           stats->sumP2P          = ctx->hostStats[kSumP2P];
-                           stats->maxP2P          = ctx->hostStats[kMaxP2P];
-                           stats->sumM2P          = ctx->hostStats[kSumM2P];
-                           stats->maxM2P          = ctx->hostStats[kMaxM2P];
-                           stats->maxStack        = ctx->hostStats[kMaxStack];
-                           stats->retries         = ctx->retries;
-                           stats->potentialEnergy = energy;
-                           for (int i = 0; i < 6; ++i)
-                           {
-                               stats->box[i] = box.limits[i];
-                               stats->ms[i]  = ms[i];
-                           }
-                       }
+                       if (!ctx->copyStream)
+                           RYO_CUDA(cudaStreamCreateWithFlags(&ctx->copyStream, cudaStreamNonBlocking));
+                       float* d[9];
+                       const char* names[9] = {"host.x", "host.y", "host.z", "host.m", "host.h",
+                                               "host.p", "host.ax", "host.ay", "host.az"};
+                       for (int k = 0; k < 9; ++k)
+                           d[k] = ctx->scratch<float>(names[k], n, s);
+                       // the copy stream starts after the work already queued on s, which may still use the buffers
+                       streamAfter(ctx, ctx->copyStream, s, 1);
+                       const size_t bytes = n * sizeof(float);
+                       RYO_CUDA(cudaMemcpyAsync(d[0], x, bytes, cudaMemcpyHostToDevice, s));
+                       RYO_CUDA(cudaMemcpyAsync(d[1], y, bytes, cudaMemcpyHostToDevice, s));
+                       RYO_CUDA(cudaMemcpyAsync(d[2], z, bytes, cudaMemcpyHostToDevice, s));
+                       RYO_CUDA(cudaMemcpyAsync(d[3], m, bytes, cudaMemcpyHostToDevice, ctx->copyStream));
+                       RYO_CUDA(cudaMemcpyAsync(d[4], h, bytes, cudaMemcpyHostToDevice, ctx->copyStream));
+                       RYO_CUDA(cudaEventRecord(ctx->pipeEvents[1], ctx->copyStream));
+                       HostPipe pipe{ctx->copyStream, ctx->pipeEvents[1], xs, ys, zs, p, ax, ay, az, order, 8};
+                       solveSingle(ctx, P, d[0], d[1], d[2], d[3], d[4], nullptr, nullptr, nullptr, n, d[5], d[6],
+                                   d[7], d[8], nullptr, stats, s, &pipe);
+                       RYO_CUDA(cudaStreamSynchronize(ctx->copyStream));
+                       RYO_CUDA(cudaStreamSynchronize(s));
                    });
 }
 

@@ -31,27 +31,36 @@ struct Arena
     float* a[kArenaArrays] = {};
     uint32_t* id           = nullptr;
     size_t capacity        = 0;
+    void* block            = nullptr; // all arrays in one allocation
 
+    //! room for at least @p n bodies; growth doubles, so a growing stream reallocates O(log n) times (each
+    //! reallocation frees, which waits for the device)
     void ensure(size_t n)
     {
         if (n <= capacity) return;
-        release();
-        size_t cap = std::max<size_t>(n, capacity + capacity / 2);
+        release_();
+        size_t cap = std::max<size_t>(n, 2 * capacity);
+        cap        = (cap + 63) / 64 * 64; // every array starts on a 256-byte boundary
+        RYO_CUDA(cudaMalloc(&block, (kArenaArrays + 1) * cap * sizeof(float)));
         for (int k = 0; k < kArenaArrays; ++k)
-            RYO_CUDA(cudaMalloc(&a[k], cap * sizeof(float)));
-        RYO_CUDA(cudaMalloc(&id, cap * sizeof(uint32_t)));
+            a[k] = static_cast<float*>(block) + size_t(k) * cap;
+        id       = reinterpret_cast<uint32_t*>(static_cast<float*>(block) + size_t(kArenaArrays) * cap);
         capacity = cap;
     }
     void release()
     {
-        for (int k = 0; k < kArenaArrays; ++k)
-        {
-            if (a[k]) cudaFree(a[k]);
-            a[k] = nullptr;
-        }
-        if (id) cudaFree(id);
-        id       = nullptr;
+        release_();
         capacity = 0;
+    }
+
+private:
+    void release_()
+    {
+        if (block) cudaFree(block);
+        block = nullptr;
+        for (int k = 0; k < kArenaArrays; ++k)
+            a[k] = nullptr;
+        id = nullptr;
     }
 };
 
@@ -352,6 +361,7 @@ extern "C" void ryo_engine_params_default(ryo_engine_params* p)
     p->hbmBudgetBytes = 120e9;
     p->bytesPerBody   = 256.0;
     p->maxSystems     = RYO_BATCH_MAX_SYSTEMS;
+    p->reserveBodies  = 0;
 }
 
 extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params* p, ryo_engine_t** out)
@@ -360,20 +370,33 @@ extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params*
     if (!(p->hbmBudgetBytes > 0) || !(p->bytesPerBody > 0) || p->maxSystems < 1 ||
         p->maxSystems > RYO_BATCH_MAX_SYSTEMS)
         return RYO_ERR_BAD_ARG;
+    ryo_engine* E = nullptr;
     try
     {
-        auto* E         = new ryo_engine();
+        E               = new ryo_engine();
         E->ctx          = ctx;
         E->solve        = p->solve;
         E->budget       = p->hbmBudgetBytes;
         E->bytesPerBody = p->bytesPerBody;
         E->maxSystems   = p->maxSystems;
-        *out            = E;
+        if (p->reserveBodies > 0)
+        {
+            E->arenas.buf[0].ensure(p->reserveBodies);
+            E->arenas.buf[1].ensure(p->reserveBodies);
+        }
+        *out = E;
         return RYO_OK;
     }
     catch (const std::bad_alloc&)
     {
+        delete E;
         return RYO_ERR_OOM;
+    }
+    catch (const CudaError& e)
+    {
+        ctx->lastError = std::string("engine_create: ") + e.what + ": " + cudaGetErrorString(e.err);
+        delete E;
+        return e.err == cudaErrorMemoryAllocation ? RYO_ERR_OOM : RYO_ERR_CUDA;
     }
 }
 
@@ -434,6 +457,10 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                        {
                            cudaStream_t s = stream;
                            ryo_engine_step_info st{};
+                           using Clock = std::chrono::steady_clock;
+                           auto since  = [](Clock::time_point t0)
+                           { return float(std::chrono::duration<double, std::milli>(Clock::now() - t0).count()); };
+                           auto t0 = Clock::now();
                            // admission: arrival order, while the budget and the system slots allow
                            std::vector<Request> admitted;
                            while (!E->queue.empty() &&
@@ -493,6 +520,8 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                            RYO_CUDA(cudaMemsetAsync(dKin, 0, sizeof(double) * ns, s));
                            engineKickDrift<<<gridFor(n, E->ctx->smCount), 256, 0, s>>>(P, n, dFirst, ns, dSys);
                            RYO_LAUNCH_CHECK();
+                           st.hostMs[0] = since(t0);
+                           auto t1      = Clock::now();
 
                            uint32_t* order = E->ctx->scratch<uint32_t>("eng.order", n, s);
                            std::vector<double> pe(ns);
@@ -503,6 +532,8 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                                                                nullptr, &ss, s);
                            if (rs != RYO_OK)
                                throw SolveFailed{rs, "engine_step: batched solve failed: " + E->ctx->lastError};
+                           st.hostMs[1] = since(t1);
+                           auto t2      = Clock::now();
                            E->solves += ns;
                            uint32_t* idTmp = E->ctx->scratch<uint32_t>("eng.idtmp", n, s);
                            engineGatherIds<<<gridFor(n, E->ctx->smCount), 256, 0, s>>>(order, A.id, idTmp, n);
@@ -513,9 +544,21 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                            std::vector<double> ke(ns);
                            RYO_CUDA(cudaMemcpyAsync(ke.data(), dKin, sizeof(double) * ns, cudaMemcpyDeviceToHost, s));
                            RYO_CUDA(cudaStreamSynchronize(s));
+                           st.hostMs[2] = since(t2);
+                           auto t3      = Clock::now();
 
-                           // advance the requests; retire the finished ones
+                           // advance the requests; retire the finished ones. Their final states are gathered into
+                           // one device buffer and copied out with a single wait at the end of the step.
                            std::vector<Request> keep;
+                           size_t outFloats = 0;
+                           for (uint32_t k = 0; k < ns; ++k)
+                           {
+                               const Request& q = E->resident[k];
+                               bool last        = q.haveForces ? q.stepsLeft <= 1 : q.stepsLeft <= 0;
+                               if (last && q.out) outFloats += 10 * size_t(q.n);
+                           }
+                           float* results = outFloats ? E->ctx->scratch<float>("eng.result", outFloats, s) : nullptr;
+                           size_t outAt   = 0;
                            for (uint32_t k = 0; k < ns; ++k)
                            {
                                Request& q = E->resident[k];
@@ -536,12 +579,12 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                                }
                                if (q.out)
                                {
-                                   float* tmp = E->ctx->scratch<float>("eng.result", 10 * size_t(q.n), s);
+                                   float* tmp = results + outAt;
+                                   outAt += 10 * size_t(q.n);
                                    engineScatterResult<<<ceilDiv(q.n, 256), 256, 0, s>>>(P, q.arenaFirst, q.n, tmp);
                                    RYO_LAUNCH_CHECK();
                                    RYO_CUDA(cudaMemcpyAsync(q.out, tmp, 10 * size_t(q.n) * sizeof(float),
                                                             cudaMemcpyDeviceToHost, s));
-                                   RYO_CUDA(cudaStreamSynchronize(s));
                                }
                                ryo_engine_result res{};
                                res.tag             = q.tag;
@@ -555,7 +598,9 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                                ++st.retired;
                                E->changed = true;
                            }
+                           if (outAt) RYO_CUDA(cudaStreamSynchronize(s));
                            E->resident.swap(keep);
+                           st.hostMs[3] = since(t3);
                            st.solved    = int(ns);
                            st.retries   = int(ss.retries);
                            st.sumP2P    = ss.sumP2P;

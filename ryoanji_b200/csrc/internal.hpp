@@ -3,6 +3,7 @@
  */
 #pragma once
 
+#include <algorithm>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -65,6 +66,8 @@ struct ryo_ctx
         double root[11]    = {};
     } solveState;
     cudaEvent_t phaseEvents[7]      = {};
+    cudaEvent_t pipeEvents[2]       = {};    // ordering between the solve and the copy stream of host solves
+    cudaStream_t copyStream         = nullptr; // host solves: copies that overlap the solve
 
     struct Buffer
     {
@@ -82,7 +85,10 @@ struct ryo_ctx
         Buffer& b = buffers[name];
         if (b.bytes < bytes)
         {
-            // growth is rare: wait for work that may still use the old buffer, then reallocate
+            // growth is rare: wait for work that may still use the old buffer, then reallocate. A buffer that
+            // grows again takes at least 1.5 times its old size, so a growing workload (a served stream)
+            // reallocates O(log n) times.
+            size_t old = b.bytes;
             if (b.ptr)
             {
                 RYO_CUDA(cudaStreamSynchronize(s));
@@ -90,7 +96,7 @@ struct ryo_ctx
                 b.ptr   = nullptr;
                 b.bytes = 0;
             }
-            size_t grow = bytes + bytes / 8;
+            size_t grow = std::max(bytes + bytes / 8, old + old / 2);
             RYO_CUDA(cudaMalloc(&b.ptr, grow));
             b.bytes = grow;
         }
@@ -101,6 +107,10 @@ struct ryo_ctx
     {
         for (auto& e : phaseEvents)
             if (e) cudaEventDestroy(e);
+        for (auto& e : pipeEvents)
+            if (e) cudaEventDestroy(e);
+        if (copyStream) cudaStreamDestroy(copyStream);
+        copyStream = nullptr;
         for (auto& kv : buffers)
             if (kv.second.ptr) cudaFree(kv.second.ptr);
         buffers.clear();

@@ -28,10 +28,10 @@ def _requests():
     ] + [dict(tag=10 + k, p=ds.plummer(300 + 50 * k, seed=20 + k), steps=1 + k % 3, box=None) for k in range(6)]
 
 
-def _submit(eng, r, dt=1e-3):
+def _submit(eng, r, dt=1e-3, out=None):
     p = r["p"]
     eng.submit(r["tag"], p.x, p.y, p.z, p.m, p.h, p.vx, p.vy, p.vz, box=r["box"], steps=r["steps"], dt=dt,
-               want_output=True)
+               want_output=True, out=out)
 
 
 def _drain(eng, max_steps=200):
@@ -62,12 +62,15 @@ def test_each_request_same_alone_and_in_the_mix():
     mixed.update(_drain(mix))
     assert sorted(mixed) == sorted(r["tag"] for r in reqs)
     for r in reqs:
-        alone = ryo.Engine(params)
-        _submit(alone, r)
+        # alone: arenas reserved up front, final state into a caller's pinned buffer
+        alone = ryo.Engine(params, reserve_bodies=20000)
+        out = torch.empty((10, r["p"].n), dtype=torch.float32).pin_memory()
+        _submit(alone, r, out=out)
         a = _drain(alone)[r["tag"]]
         b = mixed[r["tag"]]
         assert a["steps"] == b["steps"] == r["steps"]
-        sa, sb = a["state"], b["state"]
+        assert a["state"] is out
+        sa, sb = out.numpy(), b["state"]
         scale = np.abs(sa).max(axis=1, keepdims=True) + 1e-30
         rel = float((np.abs(sa - sb) / scale).max())
         assert rel <= 1e-5, (r["tag"], rel)

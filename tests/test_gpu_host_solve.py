@@ -1,0 +1,76 @@
+"""Solve from and to host memory (ryo_solve_host_f32): the same results as the device solve.
+
+Inputs come from pinned host tensors and are left unchanged; outputs (sorted positions, order, potential and
+acceleration in SFC order) land in host tensors. The traversal of an open system runs in chunks of groups whose
+results download while the next chunk runs: every group is computed by the same kernel code as in one launch, so
+the results are bit-identical, except for groups split over several warps, whose part count may differ (rounding).
+"""
+import numpy as np
+import pytest
+import torch
+
+from ryoanji_b200 import datasets as ds
+
+pytestmark = pytest.mark.gpu
+
+
+def _pinned(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+
+
+def _compare(pset, params, exact):
+    import ryoanji_b200 as ryo
+    n = pset.n
+    hin = [_pinned(a) for a in (pset.x, pset.y, pset.z, pset.m, pset.h)]
+    before = [t.clone() for t in hin]
+    hout = [torch.empty(n).pin_memory() for _ in range(4)]
+    hxyz = [torch.empty(n).pin_memory() for _ in range(3)]
+    hord = torch.empty(n, dtype=torch.int32).pin_memory()
+    ctx = ryo.Context()
+    rh = ryo.solve_host(*hin, *hout, params=params, sorted_xyz=hxyz, order=hord, ctx=ctx)
+    for a, b in zip(hin, before):
+        assert torch.equal(a, b)  # inputs untouched
+
+    d = [t.cuda() for t in hin]
+    dout = [torch.empty(n, device="cuda") for _ in range(4)]
+    dord = torch.empty(n, dtype=torch.int32, device="cuda")
+    rd = ryo.solve(*d, *dout, params=params, order=dord, ctx=ctx)
+    assert torch.equal(hord, dord.cpu())
+    for a, b in zip(hxyz, d[:3]):
+        assert torch.equal(a, b.cpu())
+    assert (rh.sum_p2p, rh.max_p2p, rh.sum_m2p, rh.max_m2p) == (rd.sum_p2p, rd.max_p2p, rd.sum_m2p, rd.max_m2p)
+    for a, b in zip(hout, dout):
+        b = b.cpu()
+        if exact:
+            assert torch.equal(a, b)
+        else:
+            scale = b.abs().max()
+            assert float((a - b).abs().max()) <= 1e-6 * float(scale)
+    assert rh.potential_energy == pytest.approx(rd.potential_energy, rel=1e-9 if exact else 1e-6)
+    return rh
+
+
+def test_host_solve_equals_device_solve_cube():
+    import ryoanji_b200 as ryo
+    _compare(ds.uniform_cube(300000, seed=3), ryo.SolveParams(theta=0.5), exact=True)
+
+
+def test_host_solve_equals_device_solve_with_split_groups():
+    import ryoanji_b200 as ryo
+    r = _compare(ds.plummer(100000, seed=1, velocities=False), ryo.SolveParams(theta=0.5), exact=False)
+    assert r.max_p2p > 16384  # the sparse outskirts took the split path
+
+
+def test_host_solve_periodic_and_small():
+    import ryoanji_b200 as ryo
+    p = ds.periodic_box(20000, seed=6, eps=0.002)
+    box = ryo.Box(*p.box, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
+    _compare(p, ryo.SolveParams(theta=0.5, box=box), exact=True)
+    _compare(ds.uniform_cube(100, seed=4, eps=0.01), ryo.SolveParams(theta=0.5), exact=True)  # fewer groups than chunks
+
+
+def test_host_solve_rejects_device_tensors():
+    import ryoanji_b200 as ryo
+    x = torch.zeros(16, device="cuda")
+    with pytest.raises(ValueError):
+        ryo.solve_host(x, x, x, x, x, x, x, x, x)
