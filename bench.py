@@ -34,6 +34,16 @@ sys.path.insert(0, ROOT)
 BASELINE_PUBLISHED_MPS = 62.2  # reference, 1x A100, theta 0.5, 67 M particles (README.md:60)
 P2P_FLOPS, M2P_FLOPS = 23, 65  # the reference's flop convention (ryoanji/test/demo.cu:108)
 TRAV_DRAM_BYTES_2E24 = 1.372e9  # one traversal launch, uniform cube N=2^24, ncu dram bytes read + write
+# bytes per body the build phases (keys, sort, permutation, leaves, upsweep) read and write in HBM
+BUILD_BYTES_PER_BODY = {
+    "keys": 12 + 8,                    # x, y, z in, key out
+    "digit_histogram": 8,              # keys in
+    "sort_passes": 8 * (12 + 12),      # 8 digit passes of (key, index) in and out
+    "pack_records": 20 + 32,           # x, y, z, m, h in, 32-byte record out
+    "gather_records": 4 + 32 + 20 + 32,  # index, record in; x, y, z, m, h and packed sources/targets out
+    "leaves": 8,                       # sorted keys in
+    "upsweep": 16 + 2,                 # packed bodies in; 64-byte node records out, about one node per 28 bodies
+}
 METRIC = "BH solve throughput (build + upsweep + traversal), theta 0.5, 1st-pct acc err vs FP64 direct"
 
 
@@ -259,9 +269,11 @@ def run_ours(args, rank, world, local_rank):
                      "kernel": "traverseKernel (M2P + P2P), 23 flops per P2P and 65 per M2P per target",
                      "peak_source": "measured FP32 FMA peak of this GPU in this run (ryo_measure_peaks)",
                      "peak_fp32x2": peaks["fp32x2_tflops"]},
-        "build_hbm": {"bytes_per_body": 296, "gbs": 296 * n / ((phase["sort"] + phase["tree"] + phase["upsweep"])
-                                                              * 1e-3) / 1e9,
-                      "peak_gbs": _measured_hbm(peaks)},
+        "build_hbm": {"bytes_per_body": sum(BUILD_BYTES_PER_BODY.values()),
+                      "gbs": sum(BUILD_BYTES_PER_BODY.values()) * n
+                      / ((phase["sort"] + phase["tree"] + phase["upsweep"]) * 1e-3) / 1e9,
+                      "peak_gbs": _measured_hbm(peaks),
+                      "bytes_note": ", ".join(f"{k} {v}" for k, v in BUILD_BYTES_PER_BODY.items())},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }

@@ -886,21 +886,6 @@ extern "C" void ryo_solve_params_default(ryo_solve_params* p)
     p->multipole                  = RYO_MULTIPOLE_QUADRUPOLE;
 }
 
-namespace
-{
-__global__ void packSolveBodies(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
-                                const float* __restrict__ m, const float* __restrict__ h, size_t n,
-                                float4* __restrict__ xyzm, float4* __restrict__ xyzh)
-{
-    size_t stride = size_t(gridDim.x) * blockDim.x;
-    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
-    {
-        float px = x[i], py = y[i], pz = z[i];
-        xyzm[i]  = make_float4(px, py, pz, m[i]);
-        xyzh[i]  = make_float4(px, py, pz, h[i]);
-    }
-}
-} // namespace
 
 namespace
 {
@@ -990,15 +975,14 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     const uint64_t* sorted = alt ? keysAlt : keys;
     const uint32_t* order  = alt ? ordAlt : ord;
 
-    // permute every per-particle array (a host solve's masses and softenings arrive on the copy stream meanwhile)
+    // permute every per-particle array through 32-byte body records, writing the traversal's packed sources and
+    // targets on the way (a host solve's masses and softenings arrive on the copy stream meanwhile)
     if (pipe) RYO_CUDA(cudaStreamWaitEvent(s, pipe->massReady, 0));
-    float* tmpF = ctx->scratch<float>("solve.tmpf", n, s);
-    for (float* a : {x, y, z, m, h, vx, vy, vz})
-    {
-        if (!a) continue;
-        launchGather(order, a, tmpF, n, s);
-        RYO_CUDA(cudaMemcpyAsync(a, tmpF, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-    }
+    float4* rec  = ctx->scratch<float4>("solve.bodyRecords", 2 * n, s);
+    float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
+    float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
+    launchPackRecords(x, y, z, m, h, vx, vy, vz, n, rec, s);
+    launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, s);
     if (orderOut)
         RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
     if (pipe)
@@ -1011,12 +995,6 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
         d2h(pipe->hz, z, n * sizeof(float), pipe->copy);
     }
     mark(ctx, P, 1, s);
-    float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
-    float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
-    packSolveBodies<<<ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
-                                                                     : unsigned(ctx->smCount * 16),
-                      256, 0, s>>>(x, y, z, m, h, n, xyzm, xyzh);
-    RYO_LAUNCH_CHECK();
 
     // leaves, links
     int cap           = int(std::min<size_t>(n / 2 + 64, size_t(1) << 30));
@@ -1398,22 +1376,14 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                                                  s, true);
                        const uint64_t* sorted = alt ? keysAlt : keys;
                        const uint32_t* order  = alt ? ordAlt : ord;
-                       float* tmpF            = ctx->scratch<float>("solve.tmpf", n, s);
-                       for (float* a : {x, y, z, m, h, vx, vy, vz})
-                       {
-                           if (!a) continue;
-                           launchGather(order, a, tmpF, n, s);
-                           RYO_CUDA(cudaMemcpyAsync(a, tmpF, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
-                       }
+                       float4* rec            = ctx->scratch<float4>("solve.bodyRecords", 2 * n, s);
+                       float4* xyzm           = ctx->scratch<float4>("solve.xyzm", n, s);
+                       float4* xyzh           = ctx->scratch<float4>("solve.xyzh", n, s);
+                       launchPackRecords(x, y, z, m, h, vx, vy, vz, n, rec, s);
+                       launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, s);
                        if (orderOut)
                            RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
                        mark(ctx, P, 1, s);
-                       float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
-                       float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
-                       packSolveBodies<<<ceilDiv(n, 256) < unsigned(ctx->smCount * 16) ? ceilDiv(n, 256)
-                                                                                        : unsigned(ctx->smCount * 16),
-                                         256, 0, s>>>(x, y, z, m, h, n, xyzm, xyzh);
-                       RYO_LAUNCH_CHECK();
 
                        // one tree over all systems: leaves holding bodies lie at or below the system level
                        int cap          = int(std::min<size_t>(n / 2 + 64 + 8 * size_t(ns), size_t(1) << 30));

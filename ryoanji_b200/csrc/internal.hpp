@@ -130,6 +130,12 @@ void launchSequence(uint32_t* v, size_t n, uint32_t first, cudaStream_t s);
 void launchGather(const uint32_t* order, const float* in, float* out, size_t n, cudaStream_t s);
 template<class T>
 void launchGatherT(const uint32_t* order, const T* in, T* out, size_t n, cudaStream_t s);
+//! rec[2 i], rec[2 i + 1] = (x, y, z, m), (h, vx, vy, vz) of body i (null velocities give zeros)
+void launchPackRecords(const float* x, const float* y, const float* z, const float* m, const float* h,
+                       const float* vx, const float* vy, const float* vz, size_t n, float4* rec, cudaStream_t s);
+//! body i of the output is record order[i]: the per-body arrays (null ones skipped) and xyzm / xyzh (may be null)
+void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, float* x, float* y, float* z, float* m,
+                         float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- scan / sort
 //! out[i] = sum(in[0:i]) for i in [0, n]; out has n + 1 entries (out[n] = total); in-place allowed

@@ -216,6 +216,63 @@ void launchGather(const uint32_t* order, const float* in, float* out, size_t n, 
     launchGatherT<float>(order, in, out, n, s);
 }
 
+//! every body as one 32-byte record (x, y, z, m, h, vx, vy, vz; absent velocities are zero), so that the permutation
+//! after the sort reads one sector per body instead of one per array
+__global__ void packRecordsKernel(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                                  const float* __restrict__ m, const float* __restrict__ h,
+                                  const float* __restrict__ vx, const float* __restrict__ vy,
+                                  const float* __restrict__ vz, size_t n, float4* __restrict__ rec)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        rec[2 * i]     = make_float4(x[i], y[i], z[i], m[i]);
+        rec[2 * i + 1] = make_float4(h[i], vx ? vx[i] : 0.f, vy ? vy[i] : 0.f, vz ? vz[i] : 0.f);
+    }
+}
+
+//! the sorted bodies from their records: the per-body arrays (overwritten in sorted order) and the packed source
+//! (x, y, z, m) and target (x, y, z, h) arrays of the traversal
+__global__ void gatherRecordsKernel(const uint32_t* __restrict__ order, const float4* __restrict__ rec, size_t n,
+                                    float* __restrict__ x, float* __restrict__ y, float* __restrict__ z,
+                                    float* __restrict__ m, float* __restrict__ h, float* __restrict__ vx,
+                                    float* __restrict__ vy, float* __restrict__ vz, float4* __restrict__ xyzm,
+                                    float4* __restrict__ xyzh)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+    {
+        size_t j = order[i];
+        float4 a = rec[2 * j], b = rec[2 * j + 1]; // one 32-byte sector
+        x[i]     = a.x;
+        y[i]     = a.y;
+        z[i]     = a.z;
+        m[i]     = a.w;
+        h[i]     = b.x;
+        if (vx) vx[i] = b.y;
+        if (vy) vy[i] = b.z;
+        if (vz) vz[i] = b.w;
+        if (xyzm) xyzm[i] = a;
+        if (xyzh) xyzh[i] = make_float4(a.x, a.y, a.z, b.x);
+    }
+}
+
+void launchPackRecords(const float* x, const float* y, const float* z, const float* m, const float* h,
+                       const float* vx, const float* vy, const float* vz, size_t n, float4* rec, cudaStream_t s)
+{
+    if (n == 0) return;
+    packRecordsKernel<<<streamGrid(n, 256), 256, 0, s>>>(x, y, z, m, h, vx, vy, vz, n, rec);
+    RYO_LAUNCH_CHECK();
+}
+
+void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, float* x, float* y, float* z, float* m,
+                         float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, cudaStream_t s)
+{
+    if (n == 0) return;
+    gatherRecordsKernel<<<streamGrid(n, 256), 256, 0, s>>>(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh);
+    RYO_LAUNCH_CHECK();
+}
+
 template void launchGatherT<float>(const uint32_t*, const float*, float*, size_t, cudaStream_t);
 template void launchGatherT<double>(const uint32_t*, const double*, double*, size_t, cudaStream_t);
 template void launchGatherT<float4>(const uint32_t*, const float4*, float4*, size_t, cudaStream_t);
