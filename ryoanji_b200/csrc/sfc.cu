@@ -5,6 +5,8 @@
  * costs 21 Hilbert levels of bit arithmetic on 12 input bytes. Threads process four consecutive points with 128-bit
  * loads when the arrays allow it; the grid is a multiple of the SM count and strides over the data.
  */
+#include <initializer_list>
+
 #include "internal.hpp"
 
 namespace ryo
@@ -257,11 +259,102 @@ __global__ void gatherRecordsKernel(const uint32_t* __restrict__ order, const fl
     }
 }
 
+//! packRecordsKernel for four bodies per thread with 16-byte loads (arrays 16-byte aligned, n4 = n / 4)
+__global__ void packRecordsKernel4(const float4* __restrict__ x, const float4* __restrict__ y,
+                                   const float4* __restrict__ z, const float4* __restrict__ m,
+                                   const float4* __restrict__ h, const float4* __restrict__ vx,
+                                   const float4* __restrict__ vy, const float4* __restrict__ vz, size_t n4,
+                                   float4* __restrict__ rec)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n4; t += stride)
+    {
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 px = x[t], py = y[t], pz = z[t], pm = m[t], ph = h[t];
+        float4 ux = vx ? vx[t] : zero, uy = vy ? vy[t] : zero, uz = vz ? vz[t] : zero;
+        float4* o = rec + 8 * t;
+        o[0]      = make_float4(px.x, py.x, pz.x, pm.x);
+        o[1]      = make_float4(ph.x, ux.x, uy.x, uz.x);
+        o[2]      = make_float4(px.y, py.y, pz.y, pm.y);
+        o[3]      = make_float4(ph.y, ux.y, uy.y, uz.y);
+        o[4]      = make_float4(px.z, py.z, pz.z, pm.z);
+        o[5]      = make_float4(ph.z, ux.z, uy.z, uz.z);
+        o[6]      = make_float4(px.w, py.w, pz.w, pm.w);
+        o[7]      = make_float4(ph.w, ux.w, uy.w, uz.w);
+    }
+}
+
+//! gatherRecordsKernel for four consecutive sorted bodies per thread: one 16-byte load of their indices, 16-byte
+//! stores of every output (arrays 16-byte aligned, n4 = n / 4)
+__global__ void gatherRecordsKernel4(const uint4* __restrict__ order, const float4* __restrict__ rec, size_t n4,
+                                     float4* __restrict__ x, float4* __restrict__ y, float4* __restrict__ z,
+                                     float4* __restrict__ m, float4* __restrict__ h, float4* __restrict__ vx,
+                                     float4* __restrict__ vy, float4* __restrict__ vz, float4* __restrict__ xyzm,
+                                     float4* __restrict__ xyzh)
+{
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n4; t += stride)
+    {
+        uint4 j = order[t];
+        float4 a0 = rec[2 * size_t(j.x)], b0 = rec[2 * size_t(j.x) + 1];
+        float4 a1 = rec[2 * size_t(j.y)], b1 = rec[2 * size_t(j.y) + 1];
+        float4 a2 = rec[2 * size_t(j.z)], b2 = rec[2 * size_t(j.z) + 1];
+        float4 a3 = rec[2 * size_t(j.w)], b3 = rec[2 * size_t(j.w) + 1];
+        x[t] = make_float4(a0.x, a1.x, a2.x, a3.x);
+        y[t] = make_float4(a0.y, a1.y, a2.y, a3.y);
+        z[t] = make_float4(a0.z, a1.z, a2.z, a3.z);
+        m[t] = make_float4(a0.w, a1.w, a2.w, a3.w);
+        h[t] = make_float4(b0.x, b1.x, b2.x, b3.x);
+        if (vx) vx[t] = make_float4(b0.y, b1.y, b2.y, b3.y);
+        if (vy) vy[t] = make_float4(b0.z, b1.z, b2.z, b3.z);
+        if (vz) vz[t] = make_float4(b0.w, b1.w, b2.w, b3.w);
+        if (xyzm)
+        {
+            float4* o = xyzm + 4 * t;
+            o[0] = a0;
+            o[1] = a1;
+            o[2] = a2;
+            o[3] = a3;
+        }
+        if (xyzh)
+        {
+            float4* o = xyzh + 4 * t;
+            o[0] = make_float4(a0.x, a0.y, a0.z, b0.x);
+            o[1] = make_float4(a1.x, a1.y, a1.z, b1.x);
+            o[2] = make_float4(a2.x, a2.y, a2.z, b2.x);
+            o[3] = make_float4(a3.x, a3.y, a3.z, b3.x);
+        }
+    }
+}
+
+namespace
+{
+bool aligned16(std::initializer_list<const void*> ptrs)
+{
+    for (const void* p : ptrs)
+        if (reinterpret_cast<uintptr_t>(p) % 16 != 0) return false;
+    return true;
+}
+} // namespace
+
 void launchPackRecords(const float* x, const float* y, const float* z, const float* m, const float* h,
                        const float* vx, const float* vy, const float* vz, size_t n, float4* rec, cudaStream_t s)
 {
     if (n == 0) return;
-    packRecordsKernel<<<streamGrid(n, 256), 256, 0, s>>>(x, y, z, m, h, vx, vy, vz, n, rec);
+    size_t done = 0;
+    if (n >= 4 && aligned16({x, y, z, m, h, vx, vy, vz, rec}))
+    {
+        size_t n4 = n / 4;
+        auto f4   = [](const float* a) { return reinterpret_cast<const float4*>(a); };
+        packRecordsKernel4<<<streamGrid(n4, 256), 256, 0, s>>>(f4(x), f4(y), f4(z), f4(m), f4(h), f4(vx), f4(vy),
+                                                               f4(vz), n4, rec);
+        RYO_LAUNCH_CHECK();
+        done = 4 * n4;
+    }
+    if (done == n) return;
+    auto off = [&](const float* a) { return a ? a + done : nullptr; };
+    packRecordsKernel<<<streamGrid(n - done, 256), 256, 0, s>>>(off(x), off(y), off(z), off(m), off(h), off(vx),
+                                                                off(vy), off(vz), n - done, rec + 2 * done);
     RYO_LAUNCH_CHECK();
 }
 
@@ -269,7 +362,23 @@ void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, flo
                          float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, cudaStream_t s)
 {
     if (n == 0) return;
-    gatherRecordsKernel<<<streamGrid(n, 256), 256, 0, s>>>(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh);
+    size_t done = 0;
+    if (n >= 4 && aligned16({order, x, y, z, m, h, vx, vy, vz, xyzm, xyzh}))
+    {
+        size_t n4 = n / 4;
+        auto f4   = [](float* a) { return reinterpret_cast<float4*>(a); };
+        gatherRecordsKernel4<<<streamGrid(n4, 256), 256, 0, s>>>(reinterpret_cast<const uint4*>(order), rec, n4,
+                                                                 f4(x), f4(y), f4(z), f4(m), f4(h), f4(vx), f4(vy),
+                                                                 f4(vz), xyzm, xyzh);
+        RYO_LAUNCH_CHECK();
+        done = 4 * n4;
+    }
+    if (done == n) return;
+    auto off  = [&](float* a) { return a ? a + done : nullptr; };
+    auto off4 = [&](float4* a) { return a ? a + done : nullptr; };
+    gatherRecordsKernel<<<streamGrid(n - done, 256), 256, 0, s>>>(order + done, rec, n - done, off(x), off(y), off(z),
+                                                                  off(m), off(h), off(vx), off(vy), off(vz), off4(xyzm),
+                                                                  off4(xyzh));
     RYO_LAUNCH_CHECK();
 }
 

@@ -217,7 +217,7 @@ __global__ void digitBases(const uint32_t* hist, uint32_t* base, int numPasses)
     }
 }
 
-__global__ void __launch_bounds__(kSortBlock) onesweepPass(const uint64_t* __restrict__ keysIn,
+__global__ void __launch_bounds__(kSortBlock, 4) onesweepPass(const uint64_t* __restrict__ keysIn,
                                                            const uint32_t* __restrict__ valsIn,
                                                            uint64_t* __restrict__ keysOut,
                                                            uint32_t* __restrict__ valsOut, size_t n, int shift,
@@ -244,25 +244,21 @@ __global__ void __launch_bounds__(kSortBlock) onesweepPass(const uint64_t* __res
     const uint32_t dmask = (1u << nbits) - 1;
     const size_t wbase   = base + size_t(warp) * (kSortItems * kWarp);
 
+    // keys now, values only once the keys are staged (fewer live registers, more tiles in flight per SM); a padding
+    // item past n has digit kDigits
     uint64_t k[kSortItems];
-    uint32_t v[kSortItems], d[kSortItems], r[kSortItems];
+    uint32_t r[kSortItems];
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i)
     {
         size_t idx = wbase + size_t(i) * kWarp + lane;
-        if (idx < n)
-        {
-            k[i] = keysIn[idx];
-            v[i] = valsIn ? valsIn[idx] : uint32_t(idx);
-            d[i] = uint32_t(k[i] >> shift) & dmask;
-        }
-        else
-        {
-            k[i] = 0;
-            v[i] = 0;
-            d[i] = kDigits;
-        }
+        k[i]       = idx < n ? keysIn[idx] : 0;
     }
+    auto digitOf = [&](int i) -> uint32_t
+    {
+        size_t idx = wbase + size_t(i) * kWarp + lane;
+        return idx < n ? uint32_t(k[i] >> shift) & dmask : uint32_t(kDigits);
+    };
 
     // rank within the warp: items in (item, lane) order, which is this warp's input order. The lanes holding the
     // same digit are found with one ballot per digit bit (plus one for the padding items past n).
@@ -270,23 +266,24 @@ __global__ void __launch_bounds__(kSortBlock) onesweepPass(const uint64_t* __res
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i)
     {
-        const bool valid = d[i] < kDigits;
+        const uint32_t di = digitOf(i);
+        const bool valid  = di < kDigits;
         const unsigned vm = __ballot_sync(0xffffffffu, valid);
         unsigned peers    = valid ? vm : ~vm;
 #pragma unroll
         for (int b = 0; b < 8; ++b)
         {
             if (b >= nbits) break; // uniform across the warp
-            const bool bit    = (d[i] >> b) & 1u;
+            const bool bit    = (di >> b) & 1u;
             const unsigned bv = __ballot_sync(0xffffffffu, bit);
             peers &= bit ? bv : ~bv;
         }
         int leader     = __ffs(peers) - 1;
         uint32_t before = 0;
-        if (lane == leader && d[i] < kDigits)
+        if (lane == leader && valid)
         {
-            before              = sHist[warp][d[i]];
-            sHist[warp][d[i]] = before + __popc(peers);
+            before          = sHist[warp][di];
+            sHist[warp][di] = before + __popc(peers);
         }
         before = __shfl_sync(0xffffffffu, before, leader);
         r[i]   = before + __popc(peers & lt);
@@ -342,12 +339,21 @@ __global__ void __launch_bounds__(kSortBlock) onesweepPass(const uint64_t* __res
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i)
     {
-        if (d[i] < kDigits)
+        const uint32_t di = digitOf(i);
+        if (di < kDigits)
         {
-            uint32_t pos = sStart[d[i]] + sHist[warp][d[i]] + r[i];
+            uint32_t pos = sStart[di] + sHist[warp][di] + r[i];
             sKeys[pos]   = k[i];
             r[i]         = pos;
         }
+    }
+    // the values, whose loads overlap the key writes below
+    uint32_t v[kSortItems];
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i)
+    {
+        size_t idx = wbase + size_t(i) * kWarp + lane;
+        v[i]       = idx < n ? (valsIn ? valsIn[idx] : uint32_t(idx)) : 0u;
     }
     __syncthreads();
     const uint32_t count = uint32_t(n - base < size_t(kSortTile) ? n - base : size_t(kSortTile));
@@ -362,7 +368,7 @@ __global__ void __launch_bounds__(kSortBlock) onesweepPass(const uint64_t* __res
     uint32_t* sVals = reinterpret_cast<uint32_t*>(sKeys);
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i)
-        if (d[i] < kDigits) sVals[r[i]] = v[i];
+        if (wbase + size_t(i) * kWarp + lane < n) sVals[r[i]] = v[i];
     __syncthreads();
     for (uint32_t p = tid; p < count; p += kSortBlock)
     {
@@ -391,6 +397,9 @@ bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_
     digitBases<<<1, kDigits, 0, s>>>(t.hist, t.base, numPasses);
     RYO_LAUNCH_CHECK();
 
+    // the whole shared memory as carveout, so that registers (four tiles per SM), not the L1 split, limit residency
+    RYO_CUDA(cudaFuncSetAttribute(onesweepPass, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  int(cudaSharedmemCarveoutMaxShared)));
     // pass p reads buffer set p % 2 and writes the other
     bool inAlt = false;
     for (int p = 0; p < numPasses; ++p)
