@@ -123,15 +123,32 @@ __global__ void batchAutoBoxes(const uint32_t* __restrict__ mm, const int* __res
     boxes[s]   = b;
 }
 
-__global__ void batchKeysKernel(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
-                                size_t n, const uint64_t* __restrict__ first, uint32_t numSystems,
-                                const DevBox<float>* __restrict__ boxes, int sysBits, uint64_t* __restrict__ keys)
+//! the two-level Hilbert tables (identical keys to hilbert3), built at compile time
+static __device__ const HilbertLut kBatchHilbertLut = makeHilbertLut();
+
+__global__ void __launch_bounds__(256) batchKeysKernel(const float* __restrict__ x, const float* __restrict__ y,
+                                                       const float* __restrict__ z, size_t n,
+                                                       const uint64_t* __restrict__ first, uint32_t numSystems,
+                                                       const DevBox<float>* __restrict__ boxes, int sysBits,
+                                                       uint64_t* __restrict__ keys)
 {
+    __shared__ uint16_t two[48 * 64];
+    __shared__ uint16_t one[48 * 8];
+    for (int i = threadIdx.x; i < 48 * 64; i += blockDim.x)
+        two[i] = kBatchHilbertLut.two[i];
+    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
+        one[i] = kBatchHilbertLut.one[i];
+    __syncthreads();
     size_t stride = size_t(gridDim.x) * blockDim.x;
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
     {
-        uint32_t s = systemOf(first, numSystems, i);
-        uint64_t k = pointKey(x[i], y[i], z[i], boxes[s]);
+        uint32_t s           = systemOf(first, numSystems, i);
+        const DevBox<float>& b = boxes[s];
+        unsigned ic[3];
+        pointCells(x[i], y[i], z[i], b, ic);
+        bool full  = b.bits[0] == unsigned(kMaxLevel) && b.bits[1] == unsigned(kMaxLevel) &&
+                    b.bits[2] == unsigned(kMaxLevel);
+        uint64_t k = full ? hilbert3Lut(ic[0], ic[1], ic[2], two, one) : hilbertKey(ic[0], ic[1], ic[2], b.bits);
         keys[i]    = (uint64_t(s) << (63 - sysBits)) | (k >> sysBits);
     }
 }

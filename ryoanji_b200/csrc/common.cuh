@@ -166,6 +166,107 @@ __host__ __device__ inline uint64_t hilbert3(unsigned px, unsigned py, unsigned 
     return key;
 }
 
+/*! hilbert3 as a state machine over 2 levels per step. The per-level update of hilbert3 is a signed permutation of
+ *  the axes, so the transform accumulated down the levels is one of 48 states (axis permutation, flip bits). For
+ *  every state and every pair of octants (original coordinate bits of two levels) the table holds the two Hilbert
+ *  digits and the next state, generated at compile time by applying hilbert3's rules; the keys are therefore
+ *  identical to hilbert3's. */
+struct HilbertLut
+{
+    uint16_t two[48 * 64]; // (digit pair) | (next state << 6)
+    uint16_t one[48 * 8];  // (digit) | (next state << 3)
+};
+
+constexpr int kHilbertPerms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+
+constexpr int hilbertPermIndex(int a, int b)
+{
+    for (int i = 0; i < 6; ++i)
+        if (kHilbertPerms[i][0] == a && kHilbertPerms[i][1] == b) return i;
+    return 0;
+}
+
+//! one level of hilbert3 for state @p state (perm index * 8 + flips x4 y2 z1) and original octant bits @p oct
+constexpr void hilbertStep(int state, unsigned oct, unsigned& digit, int& next)
+{
+    const int* perm = kHilbertPerms[state / 8];
+    unsigned fl[3]  = {unsigned(state >> 2) & 1u, unsigned(state >> 1) & 1u, unsigned(state) & 1u};
+    unsigned ob[3]  = {(oct >> 2) & 1u, (oct >> 1) & 1u, oct & 1u};
+    unsigned bx = ob[perm[0]] ^ fl[0], by = ob[perm[1]] ^ fl[1], bz = ob[perm[2]] ^ fl[2];
+    constexpr unsigned digitOf[8] = {0, 1, 3, 2, 7, 6, 4, 5};
+    digit        = digitOf[(bx << 2) | (by << 1) | bz];
+    unsigned nby = by ^ 1u, nbz = bz ^ 1u;
+    unsigned f[3] = {fl[0] ^ (bx & (nby | bz)), fl[1] ^ ((bx & (by | bz)) | (by & nbz)),
+                     fl[2] ^ ((bx & nby & nbz) | (by & nbz))};
+    int np[3]     = {perm[0], perm[1], perm[2]};
+    unsigned nf[3] = {f[0], f[1], f[2]};
+    if (bz)
+    {
+        np[0] = perm[1], np[1] = perm[2], np[2] = perm[0];
+        nf[0] = f[1], nf[1] = f[2], nf[2] = f[0];
+    }
+    else if (!by)
+    {
+        np[0] = perm[2], np[2] = perm[0];
+        nf[0] = f[2], nf[2] = f[0];
+    }
+    next = hilbertPermIndex(np[0], np[1]) * 8 + int((nf[0] << 2) | (nf[1] << 1) | nf[2]);
+}
+
+constexpr HilbertLut makeHilbertLut()
+{
+    HilbertLut t{};
+    for (int st = 0; st < 48; ++st)
+    {
+        for (unsigned o = 0; o < 8; ++o)
+        {
+            unsigned d = 0;
+            int nx     = 0;
+            hilbertStep(st, o, d, nx);
+            t.one[st * 8 + o] = uint16_t(d | (unsigned(nx) << 3));
+        }
+        for (unsigned o = 0; o < 64; ++o)
+        {
+            unsigned d1 = 0, d2 = 0;
+            int s1 = 0, s2 = 0;
+            hilbertStep(st, o >> 3, d1, s1);
+            hilbertStep(s1, o & 7u, d2, s2);
+            t.two[st * 64 + o] = uint16_t(((d1 << 3) | d2) | (unsigned(s2) << 6));
+        }
+    }
+    return t;
+}
+
+//! bits 0..20 of v spread to every third bit (v_i at bit 3 i)
+__host__ __device__ inline uint64_t spreadBits3(uint32_t v)
+{
+    uint64_t x = v & 0x1fffffu;
+    x          = (x | (x << 32)) & 0x1f00000000ffffull;
+    x          = (x | (x << 16)) & 0x1f0000ff0000ffull;
+    x          = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x          = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x          = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+//! hilbert3(px, py, pz, kMaxLevel) through the tables (level 20 first, two levels per lookup, level 0 last)
+__host__ __device__ inline uint64_t hilbert3Lut(unsigned px, unsigned py, unsigned pz, const uint16_t* two,
+                                                const uint16_t* one)
+{
+    uint64_t m   = (spreadBits3(px) << 2) | (spreadBits3(py) << 1) | spreadBits3(pz);
+    uint64_t key = 0;
+    unsigned st  = 0;
+#pragma unroll
+    for (int lvl = kMaxLevel - 1; lvl >= 2; lvl -= 2)
+    {
+        unsigned e = two[st * 64 + (unsigned(m >> (3 * (lvl - 1))) & 63u)];
+        key        = (key << 6) | (e & 63u);
+        st         = e >> 6;
+    }
+    unsigned e = one[st * 8 + unsigned(m & 7u)];
+    return (key << 3) | (e & 7u);
+}
+
 __host__ __device__ inline uint64_t hilbert2(unsigned px, unsigned py, int order)
 {
     uint64_t key = 0;
@@ -509,12 +610,11 @@ __host__ __device__ inline int cellIndex(T x, T xmin, T m)
     return int(F::sub(fa, fb)) - int(F::sub(a, fa) < F::sub(b, fb));
 }
 
-//! SFC key of a point (sfc.hpp:161-207); coordinates outside the box are clamped into it
+//! integer cell coordinates of a point for its SFC key (sfc.hpp:161-207), clamped into the box
 template<class T>
-__host__ __device__ inline uint64_t pointKey(T x, T y, T z, const DevBox<T>& box)
+__host__ __device__ inline void pointCells(T x, T y, T z, const DevBox<T>& box, unsigned ic[3])
 {
     const T v[3] = {x, y, z};
-    unsigned ic[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d)
     {
@@ -524,6 +624,14 @@ __host__ __device__ inline uint64_t pointKey(T x, T y, T z, const DevBox<T>& box
         c      = c < cm ? c : cm;
         ic[d]  = unsigned(c > 0 ? c : 0);
     }
+}
+
+//! SFC key of a point (sfc.hpp:161-207); coordinates outside the box are clamped into it
+template<class T>
+__host__ __device__ inline uint64_t pointKey(T x, T y, T z, const DevBox<T>& box)
+{
+    unsigned ic[3];
+    pointCells(x, y, z, box, ic);
     return hilbertKey(ic[0], ic[1], ic[2], box.bits);
 }
 

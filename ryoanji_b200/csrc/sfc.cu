@@ -43,6 +43,42 @@ __global__ void keysKernelVec4(const float4* __restrict__ x, const float4* __res
     }
 }
 
+//! the two-level Hilbert tables (identical keys to hilbert3), built at compile time
+__device__ const HilbertLut kHilbertLut = makeHilbertLut();
+
+//! keysKernelVec4 for boxes whose three axes use all 21 levels: the Hilbert index through the tables in shared
+//! memory (two levels per lookup instead of bit arithmetic per level)
+__global__ void __launch_bounds__(256) keysKernelVec4Lut(const float4* __restrict__ x, const float4* __restrict__ y,
+                                                         const float4* __restrict__ z, ulonglong2* __restrict__ keys,
+                                                         size_t n4, DevBox<float> box)
+{
+    __shared__ uint16_t two[48 * 64];
+    __shared__ uint16_t one[48 * 8];
+    for (int i = threadIdx.x; i < 48 * 64; i += blockDim.x)
+        two[i] = kHilbertLut.two[i];
+    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
+        one[i] = kHilbertLut.one[i];
+    __syncthreads();
+    auto key = [&](float px, float py, float pz)
+    {
+        unsigned ic[3];
+        pointCells(px, py, pz, box, ic);
+        return hilbert3Lut(ic[0], ic[1], ic[2], two, one);
+    };
+    size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n4; i += stride)
+    {
+        float4 px = x[i], py = y[i], pz = z[i];
+        ulonglong2 a, b;
+        a.x             = key(px.x, py.x, pz.x);
+        a.y             = key(px.y, py.y, pz.y);
+        b.x             = key(px.z, py.z, pz.z);
+        b.y             = key(px.w, py.w, pz.w);
+        keys[2 * i]     = a;
+        keys[2 * i + 1] = b;
+    }
+}
+
 static unsigned streamGrid(size_t work, unsigned block)
 {
     int dev = 0, sms = 148;
@@ -65,10 +101,15 @@ void launchKeys(const T* x, const T* y, const T* z, uint64_t* keys, size_t n, co
     {
         if (aligned && !keepRemoved && n >= 4)
         {
-            size_t n4 = n / 4;
-            keysKernelVec4<<<streamGrid(n4, block), block, 0, s>>>(
-                reinterpret_cast<const float4*>(x), reinterpret_cast<const float4*>(y),
-                reinterpret_cast<const float4*>(z), reinterpret_cast<ulonglong2*>(keys), n4, box);
+            size_t n4  = n / 4;
+            bool full  = box.bits[0] == unsigned(kMaxLevel) && box.bits[1] == unsigned(kMaxLevel) &&
+                        box.bits[2] == unsigned(kMaxLevel);
+            auto* x4 = reinterpret_cast<const float4*>(x);
+            auto* y4 = reinterpret_cast<const float4*>(y);
+            auto* z4 = reinterpret_cast<const float4*>(z);
+            auto* k2 = reinterpret_cast<ulonglong2*>(keys);
+            if (full) keysKernelVec4Lut<<<streamGrid(n4, block), block, 0, s>>>(x4, y4, z4, k2, n4, box);
+            else keysKernelVec4<<<streamGrid(n4, block), block, 0, s>>>(x4, y4, z4, k2, n4, box);
             RYO_LAUNCH_CHECK();
             size_t done = n4 * 4;
             if (done < n)
