@@ -34,6 +34,7 @@ constexpr int kTravThreads  = kTravWarps * kWarp;
 constexpr int kStackDefault = 1024;
 constexpr int kM2PCap       = 64;  // pending approximated cells (flushed at 32)
 constexpr int kLeafCap      = 64;  // pending direct leaves (flushed when more than 32 are pending)
+constexpr int kP2PBatch     = 2 * kWarp; // direct bodies evaluated per staging round (two per lane)
 constexpr int kRootOnly     = -2;  // stack marker: the root itself is the only cell (single-leaf tree); a marker
                                    // -(r + 2) stands for the single cell r
 
@@ -42,8 +43,9 @@ struct WarpSmem
     int m2p[kM2PCap + kWarp];
     int2 leaves[kLeafCap + kWarp];
     int leafScan[kLeafCap + kWarp];
-    // staged sources, every value duplicated: M2P 5 x 16 bytes per cell, P2P 2 x 16 + 8 bytes per body
-    float4 stage[7 * kWarp]; // M2P of dipole expansions stages 7 float4 per cell
+    // staged sources, every value duplicated: M2P 5 x 16 bytes per cell (7 for dipole expansions), P2P 2 x 16 + 8
+    // bytes per body for 64 bodies
+    float4 stage[7 * kWarp];
     // per lane: Kahan running sums [0] and compensations [1] of (-phi, ax, ay, az), both targets packed
     unsigned long long sums[2][4][kWarp];
     // evaluation batches of the current walk: the next batch's number, and which of them this warp evaluates
@@ -60,6 +62,11 @@ __device__ __forceinline__ bool ownBatch(WarpSmem& S)
     __syncwarp();
     return S.parts <= 1 || j % S.parts == S.part;
 }
+
+static_assert(2 * kP2PBatch + kP2PBatch / 2 <= 7 * kWarp, "a P2P batch must fit in the stage");
+// a P2P evaluation leaves fewer than kP2PBatch bodies, so at most kP2PBatch - 1 leaves, pending; one walk step adds
+// at most kWarp more
+static_assert(kP2PBatch - 1 + kWarp <= kLeafCap + kWarp, "the pending leaf list must hold a step's additions");
 
 // ------------------------------------------------------------------------------------------------ packed f32x2
 
@@ -437,41 +444,48 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
         total = __shfl_sync(0xffffffffu, inc, kWarp - 1);
     }
     __syncwarp();
-    int numBatches = all ? (total + kWarp - 1) / kWarp : total / kWarp;
+    int numBatches = all ? (total + kP2PBatch - 1) / kP2PBatch : total / kP2PBatch;
+    // staged body k: positions and mass at stage[2 k], stage[2 k + 1], softening pair at sth[k]
+    const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
+    const f2* sth        = reinterpret_cast<const f2*>(S.stage + 2 * kP2PBatch);
     for (int b = 0; b < numBatches; ++b)
     {
         if (!ownBatch(S)) continue;
-        int r = b * kWarp + lane;
-        if (r < total)
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
         {
-            // first leaf whose inclusive prefix exceeds r
-            int lo = 0, hi = numLeaves - 1;
-            while (lo < hi)
+            int k = half * kWarp + lane;
+            int r = b * kP2PBatch + k;
+            if (r < total)
             {
-                int mid = (lo + hi) >> 1;
-                if (S.leafScan[mid] > r) hi = mid;
-                else lo = mid + 1;
+                // first leaf whose inclusive prefix exceeds r
+                int lo = 0, hi = numLeaves - 1;
+                while (lo < hi)
+                {
+                    int mid = (lo + hi) >> 1;
+                    if (S.leafScan[mid] > r) hi = mid;
+                    else lo = mid + 1;
+                }
+                int2 lf   = S.leaves[lo];
+                int body  = lf.x + (r - (S.leafScan[lo] - lf.y));
+                float4 sj = src.vec(body);
+                float hj  = src.scalar(body);
+                S.stage[2 * k]     = make_float4(sj.x, sj.x, sj.y, sj.y);
+                S.stage[2 * k + 1] = make_float4(sj.z, sj.z, sj.w, sj.w);
+                reinterpret_cast<float2*>(S.stage + 2 * kP2PBatch)[k] = make_float2(hj, hj);
             }
-            int2 lf   = S.leaves[lo];
-            int body  = lf.x + (r - (S.leafScan[lo] - lf.y));
-            float4 sj = src.vec(body);
-            float hj  = src.scalar(body);
-            S.stage[2 * lane]     = make_float4(sj.x, sj.x, sj.y, sj.y);
-            S.stage[2 * lane + 1] = make_float4(sj.z, sj.z, sj.w, sj.w);
-            reinterpret_cast<float2*>(S.stage + 2 * kWarp)[lane] = make_float2(hj, hj);
         }
         __syncwarp();
-        int nvalid           = min(kWarp, total - b * kWarp);
-        const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
-        const f2* sth        = reinterpret_cast<const f2*>(S.stage + 2 * kWarp);
-        Acc2 part            = zero2();
+        int nvalid = min(kP2PBatch, total - b * kP2PBatch);
+        Acc2 part  = zero2();
         // equal smoothing lengths for the targets and this batch's sources: hh is one constant
         if (T.uniformH)
         {
-            float hj0, hjl, dup;
+            float hj0, ha, hb, dup;
             upk(sth[0], hj0, dup);
-            upk(sth[lane < nvalid ? lane : 0], hjl, dup);
-            if (__all_sync(0xffffffffu, hjl == hj0))
+            upk(sth[lane < nvalid ? lane : 0], ha, dup);
+            upk(sth[kWarp + lane < nvalid ? kWarp + lane : 0], hb, dup);
+            if (__all_sync(0xffffffffu, ha == hj0 && hb == hj0))
             {
                 float hij = __fadd_rn(T.h0, hj0);
                 float hh  = __fmul_rn(hij, hij);
@@ -481,10 +495,10 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
                     ulonglong2 a = st[2 * j], c = st[2 * j + 1];
                     p2p2u(pp, T.tx, T.ty, T.tz, hh, a.x, a.y, c.x, c.y);
                 };
-                if (nvalid == kWarp)
+                if (nvalid == kP2PBatch)
                 {
 #pragma unroll 4
-                    for (int j = 0; j < kWarp; j += 2)
+                    for (int j = 0; j < kP2PBatch; j += 2)
                     {
                         oneU(part, j);
                         oneU(pb, j + 1);
@@ -510,10 +524,10 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
             ulonglong2 a = st[2 * j], c = st[2 * j + 1];
             p2p2(part, T.tx, T.ty, T.tz, T.th, a.x, a.y, c.x, c.y, sth[j]);
         };
-        if (nvalid == kWarp)
+        if (nvalid == kP2PBatch)
         {
 #pragma unroll 8
-            for (int j = 0; j < kWarp; ++j)
+            for (int j = 0; j < kP2PBatch; ++j)
                 one(j);
         }
         else
@@ -525,8 +539,8 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
         __syncwarp();
     }
     if (all) return 0;
-    // keep bodies [numBatches * 32, total): drop fully consumed leaves, trim the first kept one
-    int done = numBatches * kWarp;
+    // keep bodies [numBatches * kP2PBatch, total): drop fully consumed leaves, trim the first kept one
+    int done = numBatches * kP2PBatch;
     int keepFrom = 0;
     {
         int lo = 0, hi = numLeaves; // first leaf with inclusive prefix > done
