@@ -222,7 +222,7 @@ extern "C"
     {
         uint32_t* groupM2P; /* device, numGroups entries (may be NULL): approximated cells per group */
         uint32_t* groupP2P; /* device, numGroups entries (may be NULL): directly summed source bodies per group */
-        int stackCapacity;  /* traversal stack entries per warp, 0 = default (1024); small values force splits */
+        int stackCapacity;  /* traversal stack entries per warp, 0 = default (512); small values force splits */
         int multipole;      /* RYO_MULTIPOLE_QUADRUPOLE: 8 floats per node in multipoles (default);
                                RYO_MULTIPOLE_MDQ: 12 floats per node (CartesianMDQpole, traversal_gpu.cu:641) */
     } ryo_traverse_options;

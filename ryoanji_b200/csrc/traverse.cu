@@ -31,8 +31,7 @@ namespace ryo
 
 constexpr int kTravWarps    = 4;
 constexpr int kTravThreads  = kTravWarps * kWarp;
-constexpr int kStackDefault = 1024;
-constexpr int kM2PCap       = 64;  // pending approximated cells (flushed at 32)
+constexpr int kM2PCap       = 64;  // pending approximated cells (flushed at 64, or 32 for dipole expansions)
 constexpr int kLeafCap      = 64;  // pending direct leaves (flushed when more than 32 are pending)
 constexpr int kP2PBatch     = 2 * kWarp; // direct bodies evaluated per staging round (two per lane)
 constexpr int kRootOnly     = -2;  // stack marker: the root itself is the only cell (single-leaf tree); a marker
@@ -43,9 +42,9 @@ struct WarpSmem
     int m2p[kM2PCap + kWarp];
     int2 leaves[kLeafCap + kWarp];
     int leafScan[kLeafCap + kWarp];
-    // staged sources, every value duplicated: M2P 5 x 16 bytes per cell (7 for dipole expansions), P2P 2 x 16 + 8
-    // bytes per body for 64 bodies
-    float4 stage[7 * kWarp];
+    // staged sources, every value duplicated: M2P 5 x 16 bytes per cell for 64 quadrupoles (7 for 32 dipole
+    // expansions), P2P 2 x 16 + 8 bytes per body for 64 bodies
+    float4 stage[10 * kWarp];
     // per lane: Kahan running sums [0] and compensations [1] of (-phi, ax, ay, az), both targets packed
     unsigned long long sums[2][4][kWarp];
     // evaluation batches of the current walk: the next batch's number, and which of them this warp evaluates
@@ -63,7 +62,10 @@ __device__ __forceinline__ bool ownBatch(WarpSmem& S)
     return S.parts <= 1 || j % S.parts == S.part;
 }
 
-static_assert(2 * kP2PBatch + kP2PBatch / 2 <= 7 * kWarp, "a P2P batch must fit in the stage");
+static_assert(2 * kP2PBatch + kP2PBatch / 2 <= 10 * kWarp, "a P2P batch must fit in the stage");
+static_assert(5 * 2 * kWarp <= 10 * kWarp && 7 * kWarp <= 10 * kWarp, "an M2P batch must fit in the stage");
+// an M2P flush leaves fewer than kWarp cells pending (at most 64 + 31 before it); one walk step adds at most kWarp
+static_assert(2 * kWarp - 1 + kWarp <= kM2PCap + kWarp, "the pending cell list must hold a step's additions");
 // a P2P evaluation leaves fewer than kP2PBatch bodies, so at most kP2PBatch - 1 leaves, pending; one walk step adds
 // at most kWarp more
 static_assert(kP2PBatch - 1 + kWarp <= kLeafCap + kWarp, "the pending leaf list must hold a step's additions");
@@ -366,27 +368,40 @@ __device__ __forceinline__ void addBatchS(WarpSmem& S, const Acc2& part)
     }
 }
 
-//! evaluate the first @p count (<= 32) pending cells
+//! approximated cells per evaluation batch: 64 quadrupoles (5 staged float4 each), or 32 dipole expansions (7)
+template<class Nodes>
+__host__ __device__ constexpr int m2pBatch()
+{
+    return Nodes::kDipole ? kWarp : 2 * kWarp;
+}
+
+//! evaluate the first @p count (<= m2pBatch) pending cells
 template<class Nodes>
 __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState& T)
 {
     constexpr int kStride = Nodes::kDipole ? 7 : 5; // staged float4 per cell
+    constexpr int kBatch  = m2pBatch<Nodes>();
     if (!ownBatch(S)) return;
     int lane = laneId();
-    if (lane < count)
+#pragma unroll
+    for (int half = 0; half < kBatch / kWarp; ++half)
     {
-        float4 c, q0, q1, dp = make_float4(0.f, 0.f, 0.f, 0.f);
-        nodes.multipole(S.m2p[lane], c, q0, q1, dp);
-        float4* st = S.stage + kStride * lane;
-        st[0]      = make_float4(c.x, c.x, c.y, c.y);
-        st[1]      = make_float4(c.z, c.z, q0.x, q0.x);
-        st[2]      = make_float4(q0.y, q0.y, q0.z, q0.z);
-        st[3]      = make_float4(q0.w, q0.w, q1.x, q1.x);
-        st[4]      = make_float4(q1.y, q1.y, q1.z, q1.z);
-        if (Nodes::kDipole)
+        int k = half * kWarp + lane;
+        if (k < count)
         {
-            st[5 % kStride] = make_float4(dp.x, dp.x, dp.y, dp.y);
-            st[6 % kStride] = make_float4(dp.z, dp.z, 0.f, 0.f);
+            float4 c, q0, q1, dp = make_float4(0.f, 0.f, 0.f, 0.f);
+            nodes.multipole(S.m2p[k], c, q0, q1, dp);
+            float4* st = S.stage + kStride * k;
+            st[0]      = make_float4(c.x, c.x, c.y, c.y);
+            st[1]      = make_float4(c.z, c.z, q0.x, q0.x);
+            st[2]      = make_float4(q0.y, q0.y, q0.z, q0.z);
+            st[3]      = make_float4(q0.w, q0.w, q1.x, q1.x);
+            st[4]      = make_float4(q1.y, q1.y, q1.z, q1.z);
+            if (Nodes::kDipole)
+            {
+                st[5 % kStride] = make_float4(dp.x, dp.x, dp.y, dp.y);
+                st[6 % kStride] = make_float4(dp.z, dp.z, 0.f, 0.f);
+            }
         }
     }
     __syncwarp();
@@ -404,10 +419,10 @@ __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState&
         else
             m2p2(part, T.tx, T.ty, T.tz, a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y, e.x, e.y);
     };
-    if (count == kWarp)
+    if (count == kBatch)
     {
 #pragma unroll 2
-        for (int j = 0; j < kWarp; j += 2)
+        for (int j = 0; j < kBatch; j += 2)
         {
             one(pa, j);
             one(pb, j + 1);
@@ -814,11 +829,12 @@ __global__ void __launch_bounds__(kTravThreads, 5)
                             break;
                         }
 
-                        while (nM >= kWarp)
+                        constexpr int kMB = m2pBatch<Nodes>();
+                        while (nM >= kMB)
                         {
-                            evalM2P(S, kWarp, nodes, T);
-                            nM -= kWarp;
-                            if (lane < nM) S.m2p[lane] = S.m2p[kWarp + lane];
+                            evalM2P(S, kMB, nodes, T);
+                            nM -= kMB; // fewer than kWarp cells remain: one move per lane
+                            if (lane < nM) S.m2p[lane] = S.m2p[kMB + lane];
                             __syncwarp();
                         }
                         if (nL > kLeafCap - kWarp) nL = evalP2P(S, nL, false, src, T);
