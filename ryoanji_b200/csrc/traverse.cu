@@ -463,26 +463,33 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
     // staged body k: positions and mass at stage[2 k], stage[2 k + 1], softening pair at sth[k]
     const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
     const f2* sth        = reinterpret_cast<const f2*>(S.stage + 2 * kP2PBatch);
+    int first = 0; // warp-uniform: the pending leaf that holds the batch's first body
     for (int b = 0; b < numBatches; ++b)
     {
+        // where the next 64 leaves end relative to the batch start R0: bit q of ends is set if a leaf ends after
+        // body R0 + q (its inclusive prefix is R0 + q + 1). A batch of 64 bodies meets at most 64 leaves.
+        const int R0 = b * kP2PBatch;
+        int t0 = first + lane, t1 = first + kWarp + lane;
+        int p0 = t0 < numLeaves ? S.leafScan[t0] - R0 : kP2PBatch + 1;
+        int p1 = t1 < numLeaves ? S.leafScan[t1] - R0 : kP2PBatch + 1;
+        auto bitsIn = [](int p, int lo) { return p > lo && p <= lo + kWarp ? 1u << (p - lo - 1) : 0u; };
+        unsigned endsLo = __reduce_or_sync(0xffffffffu, bitsIn(p0, 0) | bitsIn(p1, 0));
+        unsigned endsHi = __reduce_or_sync(0xffffffffu, bitsIn(p0, kWarp) | bitsIn(p1, kWarp));
+        const unsigned long long ends = (static_cast<unsigned long long>(endsHi) << 32) | endsLo;
+        const int leafBase = first;
+        first += __popcll(ends); // the leaves ending inside this batch come before the next batch's first body
         if (!ownBatch(S)) continue;
 #pragma unroll
         for (int half = 0; half < 2; ++half)
         {
             int k = half * kWarp + lane;
-            int r = b * kP2PBatch + k;
+            int r = R0 + k;
             if (r < total)
             {
-                // first leaf whose inclusive prefix exceeds r
-                int lo = 0, hi = numLeaves - 1;
-                while (lo < hi)
-                {
-                    int mid = (lo + hi) >> 1;
-                    if (S.leafScan[mid] > r) hi = mid;
-                    else lo = mid + 1;
-                }
-                int2 lf   = S.leaves[lo];
-                int body  = lf.x + (r - (S.leafScan[lo] - lf.y));
+                // body r lies in the leaf after the ones that end at or before it (ends bits 0 .. k - 1)
+                int leaf  = leafBase + (k == 0 ? 0 : __popcll(ends & (~0ull >> (64 - k))));
+                int2 lf   = S.leaves[leaf];
+                int body  = lf.x + (r - (S.leafScan[leaf] - lf.y));
                 float4 sj = src.vec(body);
                 float hj  = src.scalar(body);
                 S.stage[2 * k]     = make_float4(sj.x, sj.x, sj.y, sj.y);
