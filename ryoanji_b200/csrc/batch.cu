@@ -15,17 +15,6 @@
 namespace ryo
 {
 
-//! order-preserving map of floats to unsigned integers (min/max by integer atomics)
-__device__ __forceinline__ uint32_t orderedBits(float f)
-{
-    uint32_t u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float orderedFloat(uint32_t u)
-{
-    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
-
 //! system of body i: the last s with first[s] <= i
 __device__ __forceinline__ uint32_t systemOf(const uint64_t* __restrict__ first, uint32_t numSystems, uint64_t i)
 {

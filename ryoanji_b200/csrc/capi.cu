@@ -982,7 +982,8 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
     float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
     launchPackRecords(x, y, z, m, h, vx, vy, vz, n, rec, s);
-    launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, s);
+    uint32_t* hRange = ctx->scratch<uint32_t>("solve.softeningRange", 2, s);
+    launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, hRange, s);
     if (orderOut)
         RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
     if (pipe)
@@ -1080,6 +1081,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     t.az = az;
     t.stackCapacity = P->stackCapacity;
     t.dipoles       = dipoles;
+    t.softeningRange = hRange;
     uint32_t* gm2p  = ctx->scratch<uint32_t>("solve.groupM2P", numGroups, s);
     uint32_t* gp2p  = ctx->scratch<uint32_t>("solve.groupP2P", numGroups, s);
     RYO_CUDA(cudaMemsetAsync(gm2p, 0, sizeof(uint32_t) * numGroups, s));
@@ -1380,7 +1382,8 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        float4* xyzm           = ctx->scratch<float4>("solve.xyzm", n, s);
                        float4* xyzh           = ctx->scratch<float4>("solve.xyzh", n, s);
                        launchPackRecords(x, y, z, m, h, vx, vy, vz, n, rec, s);
-                       launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, s);
+                       uint32_t* hRange       = ctx->scratch<uint32_t>("solve.softeningRange", 2, s);
+                       launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, hRange, s);
                        if (orderOut)
                            RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
                        mark(ctx, P, 1, s);
@@ -1480,6 +1483,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        t.stackCapacity = P->stackCapacity;
                        t.groupSys      = tSys;
                        t.dipoles       = dipoles;
+                       t.softeningRange = hRange;
                        t.systems       = dTrav;
                        t.sysPotential  = sysPot;
                        double pot      = 0;

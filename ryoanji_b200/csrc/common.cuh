@@ -684,6 +684,17 @@ __host__ __device__ inline T vecMacR2(uint64_t prefix, const T com[3], float inv
 
 // ------------------------------------------------------------------------------------------------ warp helpers
 
+//! order-preserving map of floats to unsigned integers (min/max by integer atomics)
+__device__ __forceinline__ uint32_t orderedBits(float f)
+{
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float orderedFloat(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
 __device__ inline unsigned laneId() { return threadIdx.x & (kWarp - 1); }
 
 __device__ inline unsigned lanemaskLt()

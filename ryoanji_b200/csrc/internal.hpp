@@ -133,9 +133,11 @@ void launchGatherT(const uint32_t* order, const T* in, T* out, size_t n, cudaStr
 //! rec[2 i], rec[2 i + 1] = (x, y, z, m), (h, vx, vy, vz) of body i (null velocities give zeros)
 void launchPackRecords(const float* x, const float* y, const float* z, const float* m, const float* h,
                        const float* vx, const float* vy, const float* vz, size_t n, float4* rec, cudaStream_t s);
-//! body i of the output is record order[i]: the per-body arrays (null ones skipped) and xyzm / xyzh (may be null)
+//! body i of the output is record order[i]: the per-body arrays (null ones skipped) and xyzm / xyzh (may be null);
+//! hRange (may be null) receives the min and max softening as ordered bits (orderedBits)
 void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, float* x, float* y, float* z, float* m,
-                         float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, cudaStream_t s);
+                         float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, uint32_t* hRange,
+                         cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- scan / sort
 //! out[i] = sum(in[0:i]) for i in [0, n]; out has n + 1 entries (out[n] = total); in-place allowed
@@ -270,6 +272,9 @@ struct TraverseLaunch
     uint32_t numHeavy;  // second pass: queued groups
     float4* partials;   // second pass: (-phi, ax, ay, az) of the group's 64 targets, per item
     int* partStatus;    // second pass: per item, 1 if the walk overflowed the stack
+    // min and max softening of every target and source as ordered bits (null: not known). Equal values let the
+    // direct sums skip staging and comparing the sources' softening.
+    const uint32_t* softeningRange;
 };
 
 //! per-system traversal parameters of a batched solve

@@ -276,17 +276,32 @@ __global__ void packRecordsKernel(const float* __restrict__ x, const float* __re
 
 //! the sorted bodies from their records: the per-body arrays (overwritten in sorted order) and the packed source
 //! (x, y, z, m) and target (x, y, z, h) arrays of the traversal
+//! fold a thread's softening range into hRange[0] (min) and hRange[1] (max), as ordered bits; whole warps call it
+__device__ __forceinline__ void foldRange(uint32_t lo, uint32_t hi, uint32_t* hRange)
+{
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if (laneId() == 0 && lo <= hi)
+    {
+        atomicMin(hRange, lo);
+        atomicMax(hRange + 1, hi);
+    }
+}
+
 __global__ void gatherRecordsKernel(const uint32_t* __restrict__ order, const float4* __restrict__ rec, size_t n,
                                     float* __restrict__ x, float* __restrict__ y, float* __restrict__ z,
                                     float* __restrict__ m, float* __restrict__ h, float* __restrict__ vx,
                                     float* __restrict__ vy, float* __restrict__ vz, float4* __restrict__ xyzm,
-                                    float4* __restrict__ xyzh)
+                                    float4* __restrict__ xyzh, uint32_t* __restrict__ hRange)
 {
     size_t stride = size_t(gridDim.x) * blockDim.x;
+    uint32_t lo = 0xffffffffu, hi = 0u;
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
     {
         size_t j = order[i];
         float4 a = rec[2 * j], b = rec[2 * j + 1]; // one 32-byte sector
+        lo       = min(lo, orderedBits(b.x));
+        hi       = max(hi, orderedBits(b.x));
         x[i]     = a.x;
         y[i]     = a.y;
         z[i]     = a.z;
@@ -298,6 +313,7 @@ __global__ void gatherRecordsKernel(const uint32_t* __restrict__ order, const fl
         if (xyzm) xyzm[i] = a;
         if (xyzh) xyzh[i] = make_float4(a.x, a.y, a.z, b.x);
     }
+    if (hRange) foldRange(lo, hi, hRange);
 }
 
 //! packRecordsKernel for four bodies per thread with 16-byte loads (arrays 16-byte aligned, n4 = n / 4)
@@ -331,9 +347,10 @@ __global__ void gatherRecordsKernel4(const uint4* __restrict__ order, const floa
                                      float4* __restrict__ x, float4* __restrict__ y, float4* __restrict__ z,
                                      float4* __restrict__ m, float4* __restrict__ h, float4* __restrict__ vx,
                                      float4* __restrict__ vy, float4* __restrict__ vz, float4* __restrict__ xyzm,
-                                     float4* __restrict__ xyzh)
+                                     float4* __restrict__ xyzh, uint32_t* __restrict__ hRange)
 {
     size_t stride = size_t(gridDim.x) * blockDim.x;
+    uint32_t lo = 0xffffffffu, hi = 0u;
     for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n4; t += stride)
     {
         uint4 j = order[t];
@@ -341,6 +358,8 @@ __global__ void gatherRecordsKernel4(const uint4* __restrict__ order, const floa
         float4 a1 = rec[2 * size_t(j.y)], b1 = rec[2 * size_t(j.y) + 1];
         float4 a2 = rec[2 * size_t(j.z)], b2 = rec[2 * size_t(j.z) + 1];
         float4 a3 = rec[2 * size_t(j.w)], b3 = rec[2 * size_t(j.w) + 1];
+        lo = min(min(min(lo, orderedBits(b0.x)), orderedBits(b1.x)), min(orderedBits(b2.x), orderedBits(b3.x)));
+        hi = max(max(max(hi, orderedBits(b0.x)), orderedBits(b1.x)), max(orderedBits(b2.x), orderedBits(b3.x)));
         x[t] = make_float4(a0.x, a1.x, a2.x, a3.x);
         y[t] = make_float4(a0.y, a1.y, a2.y, a3.y);
         z[t] = make_float4(a0.z, a1.z, a2.z, a3.z);
@@ -366,6 +385,7 @@ __global__ void gatherRecordsKernel4(const uint4* __restrict__ order, const floa
             o[3] = make_float4(a3.x, a3.y, a3.z, b3.x);
         }
     }
+    if (hRange) foldRange(lo, hi, hRange);
 }
 
 namespace
@@ -400,8 +420,14 @@ void launchPackRecords(const float* x, const float* y, const float* z, const flo
 }
 
 void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, float* x, float* y, float* z, float* m,
-                         float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, cudaStream_t s)
+                         float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, uint32_t* hRange,
+                         cudaStream_t s)
 {
+    if (hRange)
+    {
+        RYO_CUDA(cudaMemsetAsync(hRange, 0xff, sizeof(uint32_t), s)); // min
+        RYO_CUDA(cudaMemsetAsync(hRange + 1, 0, sizeof(uint32_t), s)); // max
+    }
     if (n == 0) return;
     size_t done = 0;
     if (n >= 4 && aligned16({order, x, y, z, m, h, vx, vy, vz, xyzm, xyzh}))
@@ -410,7 +436,7 @@ void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, flo
         auto f4   = [](float* a) { return reinterpret_cast<float4*>(a); };
         gatherRecordsKernel4<<<streamGrid(n4, 256), 256, 0, s>>>(reinterpret_cast<const uint4*>(order), rec, n4,
                                                                  f4(x), f4(y), f4(z), f4(m), f4(h), f4(vx), f4(vy),
-                                                                 f4(vz), xyzm, xyzh);
+                                                                 f4(vz), xyzm, xyzh, hRange);
         RYO_LAUNCH_CHECK();
         done = 4 * n4;
     }
@@ -419,7 +445,7 @@ void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, flo
     auto off4 = [&](float4* a) { return a ? a + done : nullptr; };
     gatherRecordsKernel<<<streamGrid(n - done, 256), 256, 0, s>>>(order + done, rec, n - done, off(x), off(y), off(z),
                                                                   off(m), off(h), off(vx), off(vy), off(vz), off4(xyzm),
-                                                                  off4(xyzh));
+                                                                  off4(xyzh), hRange);
     RYO_LAUNCH_CHECK();
 }
 

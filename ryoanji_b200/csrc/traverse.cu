@@ -50,11 +50,16 @@ struct WarpSmem
     // evaluation batches of the current walk: the next batch's number, and which of them this warp evaluates
     // (batch j when j % parts == part; parts is 1 outside the split second pass)
     int batchNext, part, parts, item;
+    // 1 if every target and source of the launch has the softening of the group's targets (T.h0)
+    int allUniform, pad[3];
 };
 
-//! true if the walk's next evaluation batch belongs to this warp; counts the batch either way
+//! true if the walk's next evaluation batch belongs to this warp; counts the batch either way. Outside the split
+//! second pass (kSplit false) every batch is the warp's own.
+template<bool kSplit>
 __device__ __forceinline__ bool ownBatch(WarpSmem& S)
 {
+    if constexpr (!kSplit) return true;
     int j = S.batchNext;
     __syncwarp();
     if (laneId() == 0) S.batchNext = j + 1;
@@ -376,12 +381,12 @@ __host__ __device__ constexpr int m2pBatch()
 }
 
 //! evaluate the first @p count (<= m2pBatch) pending cells
-template<class Nodes>
+template<bool kSplit, class Nodes>
 __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState& T)
 {
     constexpr int kStride = Nodes::kDipole ? 7 : 5; // staged float4 per cell
     constexpr int kBatch  = m2pBatch<Nodes>();
-    if (!ownBatch(S)) return;
+    if (!ownBatch<kSplit>(S)) return;
     int lane = laneId();
 #pragma unroll
     for (int half = 0; half < kBatch / kWarp; ++half)
@@ -444,7 +449,7 @@ __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState&
 
 /*! evaluate pending direct leaves in batches of 32 bodies; with @p all == false only whole batches are evaluated
  *  and the remainder stays pending (the first pending leaf may be partly consumed). Returns the leaves left. */
-template<class Sources>
+template<bool kSplit, class Sources>
 __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src, TargetState& T)
 {
     int lane = laneId();
@@ -463,7 +468,8 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
     // staged body k: positions and mass at stage[2 k], stage[2 k + 1], softening pair at sth[k]
     const ulonglong2* st = reinterpret_cast<const ulonglong2*>(S.stage);
     const f2* sth        = reinterpret_cast<const f2*>(S.stage + 2 * kP2PBatch);
-    int first = 0; // warp-uniform: the pending leaf that holds the batch's first body
+    const bool allUniform = S.allUniform != 0; // no softening to stage or compare
+    int first             = 0;                  // warp-uniform: the pending leaf that holds the batch's first body
     for (int b = 0; b < numBatches; ++b)
     {
         // where the next 64 leaves end relative to the batch start R0: bit q of ends is set if a leaf ends after
@@ -478,7 +484,7 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
         const unsigned long long ends = (static_cast<unsigned long long>(endsHi) << 32) | endsLo;
         const int leafBase = first;
         first += __popcll(ends); // the leaves ending inside this batch come before the next batch's first body
-        if (!ownBatch(S)) continue;
+        if (!ownBatch<kSplit>(S)) continue;
 #pragma unroll
         for (int half = 0; half < 2; ++half)
         {
@@ -491,10 +497,13 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
                 int2 lf   = S.leaves[leaf];
                 int body  = lf.x + (r - (S.leafScan[leaf] - lf.y));
                 float4 sj = src.vec(body);
-                float hj  = src.scalar(body);
                 S.stage[2 * k]     = make_float4(sj.x, sj.x, sj.y, sj.y);
                 S.stage[2 * k + 1] = make_float4(sj.z, sj.z, sj.w, sj.w);
-                reinterpret_cast<float2*>(S.stage + 2 * kP2PBatch)[k] = make_float2(hj, hj);
+                if (!allUniform)
+                {
+                    float hj = src.scalar(body);
+                    reinterpret_cast<float2*>(S.stage + 2 * kP2PBatch)[k] = make_float2(hj, hj);
+                }
             }
         }
         __syncwarp();
@@ -503,11 +512,17 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
         // equal smoothing lengths for the targets and this batch's sources: hh is one constant
         if (T.uniformH)
         {
-            float hj0, ha, hb, dup;
-            upk(sth[0], hj0, dup);
-            upk(sth[lane < nvalid ? lane : 0], ha, dup);
-            upk(sth[kWarp + lane < nvalid ? kWarp + lane : 0], hb, dup);
-            if (__all_sync(0xffffffffu, ha == hj0 && hb == hj0))
+            float hj0 = T.h0;
+            bool same = true;
+            if (!allUniform)
+            {
+                float ha, hb, dup;
+                upk(sth[0], hj0, dup);
+                upk(sth[lane < nvalid ? lane : 0], ha, dup);
+                upk(sth[kWarp + lane < nvalid ? kWarp + lane : 0], hb, dup);
+                same = __all_sync(0xffffffffu, ha == hj0 && hb == hj0);
+            }
+            if (same)
             {
                 float hij = __fadd_rn(T.h0, hj0);
                 float hh  = __fmul_rn(hij, hij);
@@ -686,7 +701,7 @@ void launchCombineHeavy(const TraverseLaunch& t, const float* mass, cudaStream_t
     RYO_LAUNCH_CHECK();
 }
 
-template<class Nodes, class Targets, class Sources>
+template<class Nodes, class Targets, class Sources, bool kSplit>
 __global__ void __launch_bounds__(kTravThreads, 5)
     traverseKernel(TraverseLaunch P, Nodes nodes, Targets tgt, Sources src)
 {
@@ -723,6 +738,9 @@ __global__ void __launch_bounds__(kTravThreads, 5)
         T.th      = pk(t0.w, t1.w);
         T.h0       = __shfl_sync(0xffffffffu, t0.w, 0);
         T.uniformH = __all_sync(0xffffffffu, t0.w == T.h0 && t1.w == T.h0);
+        if (lane == 0)
+            S.allUniform = P.softeningRange && T.uniformH && P.softeningRange[0] == P.softeningRange[1] &&
+                           orderedFloat(P.softeningRange[0]) == T.h0;
 #pragma unroll
         for (int c = 0; c < 4; ++c)
             S.sums[0][c][lane] = S.sums[1][c][lane] = 0ull;
@@ -839,17 +857,17 @@ __global__ void __launch_bounds__(kTravThreads, 5)
                         constexpr int kMB = m2pBatch<Nodes>();
                         while (nM >= kMB)
                         {
-                            evalM2P(S, kMB, nodes, T);
+                            evalM2P<kSplit>(S, kMB, nodes, T);
                             nM -= kMB; // fewer than kWarp cells remain: one move per lane
                             if (lane < nM) S.m2p[lane] = S.m2p[kMB + lane];
                             __syncwarp();
                         }
-                        if (nL > kLeafCap - kWarp) nL = evalP2P(S, nL, false, src, T);
+                        if (nL > kLeafCap - kWarp) nL = evalP2P<kSplit>(S, nL, false, src, T);
                     }
                     if (!overflow)
                     {
-                        if (nM > 0) evalM2P(S, nM, nodes, T);
-                        if (nL > 0) evalP2P(S, nL, true, src, T);
+                        if (nM > 0) evalM2P<kSplit>(S, nM, nodes, T);
+                        if (nL > 0) evalP2P<kSplit>(S, nL, true, src, T);
                     }
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
@@ -944,7 +962,8 @@ template<class Nodes, class Targets, class Sources>
 static void launchTyped(const TraverseLaunch& t, const Nodes& nodes, const Targets& tgt, const Sources& src,
                         int smCount, cudaStream_t s)
 {
-    auto kernel = traverseKernel<Nodes, Targets, Sources>;
+    auto kernel = t.parts > 0 ? traverseKernel<Nodes, Targets, Sources, true>
+                              : traverseKernel<Nodes, Targets, Sources, false>;
     size_t smem = sizeof(int) * kTravWarps * size_t(t.stackCapacity) + sizeof(WarpSmem) * kTravWarps;
     RYO_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int perSm = 0;
