@@ -33,7 +33,7 @@ sys.path.insert(0, ROOT)
 
 BASELINE_PUBLISHED_MPS = 62.2  # reference, 1x A100, theta 0.5, 67 M particles (README.md:60)
 P2P_FLOPS, M2P_FLOPS = 23, 65  # the reference's flop convention (ryoanji/test/demo.cu:108)
-TRAV_DRAM_BYTES_2E24 = 1.372e9  # one traversal launch, uniform cube N=2^24, ncu dram bytes read + write
+TRAV_DRAM_BYTES_2E24 = 1.289e9  # one traversal launch, uniform cube N=2^24, ncu dram bytes read + write
 # bytes per body the build phases (keys, sort, permutation, leaves, upsweep) read and write in HBM
 BUILD_BYTES_PER_BODY = {
     "keys": 12 + 8,                    # x, y, z in, key out
@@ -264,7 +264,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / peaks["fp32_tflops"],
                      "traffic": TRAV_DRAM_BYTES_2E24 * n / (1 << 24),
                      "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of one traverseKernel launch "
-                                     "captured with ncu on the same uniform cube at N=2^24 (1.110 GB + 0.262 GB), "
+                                     "captured with ncu on the same uniform cube at N=2^24 (1.027 GB + 0.262 GB), "
                                      "scaled by N/2^24; bytes per body are constant at fixed interactions per body",
                      "kernel": "traverseKernel (M2P + P2P), 23 flops per P2P and 65 per M2P per target",
                      "peak_source": "measured FP32 FMA peak of this GPU in this run (ryo_measure_peaks)",
