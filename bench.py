@@ -410,7 +410,8 @@ def run_ensemble(args, ctx, dev, rank=0, world=1, max_over_ranks=lambda v: v) ->
                         "quadrupole; one solve of every system per step"
                         + (f"; LPT shares over {world} GPUs, times = max over ranks" if world > 1 else ""),
             "autotuned": {"bucket": tuned.bucket_size, "group": tuned.group_size, "stack": tuned.stack_capacity,
-                          "candidates_ms": [list(t) for t in table]},
+                          "group_tolerance": tuned.group_tolerance,
+                          "candidates_ms (bucket, group, stack, group tolerance, ms)": [list(t) for t in table]},
             "batched": {"ms_per_step": batched_ms, "solves_per_s": ns / (batched_ms * 1e-3),
                         "mparticles_per_s": n / (batched_ms * 1e-3) / 1e6, "steps": steps},
             "plain_loop": {"ms_per_step": plain_ms, "solves_per_s": ns / (plain_ms * 1e-3),
@@ -436,7 +437,9 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
         # the final state (x y z vx vy vz ax ay az p) of every request lands in pinned host memory in both arms
         result[q["tag"]] = torch.empty((10, q["n"]), dtype=torch.float32).pin_memory()
     torch.cuda.synchronize()
-    params = ryo.SolveParams(theta=0.5)
+    # both arms split each 64-body window spatially (tolFactor 2, the reference's production grouping): sparse
+    # Plummer outskirts otherwise make wide groups
+    params = ryo.SolveParams(theta=0.5, group_tolerance=2.0)
     periodic = ryo.Box(0.0, 1.0, 0.0, 1.0, 0.0, 1.0, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
     arrival = {q["tag"]: q["arrival"] for q in all_reqs}
     solves = sum(q["steps"] + 1 for q in all_reqs)
@@ -507,7 +510,8 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
         x, y, z, m, h, vx, vy, vz = (t.to(dev, non_blocking=True) for t in host[q["tag"]])
         n = q["n"]
         p, ax, ay, az = (torch.empty(n, device=dev) for _ in range(4))
-        pp = ryo.SolveParams(theta=0.5, box=periodic if q["kind"] == "periodic" else None, num_shells=1)
+        pp = ryo.SolveParams(theta=0.5, box=periodic if q["kind"] == "periodic" else None, num_shells=1,
+                             group_tolerance=2.0)
         ryo.solve(x, y, z, m, h, p, ax, ay, az, params=pp, v=(vx, vy, vz), ctx=ctx)
         hdt, dt = 0.5 * q["dt"], q["dt"]
         for _ in range(q["steps"]):
@@ -525,7 +529,7 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
     plain = summary(done, max(done.values(), default=0.0))
     return {"workload": f"{len(all_reqs)} requests, Poisson arrivals at {args.served_rate}/s, N=round(2^U[12,22]), "
                         "45% Plummer / 45% cube / 10% periodic+Ewald, K~U{1..64} KDK steps, dt=1e-3, theta 0.5, "
-                        "120 GB admission budget"
+                        "spatial groups (tolFactor 2) in both arms, 120 GB admission budget"
                         + (f"; requests routed over {world} GPUs by estimated backlog" if world > 1 else ""),
             "solves": solves, "body_solves": body_solves, "served": served, "plain": plain,
             "speedup_solves_per_s": served["solves_per_s"] / plain["solves_per_s"],
