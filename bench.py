@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--ensemble-systems", type=int, default=1024)
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--no-plummer", action="store_true", help="skip the 2^24 Plummer sphere leg")
     ap.add_argument("--served-requests", type=int, default=48)
     ap.add_argument("--served-rate", type=float, default=24.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--no-accuracy-matched", action="store_true")
@@ -322,6 +323,8 @@ def run_ours(args, rank, world, local_rank):
         line["ensemble"] = run_ensemble(args, ctx, dev, rank, world, max_over_ranks)
     if not args.no_served:
         line["served"] = run_served(args, ctx, dev, rank, world, dist)
+    if world == 1 and not args.no_plummer:
+        line["plummer_2e24"] = run_plummer(args, ctx, dev)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         kind, dt, sec = cpu_reference_solve(args.cpu_log2n, args.theta, seed=3)
@@ -417,6 +420,56 @@ def run_ensemble(args, ctx, dev, rank=0, world=1, max_over_ranks=lambda v: v) ->
             "plain_loop": {"ms_per_step": plain_ms, "solves_per_s": ns / (plain_ms * 1e-3),
                            "mparticles_per_s": n / (plain_ms * 1e-3) / 1e6},
             "speedup_solves_per_s": plain_ms / batched_ms}
+
+
+def run_plummer(args, ctx, dev, log2n: int = 24) -> dict:
+    """the plain path's second workload: one Plummer sphere of 2^24 equal masses (a = 1, total mass 1, eps = 0.01,
+    radii resampled above 50 a, seeded), theta 0.5, quadrupole, bucket 64, one full solve per step with the inputs
+    restored before each. Fixed groups of 64 (the reference demo's) and spatial groups (tolFactor 2); relative
+    acceleration error against FP64 direct sums on 16,384 random targets."""
+    import torch
+    import ryoanji_b200 as ryo
+    from ryoanji_b200 import datasets as ds
+    n = 1 << log2n
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(24)
+    x, y, z, _, _, _ = ds.plummer_device(torch.ones(n, dtype=torch.float64, device=dev), gen, velocities=False)
+    pristine = [t.float().contiguous() for t in (x, y, z)]
+    pristine += [torch.full((n,), 1.0 / n, device=dev), torch.full((n,), 0.005, device=dev)]
+    del x, y, z
+    work = [t.clone() for t in pristine]
+    out = [torch.empty(n, device=dev) for _ in range(4)]
+    order = torch.empty(n, dtype=torch.int32, device=dev)
+    rng = np.random.default_rng(3)
+    tgt = torch.from_numpy(rng.choice(n, 16384, replace=False)).to(dev)
+    _, rx, ry, rz = ryo.direct_targets_f64(tgt, *pristine)
+    ref = torch.stack([rx, ry, rz], 1)
+    res = {"workload": f"Plummer sphere N=2^{log2n}, a=1, M=1, eps=0.01 (h=0.005), rmax=50a, theta 0.5, quadrupole, "
+                       "bucket 64, groups of 64; one full solve per step"}
+    for label, tol in (("fixed_groups", 0.0), ("spatial_groups", 2.0)):
+        params = ryo.SolveParams(theta=0.5, bucket_size=64, group_size=64, group_tolerance=tol, timing=True)
+        times = []
+        for i in range(6):
+            for w, p in zip(work, pristine):
+                w.copy_(p)
+            e0, e1 = _events()
+            e0.record()
+            r = ryo.solve(*work, *out, params=params, order=order, ctx=ctx)
+            e1.record()
+            e1.synchronize()
+            if i >= 3:
+                times.append(e0.elapsed_time(e1))
+        ms = sum(times) / len(times)
+        inv = torch.empty_like(order)
+        inv[order.long()] = torch.arange(n, dtype=torch.int32, device=dev)
+        acc = torch.stack([a[inv[tgt].long()] for a in out[1:]], 1).double()
+        err = (torch.linalg.norm(acc - ref, dim=1) / torch.linalg.norm(ref, dim=1)).cpu().numpy()
+        res[label] = {"ms_per_step": ms, "mparticles_per_s": n / (ms * 1e-3) / 1e6, "groups": r.num_groups,
+                      "phase_ms": {k: round(v, 3) for k, v in r.ms.items()},
+                      "p2p_per_body": r.sum_p2p / n, "m2p_per_body": r.sum_m2p / n, "max_p2p": r.max_p2p,
+                      "err_p99_1st_pct": float(np.percentile(err, 99)), "err_max": float(err.max()),
+                      "err_median": float(np.median(err))}
+    return res
 
 
 def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
