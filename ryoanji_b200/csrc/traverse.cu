@@ -426,7 +426,7 @@ __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState&
     };
     if (count == kBatch)
     {
-#pragma unroll 2
+#pragma unroll 4
         for (int j = 0; j < kBatch; j += 2)
         {
             one(pa, j);
@@ -534,7 +534,7 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
                 };
                 if (nvalid == kP2PBatch)
                 {
-#pragma unroll 4
+#pragma unroll 8
                     for (int j = 0; j < kP2PBatch; j += 2)
                     {
                         oneU(part, j);
