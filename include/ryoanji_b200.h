@@ -370,8 +370,9 @@ extern "C"
     /* The same solve from and to HOST memory (pinned memory copies fastest): x, y, z, m, h are read (not changed);
      * xs, ys, zs (may be NULL) receive the positions in SFC order, p, ax, ay, az the potential and acceleration in
      * that order, order (may be NULL) the original index of each sorted body. The copies overlap the solve: m and h
-     * upload during the key sort, the order and sorted positions download while the tree is built, and for an open
-     * box with fixed groups the traversal runs in 8 launches whose results download while the next one runs.
+     * upload during the key sort and the leaf and link construction, the order downloads while the tree is built and
+     * the sorted positions during the upsweep, and for an open box with fixed groups the traversal runs in 8
+     * launches whose results download while the next one runs.
      * Returns when every output is in host memory. Device buffers are context scratch. */
     RYO_API ryo_status ryo_solve_host_f32(ryo_ctx_t* ctx, const ryo_solve_params* params, const float* x,
                                           const float* y, const float* z, const float* m, const float* h, size_t n,

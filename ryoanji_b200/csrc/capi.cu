@@ -975,26 +975,36 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     const uint64_t* sorted = alt ? keysAlt : keys;
     const uint32_t* order  = alt ? ordAlt : ord;
 
-    // permute every per-particle array through 32-byte body records, writing the traversal's packed sources and
-    // targets on the way (a host solve's masses and softenings arrive on the copy stream meanwhile)
-    if (pipe) RYO_CUDA(cudaStreamWaitEvent(s, pipe->massReady, 0));
-    float4* rec  = ctx->scratch<float4>("solve.bodyRecords", 2 * n, s);
-    float4* xyzm = ctx->scratch<float4>("solve.xyzm", n, s);
-    float4* xyzh = ctx->scratch<float4>("solve.xyzh", n, s);
-    launchPackRecords(x, y, z, m, h, vx, vy, vz, n, rec, s);
-    uint32_t* hRange = ctx->scratch<uint32_t>("solve.softeningRange", 2, s);
-    launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, hRange, s);
     if (orderOut)
         RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    // permute every per-particle array through 32-byte body records, writing the traversal's packed sources and
+    // targets on the way. A host solve's masses and softenings arrive on the copy stream meanwhile: it builds the
+    // leaves and links first, which need only the sorted keys, and permutes after them.
+    float4* rec      = ctx->scratch<float4>("solve.bodyRecords", 2 * n, s);
+    float4* xyzm     = ctx->scratch<float4>("solve.xyzm", n, s);
+    float4* xyzh     = ctx->scratch<float4>("solve.xyzh", n, s);
+    uint32_t* hRange = ctx->scratch<uint32_t>("solve.softeningRange", 2, s);
+    auto permute     = [&]()
+    {
+        if (pipe) RYO_CUDA(cudaStreamWaitEvent(s, pipe->massReady, 0));
+        launchPackRecords(x, y, z, m, h, vx, vy, vz, n, rec, s);
+        launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, hRange, s);
+        if (pipe)
+        {
+            // the sorted positions are final: copy them out while the upsweep and the traversal run
+            streamAfter(ctx, pipe->copy, s, 0);
+            d2h(pipe->hx, x, n * sizeof(float), pipe->copy);
+            d2h(pipe->hy, y, n * sizeof(float), pipe->copy);
+            d2h(pipe->hz, z, n * sizeof(float), pipe->copy);
+        }
+    };
     if (pipe)
     {
-        // the permutation and the sorted positions are final: copy them out while the tree is built
+        // the permutation is final
         streamAfter(ctx, pipe->copy, s, 0);
         d2h(pipe->horder, order, n * sizeof(uint32_t), pipe->copy);
-        d2h(pipe->hx, x, n * sizeof(float), pipe->copy);
-        d2h(pipe->hy, y, n * sizeof(float), pipe->copy);
-        d2h(pipe->hz, z, n * sizeof(float), pipe->copy);
     }
+    else permute();
     mark(ctx, P, 1, s);
 
     // leaves, links
@@ -1021,6 +1031,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     oct.d_levelRange   = ctx->scratch<int>("solve.levelRange", kMaxLevel + 2, s);
     int levelRange[kMaxLevel + 2];
     linkOctree(ctx, leaves, nl, oct, levelRange, s);
+    if (pipe) permute();
 
     mark(ctx, P, 2, s);
     // fused upsweep: node records + FP64 root expansion
