@@ -31,7 +31,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BASELINE_PUBLISHED_MPS = 62.2  # reference, 1x A100, theta 0.5, 67 M particles (README.md:60)
+REFERENCE_PUBLISHED_MPS = 62.2  # reference, 1x A100, theta 0.5, 67 M particles (README.md:60)
 P2P_FLOPS, M2P_FLOPS = 23, 65  # the reference's flop convention (ryoanji/test/demo.cu:108)
 TRAV_DRAM_BYTES_2E24 = 1.289e9  # one traversal launch, uniform cube N=2^24, ncu dram bytes read + write
 # bytes per body the build phases (keys, sort, permutation, leaves, upsweep) read and write in HBM
@@ -255,7 +255,7 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC,
         "value": value, "unit": "Mparticles/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": value / world / BASELINE_PUBLISHED_MPS, "dtype": "f32", "data": "synthetic",
+        "vs_baseline": value / world / REFERENCE_PUBLISHED_MPS, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args, world),
         "phase_ms": phase,
         "interactions": {"p2p_per_body": res.sum_p2p / n, "m2p_per_body": res.sum_m2p / n, "max_p2p": res.max_p2p,
