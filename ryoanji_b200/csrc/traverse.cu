@@ -13,8 +13,9 @@
  *     four entries, 32 cells, are tested per step), bounded by the stack capacity; a group that would exceed it is
  *     reported and split by the host, as the reference does with its global queue;
  *   - approximated cells and direct leaves are appended to per-warp lists in shared memory with ballot/popc
- *     compaction and evaluated in dense batches of 32 cells or 32 bodies whose data is staged in shared memory and
- *     read with broadcast loads, so the inner loops are FP32 arithmetic plus one rsqrt per interaction;
+ *     compaction and evaluated in dense batches (64 bodies, 64 quadrupole cells or 32 dipole expansions, two per
+ *     lane) whose data is staged in shared memory and read with broadcast loads, so the inner loops are FP32
+ *     arithmetic plus one rsqrt per interaction;
  *   - the two targets of a lane are processed together with the packed f32x2 FMA/ADD/MUL of sm_100a, and the
  *     staged sources are stored pre-duplicated (s, s) so every source operand is a ready register pair: one
  *     instruction issues the work of two targets and the freed issue slots carry the rsqrt, shared-memory and
@@ -447,7 +448,7 @@ __device__ void evalM2P(WarpSmem& S, int count, const Nodes& nodes, TargetState&
     __syncwarp();
 }
 
-/*! evaluate pending direct leaves in batches of 32 bodies; with @p all == false only whole batches are evaluated
+/*! evaluate pending direct leaves in batches of kP2PBatch bodies; with @p all == false only whole batches are evaluated
  *  and the remainder stays pending (the first pending leaf may be partly consumed). Returns the leaves left. */
 template<bool kSplit, class Sources>
 __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src, TargetState& T)
