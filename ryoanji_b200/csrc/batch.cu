@@ -177,6 +177,8 @@ __global__ void batchRootsKernel(uint32_t numSystems, const uint64_t* __restrict
     t.boxL[1]   = boxes[s].len[1];
     t.boxL[2]   = boxes[s].len[2];
     t.pad       = 0;
+    t.hLo       = 0xffffffffu; // filled by batchSofteningRange
+    t.hHi       = 0u;
     out[s]      = t;
 }
 
@@ -223,6 +225,48 @@ void launchBatchKeys(const float* x, const float* y, const float* z, size_t n, c
     size_t cap  = size_t(smCount) * 16;
     batchKeysKernel<<<unsigned(want < cap ? want : cap), 256, 0, s>>>(x, y, z, n, first, numSystems, boxes,
                                                                       3 * sysLevel, keys);
+    RYO_LAUNCH_CHECK();
+}
+
+//! one block per system: min and max softening of its bodies (systems are contiguous runs of bodies)
+__global__ void __launch_bounds__(256) batchSofteningRange(const float* __restrict__ h,
+                                                           const uint64_t* __restrict__ first, SysTrav* trav)
+{
+    __shared__ uint32_t sLo[8], sHi[8];
+    const uint32_t s = blockIdx.x;
+    uint32_t lo = 0xffffffffu, hi = 0u;
+    for (uint64_t i = first[s] + threadIdx.x; i < first[s + 1]; i += blockDim.x)
+    {
+        uint32_t b = orderedBits(h[i]);
+        lo         = min(lo, b);
+        hi         = max(hi, b);
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned warp = threadIdx.x / kWarp;
+    if (laneId() == 0)
+    {
+        sLo[warp] = lo;
+        sHi[warp] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (unsigned w = 1; w < blockDim.x / kWarp; ++w)
+        {
+            lo = min(lo, sLo[w]);
+            hi = max(hi, sHi[w]);
+        }
+        trav[s].hLo = lo;
+        trav[s].hHi = hi;
+    }
+}
+
+void launchBatchSofteningRange(const float* h, const uint64_t* first, uint32_t numSystems, SysTrav* trav,
+                               cudaStream_t s)
+{
+    if (numSystems == 0) return;
+    batchSofteningRange<<<numSystems, 256, 0, s>>>(h, first, trav);
     RYO_LAUNCH_CHECK();
 }
 

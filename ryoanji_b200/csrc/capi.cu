@@ -1471,6 +1471,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        RYO_CUDA(cudaMemsetAsync(rootErr, 0, sizeof(unsigned int), s));
                        launchBatchRoots(ns, oct.prefixes, levelRange[sysLevel], levelRange[sysLevel + 1],
                                         oct.childOffsets, sysLevel, dBx, dShells, dTrav, dRootNode, rootErr, s);
+                       launchBatchSofteningRange(h, dFirst, ns, dTrav, s);
                        double* sysPot = ctx->scratch<double>("batch.pot", 2 * size_t(ns), s); // tree, Ewald
                        RYO_CUDA(cudaMemsetAsync(sysPot, 0, sizeof(double) * 2 * ns, s));
                        for (float* a : {p, ax, ay, az})

@@ -283,8 +283,12 @@ struct SysTrav
     int entry;     // first stack entry: first child of the system's root, or -(root + 2) for a single-cell tree
     int numShells; // periodic replicas per dimension
     float boxL[3];
+    uint32_t hLo, hHi; // min and max softening of the system's bodies as ordered bits (hLo > hHi: not known)
     int pad;
 };
+//! per-system softening range of a batched solve into trav[s].hLo / hHi (one block per system)
+void launchBatchSofteningRange(const float* h, const uint64_t* first, uint32_t numSystems, SysTrav* trav,
+                               cudaStream_t s);
 void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s);
 /*! after a second pass: per queued group, the parts' partial sums added in part order into the outputs (and the
  *  potential); a group whose walk overflowed the stack goes to t.failedGroups instead. @p mass: target masses */

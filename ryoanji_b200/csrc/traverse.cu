@@ -766,6 +766,9 @@ __global__ void __launch_bounds__(kTravThreads, 5)
             sys               = P.groupSys[g];
             const SysTrav& st = P.systems[sys];
             rootEntry         = st.entry;
+            // a system's groups meet only its own bodies: its own softening range decides
+            if (lane == 0)
+                S.allUniform = T.uniformH && st.hLo == st.hHi && orderedFloat(st.hLo) == T.h0;
             shells            = st.numShells;
             boxL[0]           = st.boxL[0];
             boxL[1]           = st.boxL[1];
