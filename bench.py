@@ -596,7 +596,7 @@ def run_accuracy_matched(args, ctx, dev, work, out, pristine, n) -> dict:
     import ryoanji_b200 as ryo
     rng = np.random.default_rng(7)
     tgt = torch.from_numpy(rng.choice(n, 4096, replace=False)).to(dev)
-    for theta in (0.45, 0.42, 0.40, 0.38):
+    for theta in (0.45, 0.44, 0.43, 0.42, 0.41, 0.40, 0.38):
         params = ryo.SolveParams(theta=theta, bucket_size=64, group_size=64, box=ryo.Box.cube(-1.0, 1.0),
                                  timing=True)
         times = []
