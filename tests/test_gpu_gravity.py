@@ -384,3 +384,55 @@ def test_single_leaf_tree_solve():
     rp, rx, ry, rz = ryo.direct_targets_f64(t, x, y, z, m, h)
     e = rel_err(host(ax), host(ay), host(az), host(rx), host(ry), host(rz))
     assert e.max() < 1e-5
+
+
+def test_coincident_bodies_and_tiny_sets(oracle):
+    """300 bodies at one point beside 5,000 others: their keys are equal, so one leaf at the deepest level holds more
+    than the bucket size. Tree, per-group counts and forces against the oracle; then one and two bodies."""
+    import ryoanji_b200 as ryo
+    rng = np.random.default_rng(4)
+    pos = rng.uniform(-1, 1, (5300, 3)).astype(np.float32)
+    pos[5000:] = np.float32(0.123456)
+    hx, hy, hz = (np.ascontiguousarray(pos[:, d]) for d in range(3))
+    n = len(hx)
+    hm = np.full(n, 1.0 / n, np.float32)
+    hh = np.full(n, 0.01, np.float32)
+    box6 = np.array([-1, 1] * 3, np.float32)
+    x, y, z, m, h = (dev(a) for a in (hx, hy, hz, hm, hh))
+    p, ax, ay, az = (torch.empty(n, device="cuda") for _ in range(4))
+    order = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx = ryo.Context()
+    res = ryo.solve(x, y, z, m, h, p, ax, ay, az, ryo.SolveParams(theta=0.5, box=ryo.Box.cube(-1.0, 1.0)),
+                    order=order, ctx=ctx)
+    keys = oracle.sfc_keys(hx, hy, hz, box6)
+    sk, o = oracle.sort_keys(keys)
+    assert np.array_equal(host(order).view(np.uint32), o)
+    l_ref, c_ref = oracle.octree_leaves(sk, 64)
+    assert c_ref.max() == 300  # the coincident bodies share one leaf
+    arr = ryo.solve_arrays(ctx)
+    assert np.array_equal(host(arr["leaves"]).view(np.uint64), l_ref)
+    g = host(arr["groups"]).view(np.uint32)
+    tree = dict(childOffsets=host(arr["childOffsets"]), internalToLeaf=host(arr["internalToLeaf"]))
+    m2p, p2p, acc = oracle.traverse_rule(g[:-1], g[1:], host(x), host(y), host(z), host(h), host(m), tree,
+                                         host(arr["layout"]).view(np.uint32), np.ascontiguousarray(host(arr["centers"])),
+                                         np.ascontiguousarray(host(arr["multipoles"])), evaluate=True)
+    assert np.array_equal(host(arr["groupM2P"]).view(np.uint32), m2p)
+    assert np.array_equal(host(arr["groupP2P"]).view(np.uint32), p2p)
+    assert res.sum_p2p == int((p2p.astype(np.int64) * np.diff(g)).sum())
+    gx, gy, gz = host(ax), host(ay), host(az)
+    assert np.isfinite(gx).all() and np.isfinite(host(p)).all()
+    # the coincident bodies pull each other with zero force; their acceleration is the rest's
+    e = rel_err(gx, gy, gz, acc[:, 1], acc[:, 2], acc[:, 3])
+    assert np.percentile(e, 99) < 2e-6 and e.max() < 5e-5
+
+    for k in (1, 2):
+        xs, ys, zs, ms, hs = (dev(a) for a in (hx[:k], hy[:k], hz[:k], hm[:k], hh[:k]))
+        out = [torch.empty(k, device="cuda") for _ in range(4)]
+        r = ryo.solve(xs, ys, zs, ms, hs, *out)
+        assert r.sum_p2p == k * k and r.sum_m2p == 0
+        t = torch.arange(k, device="cuda")
+        rp, rx, ry, rz = ryo.direct_targets_f64(t, xs, ys, zs, ms, hs)
+        for got, want in zip(out[1:], (rx, ry, rz)):
+            assert np.allclose(host(got), host(want), rtol=1e-5, atol=1e-7)
+        if k == 1:
+            assert float(out[1].abs().max()) == 0.0
