@@ -113,7 +113,8 @@ extern "C"
 
     /* cstone::sortByKey with caller buffers (cstone/include/cstone/primitives/primitives_gpu.cu:311-356): stable
      * ascending sort of keys[0:n) carrying values along; keyBuf/valueBuf hold n elements each; tmp holds
-     * ryo_sort_by_key_temp_bytes(n) bytes. Onesweep radix sort over bits [0, 64). */
+     * ryo_sort_by_key_temp_bytes(n) bytes. Onesweep radix sort over bits [0, 64). n must be below 2^32 (the
+     * sort's digit offsets are 32-bit); a larger n returns RYO_ERR_BAD_ARG. */
     RYO_API size_t ryo_sort_by_key_temp_bytes(size_t n);
     RYO_API ryo_status ryo_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf,
                                        uint32_t* valueBuf, void* tmp, size_t tmpBytes, ryo_stream_t stream);
@@ -131,7 +132,8 @@ extern "C"
     /* cstone::computeOctree / updateOctreeGpu to convergence (cstone/include/cstone/tree/csarray.hpp:409-440,
      * update_gpu.cuh:43-68): the cornerstone leaf array of sorted keys with at most @p bucketSize particles per
      * leaf. Built in one pass (no host-synchronised rebalance loop); identical to the reference's fixed point.
-     * Writes leaves[numLeaves + 1] and counts[numLeaves] if numLeaves <= capacity; *numLeaves (host) always. */
+     * Writes leaves[numLeaves + 1] and counts[numLeaves] if numLeaves <= capacity; *numLeaves (host) always.
+     * n must be below 2^32. */
     RYO_API ryo_status ryo_compute_octree(ryo_ctx_t* ctx, const uint64_t* sortedKeys, size_t n, unsigned bucketSize,
                                           uint64_t* leaves, uint32_t* counts, int capacity, int* numLeaves,
                                           ryo_stream_t stream);

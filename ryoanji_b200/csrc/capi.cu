@@ -224,6 +224,7 @@ extern "C" ryo_status ryo_sort_by_key(uint64_t* keys, uint32_t* values, size_t n
                    {
                        if (n == 0) return;
                        REQUIRE(keys && values && keyBuf && valueBuf && tmp, "sort_by_key: null argument");
+                       REQUIRE(n < (size_t(1) << 32), "sort_by_key: key count must be below 2^32");
                        if (tmpBytes < ryo_sort_by_key_temp_bytes(n))
                            throw ApiError{RYO_ERR_CAPACITY, "sort_by_key: temporary storage too small"};
                        // the last 64 bytes of tmp hold the wait-timeout flag
@@ -271,6 +272,7 @@ extern "C" ryo_status ryo_compute_octree(ryo_ctx_t* ctx, const uint64_t* sortedK
                    [&]
                    {
                        REQUIRE(numLeaves && bucketSize > 0 && (n == 0 || sortedKeys), "compute_octree: bad argument");
+                       REQUIRE(n < (size_t(1) << 32), "compute_octree: key count must be below 2^32");
                        int nl     = buildLeaves(ctx, sortedKeys, n, bucketSize, leaves, counts, nullptr, capacity,
                                                 stream);
                        *numLeaves = nl;

@@ -58,6 +58,16 @@ def test_bad_arguments_return_status_not_crash():
     assert ryo.lib.ryo_traverse_f32(*args) == 2
 
 
+def test_sort_rejects_counts_beyond_32_bits():
+    """the sort's digit offsets are 32-bit: 2^32 keys are refused before any pointer is used or kernel launched"""
+    import ryoanji_b200 as ryo
+    fake = C.c_void_p(16)  # never dereferenced: the count check comes first
+    n = 1 << 32
+    st = ryo.lib.ryo_sort_by_key(fake, fake, n, fake, fake, fake, ryo.lib.ryo_sort_by_key_temp_bytes(n), None)
+    assert st == 2
+    assert b"2^32" in ryo.lib.ryo_ctx_last_error(None)
+
+
 @pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-device path")
 def test_context_without_device_fails_cleanly():
     import ryoanji_b200 as ryo
