@@ -20,13 +20,14 @@ from ._abi import (BOUNDARY_CUBIC_OPEN, BOUNDARY_FIXED, BOUNDARY_OPEN, BOUNDARY_
 
 __all__ = [
     "Box", "Context", "RyoError", "TreeBuilder", "SolveParams", "SolveResult", "EwaldSettings", "lib",
+    "default_context",
     "compute_sfc_keys", "compute_bounding_box", "sequence", "sort_by_key", "compute_octree", "build_octree",
-    "compute_fixed_groups", "compute_leaf_source_center", "upsweep_centers", "compute_leaf_multipoles",
-    "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats", "read_traversal_retries", "solve_batch", "compute_group_splits", "solve_targets",
-    "BatchSystem", "BatchResult", "Engine", "ewald_targets_f64",
-    "compute_gravity_ewald", "direct_sum", "direct_targets_f64", "solve", "solve_arrays", "bh_max_target_size",
+    "compute_fixed_groups", "compute_group_splits", "compute_leaf_source_center", "upsweep_centers",
+    "compute_leaf_multipoles", "upsweep_multipoles", "set_mac", "traverse", "read_bh_stats",
+    "read_traversal_retries", "bh_max_target_size", "stack_size",
+    "compute_gravity_ewald", "ewald_targets_f64", "direct_sum", "direct_targets_f64",
+    "solve", "solve_host", "solve_targets", "solve_arrays", "solve_batch", "BatchSystem", "BatchResult", "Engine",
     "kernel_launches", "measure_peaks",
-    "stack_size",
     "BOUNDARY_OPEN", "BOUNDARY_PERIODIC", "BOUNDARY_FIXED", "BOUNDARY_CUBIC_OPEN", "MAX_TREE_LEVEL",
 ]
 

@@ -112,3 +112,14 @@ int main() {
     assert r.returncode == 0, r.stderr
     run = subprocess.run([str(exe)], capture_output=True, text=True)
     assert run.returncode == 0, (run.returncode, run.stdout, run.stderr)
+
+
+def test_public_api_is_exported():
+    """every name in ryoanji_b200.__all__ exists, and every public function and class of the package is listed"""
+    import inspect
+    import ryoanji_b200 as ryo
+    missing = [n for n in ryo.__all__ if not hasattr(ryo, n)]
+    assert not missing, missing
+    own = [n for n, v in vars(ryo).items() if not n.startswith("_") and (inspect.isfunction(v) or inspect.isclass(v))
+           and getattr(v, "__module__", "") == ryo.__name__]
+    assert set(own) <= set(ryo.__all__), set(own) - set(ryo.__all__)
