@@ -465,7 +465,8 @@ extern "C"
     RYO_API ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params* params, ryo_engine_t** out);
     RYO_API void ryo_engine_destroy(ryo_engine_t* engine);
     RYO_API const char* ryo_engine_last_error(const ryo_engine_t* engine);
-    /* queue a request; RYO_ERR_CAPACITY if it alone exceeds the budget */
+    /* queue a request; RYO_ERR_CAPACITY if it alone exceeds the budget, RYO_ERR_NOT_CUBIC for a periodic box that is
+     * not a cube and RYO_ERR_BAD_ARG for replica shells outside [0, 4] (refused here rather than at a later step) */
     RYO_API ryo_status ryo_engine_submit(ryo_engine_t* engine, const ryo_engine_request* request);
     /* admit, kick-drift, one batched solve of every resident request, kick, retire the finished ones */
     RYO_API ryo_status ryo_engine_step(ryo_engine_t* engine, ryo_engine_step_info* info, ryo_stream_t stream);

@@ -425,6 +425,23 @@ extern "C" ryo_status ryo_engine_submit(ryo_engine_t* E, const ryo_engine_reques
                 E->lastError = "engine_submit: every box axis needs max > min";
                 return RYO_ERR_BAD_ARG;
             }
+        // the batched solve's checks of a periodic system, made here so that one bad request cannot fail every
+        // step of the requests resident beside it
+        const int* b = r->box.boundary;
+        if (b[0] == RYO_BOUNDARY_PERIODIC && b[1] == RYO_BOUNDARY_PERIODIC && b[2] == RYO_BOUNDARY_PERIODIC)
+        {
+            DevBox<float> box = makeDevBox<float>(l, 1);
+            if (!(box.len[0] == box.len[1] && box.len[1] == box.len[2]))
+            {
+                E->lastError = "engine_submit: Ewald needs a cubic periodic box";
+                return RYO_ERR_NOT_CUBIC;
+            }
+            if (r->numShells < 0 || r->numShells > 4)
+            {
+                E->lastError = "engine_submit: numShells in [0, 4]";
+                return RYO_ERR_BAD_ARG;
+            }
+        }
     }
     Request q{};
     q.tag                = r->tag;

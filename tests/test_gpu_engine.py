@@ -141,3 +141,25 @@ def test_admission_respects_budget():
     with pytest.raises(ryo.RyoError):
         eng.submit(99, big.x, big.y, big.z, big.m, big.h, steps=1)
     eng.close()
+
+
+def test_submit_rejects_bad_periodic_requests():
+    """a periodic request the batched solve would refuse (non-cubic box, replica shells outside [0, 4]) is refused at
+    submission, and the requests already resident keep running"""
+    import ryoanji_b200 as ryo
+    eng = ryo.Engine(ryo.SolveParams())
+    ok = ds.plummer(500, seed=50)
+    eng.submit(1, ok.x, ok.y, ok.z, ok.m, ok.h, ok.vx, ok.vy, ok.vz, steps=2, dt=1e-3)
+    eng.step()
+    pb = ds.periodic_box(400, seed=51, eps=0.01)
+    per = (ryo.BOUNDARY_PERIODIC,) * 3
+    lo, hi = pb.box[0], pb.box[1]
+    with pytest.raises(ryo.RyoError) as e:
+        eng.submit(2, pb.x, pb.y, pb.z, pb.m, pb.h, box=ryo.Box(lo, hi, lo, hi, lo, hi + 0.5, per), steps=1)
+    assert e.value.status == ryo._abi.ERR_NOT_CUBIC
+    with pytest.raises(ryo.RyoError) as e:
+        eng.submit(3, pb.x, pb.y, pb.z, pb.m, pb.h, box=ryo.Box(*pb.box, boundary=per), num_shells=5, steps=1)
+    assert e.value.status == ryo._abi.ERR_BAD_ARG
+    done = _drain(eng)
+    assert sorted(done) == [1]
+    eng.close()
