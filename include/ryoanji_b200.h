@@ -38,7 +38,9 @@ extern "C"
         RYO_ERR_TIMEOUT                     = 5, /* a bounded device wait gave up (error flag set by a kernel) */
         RYO_ERR_CAPACITY                    = 6, /* a caller-provided buffer is too small; see the size out-arg */
         RYO_ERR_NOT_CUBIC                   = 7, /* Ewald needs a cubic periodic box */
-        RYO_ERR_NO_DEVICE                   = 8
+        RYO_ERR_NO_DEVICE                   = 8,
+        RYO_ERR_INTERNAL                    = 9  /* an unexpected host-side failure inside the library (a C++ exception
+                                                  that is no CUDA, argument or allocation error); see the last error */
     } ryo_status;
 
     /* cstone::BoundaryType (cstone/include/cstone/sfc/box.hpp:84-90) */

@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libryoanji_b200.so")
 
 BOUNDARY_OPEN, BOUNDARY_PERIODIC, BOUNDARY_FIXED, BOUNDARY_CUBIC_OPEN = 0, 1, 2, 3
-OK, ERR_CUDA, ERR_BAD_ARG, ERR_OOM, ERR_STACK_OVERFLOW, ERR_TIMEOUT, ERR_CAPACITY, ERR_NOT_CUBIC, ERR_NO_DEVICE = \
-    range(9)
+OK, ERR_CUDA, ERR_BAD_ARG, ERR_OOM, ERR_STACK_OVERFLOW, ERR_TIMEOUT, ERR_CAPACITY, ERR_NOT_CUBIC, ERR_NO_DEVICE, \
+    ERR_INTERNAL = range(10)
 
 
 class RyoError(RuntimeError):

@@ -7,8 +7,11 @@
  * The one exception is ryo_sort_by_key_static, whose scratch is a fixed device array shared by all its callers.
  */
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <memory>
+#include <new>
 #include <stdexcept>
 
 #include "internal.hpp"
@@ -55,6 +58,17 @@ ryo_status guarded(std::string& msg, F&& f)
     {
         msg = "host allocation failed";
         return RYO_ERR_OOM;
+    }
+    catch (const std::exception& e)
+    {
+        // no exception may cross the C ABI: anything else becomes a status too
+        msg = std::string("internal error: ") + e.what();
+        return RYO_ERR_INTERNAL;
+    }
+    catch (...)
+    {
+        msg = "internal error";
+        return RYO_ERR_INTERNAL;
     }
 }
 
@@ -120,6 +134,7 @@ extern "C" const char* ryo_status_string(ryo_status s)
         case RYO_ERR_CAPACITY: return "buffer capacity too small";
         case RYO_ERR_NOT_CUBIC: return "Ewald needs a cubic periodic box";
         case RYO_ERR_NO_DEVICE: return "no CUDA device";
+        case RYO_ERR_INTERNAL: return "internal error";
     }
     return "unknown status";
 }
@@ -129,8 +144,13 @@ extern "C" const char* ryo_version(void) { return "0.1.0"; }
 extern "C" ryo_status ryo_ctx_create(int device, ryo_ctx_t** out)
 {
     if (!out) return RYO_ERR_BAD_ARG;
-    *out = nullptr;
-    ryo_ctx* ctx = new ryo_ctx();
+    *out         = nullptr;
+    ryo_ctx* ctx = new (std::nothrow) ryo_ctx();
+    if (!ctx)
+    {
+        tlsError = "ctx_create: host allocation failed";
+        return RYO_ERR_OOM;
+    }
     ryo_status st = guarded(tlsError,
                             [&]
                             {
@@ -791,13 +811,17 @@ void treebuilderUpdate(ryo_treebuilder* tb, T* x, T* y, T* z, size_t n, const De
 extern "C" ryo_status ryo_treebuilder_create(ryo_ctx_t* ctx, unsigned ncrit, ryo_treebuilder_t** out)
 {
     if (!ctx || !out || ncrit == 0) return RYO_ERR_BAD_ARG;
-    static unsigned long long counter = 0;
-    auto* tb  = new ryo_treebuilder();
-    tb->ctx   = ctx;
-    tb->ncrit = ncrit;
-    tb->tag   = "tb" + std::to_string(++counter);
-    *out      = tb;
-    return RYO_OK;
+    // the tag names the builder's buffers in the context: unique across threads
+    static std::atomic<unsigned long long> counter{0};
+    return guarded(ctx->lastError,
+                   [&]
+                   {
+                       auto tb   = std::make_unique<ryo_treebuilder>();
+                       tb->ctx   = ctx;
+                       tb->ncrit = ncrit;
+                       tb->tag   = "tb" + std::to_string(++counter);
+                       *out      = tb.release();
+                   });
 }
 
 extern "C" void ryo_treebuilder_destroy(ryo_treebuilder_t* tb)

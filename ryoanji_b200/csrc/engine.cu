@@ -350,6 +350,17 @@ ryo_status engineGuard(ryo_engine* E, const std::function<void()>& f)
         E->lastError = "host allocation failed";
         return RYO_ERR_OOM;
     }
+    catch (const std::exception& e)
+    {
+        // no exception may cross the C ABI
+        E->lastError = std::string("internal error: ") + e.what();
+        return RYO_ERR_INTERNAL;
+    }
+    catch (...)
+    {
+        E->lastError = "internal error";
+        return RYO_ERR_INTERNAL;
+    }
 }
 } // namespace
 
@@ -397,6 +408,12 @@ extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params*
         ctx->lastError = std::string("engine_create: ") + e.what + ": " + cudaGetErrorString(e.err);
         delete E;
         return e.err == cudaErrorMemoryAllocation ? RYO_ERR_OOM : RYO_ERR_CUDA;
+    }
+    catch (...)
+    {
+        ctx->lastError = "engine_create: internal error";
+        delete E;
+        return RYO_ERR_INTERNAL;
     }
 }
 
@@ -462,7 +479,15 @@ extern "C" ryo_status ryo_engine_submit(ryo_engine_t* E, const ryo_engine_reques
         E->lastError = "engine_submit: the request alone exceeds the HBM budget";
         return RYO_ERR_CAPACITY;
     }
-    E->queue.push_back(q);
+    try
+    {
+        E->queue.push_back(q);
+    }
+    catch (const std::bad_alloc&)
+    {
+        E->lastError = "engine_submit: host allocation failed";
+        return RYO_ERR_OOM;
+    }
     return RYO_OK;
 }
 

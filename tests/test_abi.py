@@ -45,6 +45,8 @@ def test_status_strings_and_version():
     assert ryo.lib.ryo_version() == b"0.1.0"
     assert ryo.lib.ryo_status_string(0) == b"ok"
     assert b"stack" in ryo.lib.ryo_status_string(4)
+    assert ryo.lib.ryo_status_string(ryo._abi.ERR_INTERNAL) == b"internal error"
+    assert ryo.lib.ryo_status_string(ryo._abi.ERR_INTERNAL + 1) == b"unknown status"
     assert ryo.bh_max_target_size() == 64
     assert ryo.stack_size(1000) == 0
 
