@@ -92,9 +92,13 @@ extern "C"
     /* library version "major.minor.patch" */
     RYO_API const char* ryo_version(void);
     /* A context owns scratch memory, per-call counters and statistics on one device (no global device state, so
-     * several contexts may run concurrently on different streams). */
+     * several contexts may run concurrently on different streams). A context is not locked: calls on one context
+     * (and on the tree builders and engines made from it) must not overlap from several host threads; give each
+     * thread its own context. */
     RYO_API ryo_status ryo_ctx_create(int device, ryo_ctx_t** out);
     RYO_API void ryo_ctx_destroy(ryo_ctx_t* ctx);
+    /* the message of the context's last failed call; with NULL, that of the calling thread's last failed call of a
+     * function that takes no context (and of a failed ryo_ctx_create) */
     RYO_API const char* ryo_ctx_last_error(const ryo_ctx_t* ctx);
 
     /* ------------------------------------------------------------------------------------------ cstone layer */
