@@ -1,9 +1,12 @@
 /*
  * ryoanji-b200 — C ABI of the single-GPU Barnes-Hut gravity path for NVIDIA B200 (sm_100a).
  *
- * Plain pointers and sizes only. Every device array argument is device memory of the current device unless the
- * comment says "host". Each entry point names the reference interface it replaces (paths relative to the
- * reference project root, tischwab0911/ryoanji). Functions return a ryo_status and never exit the process.
+ * Plain pointers and sizes only. A function that takes a context (or a tree builder or engine made from one) runs
+ * on the context's device, which it makes current for the call and restores afterwards; the others run on the
+ * calling thread's current device. Every device array argument is memory of that device, and every stream one of
+ * its streams, unless the comment says "host". Each entry point names the reference interface it replaces (paths
+ * relative to the reference project root, tischwab0911/ryoanji). Functions return a ryo_status and never exit the
+ * process.
  *
  * Conventions shared with the reference:
  *   - 64-bit Hilbert keys, 21 levels; keys equal to 2^63 mark removed particles.

@@ -55,6 +55,13 @@ def _check(status: int, ctx: "Context | None" = None) -> None:
         raise RyoError(status, (msg or b"").decode(errors="replace"))
 
 
+def _same_device(ctx: "Context", *tensors) -> None:
+    """a context's calls run on the context's device, so its device arrays must live there"""
+    for t in tensors:
+        if isinstance(t, torch.Tensor) and t.is_cuda and t.device.index != ctx.device:
+            raise ValueError(f"a tensor on {t.device} was passed with a context on cuda:{ctx.device}")
+
+
 @dataclass
 class Box:
     """cstone::Box (cstone/include/cstone/sfc/box.hpp:99-214): limits x0, x1, y0, y1, z0, z1 and boundaries"""
@@ -170,6 +177,7 @@ def compute_sfc_keys(x, y, z, box: Box, keys=None, stream=None) -> torch.Tensor:
 
 def compute_bounding_box(x, y, z, ctx: Context | None = None, stream=None) -> list[float]:
     ctx = ctx or default_context()
+    _same_device(ctx, x, y, z)
     out = (C.c_float * 6)()
     _check(lib.ryo_compute_bounding_box_f32(ctx.handle, _ptr(x), _ptr(y), _ptr(z), C.c_size_t(x.numel()), out,
                                             _stream(stream)), ctx)
@@ -195,6 +203,7 @@ def sort_by_key(keys: torch.Tensor, values: torch.Tensor, stream=None) -> None:
 def compute_octree(sorted_keys: torch.Tensor, bucket_size: int, ctx: Context | None = None, stream=None):
     """cstone::computeOctree on the GPU: (leaves[numLeaves + 1] int64, counts[numLeaves] int32)"""
     ctx = ctx or default_context()
+    _same_device(ctx, sorted_keys)
     n = sorted_keys.numel()
     num = C.c_int(0)
     st = lib.ryo_compute_octree(ctx.handle, _ptr(sorted_keys), C.c_size_t(n), C.c_uint(bucket_size), None, None, 0,
@@ -211,6 +220,7 @@ def compute_octree(sorted_keys: torch.Tensor, bucket_size: int, ctx: Context | N
 def build_octree(leaves: torch.Tensor, ctx: Context | None = None, stream=None) -> dict:
     """cstone::buildOctreeGpu: the linked octree of a cornerstone leaf array"""
     ctx = ctx or default_context()
+    _same_device(ctx, leaves)
     nl = leaves.numel() - 1
     ni = (nl - 1) // 7
     nn = nl + ni
@@ -247,6 +257,7 @@ def compute_group_splits(x, y, z, h, leaves, layout, box: Box, group_size: int =
     """cstone::computeGroupSplits: spatial target groups of SFC-sorted bodies (int32 tensor of numGroups + 1
     entries: group starts, then last); leaves/layout are the cornerstone leaf array and body layout"""
     ctx = ctx or default_context()
+    _same_device(ctx, x, y, z, h, leaves, layout)
     last = x.numel() if last is None else last
     cap = (last - first) + 2
     groups = torch.empty(cap, dtype=torch.int32, device=x.device)
@@ -313,6 +324,8 @@ def traverse(groups: torch.Tensor, init_node: int, xt, yt, zt, mt, ht, xs, ys, z
     0.5 G sum(m phi) and, with group_counts, the per-group (M2P cells, P2P bodies) counts.
     """
     ctx = ctx or default_context()
+    _same_device(ctx, groups, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, child_offsets, internal_to_leaf, layout, source_center,
+                 multipoles, p, ax, ay, az)
     ng = groups.numel() - 1
     gv = _abi.GroupView(first_body, last_body if last_body is not None else xt.numel(), ng,
                         C.c_void_p(groups.data_ptr()), C.c_void_p(groups.data_ptr() + 4))
@@ -356,6 +369,7 @@ def compute_gravity_ewald(root_center, m_root, groups: torch.Tensor, x, y, z, m,
                           az, settings: EwaldSettings | None = None, ctx: Context | None = None, stream=None) -> float:
     """ryoanji::computeGravityEwaldGpu; returns the Ewald potential energy 0.5 G sum(m phi_ewald)"""
     ctx = ctx or default_context()
+    _same_device(ctx, groups, x, y, z, m, ugrav, ax, ay, az)
     settings = settings or EwaldSettings()
     ng = groups.numel() - 1
     gv = _abi.GroupView(0, x.numel(), ng, C.c_void_p(groups.data_ptr()), C.c_void_p(groups.data_ptr() + 4))
@@ -400,6 +414,7 @@ def ewald_targets_f64(targets: torch.Tensor, x, y, z, m, h, L: float, G: float =
     """FP64 periodic sum for chosen targets of a cubic box [x0, x0 + L)^3: direct sum over the replica shells plus
     the particle-level Ewald correction; (pot = G m phi, ax, ay, az) float64 tensors"""
     ctx = ctx or default_context()
+    _same_device(ctx, targets, x, y, z, m, h)
     e = (ewald or EwaldSettings()).c()
     out = direct_targets_f64(targets, x, y, z, m, h, G=G, box_l=(L, L, L), num_shells=e.numReplicaShells,
                              stream=stream)
@@ -431,6 +446,7 @@ class TreeBuilder:
 
     def update(self, x, y, z, box: Box, stream=None) -> int:
         """sorts x, y, z in place into SFC order and builds the tree; returns the number of nodes"""
+        _same_device(self.ctx, x, y, z)
         nn = C.c_int(0)
         if x.dtype == torch.float32:
             b = box.f32()
@@ -553,6 +569,7 @@ def solve(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, v=Non
     """The fused single-system solve. x, y, z, m, h (and v = (vx, vy, vz) if given) are sorted in place into SFC
     order; p, ax, ay, az receive G m phi and G a in that order; order (int32, optional) the original indices."""
     ctx = ctx or default_context()
+    _same_device(ctx, x, y, z, m, h, p, ax, ay, az, order, *(v or ()))
     params = params or SolveParams()
     pc = params.c()
     st = _abi.SolveStats()
@@ -615,6 +632,7 @@ def solve_batch(systems, x, y, z, m, h, p, ax, ay, az, params: SolveParams | Non
     """Solve many independent systems in one launch per phase. The arrays hold the systems' bodies concatenated in
     the order of @p systems (a list of BatchSystem); each system is sorted in place within its own range."""
     ctx = ctx or default_context()
+    _same_device(ctx, x, y, z, m, h, p, ax, ay, az, order, *(v or ()))
     params = params or SolveParams()
     pc = params.c()
     ns = len(systems)
@@ -757,6 +775,7 @@ def solve_targets(xt, yt, zt, mt=None, ht=None, ctx: Context | None = None, stre
     """field of the last solve() on @p ctx at separate targets (MultipoleHolder::compute with distinct targets):
     (p = G m phi, ax, ay, az) in the targets' order, and the interaction statistics"""
     ctx = ctx or default_context()
+    _same_device(ctx, xt, yt, zt, mt, ht)
     n = xt.numel()
     p, ax, ay, az = (torch.empty(n, device=xt.device) for _ in range(4))
     st = _abi.SolveStats()

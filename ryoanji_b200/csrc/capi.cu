@@ -72,6 +72,14 @@ ryo_status guarded(std::string& msg, F&& f)
     }
 }
 
+//! guarded, with the context's device current for the call
+template<class F>
+ryo_status guardedCtx(ryo_ctx* ctx, F&& f)
+{
+    DeviceScope device(ctx->device);
+    return guarded(ctx->lastError, std::forward<F>(f));
+}
+
 #define REQUIRE(cond, msg)                                                                                             \
     do                                                                                                                 \
     {                                                                                                                  \
@@ -151,6 +159,7 @@ extern "C" ryo_status ryo_ctx_create(int device, ryo_ctx_t** out)
         tlsError = "ctx_create: host allocation failed";
         return RYO_ERR_OOM;
     }
+    DeviceScope scope(device); // the caller's current device is restored on return
     ryo_status st = guarded(tlsError,
                             [&]
                             {
@@ -172,6 +181,7 @@ extern "C" ryo_status ryo_ctx_create(int device, ryo_ctx_t** out)
 extern "C" void ryo_ctx_destroy(ryo_ctx_t* ctx)
 {
     if (!ctx) return;
+    DeviceScope device(ctx->device);
     cudaDeviceSynchronize();
     ctx->releaseAll();
     if (ctx->ctl) cudaFree(ctx->ctl);
@@ -210,7 +220,7 @@ extern "C" ryo_status ryo_compute_bounding_box_f32(ryo_ctx_t* ctx, const float* 
                                                    size_t n, float* limits6, ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(limits6 && n > 0 && x && y && z, "compute_bounding_box: bad argument");
@@ -288,7 +298,7 @@ extern "C" ryo_status ryo_compute_octree(ryo_ctx_t* ctx, const uint64_t* sortedK
                                          ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(numLeaves && bucketSize > 0 && (n == 0 || sortedKeys), "compute_octree: bad argument");
@@ -306,7 +316,7 @@ extern "C" ryo_status ryo_build_octree(ryo_ctx_t* ctx, const uint64_t* leaves, i
                                        int* internalToLeaf, int* leafToInternal, ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(numLeaves >= 1 && leaves && prefixes && childOffsets && parents && levelRange &&
@@ -337,7 +347,7 @@ extern "C" ryo_status ryo_compute_group_splits_f32(ryo_ctx_t* ctx, uint32_t firs
                                                    uint32_t* numGroups, ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(numGroups && box && last >= first, "compute_group_splits: bad argument");
@@ -594,7 +604,7 @@ extern "C" ryo_status ryo_traverse_ex_f32(ryo_ctx_t* ctx, const ryo_group_view* 
                                           ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(grp && xt && yt && zt && mt && ht && xs && ys && zs && ms && hs && childOffsets &&
@@ -668,7 +678,7 @@ extern "C" ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float*
                                                     const ryo_ewald_settings* settings, ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(rootCenter && Mroot && grp && x && y && z && m && box && ax && ay && az && settings,
@@ -813,7 +823,7 @@ extern "C" ryo_status ryo_treebuilder_create(ryo_ctx_t* ctx, unsigned ncrit, ryo
     if (!ctx || !out || ncrit == 0) return RYO_ERR_BAD_ARG;
     // the tag names the builder's buffers in the context: unique across threads
     static std::atomic<unsigned long long> counter{0};
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        auto tb   = std::make_unique<ryo_treebuilder>();
@@ -827,6 +837,7 @@ extern "C" ryo_status ryo_treebuilder_create(ryo_ctx_t* ctx, unsigned ncrit, ryo
 extern "C" void ryo_treebuilder_destroy(ryo_treebuilder_t* tb)
 {
     if (!tb) return;
+    DeviceScope device(tb->ctx->device);
     cudaDeviceSynchronize();
     for (auto it = tb->ctx->buffers.begin(); it != tb->ctx->buffers.end();)
     {
@@ -844,7 +855,7 @@ extern "C" ryo_status ryo_treebuilder_update_f32(ryo_treebuilder_t* tb, float* x
                                                  const ryo_box_f32* box, int* numNodes, ryo_stream_t stream)
 {
     if (!tb) return RYO_ERR_BAD_ARG;
-    return guarded(tb->ctx->lastError,
+    return guardedCtx(tb->ctx,
                    [&]
                    {
                        REQUIRE(x && y && z && box, "treebuilder_update: null argument");
@@ -858,7 +869,7 @@ extern "C" ryo_status ryo_treebuilder_update_f64(ryo_treebuilder_t* tb, double* 
                                                  const ryo_box_f64* box, int* numNodes, ryo_stream_t stream)
 {
     if (!tb) return RYO_ERR_BAD_ARG;
-    return guarded(tb->ctx->lastError,
+    return guardedCtx(tb->ctx,
                    [&]
                    {
                        REQUIRE(x && y && z && box, "treebuilder_update: null argument");
@@ -1278,7 +1289,7 @@ extern "C" ryo_status ryo_solve_f32(ryo_ctx_t* ctx, const ryo_solve_params* P, f
                                     ryo_stream_t stream)
 {
     if (!ctx || !P) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&] { solveSingle(ctx, P, x, y, z, m, h, vx, vy, vz, n, p, ax, ay, az, orderOut, stats, stream,
                                      nullptr); });
 }
@@ -1289,7 +1300,7 @@ extern "C" ryo_status ryo_solve_host_f32(ryo_ctx_t* ctx, const ryo_solve_params*
                                          uint32_t* order, ryo_solve_stats* stats, ryo_stream_t stream)
 {
     if (!ctx || !P) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(x && y && z && m && h && p && ax && ay && az, "solve_host: null argument");
@@ -1335,7 +1346,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                                           ryo_solve_stats* stats, ryo_stream_t stream)
 {
     if (!ctx || !P) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(systems && numSystems >= 1 && numSystems <= RYO_BATCH_MAX_SYSTEMS,
@@ -1608,7 +1619,7 @@ extern "C" ryo_status ryo_ewald_targets_f64(ryo_ctx_t* ctx, const int64_t* targe
                                             double* pot, double* ax, double* ay, double* az, ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        REQUIRE(settings && L > 0, "ewald_targets: bad settings or box");
@@ -1666,7 +1677,7 @@ extern "C" ryo_status ryo_solve_targets_f32(ryo_ctx_t* ctx, const float* xt, con
                                            float* ay, float* az, ryo_solve_stats* stats, ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError,
+    return guardedCtx(ctx,
                    [&]
                    {
                        const auto& S = ctx->solveState;
@@ -1779,5 +1790,5 @@ extern "C" uint64_t ryo_kernel_launches(void) { return ryo::launchCounter(); }
 extern "C" ryo_status ryo_measure_peaks(ryo_ctx_t* ctx, double* out3, ryo_stream_t stream)
 {
     if (!ctx || !out3) return RYO_ERR_BAD_ARG;
-    return guarded(ctx->lastError, [&] { measurePeaks(ctx->smCount, out3, out3 + 1, out3 + 2, stream); });
+    return guardedCtx(ctx, [&] { measurePeaks(ctx->smCount, out3, out3 + 1, out3 + 2, stream); });
 }

@@ -330,6 +330,7 @@ struct SolveFailed
 
 ryo_status engineGuard(ryo_engine* E, const std::function<void()>& f)
 {
+    DeviceScope device(E->ctx->device);
     try
     {
         f();
@@ -382,6 +383,7 @@ extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params*
         p->maxSystems > RYO_BATCH_MAX_SYSTEMS)
         return RYO_ERR_BAD_ARG;
     ryo_engine* E = nullptr;
+    DeviceScope device(ctx->device);
     try
     {
         E               = new ryo_engine();
@@ -419,7 +421,9 @@ extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params*
 
 extern "C" void ryo_engine_destroy(ryo_engine_t* E)
 {
-    if (E) cudaDeviceSynchronize();
+    if (!E) return;
+    DeviceScope device(E->ctx->device);
+    cudaDeviceSynchronize();
     delete E;
 }
 

@@ -36,6 +36,27 @@ enum BhStat
     kMaxStack
 };
 
+//! makes @p device the current device for its scope and restores the caller's afterwards, so that a context's calls
+//! allocate and launch on the context's device whatever device the calling thread has current
+class DeviceScope
+{
+public:
+    explicit DeviceScope(int device)
+    {
+        if (cudaGetDevice(&prev_) == cudaSuccess && prev_ != device) switched_ = cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceScope()
+    {
+        if (switched_) cudaSetDevice(prev_);
+    }
+    DeviceScope(const DeviceScope&)            = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+
+private:
+    int prev_      = 0;
+    bool switched_ = false;
+};
+
 } // namespace ryo
 
 struct ryo_ctx
