@@ -296,3 +296,24 @@ def test_mdq_p2m_m2m_m2p_match_reference(oracle, ref_oracle):
         r = np.sqrt((d * d).sum(0))
         direct = np.array([-(m / r).sum(), *(m * d / r ** 3).sum(1)])
         assert np.allclose(a_r, direct, atol=1e-3)
+
+
+def test_fixtures_regenerate_from_the_reference(ref_oracle):
+    """every committed golden case is what the reference's own CPU code (oracle/_ref) produces for the case's seeded
+    inputs today: the fixtures are the reference's outputs, not the restatement's. Arrays are compared bit for bit;
+    the total energies to 1e-5, since the reference sums them in an OpenMP reduction whose order follows the thread
+    count"""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(os.path.dirname(__file__), "golden",
+                                                                              "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    for kind, n, seed, bucket in mg.CASES:
+        fresh = mg.make_case(ref_oracle, kind, n, seed, bucket)
+        stored = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"case_{kind}_{n}.npz")))
+        assert set(fresh) == set(stored), (kind, set(fresh) ^ set(stored))
+        for k, v in fresh.items():
+            if k.endswith("_u"):
+                assert abs(float(v) - float(stored[k])) <= 1e-5 * abs(float(stored[k])), (kind, k)
+            else:
+                assert np.array_equal(np.asarray(v), stored[k]), (kind, k)
