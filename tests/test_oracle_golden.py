@@ -317,3 +317,37 @@ def test_fixtures_regenerate_from_the_reference(ref_oracle):
                 assert abs(float(v) - float(stored[k])) <= 1e-5 * abs(float(stored[k])), (kind, k)
             else:
                 assert np.array_equal(np.asarray(v), stored[k]), (kind, k)
+
+
+def _edge_sets():
+    rng = np.random.default_rng(123)
+    yield "empty", np.zeros(0, np.float32), np.zeros(0, np.float32), np.zeros(0, np.float32), [0, 1, 0, 1, 0, 1], 16
+    one = np.array([0.3], np.float32)
+    yield "one", one, one, one, [0, 1, 0, 1, 0, 1], 16
+    same = np.full(700, 0.25, np.float32)  # 700 coincident bodies: a deepest-level leaf above the bucket size
+    yield "coincident", same, same, same, [0, 1, 0, 1, 0, 1], 64
+    x, y, z = (rng.uniform(0, 1, 500).astype(np.float32) for _ in range(3))
+    yield "bucket1", x, y, z, [0, 1, 0, 1, 0, 1], 1
+    x = rng.uniform(0, 16, 2000).astype(np.float32)
+    y, z = (rng.uniform(0, 0.01, 2000).astype(np.float32) for _ in range(2))
+    yield "reduced_axes", x, y, z, [0, 16, 0, 0.01, 0, 0.01], 8
+
+
+@pytest.mark.parametrize("name", ["empty", "one", "coincident", "bucket1", "reduced_axes"])
+def test_reference_wrapper_agrees_on_edge_cases(oracle, ref_oracle, name):
+    """the restatement equals the reference's own code on the edge cases its tests cover: no bodies, one body,
+    coincident bodies, bucket size 1 and a box with reduced axes (keys, leaves, counts and the linked octree)"""
+    x, y, z, box, bucket = next((s[1:] for s in _edge_sets() if s[0] == name))
+    box = np.asarray(box, np.float32)
+    k1, k2 = oracle.sfc_keys(x, y, z, box), ref_oracle.sfc_keys(x, y, z, box)
+    assert np.array_equal(k1, k2)
+    assert np.array_equal(oracle.box_dim_bits(box), ref_oracle.box_dim_bits(box))
+    s1, o1 = oracle.sort_keys(k1)
+    s2, o2 = ref_oracle.sort_keys(k2)
+    assert np.array_equal(s1, s2) and np.array_equal(o1, o2)
+    l1, c1 = oracle.octree_leaves(s1, bucket)
+    l2, c2 = ref_oracle.octree_leaves(s1, bucket)
+    assert np.array_equal(l1, l2) and np.array_equal(c1, c2)
+    t1, t2 = oracle.octree_link(l1), ref_oracle.octree_link(l1)
+    for k in t1:
+        assert np.array_equal(np.asarray(t1[k]), np.asarray(t2[k])), k
