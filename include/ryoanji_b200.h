@@ -76,7 +76,9 @@ extern "C"
         const uint32_t* groupEnd;
     } ryo_group_view;
 
-    /* ryoanji::EwaldSettings (ryoanji/src/ryoanji/nbody/ewald.h:23-31) */
+    /* ryoanji::EwaldSettings (ryoanji/src/ryoanji/nbody/ewald.h:23-31). As in the reference, ceil(hCut) must be at
+     * most 3 (ewald.hpp:52-60); no value may be negative, and alpha_scale must be positive unless lCut, hCut and
+     * alpha_scale are all 0 (Ewald off). Other settings give RYO_ERR_BAD_ARG wherever a periodic box uses them. */
     typedef struct ryo_ewald_settings
     {
         int numReplicaShells;        /* 1 */

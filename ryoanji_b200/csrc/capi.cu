@@ -86,6 +86,13 @@ ryo_status guardedCtx(ryo_ctx* ctx, F&& f)
         if (!(cond)) throw ApiError{RYO_ERR_BAD_ARG, msg};                                                             \
     } while (0)
 
+//! refuses the Ewald settings the reference refuses (ewaldSettingsError)
+void checkEwald(const ryo_ewald_settings* e)
+{
+    REQUIRE(e, "ewald: null settings");
+    if (const char* why = ewaldSettingsError(*e)) throw ApiError{RYO_ERR_BAD_ARG, why};
+}
+
 DevBox<float> boxOf(const ryo_box_f32* b)
 {
     int periodic = b->boundary[0] == RYO_BOUNDARY_PERIODIC && b->boundary[1] == RYO_BOUNDARY_PERIODIC &&
@@ -681,6 +688,7 @@ extern "C" ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float*
     return guardedCtx(ctx,
                    [&]
                    {
+                       checkEwald(settings);
                        REQUIRE(rootCenter && Mroot && grp && x && y && z && m && box && ax && ay && az && settings,
                                "compute_gravity_ewald: null argument");
                        float lx = box->limits[1] - box->limits[0], ly = box->limits[3] - box->limits[2],
@@ -998,6 +1006,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     checkBox(box.limits);
     DevBox<float> dbox = boxOf(&box);
     bool periodic      = dbox.periodic;
+    if (periodic) checkEwald(&P->ewald);
 
     // keys and sort
     uint64_t* keys    = ctx->scratch<uint64_t>("solve.keys", n, s);
@@ -1385,6 +1394,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                                        throw ApiError{RYO_ERR_NOT_CUBIC,
                                                       "solve_batch: Ewald needs a cubic periodic box"};
                                    REQUIRE(sy.numShells >= 0 && sy.numShells <= 4, "solve_batch: numShells in [0, 4]");
+                                   checkEwald(&P->ewald);
                                    shells[k] = sy.numShells;
                                }
                            }
@@ -1622,7 +1632,8 @@ extern "C" ryo_status ryo_ewald_targets_f64(ryo_ctx_t* ctx, const int64_t* targe
     return guardedCtx(ctx,
                    [&]
                    {
-                       REQUIRE(settings && L > 0, "ewald_targets: bad settings or box");
+                       checkEwald(settings);
+                       REQUIRE(L > 0, "ewald_targets: bad box");
                        REQUIRE(numTargets == 0 || (targets && x && y && z && m && pot && ax && ay && az),
                                "ewald_targets: null argument");
                        launchEwaldTargetsF64(ctx, targets, numTargets, x, y, z, m, numBodies, L,

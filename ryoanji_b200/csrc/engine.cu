@@ -382,6 +382,12 @@ extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params*
     if (!(p->hbmBudgetBytes > 0) || !(p->bytesPerBody > 0) || p->maxSystems < 1 ||
         p->maxSystems > RYO_BATCH_MAX_SYSTEMS)
         return RYO_ERR_BAD_ARG;
+    if (const char* why = ewaldSettingsError(p->solve.ewald))
+    {
+        // periodic requests would fail every step: refuse the settings now
+        ctx->lastError = std::string("engine_create: ") + why;
+        return RYO_ERR_BAD_ARG;
+    }
     ryo_engine* E = nullptr;
     DeviceScope device(ctx->device);
     try

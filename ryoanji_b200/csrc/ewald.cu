@@ -25,9 +25,9 @@ struct EwaldKernelParams
     int replicaShells, ewaldShells;
     int numK;
     double twoPiOverL;
-    signed char h[343][3];
-    double fc[343];
-    double fs[343];
+    signed char h[kEwaldMaxK][3];
+    double fc[kEwaldMaxK];
+    double fs[kEwaldMaxK];
 };
 
 //! ewaldEvalMultipoleComplete (ewald.hpp:90-115)
@@ -77,6 +77,8 @@ EwaldHost ewaldSetup(const double* mroot, const double* center, int replicaShell
                 double hr[3] = {double(hx), double(hy), double(hz)};
                 double h2    = hr[0] * hr[0] + (hr[1] * hr[1] + hr[2] * hr[2]);
                 if (h2 == 0 || h2 > hCut * hCut) continue;
+                if (e.numK >= kEwaldMaxK) // callers check hCut first; this keeps the tables in bounds regardless
+                    throw CudaError{cudaErrorInvalidValue, "ewald: more wave vectors than hCut <= 3 gives"};
                 double g0 = std::exp(-k4 * h2) / (M_PI * h2 * L);
                 double g1 = 2 * M_PI / L * g0;
                 double g2 = -2 * M_PI / L * g1;

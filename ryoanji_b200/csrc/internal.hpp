@@ -4,6 +4,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -35,6 +36,19 @@ enum BhStat
     kMaxM2P,
     kMaxStack
 };
+
+//! why the reference would refuse these Ewald settings, or nullptr: ceil(hCut) <= 3 (ryoanji/src/ryoanji/nbody/
+//! ewald.hpp:52-60, which also bounds the wave-vector tables here), no negative value, and a positive alpha_scale
+//! unless lCut, hCut and alpha_scale are all 0 (Ewald off)
+inline const char* ewaldSettingsError(const ryo_ewald_settings& e)
+{
+    if (!(e.numReplicaShells >= 0 && e.lCut >= 0 && e.hCut >= 0 && e.alpha_scale >= 0 && e.small_R_scale_factor >= 0))
+        return "ewald: settings must not be negative";
+    if (!(std::ceil(e.hCut) <= 3)) return "ewald: hCut must be at most 3, as in the reference";
+    bool off = e.lCut == 0 && e.hCut == 0 && e.alpha_scale == 0;
+    if (!(off || e.alpha_scale > 0)) return "ewald: alpha_scale must be positive";
+    return nullptr;
+}
 
 //! makes @p device the current device for its scope and restores the caller's afterwards, so that a context's calls
 //! allocate and launch on the context's device whatever device the calling thread has current
@@ -349,6 +363,9 @@ void launchBatchGroups(uint32_t numGroups, const uint64_t* first, const uint32_t
                        uint32_t groupSize, uint32_t* start, uint32_t* end, uint32_t* sys, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- ewald.cu
+//! wave vectors of the k-space sum for ceil(hCut) <= 3: at most the 7^3 - 1 non-zero vectors of [-3, 3]^3
+constexpr int kEwaldMaxK = 343;
+
 struct EwaldHost
 {
     double mroot[8];
@@ -356,7 +373,7 @@ struct EwaldHost
     int replicaShells, ewaldShells;
     double L, lCut, hCut, alphaScale, smallR;
     int numK;
-    double kdata[343 * 5]; // per k vector: hs[3], fc, fs
+    double kdata[kEwaldMaxK * 5]; // per k vector: hs[3], fc, fs
 };
 EwaldHost ewaldSetup(const double* mroot, const double* center, int replicaShells, double L, double lCut,
                      double hCut, double alphaScale, double smallR);

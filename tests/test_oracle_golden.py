@@ -379,3 +379,22 @@ def test_reference_wrapper_agrees_on_edge_case_upsweep_and_walk(oracle, ref_orac
         assert np.array_equal(a[:full], b[:full])
     if full == n:
         assert abs(g1[0] - g2[0]) <= 1e-5 * max(abs(g2[0]), 1e-30)
+
+
+@pytest.mark.parametrize("shells,lcut,hcut", [(0, 2.6, 2.8), (1, 2.6, 2.8), (2, 3.2, 3.0), (1, 1.5, 1.6)])
+def test_ewald_restatement_against_reference_settings(oracle, ref_oracle, shells, lcut, hcut):
+    """the root-multipole Ewald correction against the reference's own code at other replica shells and cut-offs,
+    in an offset box of length 3 (ryoanji/src/ryoanji/nbody/ewald.hpp:200-389); hCut stays within the reference's
+    ceil(hCut) <= 3"""
+    rng = np.random.default_rng(17 + shells)
+    n = 300
+    x, y, z = (rng.uniform(-1.0, 2.0, n) for _ in range(3))
+    m = rng.uniform(0.5, 1.5, n) / n
+    box = np.array([-1.0, 2.0, -1.0, 2.0, -1.0, 2.0])
+    c, q = oracle.p2m(x, y, z, m)
+    rc, mr = np.asarray(c[:3], np.float64), np.asarray(q, np.float64)
+    u1, *f1 = oracle.ewald(rc, mr, x, y, z, m, box, G=1.0, replica_shells=shells, lcut=lcut, hcut=hcut)
+    u2, *f2 = ref_oracle.ewald(rc, mr, x, y, z, m, box, G=1.0, replica_shells=shells, lcut=lcut, hcut=hcut)
+    for a, b in zip(f1, f2):
+        assert np.allclose(a, b, rtol=1e-12, atol=1e-12 * np.abs(b).max())
+    assert abs(u1 - u2) <= 1e-12 * abs(u2)
