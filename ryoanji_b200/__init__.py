@@ -34,8 +34,9 @@ __all__ = [
 MAX_TREE_LEVEL = 21
 
 
-def _stream(stream=None) -> C.c_void_p:
-    s = stream if stream is not None else torch.cuda.current_stream()
+def _stream(stream=None, ctx: "Context | None" = None) -> C.c_void_p:
+    """the caller's stream, else the current stream of the context's device (of the current device without one)"""
+    s = stream if stream is not None else torch.cuda.current_stream(ctx.device if ctx is not None else None)
     return C.c_void_p(s.cuda_stream)
 
 
@@ -180,7 +181,7 @@ def compute_bounding_box(x, y, z, ctx: Context | None = None, stream=None) -> li
     _same_device(ctx, x, y, z)
     out = (C.c_float * 6)()
     _check(lib.ryo_compute_bounding_box_f32(ctx.handle, _ptr(x), _ptr(y), _ptr(z), C.c_size_t(x.numel()), out,
-                                            _stream(stream)), ctx)
+                                            _stream(stream, ctx)), ctx)
     return list(out)
 
 
@@ -207,13 +208,13 @@ def compute_octree(sorted_keys: torch.Tensor, bucket_size: int, ctx: Context | N
     n = sorted_keys.numel()
     num = C.c_int(0)
     st = lib.ryo_compute_octree(ctx.handle, _ptr(sorted_keys), C.c_size_t(n), C.c_uint(bucket_size), None, None, 0,
-                                C.byref(num), _stream(stream))
+                                C.byref(num), _stream(stream, ctx))
     if st not in (0, _abi.ERR_CAPACITY):
         _check(st, ctx)
     leaves = torch.empty(num.value + 1, dtype=torch.int64, device=sorted_keys.device)
     counts = torch.empty(num.value, dtype=torch.int32, device=sorted_keys.device)
     _check(lib.ryo_compute_octree(ctx.handle, _ptr(sorted_keys), C.c_size_t(n), C.c_uint(bucket_size), _ptr(leaves),
-                                  _ptr(counts), num.value, C.byref(num), _stream(stream)), ctx)
+                                  _ptr(counts), num.value, C.byref(num), _stream(stream, ctx)), ctx)
     return leaves, counts
 
 
@@ -236,7 +237,7 @@ def build_octree(leaves: torch.Tensor, ctx: Context | None = None, stream=None) 
     lr = (C.c_int * (MAX_TREE_LEVEL + 2))()
     _check(lib.ryo_build_octree(ctx.handle, _ptr(leaves), nl, _ptr(t["prefixes"]), _ptr(t["childOffsets"]),
                                 _ptr(t["parents"]), lr, _ptr(t["d_levelRange"]), _ptr(t["internalToLeaf"]),
-                                _ptr(t["leafToInternal"]), _stream(stream)), ctx)
+                                _ptr(t["leafToInternal"]), _stream(stream, ctx)), ctx)
     t["childOffsets"] = t["childOffsets"][:nn]
     t.update(levelRange=list(lr), numLeafNodes=nl, numInternalNodes=ni, numNodes=nn)
     return t
@@ -267,7 +268,7 @@ def compute_group_splits(x, y, z, h, leaves, layout, box: Box, group_size: int =
                                             _ptr(z), _ptr(h), _ptr(leaves), C.c_int(leaves.numel() - 1),
                                             _ptr(layout), C.byref(bx), C.c_uint(group_size), C.c_float(tol_factor),
                                             C.c_float(extent_ratio), _ptr(groups), C.c_uint32(cap), C.byref(num),
-                                            _stream(stream)), ctx)
+                                            _stream(stream, ctx)), ctx)
     return groups[:num.value + 1]
 
 
@@ -344,7 +345,7 @@ def traverse(groups: torch.Tensor, init_node: int, xt, yt, zt, mt, ht, xs, ys, z
                                    _ptr(ht), _ptr(xs), _ptr(ys), _ptr(zs), _ptr(ms), _ptr(hs), _ptr(child_offsets),
                                    _ptr(internal_to_leaf), _ptr(layout), _ptr(source_center), _ptr(multipoles),
                                    C.c_float(G), num_shells, bl, _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), C.byref(pot),
-                                   C.byref(opts), _stream(stream)), ctx)
+                                   C.byref(opts), _stream(stream, ctx)), ctx)
     if group_counts:
         return pot.value, m2p, p2p
     return pot.value
@@ -380,7 +381,7 @@ def compute_gravity_ewald(root_center, m_root, groups: torch.Tensor, x, y, z, m,
     s = settings.c()
     _check(lib.ryo_compute_gravity_ewald_f32(ctx.handle, rc, mr, C.byref(gv), _ptr(x), _ptr(y), _ptr(z), _ptr(m),
                                              C.byref(b), C.c_float(G), _ptr(ugrav), _ptr(ax), _ptr(ay), _ptr(az),
-                                             C.byref(tot), C.byref(s), _stream(stream)), ctx)
+                                             C.byref(tot), C.byref(s), _stream(stream, ctx)), ctx)
     return tot.value
 
 
@@ -420,7 +421,7 @@ def ewald_targets_f64(targets: torch.Tensor, x, y, z, m, h, L: float, G: float =
                              stream=stream)
     _check(lib.ryo_ewald_targets_f64(ctx.handle, _ptr(targets), C.c_size_t(targets.numel()), _ptr(x), _ptr(y),
                                      _ptr(z), _ptr(m), C.c_size_t(x.numel()), C.c_double(L), C.byref(e),
-                                     C.c_double(G), *[_ptr(o) for o in out], _stream(stream)), ctx)
+                                     C.c_double(G), *[_ptr(o) for o in out], _stream(stream, ctx)), ctx)
     return out
 
 
@@ -455,7 +456,7 @@ class TreeBuilder:
             b = box.f64()
             fn = lib.ryo_treebuilder_update_f64
         _check(fn(self.handle, _ptr(x), _ptr(y), _ptr(z), C.c_size_t(x.numel()), C.byref(b), C.byref(nn),
-                  _stream(stream)), self.ctx)
+                  _stream(stream, self.ctx)), self.ctx)
         v = _abi.TreeView()
         _check(lib.ryo_treebuilder_view(self.handle, C.byref(v)))
         self._view = v
@@ -576,7 +577,7 @@ def solve(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, v=Non
     vx, vy, vz = v if v is not None else (None, None, None)
     _check(lib.ryo_solve_f32(ctx.handle, C.byref(pc), _ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(h), _ptr(vx), _ptr(vy),
                              _ptr(vz), C.c_size_t(x.numel()), _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), _ptr(order),
-                             C.byref(st), _stream(stream)), ctx)
+                             C.byref(st), _stream(stream, ctx)), ctx)
     _solve_n[id(ctx)] = x.numel()
     ms = dict(zip(("sort", "tree", "upsweep", "traverse", "ewald", "total"), list(st.ms)))
     return SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
@@ -602,7 +603,7 @@ def solve_host(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, 
     hp = lambda t: None if t is None else C.c_void_p(t.data_ptr())  # noqa: E731  (host pointers, checked above)
     _check(lib.ryo_solve_host_f32(ctx.handle, C.byref(pc), hp(x), hp(y), hp(z), hp(m), hp(h), C.c_size_t(x.numel()),
                                   hp(xs), hp(ys), hp(zs), hp(p), hp(ax), hp(ay), hp(az), hp(order), C.byref(st),
-                                  _stream(stream)), ctx)
+                                  _stream(stream, ctx)), ctx)
     _solve_n[id(ctx)] = x.numel()
     ms = dict(zip(("sort", "tree", "upsweep", "traverse", "ewald", "total"), list(st.ms)))
     return SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
@@ -652,7 +653,7 @@ def solve_batch(systems, x, y, z, m, h, p, ax, ay, az, params: SolveParams | Non
     vx, vy, vz = v if v is not None else (None, None, None)
     _check(lib.ryo_solve_batch_f32(ctx.handle, C.byref(pc), arr, ns, _ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(h),
                                    _ptr(vx), _ptr(vy), _ptr(vz), C.c_size_t(x.numel()), _ptr(p), _ptr(ax), _ptr(ay),
-                                   _ptr(az), _ptr(order), energies, boxes, C.byref(st), _stream(stream)), ctx)
+                                   _ptr(az), _ptr(order), energies, boxes, C.byref(st), _stream(stream, ctx)), ctx)
     ms = dict(zip(("sort", "tree", "upsweep", "traverse", "ewald", "total"), list(st.ms)))
     res = SolveResult(st.numLeaves, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P,
                       st.maxStack, st.retries, st.potentialEnergy, [], ms)
@@ -730,7 +731,7 @@ class Engine:
 
     def step(self, stream=None) -> dict:
         info = _abi.EngineStepInfo()
-        self._err(lib.ryo_engine_step(self.handle, C.byref(info), _stream(stream)))
+        self._err(lib.ryo_engine_step(self.handle, C.byref(info), _stream(stream, self.ctx)))
         d = {k: getattr(info, k) for k in ("admitted", "retired", "resident", "queued", "solved", "retries",
                                            "residentBodies", "sumP2P", "maxP2P", "sumM2P", "maxM2P")}
         d["ms"] = list(info.ms)
@@ -780,7 +781,7 @@ def solve_targets(xt, yt, zt, mt=None, ht=None, ctx: Context | None = None, stre
     p, ax, ay, az = (torch.empty(n, device=xt.device) for _ in range(4))
     st = _abi.SolveStats()
     _check(lib.ryo_solve_targets_f32(ctx.handle, _ptr(xt), _ptr(yt), _ptr(zt), _ptr(mt), _ptr(ht), C.c_size_t(n),
-                                     _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), C.byref(st), _stream(stream)), ctx)
+                                     _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), C.byref(st), _stream(stream, ctx)), ctx)
     res = SolveResult(0, st.numNodes, st.numGroups, st.sumP2P, st.maxP2P, st.sumM2P, st.maxM2P, st.maxStack,
                       st.retries, st.potentialEnergy, list(st.box), {})
     return (p, ax, ay, az), res
@@ -802,7 +803,7 @@ def measure_peaks(ctx: Context | None = None, stream=None) -> dict:
     """FP32 FMA peak (scalar and packed f32x2) in TFLOP/s and streaming-copy GB/s, measured now"""
     ctx = ctx or default_context()
     out = (C.c_double * 3)()
-    _check(lib.ryo_measure_peaks(ctx.handle, out, _stream(stream)), ctx)
+    _check(lib.ryo_measure_peaks(ctx.handle, out, _stream(stream, ctx)), ctx)
     return dict(fp32_tflops=out[0], fp32x2_tflops=out[1], copy_gbs=out[2])
 
 
