@@ -244,6 +244,77 @@ inline void computeFixedGroups(LocalIndex first, LocalIndex last, unsigned group
     check(ryo_compute_fixed_groups(first, last, groupSize, groups, stream));
 }
 
+//! cstone::sequence (cstone/include/cstone/primitives/primitives_gpu.h:92): input[i] = init + i
+inline void sequence(LocalIndex* input, size_t numElements, LocalIndex init, ryo_stream_t stream = nullptr)
+{
+    check(ryo_sequence(input, numElements, init, stream));
+}
+
+//! cstone::sortByKeyTempStorage (primitives_gpu.h:118-120) for 64-bit keys and 32-bit values, in bytes
+template<class KeyType, class ValueType>
+uint64_t sortByKeyTempStorage(uint64_t numElements)
+{
+    static_assert(std::is_same_v<KeyType, uint64_t> && sizeof(ValueType) == 4, "64-bit keys, 32-bit values");
+    return ryo_sort_by_key_temp_bytes(numElements);
+}
+
+/*! cstone::sortByKey (primitives_gpu.h:122-130): stable ascending sort of the keys [first, last), carrying values
+ *  along; keyBuf and valueBuf hold last - first elements, tmp sortByKeyTempStorage bytes. Fewer than 2^32 keys. */
+template<class ValueType>
+void sortByKey(uint64_t* first, uint64_t* last, ValueType* values, uint64_t* keyBuf, ValueType* valueBuf, void* tmp,
+               uint64_t tmpBytes, ryo_stream_t stream = nullptr)
+{
+    static_assert(sizeof(ValueType) == 4, "32-bit values");
+    check(ryo_sort_by_key(first, reinterpret_cast<uint32_t*>(values), size_t(last - first), keyBuf,
+                          reinterpret_cast<uint32_t*>(valueBuf), tmp, tmpBytes, stream));
+}
+
+/*! cstone::computeOctree / updateOctreeGpu run to their fixed point (cstone/include/cstone/tree/csarray.hpp:409-440,
+ *  update_gpu.cuh:43-68) for sorted 64-bit keys: the cornerstone leaves (numLeaves + 1 keys) and counts of at most
+ *  @p bucketSize keys per leaf, in one pass. Returns numLeaves; when it exceeds @p capacity nothing is written, and
+ *  a second call with that capacity writes the arrays. */
+inline TreeNodeIndex computeOctreeGpu(const uint64_t* sortedKeys, size_t numKeys, unsigned bucketSize,
+                                      uint64_t* leaves, LocalIndex* counts, TreeNodeIndex capacity,
+                                      Context& ctx = defaultContext(), ryo_stream_t stream = nullptr)
+{
+    int numLeaves = 0;
+    ryo_status s =
+        ryo_compute_octree(ctx.get(), sortedKeys, numKeys, bucketSize, leaves, counts, capacity, &numLeaves, stream);
+    if (s != RYO_ERR_CAPACITY) check(s, ctx.get());
+    return numLeaves;
+}
+
+//! cstone::OctreeView (cstone/include/cstone/tree/octree.hpp:235-256) for 64-bit keys: where buildOctreeGpu writes
+//! the linked octree. levelRange is host memory and d_levelRange device memory (may be null), as in the reference.
+template<class KeyType>
+struct OctreeView
+{
+    TreeNodeIndex numLeafNodes;
+    TreeNodeIndex numInternalNodes;
+    TreeNodeIndex numNodes;
+    TreeNodeIndex numParents;
+
+    KeyType* prefixes;
+    TreeNodeIndex* childOffsets;
+    TreeNodeIndex* parents;
+    TreeNodeIndex* levelRange;
+    TreeNodeIndex* d_levelRange;
+    TreeNodeIndex* internalToLeaf;
+    TreeNodeIndex* leafToInternal;
+    KeyType* leaves{nullptr};
+};
+
+//! cstone::buildOctreeGpu (cstone/include/cstone/tree/octree_gpu.h:36) from the cornerstone leaves
+template<class KeyType>
+void buildOctreeGpu(const KeyType* cstoneTree, OctreeView<KeyType> d, Context& ctx = defaultContext(),
+                    ryo_stream_t stream = nullptr)
+{
+    static_assert(std::is_same_v<KeyType, uint64_t>, "the B200 library builds 64-bit key trees");
+    check(ryo_build_octree(ctx.get(), cstoneTree, d.numLeafNodes, d.prefixes, d.childOffsets, d.parents, d.levelRange,
+                           d.d_levelRange, d.internalToLeaf, d.leafToInternal, stream),
+          ctx.get());
+}
+
 //! cstone::computeLeafSourceCenterGpu (cstone/include/cstone/focus/source_center_gpu.h)
 inline void computeLeafSourceCenterGpu(const float* x, const float* y, const float* z, const float* m,
                                        const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,

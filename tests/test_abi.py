@@ -101,6 +101,10 @@ def test_cpp_shim_links_and_reports_errors(tmp_path):
 #include <cstdio>
 int main() {
     if (ryo::bhMaxTargetSize() != 64 || ryo::stackSize(1000) != 0) return 2;
+    // the cstone primitives: sizes and empty inputs need no device
+    if (ryo::sortByKeyTempStorage<uint64_t, unsigned>(1000) != ryo_sort_by_key_temp_bytes(1000)) return 6;
+    ryo::sortByKey<unsigned>(nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0);
+    ryo::sequence(nullptr, 0, 0);
     ryo::Box<float> box(-1.f, 1.f);
     if (box.lx() != 2.f || box.boundaryX() != ryo::BoundaryType::open) return 3;
     try { ryo::Context ctx(0); return 4; }
