@@ -221,7 +221,9 @@ extern "C"
      * initNodeIdx. numShells > 0 adds the (2 numShells + 1)^3 periodic replicas of edge boxL (3 floats, host).
      * Accumulates G m phi into p (if not NULL) and G a into ax, ay, az. *totalPotential (host, may be NULL)
      * receives 0.5 G sum(m phi) over the traversed targets. Groups whose traversal overflows the stack are split
-     * and traversed again (ryoanji/src/ryoanji/nbody/traversal_gpu.cu:582-618). */
+     * and traversed again (ryoanji/src/ryoanji/nbody/traversal_gpu.cu:582-618). Every group must hold 1 to 64
+     * targets within [firstBody, lastBody) (RYO_ERR_BAD_ARG otherwise; the call reads the group arrays back to check
+     * them). */
     RYO_API ryo_status ryo_traverse_f32(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const float* xt,
                                         const float* yt, const float* zt, const float* mt, const float* ht,
                                         const float* xs, const float* ys, const float* zs, const float* ms,

@@ -618,6 +618,23 @@ extern "C" ryo_status ryo_traverse_ex_f32(ryo_ctx_t* ctx, const ryo_group_view* 
                                    internalToLeaf && layout && sourceCenter && multipoles && ax && ay && az,
                                "traverse: null argument");
                        REQUIRE(numShells >= 0 && (numShells == 0 || boxL), "traverse: replicas need boxL");
+                       // the groups are the caller's: each must hold 1 to 64 targets inside [firstBody, lastBody). A
+                       // warp evaluates at most 64 targets, and an empty group would read before its start. The
+                       // reference refuses unsupported group sizes too (cstone/traversal/groups_gpu.cu:150).
+                       if (grp->numGroups > 0)
+                       {
+                           REQUIRE(grp->groupStart && grp->groupEnd, "traverse: null group arrays");
+                           std::vector<uint32_t> gs(grp->numGroups), ge(grp->numGroups);
+                           RYO_CUDA(cudaMemcpyAsync(gs.data(), grp->groupStart, gs.size() * sizeof(uint32_t),
+                                                    cudaMemcpyDeviceToHost, stream));
+                           RYO_CUDA(cudaMemcpyAsync(ge.data(), grp->groupEnd, ge.size() * sizeof(uint32_t),
+                                                    cudaMemcpyDeviceToHost, stream));
+                           RYO_CUDA(cudaStreamSynchronize(stream));
+                           for (size_t g = 0; g < gs.size(); ++g)
+                               REQUIRE(gs[g] >= grp->firstBody && ge[g] <= grp->lastBody && ge[g] > gs[g] &&
+                                           ge[g] - gs[g] <= 64,
+                                       "traverse: every group needs 1 to 64 targets within [firstBody, lastBody)");
+                       }
                        TraverseLaunch t{};
                        t.groupStart     = grp->groupStart;
                        t.groupEnd       = grp->groupEnd;
