@@ -272,7 +272,8 @@ extern "C"
     /* ------------------------------------------------------------------------------------------ direct sums */
 
     /* ryoanji::directSum (ryoanji/src/ryoanji/nbody/direct.cuh:87-107): all-pairs sum for targets [first, last)
-     * over numBodies sources with (2 numShells + 1)^3 replicas; adds m phi to p and a to ax, ay, az (no G). */
+     * over numBodies sources with (2 numShells + 1)^3 replicas; adds m phi to p and a to ax, ay, az (no G).
+     * first <= last <= numBodies, and replicas need boxL (RYO_ERR_BAD_ARG otherwise). */
     RYO_API ryo_status ryo_direct_sum_f32(size_t first, size_t last, size_t numBodies, const float* boxL,
                                           int numShells, const float* x, const float* y, const float* z,
                                           const float* m, const float* h, float* p, float* ax, float* ay, float* az,
@@ -282,7 +283,8 @@ extern "C"
                                           const double* m, const double* h, double* p, double* ax, double* ay,
                                           double* az, ryo_stream_t stream);
     /* accuracy reference: double-precision direct sum for selected targets of float data, exact 1/sqrt
-     * (the P2P<true> form, ryoanji/src/ryoanji/nbody/kernel.hpp:55-120); writes G m phi and G a per target */
+     * (the P2P<true> form, ryoanji/src/ryoanji/nbody/kernel.hpp:55-120); writes G m phi and G a per target. Every
+     * target index must be a body (the call reads the indices back to check them; RYO_ERR_BAD_ARG otherwise). */
     RYO_API ryo_status ryo_direct_targets_f64(const int64_t* targets, size_t numTargets, const float* x,
                                               const float* y, const float* z, const float* m, const float* h,
                                               size_t numBodies, double G, const double* boxL, int numShells,

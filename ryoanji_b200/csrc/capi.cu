@@ -738,8 +738,15 @@ extern "C" ryo_status ryo_direct_sum_f32(size_t first, size_t last, size_t numBo
                                          ryo_stream_t stream)
 {
     return guarded(tlsError,
-                   [&] { launchDirect<float>(first, last, numBodies, boxL, numShells, x, y, z, m, h, p, ax, ay, az,
-                                             stream); });
+                   [&]
+                   {
+                       REQUIRE(first <= last && last <= numBodies, "direct_sum: targets must be within the bodies");
+                       REQUIRE(numShells >= 0 && (numShells == 0 || boxL), "direct_sum: replicas need boxL");
+                       REQUIRE(last == first || (x && y && z && m && h && ax && ay && az),
+                               "direct_sum: null argument");
+                       launchDirect<float>(first, last, numBodies, boxL, numShells, x, y, z, m, h, p, ax, ay, az,
+                                         stream);
+                   });
 }
 
 extern "C" ryo_status ryo_direct_sum_f64(size_t first, size_t last, size_t numBodies, const double* boxL,
@@ -748,8 +755,15 @@ extern "C" ryo_status ryo_direct_sum_f64(size_t first, size_t last, size_t numBo
                                          double* az, ryo_stream_t stream)
 {
     return guarded(tlsError,
-                   [&] { launchDirect<double>(first, last, numBodies, boxL, numShells, x, y, z, m, h, p, ax, ay, az,
-                                              stream); });
+                   [&]
+                   {
+                       REQUIRE(first <= last && last <= numBodies, "direct_sum: targets must be within the bodies");
+                       REQUIRE(numShells >= 0 && (numShells == 0 || boxL), "direct_sum: replicas need boxL");
+                       REQUIRE(last == first || (x && y && z && m && h && ax && ay && az),
+                               "direct_sum: null argument");
+                       launchDirect<double>(first, last, numBodies, boxL, numShells, x, y, z, m, h, p, ax, ay, az,
+                                         stream);
+                   });
 }
 
 extern "C" ryo_status ryo_direct_targets_f64(const int64_t* targets, size_t numTargets, const float* x, const float* y,
@@ -760,6 +774,17 @@ extern "C" ryo_status ryo_direct_targets_f64(const int64_t* targets, size_t numT
     return guarded(tlsError,
                    [&]
                    {
+                       REQUIRE(numShells >= 0 && (numShells == 0 || boxL), "direct_targets: replicas need boxL");
+                       if (numTargets == 0) return;
+                       REQUIRE(targets && x && y && z && m && h && pot && ax && ay && az,
+                               "direct_targets: null argument");
+                       // every target must index a body: the kernel reads its position
+                       std::vector<int64_t> t(numTargets);
+                       RYO_CUDA(cudaMemcpyAsync(t.data(), targets, numTargets * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                                stream));
+                       RYO_CUDA(cudaStreamSynchronize(stream));
+                       for (int64_t i : t)
+                           REQUIRE(i >= 0 && uint64_t(i) < numBodies, "direct_targets: a target index is not a body");
                        launchDirectTargets(targets, numTargets, x, y, z, m, h, numBodies, G, boxL, numShells, pot, ax,
                                            ay, az, stream);
                    });

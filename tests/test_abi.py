@@ -60,6 +60,18 @@ def test_bad_arguments_return_status_not_crash():
     assert ryo.lib.ryo_traverse_f32(*args) == 2
 
 
+def test_direct_sums_check_ranges_before_any_launch():
+    """targets past the body count, replicas without a box and negative shells are refused on the host"""
+    import ryoanji_b200 as ryo
+    fake = C.c_void_p(16)  # never dereferenced: the checks come first
+    arrays = [fake] * 9
+    assert ryo.lib.ryo_direct_sum_f32(0, 10, 5, None, 0, *arrays, None) == 2
+    assert ryo.lib.ryo_direct_sum_f32(0, 5, 5, None, 1, *arrays, None) == 2
+    assert ryo.lib.ryo_direct_sum_f64(6, 5, 10, None, 0, *arrays, None) == 2
+    assert ryo.lib.ryo_direct_targets_f64(fake, 4, *[fake] * 5, 10, 1.0, None, -1, *[fake] * 4, None) == 2
+    assert b"replicas" in ryo.lib.ryo_ctx_last_error(None)
+
+
 def test_sort_rejects_counts_beyond_32_bits():
     """the sort's digit offsets are 32-bit: 2^32 keys are refused before any pointer is used or kernel launched"""
     import ryoanji_b200 as ryo
