@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--log2n", type=int, default=26)
     ap.add_argument("--theta", type=float, default=0.5)
     ap.add_argument("--accuracy-targets", type=int, default=16384)
-    ap.add_argument("--cpu-log2n", type=int, default=21, help="CPU baseline sample size")
+    ap.add_argument("--cpu-log2n", type=int, default=22, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--served-requests", type=int, default=48)
     ap.add_argument("--served-rate", type=float, default=24.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--no-accuracy-matched", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision-study leg (halos, periodic box)")
     ap.add_argument("--precision", action="store_true",
                     help="run the precision study (clustered halos and periodic box at theta 0.3/0.5/0.7) instead")
     return ap.parse_args()
@@ -139,13 +140,14 @@ class ClockSampler:
 
 # ------------------------------------------------------------------------------------------------------ arms
 
-def cpu_reference_solve(log2n: int, theta: float, seed: int = 0):
-    """the reference's CPU path (oracle/_ref) or, where it could not be built, the restated oracle"""
+def cpu_reference_solve(log2n: int, theta: float, seed: int = 0, library: str | None = None):
+    """one solve of the reference's CPU path (oracle/_ref; @p library picks one of its builds) or, where it could not
+    be built, the restated oracle; returns (kind, seconds, phase seconds)"""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import Oracle, have_reference
     from ryoanji_b200 import datasets as ds
     kind = "reference" if have_reference() else "port"
-    orc = Oracle(reference=(kind == "reference"))
+    orc = Oracle(reference=(kind == "reference"), library=library)
     p = ds.uniform_cube(1 << log2n, seed=seed)
     t0 = time.perf_counter()
     u, *_ , sec = orc.solve(p.x, p.y, p.z, p.m, p.h, [-1, 1, -1, 1, -1, 1], bucket=64, theta=theta, G=1.0)
@@ -153,15 +155,31 @@ def cpu_reference_solve(log2n: int, theta: float, seed: int = 0):
     return kind, dt, sec
 
 
+def fastest_cpu_build(theta: float, log2n: int = 20):
+    """the fastest build of the reference's CPU path on this host (one untimed solve of 2^log2n bodies each): the
+    -O3 -fopenmp builds for the host's vector ISAs and the parity build. Returns (library, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import have_reference, timing_builds, cpu_model
+    if not have_reference():
+        return None, f"restated oracle, g++ -O3 -fopenmp; {cpu_model()}"
+    best = None
+    for path, flags in timing_builds():
+        _, dt, _ = cpu_reference_solve(log2n, theta, seed=1, library=path)
+        if best is None or dt < best[0]:
+            best = (dt, path, flags)
+    return best[1], f"{best[2]} (fastest of {len(timing_builds())} builds on this host); {cpu_model()}"
+
+
 def run_reference_arm(args, rank):
     if rank != 0:
         return
+    library, build = fastest_cpu_build(args.theta, min(20, args.cpu_log2n))
     for _ in range(args.warmup):
-        cpu_reference_solve(args.cpu_log2n, args.theta, seed=1)
+        cpu_reference_solve(args.cpu_log2n, args.theta, seed=1, library=library)
     times = []
     kind = "port"
     for i in range(args.steps):
-        kind, dt, _ = cpu_reference_solve(args.cpu_log2n, args.theta, seed=2 + i)
+        kind, dt, _ = cpu_reference_solve(args.cpu_log2n, args.theta, seed=2 + i, library=library)
         times.append(dt)
     n = 1 << args.cpu_log2n
     value = n * len(times) / sum(times) / 1e6
@@ -172,13 +190,74 @@ def run_reference_arm(args, rank):
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args, args.gpus),
-        "cpu_baseline": {"value": value, "unit": "Mparticles/s", "cores": cores, "kind": kind,
+        "cpu_baseline": {"value": value, "unit": "Mparticles/s", "cores": cores, "kind": kind, "build": build,
                          "sample": f"each step: one full CPU solve (keys, sort, computeOctree, links, upsweep, "
                                    f"computeGravity) of N=2^{args.cpu_log2n} bodies of the same uniform-cube "
                                    f"distribution, OpenMP on {cores} threads"},
         "e2e": {"value": value, "unit": "Mparticles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    gpu = reference_gpu_plain(args)
+    if gpu is not None:
+        line["reference_gpu"] = gpu
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_plain(args) -> dict | None:
+    """the reference's own plain GPU path on this box's GPU (oracle/_ref/libryo_ref_gpu.so, compiled from the
+    reference sources for sm_100a): TreeBuilder, the demo's upsweep, computeFixedGroups(64) and traverse
+    (ryoanji/test/demo.cu:82-104, :171-190), on the uniform cube at 2^24 and 2^26 with h = 1e-6; device time per solve
+    with CUDA events, inputs restored before every solve. None when no GPU or no such library is present."""
+    import ctypes as C
+    path = os.path.join(ROOT, "oracle", "_ref", "libryo_ref_gpu.so")
+    try:
+        import torch
+        if not (os.path.exists(path) and torch.cuda.is_available()):
+            return None
+    except ImportError:
+        return None
+    lib = C.CDLL(path)
+    lib.ref_gpu_solve_f32.restype = C.c_double
+    lib.ref_gpu_solve_f32.argtypes = ([C.c_uint, C.c_float] + [C.c_void_p] * 5 + [C.c_size_t, C.c_void_p, C.c_float]
+                                      + [C.c_void_p] * 6)
+    dev = torch.device("cuda", 0)
+    box = np.array([-1, 1, -1, 1, -1, 1], np.float32)
+    out = {"workload": f"uniform cube in [-1,1]^3, masses 1/N, h=1e-6, theta={args.theta}, bucket 64, groups 64; "
+                       "one build + upsweep + traverse per solve, on the GPU of this box"}
+    for log2n in (24, 26):
+        n = 1 << log2n
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(1234)
+        pristine = [torch.rand(n, device=dev, generator=gen) * 2 - 1 for _ in range(3)]
+        m, h = torch.full((n,), 1.0 / n, device=dev), torch.full((n,), 1e-6, device=dev)
+        work = [t.clone() for t in pristine]
+        acc = [torch.zeros(n, device=dev) for _ in range(4)]
+        stats = (C.c_uint64 * 5)()
+        ms3 = (C.c_float * 3)()
+        ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        times, parts = [], []
+        for i in range(args.warmup + max(2, min(args.steps, 4))):
+            for w, p in zip(work, pristine):
+                w.copy_(p)
+            for a in acc:
+                a.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            lib.ref_gpu_solve_f32(64, C.c_float(args.theta), *[ptr(t) for t in work], ptr(m), ptr(h), n,
+                                  box.ctypes.data_as(C.c_void_p), C.c_float(1.0), *[ptr(a) for a in acc], stats, ms3)
+            e1.record()
+            e1.synchronize()
+            if i >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+                parts.append(list(ms3))
+        ms = float(np.mean(times))
+        out[f"2^{log2n}"] = {"ms_per_solve": ms, "mparticles_per_s": n / (ms * 1e-3) / 1e6,
+                             "phase_ms": dict(zip(("build", "upsweep", "groups_traverse"),
+                                                  np.mean(parts, axis=0).round(3).tolist())),
+                             "p2p_per_body": stats[0] / n, "m2p_per_body": stats[2] / n}
+        del pristine, work, acc, m, h
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -325,19 +404,69 @@ def run_ours(args, rank, world, local_rank):
         line["served"] = run_served(args, ctx, dev, rank, world, dist)
     if world == 1 and not args.no_plummer:
         line["plummer_2e24"] = run_plummer(args, ctx, dev)
+    if world == 1 and not args.no_precision:
+        line["precision"] = run_precision(args, ctx, dev)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        kind, dt, sec = cpu_reference_solve(args.cpu_log2n, args.theta, seed=3)
+        library, build = fastest_cpu_build(args.theta, min(20, args.cpu_log2n))
+        kind, dt, sec = cpu_reference_solve(args.cpu_log2n, args.theta, seed=3, library=library)
         line["cpu_baseline"] = {"value": (1 << args.cpu_log2n) / dt / 1e6, "unit": "Mparticles/s",
-                                "cores": os.cpu_count(), "kind": kind,
+                                "cores": os.cpu_count(), "kind": kind, "build": build,
                                 "sample": f"one solve of N=2^{args.cpu_log2n} uniform cube (bounded sample), "
                                           f"OpenMP on {os.cpu_count()} threads; build/upsweep/gravity s = "
                                           f"{[round(float(s), 3) for s in sec]}"}
+    if "accuracy" in line:
+        acc = line["accuracy"]
+        line["config"]["workload"] += (f"; measured 1st-pct acc err {acc['err_p99_1st_pct']:.2e} (max "
+                                       f"{acc['err_max']:.2e}) vs FP64 direct on {acc['targets']} targets")
+    # the compact summary goes last: it lands in the tail of the output that the driver keeps
+    line["summary"] = summarize(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _r(v, digits=4):
+    """round a float to a few significant digits for the summary"""
+    if isinstance(v, float):
+        return float(f"{v:.{digits}g}")
+    if isinstance(v, dict):
+        return {k: _r(x, digits) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [_r(x, digits) for x in v]
+    return v
+
+
+def summarize(line: dict) -> dict:
+    """the figures of every leg in a few hundred characters, rounded"""
+    s = {"mps": line["value"], "e2e_mps": line.get("e2e", {}).get("value"),
+         "trav_frac_fp32": line["roofline"]["frac"], "build_hbm_frac": line["build_hbm"]["gbs"]
+         / line["build_hbm"]["peak_gbs"] if line["build_hbm"].get("peak_gbs") else None,
+         "phase_ms": line["phase_ms"],
+         "per_body": [line["interactions"]["p2p_per_body"], line["interactions"]["m2p_per_body"]]}
+    if "accuracy" in line:
+        a = line["accuracy"]
+        s["acc_theta_0.5"] = {"p99": a["err_p99_1st_pct"], "max": a["err_max"]}
+    if "accuracy_matched" in line:
+        a = line["accuracy_matched"]
+        s["acc_matched"] = {k: a.get(k) for k in ("theta", "mparticles_per_s", "err_p99_1st_pct")}
+    if "ensemble" in line:
+        e = line["ensemble"]
+        s["ensemble"] = {"batched_sps": e.get("batched", {}).get("solves_per_s"),
+                         "plain_sps": e.get("plain_loop", {}).get("solves_per_s"), "x": e.get("speedup_solves_per_s")}
+    if "served" in line:
+        v = line["served"]
+        s["served"] = {"x": v.get("speedup_solves_per_s"),
+                       **{f"{arm}_{k}": v.get(arm, {}).get(k) for arm in ("served", "plain")
+                          for k in ("solves_per_s", "latency_p50_s", "latency_p99_s")}}
+    if "plummer_2e24" in line:
+        p = line["plummer_2e24"]["fixed_groups"]
+        s["plummer_2e24"] = {"mps": p["mparticles_per_s"], "p99": p["err_p99_1st_pct"], "max": p["err_max"]}
+    if "precision" in line:
+        s["precision"] = line["precision"].get("summary")
+    return _r(s)
 
 
 # ------------------------------------------------------------------------------------------------------ legs
@@ -414,7 +543,8 @@ def run_ensemble(args, ctx, dev, rank=0, world=1, max_over_ranks=lambda v: v) ->
                         + (f"; LPT shares over {world} GPUs, times = max over ranks" if world > 1 else ""),
             "autotuned": {"bucket": tuned.bucket_size, "group": tuned.group_size, "stack": tuned.stack_capacity,
                           "group_tolerance": tuned.group_tolerance,
-                          "candidates_ms (bucket, group, stack, group tolerance, ms)": [list(t) for t in table]},
+                          "best_candidates_ms (bucket, group, stack, group tolerance, ms)":
+                              [list(t) for t in sorted(table, key=lambda t: t[-1])[:3]], "candidates": len(table)},
             "batched": {"ms_per_step": batched_ms, "solves_per_s": ns / (batched_ms * 1e-3),
                         "mparticles_per_s": n / (batched_ms * 1e-3) / 1e6, "steps": steps},
             "plain_loop": {"ms_per_step": plain_ms, "solves_per_s": ns / (plain_ms * 1e-3),
@@ -624,16 +754,17 @@ def run_accuracy_matched(args, ctx, dev, work, out, pristine, n) -> dict:
     return {"theta": None, "note": "no theta in the list met 5e-4"}
 
 
-def run_precision(args) -> dict:
+def run_precision(args, ctx=None, dev=None) -> dict:
     """precision study: 64 Hernquist halos (N = 2^24) against FP64 direct sums on 16384 targets, and a periodic unit
     box (N = 2^22, Ewald defaults, one replica shell) against the FP64 particle-level Ewald sum on 1024 targets, at
     theta 0.3, 0.5 and 0.7; reports the 1st-percentile and maximum relative acceleration error and the relative error
-    of the targets' summed potential"""
+    of the targets' summed potential. The net accelerations of a uniform periodic box are near zero, so its errors
+    are also given normalised by the rms |a| of the reference (err_rms_norm_*)."""
     import torch
     import ryoanji_b200 as ryo
     from ryoanji_b200 import datasets as ds
-    dev = torch.device("cuda", 0)
-    ctx = ryo.Context(0)
+    dev = dev or torch.device("cuda", 0)
+    ctx = ctx or ryo.Context(0)
     out = {}
 
     def errors(ax, ay, az, pot, tgt, ref, periodic):
@@ -643,6 +774,11 @@ def run_precision(args) -> dict:
         err = (torch.linalg.norm(a - r, dim=1) / torch.linalg.norm(r, dim=1)).cpu().numpy()
         out = {"err_p99_1st_pct": float(np.percentile(err, 99)), "err_max": float(err.max()),
                "err_median": float(np.median(err))}
+        if periodic:
+            rms = float(torch.sqrt((r * r).sum(1).mean()))
+            dn = (torch.linalg.norm(a - r, dim=1) / rms).cpu().numpy()
+            out["err_rms_norm_p99"] = float(np.percentile(dn, 99))
+            out["err_rms_norm_max"] = float(dn.max())
         pt = pot[tgt].double()
         if periodic:
             # periodic potentials are defined up to a constant, and the two Ewald forms place it differently
@@ -686,8 +822,13 @@ def run_precision(args) -> dict:
         res["reference"] = ("FP64 particle-level Ewald sum (replica shells + every source's monopole correction)"
                             if L else "FP64 direct sum") + f" on {nt} targets, {ref_s:.1f} s"
         out[name] = res
+    summ = {}
+    for name, res in out.items():
+        key = "err_rms_norm_p99" if "periodic" in name else "err_p99_1st_pct"
+        summ[name.split("_")[0]] = {t.split("_")[1]: res[t][key] for t in res if t.startswith("theta_")}
     return {"precision_study": out, "dtype": "f32 bulk, FP64 upsweep/Ewald k-space/potential",
-            "data": "synthetic, seeded"}
+            "data": "synthetic, seeded",
+            "summary": {"note": "hernquist: 1st-pct rel err; periodic: p99 err / rms|a|", **summ}}
 
 
 def _measured_hbm(peaks):

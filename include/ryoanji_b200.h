@@ -135,7 +135,9 @@ extern "C"
      * reference. Its scratch is one fixed device array per device, so it takes no tmp argument and allocates
      * nothing; n is at most RYO_SORT_STATIC_MAX_KEYS, a larger n returns RYO_ERR_CAPACITY and sorts nothing.
      * The first call on a device looks up that array's address (which may load the module): make it before any
-     * stream capture. Calls on one device share the array: calls that overlap in time race, so serialise them. */
+     * stream capture. A cudaDeviceReset ends the context that held the array; the next call on that device finds it
+     * again in the new context (and is then a first call). Calls on one device share the array: calls that overlap
+     * in time race, so serialise them. */
 #define RYO_SORT_STATIC_MAX_KEYS (1u << 24)
     RYO_API ryo_status ryo_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf,
                                               uint32_t* valueBuf, ryo_stream_t stream);
@@ -349,8 +351,12 @@ extern "C"
         float G;                     /* gravitational constant (1) */
         int useBox;                  /* 1: use @p box; 0: bounding box of the data (open boundaries) */
         ryo_box_f32 box;             /* coordinate box; periodic boundary on all axes enables replicas + Ewald */
-        int numShells;               /* periodic replica shells when periodic (1) */
-        ryo_ewald_settings ewald;    /* Ewald settings when periodic */
+        int numShells;               /* periodic replica shells of the traversal when periodic, in [0, 4] (1) */
+        ryo_ewald_settings ewald;    /* Ewald settings when periodic. As in the reference (the traverse and
+                                        computeGravityEwaldGpu calls of MultipoleHolder take them separately),
+                                        ewald.numReplicaShells, the shells the correction assumes the tree has
+                                        summed, is not tied to numShells; a consistent periodic solve sets both to
+                                        the same value. */
         int stackCapacity;           /* 0 = default */
         int timing;                  /* 1: record per-phase device times into ryo_solve_stats.ms */
         float groupTolerance;        /* > 0: spatial target groups (ryo_compute_group_splits_f32) with this
@@ -481,7 +487,9 @@ extern "C"
     RYO_API void ryo_engine_destroy(ryo_engine_t* engine);
     RYO_API const char* ryo_engine_last_error(const ryo_engine_t* engine);
     /* queue a request; RYO_ERR_CAPACITY if it alone exceeds the budget, RYO_ERR_NOT_CUBIC for a periodic box that is
-     * not a cube and RYO_ERR_BAD_ARG for replica shells outside [0, 4] (refused here rather than at a later step) */
+     * not a cube and RYO_ERR_BAD_ARG for replica shells outside [0, 4] or, for a periodic request, Ewald settings
+     * that the single-system solve refuses (refused here rather than at a later step; engine creation accepts any
+     * Ewald settings, which open requests never use) */
     RYO_API ryo_status ryo_engine_submit(ryo_engine_t* engine, const ryo_engine_request* request);
     /* admit, kick-drift, one batched solve of every resident request, kick, retire the finished ones */
     RYO_API ryo_status ryo_engine_step(ryo_engine_t* engine, ryo_engine_step_info* info, ryo_stream_t stream);

@@ -30,6 +30,42 @@ def have_reference() -> bool:
     return os.path.exists(REF_SO)
 
 
+def _cpu_flags() -> set:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def timing_builds() -> list[tuple[str, str]]:
+    """the builds of the reference's CPU path this host can run, with their compiler flags: the -O3 -fopenmp builds
+    for the vector ISAs the host supports (oracle/Makefile target reffast) and the parity build"""
+    flags = _cpu_flags()
+    need = {"v4": {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}, "v3": {"avx2", "fma", "bmi2", "movbe"}}
+    out = []
+    for level in ("v4", "v3"):
+        path = os.path.join(HERE, "_ref", f"libryo_ref_fast_{level}.so")
+        if need[level] <= flags and os.path.exists(path):
+            out.append((path, f"g++ -O3 -march=x86-64-{level} -fopenmp (default FP contraction)"))
+    out.append((REF_SO, "g++ -O3 -fopenmp -ffp-contract=off (x86-64 baseline)"))
+    return out
+
+
 def _ptr(a):
     return a.ctypes.data_as(_p) if a is not None else None
 
@@ -37,8 +73,12 @@ def _ptr(a):
 class Oracle:
     """The CPU path with one Python interface for both the restatement (orc_*) and the reference (ref_*)."""
 
-    def __init__(self, reference: bool = False):
+    def __init__(self, reference: bool = False, library: str | None = None):
+        """library (with reference=True) loads another build of the reference's CPU path (timing_builds) in place of
+        the parity build; its results follow that build's FP contraction and are for timing only"""
         path = REF_SO if reference else ORACLE_SO
+        if reference and library:
+            path = library
         if not os.path.exists(path):
             build(reference)
         self.reference = reference

@@ -1048,7 +1048,13 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     checkBox(box.limits);
     DevBox<float> dbox = boxOf(&box);
     bool periodic      = dbox.periodic;
-    if (periodic) checkEwald(&P->ewald);
+    if (periodic)
+    {
+        checkEwald(&P->ewald);
+        // the traversal's replica shells: a negative count would traverse nothing, and every further shell costs
+        // (2 n + 1)^3 traversals (the batched solve and the engine refuse the same range)
+        REQUIRE(P->numShells >= 0 && P->numShells <= 4, "solve: numShells must be in [0, 4] for a periodic box");
+    }
 
     // keys and sort
     uint64_t* keys    = ctx->scratch<uint64_t>("solve.keys", n, s);

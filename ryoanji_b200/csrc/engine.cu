@@ -382,12 +382,6 @@ extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params*
     if (!(p->hbmBudgetBytes > 0) || !(p->bytesPerBody > 0) || p->maxSystems < 1 ||
         p->maxSystems > RYO_BATCH_MAX_SYSTEMS)
         return RYO_ERR_BAD_ARG;
-    if (const char* why = ewaldSettingsError(p->solve.ewald))
-    {
-        // periodic requests would fail every step: refuse the settings now
-        ctx->lastError = std::string("engine_create: ") + why;
-        return RYO_ERR_BAD_ARG;
-    }
     ryo_engine* E = nullptr;
     DeviceScope device(ctx->device);
     try
@@ -466,6 +460,12 @@ extern "C" ryo_status ryo_engine_submit(ryo_engine_t* E, const ryo_engine_reques
             if (r->numShells < 0 || r->numShells > 4)
             {
                 E->lastError = "engine_submit: numShells in [0, 4]";
+                return RYO_ERR_BAD_ARG;
+            }
+            // the engine's Ewald settings apply to periodic requests only, as in the single-system solve
+            if (const char* why = ewaldSettingsError(E->solve.ewald))
+            {
+                E->lastError = std::string("engine_submit: ") + why;
                 return RYO_ERR_BAD_ARG;
             }
         }

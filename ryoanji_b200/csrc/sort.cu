@@ -439,22 +439,46 @@ static __device__ __align__(256) unsigned char staticSortScratch[kStaticSortByte
 
 size_t staticSortMaxKeys() { return kStaticSortMaxKeys; }
 
-//! the array's device address on the current device, looked up on the first call for that device
+//! the current CUDA context (the driver's handle), looked up through the runtime so that the library needs no link
+//! to the driver library; null if the driver does not offer the call
+static void* currentContext()
+{
+    using GetCtx = int (*)(void**);
+    static GetCtx fn = []
+    {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<GetCtx>(f);
+    }();
+    void* c = nullptr;
+    if (fn && fn(&c) != 0) c = nullptr;
+    return c;
+}
+
+//! the array's device address on the current device. It is looked up (cudaGetSymbolAddress) on the first call for
+//! that device and again whenever the device's context has changed since: a cudaDeviceReset by the caller ends the
+//! context that held the array, and the next call on that device then finds it in the new one.
 static void* staticSortScratchAddress()
 {
     constexpr int kMaxDevices = 64;
     static std::mutex lock;
     static void* address[kMaxDevices] = {};
+    static void* context[kMaxDevices] = {};
     int dev = 0;
     RYO_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw CudaError{cudaErrorInvalidDevice, "static sort: device ordinal"};
+    void* ctxNow = currentContext();
     std::lock_guard<std::mutex> guard(lock);
-    if (!address[dev])
+    if (!address[dev] || context[dev] != ctxNow)
     {
         void* p = nullptr;
-        RYO_CUDA(cudaGetSymbolAddress(&p, staticSortScratch));
+        RYO_CUDA(cudaGetSymbolAddress(&p, staticSortScratch)); // also makes the device's context current
         if (!p) throw CudaError{cudaErrorInvalidSymbol, "static sort: scratch symbol has no address"};
         address[dev] = p;
+        context[dev] = currentContext();
     }
     return address[dev];
 }

@@ -29,6 +29,7 @@ def _check_line(d, n_gpus):
     assert d["impl"] == "reference" and d["n_gpus"] == n_gpus and d["steps"] == 1 and d["warmup"] == 1
     assert d["value"] > 0 and d["unit"] == "Mparticles/s" and d["higher_is_better"] is True
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+    assert "g++ -O3" in d["cpu_baseline"]["build"]  # the compiler flags and CPU model of the timed build
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert "workload" in d["config"]
 
@@ -60,3 +61,33 @@ def test_reference_arm_two_ranks_only_rank0_prints():
     lines = _json_lines(r.stdout)
     assert len(lines) == 1, r.stdout
     _check_line(lines[0], 2)
+
+
+def test_summary_is_last_and_fits_the_kept_tail():
+    """the driver keeps the last 1500 characters of the output: the summary of every leg goes last and fits there"""
+    sys.path.insert(0, ROOT)
+    import bench
+    leg = {"ms_per_step": 1.2345678, "solves_per_s": 1234.5678, "mparticles_per_s": 123.45678,
+           "latency_p50_s": 1.23456, "latency_p99_s": 2.3456}
+    line = {"value": 265.123456, "e2e": {"value": 244.6789}, "roofline": {"frac": 0.6678901},
+            "build_hbm": {"gbs": 1900.12345, "peak_gbs": 6456.0},
+            "phase_ms": {k: 12.3456789 for k in ("sort", "tree", "upsweep", "traverse", "total")},
+            "interactions": {"p2p_per_body": 3788.123456, "m2p_per_body": 1291.987654},
+            "accuracy": {"err_p99_1st_pct": 7.3456789e-4, "err_max": 1.23456e-2},
+            "accuracy_matched": {"theta": 0.43, "mparticles_per_s": 197.123456, "err_p99_1st_pct": 4.7123e-4},
+            "ensemble": {"batched": leg, "plain_loop": leg, "speedup_solves_per_s": 9.3456},
+            "served": {"served": leg, "plain": leg, "speedup_solves_per_s": 1.3345},
+            "plummer_2e24": {"fixed_groups": {"mparticles_per_s": 161.7123, "err_p99_1st_pct": 4.47e-4,
+                                              "err_max": 1.549e-3}},
+            "precision": {"summary": {"note": "hernquist: 1st-pct rel err; periodic: p99 err / rms|a|",
+                                      "hernquist": {"0.3": 2.1123e-4, "0.5": 1.9123e-3, "0.7": 6.9123e-3},
+                                      "periodic": {"0.3": 1.7123e-3, "0.5": 2.2123e-3, "0.7": 6.4123e-3}}}}
+    line["summary"] = bench.summarize(line)
+    text = json.dumps(line)
+    assert list(line)[-1] == "summary"
+    tail = json.dumps({"summary": line["summary"]})
+    assert len(tail) < 1400, len(tail)
+    assert text.endswith(tail[1:])
+    s = line["summary"]
+    assert s["acc_theta_0.5"]["p99"] == 7.346e-4 and s["acc_matched"]["theta"] == 0.43
+    assert s["ensemble"]["x"] == 9.346 and s["served"]["served_latency_p99_s"] == 2.346

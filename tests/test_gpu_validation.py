@@ -40,11 +40,27 @@ def test_ewald_at_the_limit_still_runs():
 
 
 def test_engine_and_particle_ewald_refuse_them_too():
+    """the engine applies its Ewald settings to periodic requests only, as the single-system solve does: creation
+    and open requests accept them, a periodic submission is refused"""
     import ryoanji_b200 as ryo
     bad = ryo.EwaldSettings(hCut=3.5)
-    with pytest.raises(ryo.RyoError) as e:
-        ryo.Engine(ryo.SolveParams(ewald=bad))
-    assert e.value.status == ryo._abi.ERR_BAD_ARG
+    eng = ryo.Engine(ryo.SolveParams(ewald=bad))
+    try:
+        q = ds.uniform_cube(300, seed=13, eps=0.01)
+        zero = np.zeros(q.n, np.float32)
+        eng.submit(1, *(torch.from_numpy(a) for a in (q.x, q.y, q.z, q.m, q.h, zero, zero, zero)), steps=1,
+                   dt=1e-3)
+        pb = ds.periodic_box(300, seed=14, eps=0.01)
+        box = ryo.Box(*pb.box, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
+        with pytest.raises(ryo.RyoError) as e:
+            eng.submit(2, *(torch.from_numpy(a) for a in (pb.x, pb.y, pb.z, pb.m, pb.h, zero, zero, zero)),
+                       box=box, steps=1, dt=1e-3)
+        assert e.value.status == ryo._abi.ERR_BAD_ARG and "ewald" in str(e.value).lower()
+        while eng.status()["queued"] or eng.status()["resident"]:
+            eng.step()
+        assert [d["tag"] for d in eng.poll()] == [1]
+    finally:
+        eng.close()
     p = ds.periodic_box(500, seed=12, eps=0.01)
     dev = [torch.from_numpy(a).cuda() for a in (p.x, p.y, p.z, p.m, p.h)]
     targets = torch.arange(0, 500, 50, dtype=torch.int64, device="cuda")
@@ -52,3 +68,69 @@ def test_engine_and_particle_ewald_refuse_them_too():
         ryo.ewald_targets_f64(targets, *dev, L=1.0, ewald=bad)
     assert e.value.status == ryo._abi.ERR_BAD_ARG
     np.testing.assert_equal(p.n, 500)
+
+
+@pytest.mark.parametrize("shells", [-1, 5])
+def test_solve_refuses_replica_shells_outside_0_4(shells):
+    """a negative count would traverse nothing and return zero forces; the batched solve and the engine refuse the
+    same range"""
+    import ryoanji_b200 as ryo
+    p = ds.periodic_box(1000, seed=15, eps=0.01)
+    box = ryo.Box(*p.box, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
+    with pytest.raises(ryo.RyoError) as e:
+        ryo.solve(*_arrays(p), params=ryo.SolveParams(box=box, num_shells=shells))
+    assert e.value.status == ryo._abi.ERR_BAD_ARG and "numShells" in str(e.value)
+
+
+def _tiny_tree():
+    import ryoanji_b200 as ryo
+    p = ds.uniform_cube(512, seed=16, eps=0.01)
+    x, y, z, m, h = (torch.from_numpy(a).cuda() for a in (p.x, p.y, p.z, p.m, p.h))
+    tb = ryo.TreeBuilder(16)
+    box = ryo.Box(-1.0, 1.0, -1.0, 1.0, -1.0, 1.0)
+    nn = tb.update(x, y, z, box)
+    centers = torch.zeros(nn, 4, device="cuda")
+    mp = torch.zeros(nn, 8, device="cuda")
+    return tb, box, (x, y, z, m, h), centers, mp
+
+
+@pytest.mark.parametrize("kind", ["empty", "over_64", "before_first", "past_last"])
+def test_traverse_refuses_bad_caller_groups(kind):
+    """every caller group must hold 1 to 64 targets inside [firstBody, lastBody)"""
+    import ryoanji_b200 as ryo
+    tb, box, (x, y, z, m, h), centers, mp = _tiny_tree()
+    g = {"empty": [0, 64, 64, 128], "over_64": [0, 65, 128], "before_first": [0, 64, 128],
+         "past_last": [448, 512, 576]}[kind]
+    groups = torch.tensor(g, dtype=torch.int32, device="cuda")
+    first = 64 if kind == "before_first" else 0
+    last = 512 if kind != "past_last" else 512
+    p, ax, ay, az = (torch.zeros(x.numel(), device="cuda") for _ in range(4))
+    with pytest.raises(ryo.RyoError) as e:
+        ryo.traverse(groups, 1, x, y, z, m, h, x, y, z, m, h, tb.childOffsets(), tb.internalToLeaf(), tb.layout(),
+                     centers, mp, 1.0, 0, None, p, ax, ay, az, first_body=first, last_body=last)
+    assert e.value.status == ryo._abi.ERR_BAD_ARG
+
+
+@pytest.mark.parametrize("bad", [-1, 500])
+def test_direct_targets_refuse_an_index_outside_the_bodies(bad):
+    import ryoanji_b200 as ryo
+    p = ds.uniform_cube(500, seed=17, eps=0.01)
+    dev = [torch.from_numpy(a).cuda() for a in (p.x, p.y, p.z, p.m, p.h)]
+    targets = torch.tensor([0, 7, bad], dtype=torch.int64, device="cuda")
+    with pytest.raises(ryo.RyoError) as e:
+        ryo.direct_targets_f64(targets, *dev)
+    assert e.value.status == ryo._abi.ERR_BAD_ARG
+
+
+def test_bounding_box_is_the_exact_min_and_max():
+    """ryo_compute_bounding_box_f32: exact FP64 minimum and maximum of every axis (no rounding: float inputs)"""
+    import ryoanji_b200 as ryo
+    rng = np.random.default_rng(18)
+    for n in (1, 7, 1000, 1 << 20):
+        xyz = [rng.standard_normal(n).astype(np.float32) * s for s in (1.0, 1e-3, 1e4)]
+        if n > 8:
+            xyz[0][n // 3] = np.float32(-3.5e7)
+            xyz[2][-1] = np.float32(np.nextafter(np.float32(9e5), np.float32(1e9)))
+        b = ryo.compute_bounding_box(*(torch.from_numpy(a).cuda() for a in xyz))
+        want = [v for a in xyz for v in (float(a.min()), float(a.max()))]
+        assert list(b) == want, (n, list(b), want)
