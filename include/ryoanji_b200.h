@@ -197,7 +197,6 @@ extern "C"
     /* ryoanji::upsweepMultipoles (upsweep_gpu.h:33-41): M2M for cells [firstCell, lastCell) */
     RYO_API ryo_status ryo_upsweep_multipoles_f32(int firstCell, int lastCell, const int* childOffsets,
                                                   const float* centers, float* multipoles, ryo_stream_t stream);
-    /* cstone::setMacGpu (source_center_gpu.h:104-116): centers[i][3] = squared vector-MAC radius, 0 if massless */
     /* the same two steps for CartesianMDQpole (INSTANTIATE_MULTIPOLE(CartesianMDQpole), upsweep_gpu.cu:143):
      * 12 floats per node (mass, qxx, qxy, qxz, qyy, qyz, qzz, trace, px, py, pz, 0), FP64 sums */
     RYO_API ryo_status ryo_compute_leaf_multipoles_mdq_f32(const float* x, const float* y, const float* z,
@@ -207,6 +206,50 @@ extern "C"
     RYO_API ryo_status ryo_upsweep_multipoles_mdq_f32(int firstCell, int lastCell, const int* childOffsets,
                                                       const float* centers, float* multipoles, ryo_stream_t stream);
 
+    /* The steps above for the reference's other two type sets (COMPUTE_LEAF_SOURCE_CENTER_GPU,
+     * source_center_gpu.cu:164-170; upsweepCentersGpu, :204-209; INSTANTIATE_MULTIPOLE, upsweep_gpu.cu:134-143;
+     * SET_MAC_GPU, source_center_gpu.cu:312-319): _f64 takes double coordinates, masses, centres (4 doubles per
+     * node) and multipoles (8 or 12 doubles per node); _mixed takes double coordinates and centres with float masses
+     * and multipoles. The sums run in double as in _f32; stored values are rounded once to their type. */
+    RYO_API ryo_status ryo_compute_leaf_source_center_f64(const double* x, const double* y, const double* z,
+                                                          const double* m, const int* leafToInternal, int numLeaves,
+                                                          const uint32_t* layout, double* centers,
+                                                          ryo_stream_t stream);
+    RYO_API ryo_status ryo_compute_leaf_source_center_mixed(const double* x, const double* y, const double* z,
+                                                            const float* m, const int* leafToInternal, int numLeaves,
+                                                            const uint32_t* layout, double* centers,
+                                                            ryo_stream_t stream);
+    RYO_API ryo_status ryo_upsweep_centers_f64(int numLevels, const int* levelRange, const int* childOffsets,
+                                               double* centers, ryo_stream_t stream);
+    RYO_API ryo_status ryo_compute_leaf_multipoles_f64(const double* x, const double* y, const double* z,
+                                                       const double* m, const int* leafToInternal, int numLeaves,
+                                                       const uint32_t* layout, const double* centers,
+                                                       double* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_compute_leaf_multipoles_mixed(const double* x, const double* y, const double* z,
+                                                         const float* m, const int* leafToInternal, int numLeaves,
+                                                         const uint32_t* layout, const double* centers,
+                                                         float* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_compute_leaf_multipoles_mdq_f64(const double* x, const double* y, const double* z,
+                                                           const double* m, const int* leafToInternal, int numLeaves,
+                                                           const uint32_t* layout, const double* centers,
+                                                           double* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_compute_leaf_multipoles_mdq_mixed(const double* x, const double* y, const double* z,
+                                                             const float* m, const int* leafToInternal, int numLeaves,
+                                                             const uint32_t* layout, const double* centers,
+                                                             float* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_upsweep_multipoles_f64(int firstCell, int lastCell, const int* childOffsets,
+                                                  const double* centers, double* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_upsweep_multipoles_mixed(int firstCell, int lastCell, const int* childOffsets,
+                                                    const double* centers, float* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_upsweep_multipoles_mdq_f64(int firstCell, int lastCell, const int* childOffsets,
+                                                      const double* centers, double* multipoles, ryo_stream_t stream);
+    RYO_API ryo_status ryo_upsweep_multipoles_mdq_mixed(int firstCell, int lastCell, const int* childOffsets,
+                                                        const double* centers, float* multipoles,
+                                                        ryo_stream_t stream);
+    RYO_API ryo_status ryo_set_mac_f64(const uint64_t* prefixes, int numNodes, double* centers, float invTheta,
+                                       const ryo_box_f64* box, ryo_stream_t stream);
+
+    /* cstone::setMacGpu (source_center_gpu.h:104-116): centers[i][3] = squared vector-MAC radius, 0 if massless */
     RYO_API ryo_status ryo_set_mac_f32(const uint64_t* prefixes, int numNodes, float* centers, float invTheta,
                                        const ryo_box_f32* box, ryo_stream_t stream);
 
@@ -253,6 +296,30 @@ extern "C"
                                            const float* boxL, float* p, float* ax, float* ay, float* az,
                                            double* totalPotential, const ryo_traverse_options* options,
                                            ryo_stream_t stream);
+
+    /* ryoanji::traverse, the two double-coordinate instantiations (TRAVERSE_MPOLE, traversal_gpu.cu:635-641): _f64
+     * is (double, double, double, double, double, multipoles of doubles); _mixed is (Tc = double, Th = Tm = Ta =
+     * float, Tf = double, multipoles of floats), the caller side of codes whose particle positions are double. As in
+     * the reference, the MAC and the sums run in double with the single-precision rsqrt of the double argument
+     * (kernel.hpp:38-52). Centres are 4 doubles per node; multipoles 8 values per node, or 12 with options->multipole
+     * = RYO_MULTIPOLE_MDQ. Semantics, checks and statistics are those of ryo_traverse_ex_f32 (options may be NULL).
+     * A group too costly for one warp is evaluated by one warp here (no split second pass). */
+    RYO_API ryo_status ryo_traverse_f64(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const double* xt,
+                                        const double* yt, const double* zt, const double* mt, const double* ht,
+                                        const double* xs, const double* ys, const double* zs, const double* ms,
+                                        const double* hs, const int* childOffsets, const int* internalToLeaf,
+                                        const uint32_t* layout, const double* sourceCenter, const double* multipoles,
+                                        double G, int numShells, const double* boxL, double* p, double* ax,
+                                        double* ay, double* az, double* totalPotential,
+                                        const ryo_traverse_options* options, ryo_stream_t stream);
+    RYO_API ryo_status ryo_traverse_mixed(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const double* xt,
+                                          const double* yt, const double* zt, const float* mt, const float* ht,
+                                          const double* xs, const double* ys, const double* zs, const float* ms,
+                                          const float* hs, const int* childOffsets, const int* internalToLeaf,
+                                          const uint32_t* layout, const double* sourceCenter,
+                                          const float* multipoles, double G, int numShells, const double* boxL,
+                                          float* p, float* ax, float* ay, float* az, double* totalPotential,
+                                          const ryo_traverse_options* options, ryo_stream_t stream);
 
     /* ryoanji::readBhStats (traversal_gpu.h:64-65): {sumP2P, maxP2P, sumM2P, maxM2P, maxStack} of the last
      * traversal on this context; maxP2P is 0xFFFFFFFF if a single target could not be traversed */

@@ -47,9 +47,9 @@ cstone::Box<T> makeBox(const T* b6)
     return cstone::Box<T>(b6[0], b6[1], b6[2], b6[3], b6[4], b6[5]);
 }
 
-//! the demo's upsweep (ryoanji/test/demo.cu:205-226) for coordinate type T and multipole MType
-template<class T, class MType>
-void upsweepFlow(RefTree& r, const T* x, const T* y, const T* z, const T* m, const cstone::Box<T>& box, float theta,
+//! the demo's upsweep (ryoanji/test/demo.cu:205-226) for coordinate type T, mass type Tm and multipole MType
+template<class T, class Tm, class MType>
+void upsweepFlow(RefTree& r, const T* x, const T* y, const T* z, const Tm* m, const cstone::Box<T>& box, float theta,
                  ryoanji::Vec4<T>* centers, MType* multipoles)
 {
     const Builder& tb = r.tb;
@@ -168,6 +168,20 @@ extern "C"
         else
             upsweepFlow(r, x, y, z, m, box, theta, c,
                         reinterpret_cast<ryoanji::CartesianQuadrupole<double>*>(multipoles));
+    }
+
+    /*! the mixed type set: double coordinates and centres, float masses and multipoles */
+    void ref_gpu_upsweep_mixed(void* h, const double* x, const double* y, const double* z, const float* m,
+                               const double* box6, float theta, double* centers, float* multipoles, int mdq)
+    {
+        auto& r  = *static_cast<RefTree*>(h);
+        auto box = makeBox(box6);
+        auto* c  = reinterpret_cast<ryoanji::Vec4<double>*>(centers);
+        if (mdq)
+            upsweepFlow(r, x, y, z, m, box, theta, c, reinterpret_cast<ryoanji::CartesianMDQpole<float>*>(multipoles));
+        else
+            upsweepFlow(r, x, y, z, m, box, theta, c,
+                        reinterpret_cast<ryoanji::CartesianQuadrupole<float>*>(multipoles));
     }
 
     /*! cstone::computeFixedGroups (cstone/include/cstone/traversal/groups_gpu.cu:45-58): writes the group boundaries

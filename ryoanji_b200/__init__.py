@@ -274,35 +274,56 @@ def compute_group_splits(x, y, z, h, leaves, layout, box: Box, group_size: int =
 
 # ---------------------------------------------------------------------------------------------------- upsweep
 
+def _type_set(x, m) -> str:
+    """the reference's type set of a step from its coordinate and mass dtypes: f32, f64 or mixed (double
+    coordinates, float masses)"""
+    if x.dtype == torch.float32:
+        return "f32"
+    if x.dtype == torch.float64:
+        return "f64" if m is None or m.dtype == torch.float64 else "mixed"
+    raise TypeError("coordinates must be float32 or float64")
+
+
 def compute_leaf_source_center(x, y, z, m, leaf_to_internal, layout, centers, stream=None):
+    """cstone::computeLeafSourceCenterGpu; float32 coordinates give float centres, float64 coordinates double
+    centres (masses float64 or float32)"""
     nl = leaf_to_internal.numel()
-    _check(lib.ryo_compute_leaf_source_center_f32(_ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(leaf_to_internal), nl,
-                                                  _ptr(layout), _ptr(centers), _stream(stream)))
+    fn = getattr(lib, "ryo_compute_leaf_source_center_" + _type_set(x, m))
+    _check(fn(_ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(leaf_to_internal), nl, _ptr(layout), _ptr(centers),
+              _stream(stream)))
 
 
 def upsweep_centers(num_levels: int, level_range, child_offsets, centers, stream=None):
     lr = (C.c_int * (MAX_TREE_LEVEL + 2))(*level_range)
-    _check(lib.ryo_upsweep_centers_f32(num_levels, lr, _ptr(child_offsets), _ptr(centers), _stream(stream)))
+    fn = lib.ryo_upsweep_centers_f64 if centers.dtype == torch.float64 else lib.ryo_upsweep_centers_f32
+    _check(fn(num_levels, lr, _ptr(child_offsets), _ptr(centers), _stream(stream)))
 
 
 def compute_leaf_multipoles(x, y, z, m, leaf_to_internal, layout, centers, multipoles, stream=None, mdq=False):
-    """ryoanji::computeLeafMultipoles: 8 floats per node, or 12 with mdq (CartesianMDQpole)"""
+    """ryoanji::computeLeafMultipoles: 8 values per node, or 12 with mdq (CartesianMDQpole); the type set follows
+    the coordinates and masses (f32, f64, or mixed: double coordinates and centres, float masses and multipoles)"""
     nl = leaf_to_internal.numel()
-    fn = lib.ryo_compute_leaf_multipoles_mdq_f32 if mdq else lib.ryo_compute_leaf_multipoles_f32
+    fn = getattr(lib, "ryo_compute_leaf_multipoles_" + ("mdq_" if mdq else "") + _type_set(x, m))
     _check(fn(_ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(leaf_to_internal), nl, _ptr(layout), _ptr(centers),
               _ptr(multipoles), _stream(stream)))
 
 
 def upsweep_multipoles(first_cell: int, last_cell: int, child_offsets, centers, multipoles, stream=None, mdq=False):
-    """ryoanji::upsweepMultipoles for the cells [first_cell, last_cell) of one level"""
-    fn = lib.ryo_upsweep_multipoles_mdq_f32 if mdq else lib.ryo_upsweep_multipoles_f32
+    """ryoanji::upsweepMultipoles for the cells [first_cell, last_cell) of one level; double centres with double
+    multipoles are the f64 set, double centres with float multipoles the mixed one"""
+    kind = "f32" if centers.dtype == torch.float32 else ("f64" if multipoles.dtype == torch.float64 else "mixed")
+    fn = getattr(lib, "ryo_upsweep_multipoles_" + ("mdq_" if mdq else "") + kind)
     _check(fn(first_cell, last_cell, _ptr(child_offsets), _ptr(centers), _ptr(multipoles), _stream(stream)))
 
 
 def set_mac(prefixes, centers, inv_theta: float, box: Box, stream=None):
-    b = box.f32()
-    _check(lib.ryo_set_mac_f32(_ptr(prefixes), prefixes.numel(), _ptr(centers), C.c_float(inv_theta), C.byref(b),
-                               _stream(stream)))
+    if centers.dtype == torch.float64:
+        b = box.f64()
+        fn = lib.ryo_set_mac_f64
+    else:
+        b = box.f32()
+        fn = lib.ryo_set_mac_f32
+    _check(fn(_ptr(prefixes), prefixes.numel(), _ptr(centers), C.c_float(inv_theta), C.byref(b), _stream(stream)))
 
 
 # ---------------------------------------------------------------------------------------------------- traversal
@@ -320,6 +341,9 @@ def traverse(groups: torch.Tensor, init_node: int, xt, yt, zt, mt, ht, xs, ys, z
              ctx: Context | None = None, stack_capacity: int = 0, group_counts: bool = False, first_body: int = 0,
              last_body: int | None = None, stream=None, mdq: bool = False):
     """ryoanji::traverse: accumulates G m phi into p (may be None) and G a into ax, ay, az.
+
+    The instantiation follows the dtypes (traversal_gpu.cu:635-641): float32 everything; float64 everything; or
+    float64 coordinates and centres with float32 masses, softenings, multipoles and outputs ("mixed").
 
     ``groups`` holds numGroups + 1 boundaries (computeFixedGroups layout). Returns the total potential
     0.5 G sum(m phi) and, with group_counts, the per-group (M2P cells, P2P bodies) counts.
@@ -339,13 +363,15 @@ def traverse(groups: torch.Tensor, init_node: int, xt, yt, zt, mt, ht, xs, ys, z
         opts.groupM2P = C.c_void_p(m2p.data_ptr())
         opts.groupP2P = C.c_void_p(p2p.data_ptr())
     opts.stackCapacity = stack_capacity
-    bl = (C.c_float * 3)(*(list(box_l) if box_l is not None else [0.0, 0.0, 0.0]))
+    kind = _type_set(xt, mt)
+    real = C.c_float if kind == "f32" else C.c_double
+    bl = (real * 3)(*(list(box_l) if box_l is not None else [0.0, 0.0, 0.0]))
     pot = C.c_double(0)
-    _check(lib.ryo_traverse_ex_f32(ctx.handle, C.byref(gv), init_node, _ptr(xt), _ptr(yt), _ptr(zt), _ptr(mt),
-                                   _ptr(ht), _ptr(xs), _ptr(ys), _ptr(zs), _ptr(ms), _ptr(hs), _ptr(child_offsets),
-                                   _ptr(internal_to_leaf), _ptr(layout), _ptr(source_center), _ptr(multipoles),
-                                   C.c_float(G), num_shells, bl, _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), C.byref(pot),
-                                   C.byref(opts), _stream(stream, ctx)), ctx)
+    fn = {"f32": lib.ryo_traverse_ex_f32, "f64": lib.ryo_traverse_f64, "mixed": lib.ryo_traverse_mixed}[kind]
+    _check(fn(ctx.handle, C.byref(gv), init_node, _ptr(xt), _ptr(yt), _ptr(zt), _ptr(mt), _ptr(ht), _ptr(xs),
+              _ptr(ys), _ptr(zs), _ptr(ms), _ptr(hs), _ptr(child_offsets), _ptr(internal_to_leaf), _ptr(layout),
+              _ptr(source_center), _ptr(multipoles), real(G), num_shells, bl, _ptr(p), _ptr(ax), _ptr(ay), _ptr(az),
+              C.byref(pot), C.byref(opts), _stream(stream, ctx)), ctx)
     if group_counts:
         return pot.value, m2p, p2p
     return pot.value

@@ -140,6 +140,18 @@ SIGNATURES = {
     "ryo_compute_leaf_multipoles_mdq_f32": (_i, [_p] * 5 + [_i] + [_p] * 4),
     "ryo_upsweep_multipoles_mdq_f32": (_i, [_i, _i] + [_p] * 4),
     "ryo_set_mac_f32": (_i, [_p, _i, _p, _f, C.POINTER(BoxF32), _p]),
+    "ryo_compute_leaf_source_center_f64": (_i, [_p, _p, _p, _p, _p, _i, _p, _p, _p]),
+    "ryo_compute_leaf_source_center_mixed": (_i, [_p, _p, _p, _p, _p, _i, _p, _p, _p]),
+    "ryo_upsweep_centers_f64": (_i, [_i, C.POINTER(_i), _p, _p, _p]),
+    "ryo_compute_leaf_multipoles_f64": (_i, [_p] * 5 + [_i] + [_p] * 4),
+    "ryo_compute_leaf_multipoles_mixed": (_i, [_p] * 5 + [_i] + [_p] * 4),
+    "ryo_compute_leaf_multipoles_mdq_f64": (_i, [_p] * 5 + [_i] + [_p] * 4),
+    "ryo_compute_leaf_multipoles_mdq_mixed": (_i, [_p] * 5 + [_i] + [_p] * 4),
+    "ryo_upsweep_multipoles_f64": (_i, [_i, _i] + [_p] * 4),
+    "ryo_upsweep_multipoles_mixed": (_i, [_i, _i] + [_p] * 4),
+    "ryo_upsweep_multipoles_mdq_f64": (_i, [_i, _i] + [_p] * 4),
+    "ryo_upsweep_multipoles_mdq_mixed": (_i, [_i, _i] + [_p] * 4),
+    "ryo_set_mac_f64": (_i, [_p, _i, _p, _f, C.POINTER(BoxF64), _p]),
     "ryo_bh_max_target_size": (_i, []),
     "ryo_stack_size": (_u32, [_u32]),
     "ryo_traverse_f32": (_i, [_p, C.POINTER(GroupView), _i] + [_p] * 15 + [_f, _i, C.POINTER(_f), _p, _p, _p, _p,
@@ -147,6 +159,12 @@ SIGNATURES = {
     "ryo_traverse_ex_f32": (_i, [_p, C.POINTER(GroupView), _i] + [_p] * 15 + [_f, _i, C.POINTER(_f), _p, _p, _p, _p,
                                                                                C.POINTER(_d),
                                                                                C.POINTER(TraverseOptions), _p]),
+    "ryo_traverse_f64": (_i, [_p, C.POINTER(GroupView), _i] + [_p] * 15 + [_d, _i, C.POINTER(_d), _p, _p, _p, _p,
+                                                                           C.POINTER(_d), C.POINTER(TraverseOptions),
+                                                                           _p]),
+    "ryo_traverse_mixed": (_i, [_p, C.POINTER(GroupView), _i] + [_p] * 15 + [_d, _i, C.POINTER(_d), _p, _p, _p, _p,
+                                                                             C.POINTER(_d), C.POINTER(TraverseOptions),
+                                                                             _p]),
     "ryo_read_bh_stats": (_i, [_p, C.POINTER(C.c_uint64)]),
     "ryo_read_traversal_retries": (C.c_uint64, [_p]),
     "ryo_compute_gravity_ewald_f32": (_i, [_p, C.POINTER(_f), C.POINTER(_f), C.POINTER(GroupView), _p, _p, _p, _p,

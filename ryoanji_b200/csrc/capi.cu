@@ -375,91 +375,151 @@ extern "C" ryo_status ryo_compute_group_splits_f32(ryo_ctx_t* ctx, uint32_t firs
 }
 
 // ==================================================================================================== upsweep
+//
+// Each step exists for the reference's three type sets: _f32 (all float), _f64 (all double) and _mixed (double
+// coordinates and centres, float masses and multipoles).
 
-extern "C" ryo_status ryo_compute_leaf_source_center_f32(const float* x, const float* y, const float* z,
-                                                         const float* m, const int* leafToInternal, int numLeaves,
-                                                         const uint32_t* layout, float* centers, ryo_stream_t stream)
+namespace
+{
+template<class Tc, class Tm, class Tf>
+ryo_status leafSourceCenter(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const int* leafToInternal,
+                            int numLeaves, const uint32_t* layout, Tf* centers, ryo_stream_t stream)
 {
     return guarded(tlsError,
                    [&]
                    {
-                       launchLeafCenters(x, y, z, m, leafToInternal, numLeaves, layout,
-                                         reinterpret_cast<float4*>(centers), stream);
+                       REQUIRE(numLeaves == 0 || (x && y && z && m && leafToInternal && layout && centers),
+                               "compute_leaf_source_center: null argument");
+                       launchLeafCenters(x, y, z, m, leafToInternal, numLeaves, layout, centers, stream);
                    });
 }
 
-extern "C" ryo_status ryo_upsweep_centers_f32(int numLevels, const int* levelRange, const int* childOffsets,
-                                              float* centers, ryo_stream_t stream)
+template<class Tf>
+ryo_status upsweepCenters(int numLevels, const int* levelRange, const int* childOffsets, Tf* centers,
+                          ryo_stream_t stream)
 {
     return guarded(tlsError,
                    [&]
                    {
                        REQUIRE(levelRange && numLevels <= kMaxLevel + 1, "upsweep_centers: bad argument");
                        for (int level = numLevels - 1; level >= 0; --level)
-                           launchUpsweepCenters(levelRange[level], levelRange[level + 1], childOffsets,
-                                                reinterpret_cast<float4*>(centers), stream);
+                           launchUpsweepCenters(levelRange[level], levelRange[level + 1], childOffsets, centers,
+                                                stream);
                    });
 }
 
-extern "C" ryo_status ryo_compute_leaf_multipoles_f32(const float* x, const float* y, const float* z, const float* m,
-                                                      const int* leafToInternal, int numLeaves,
-                                                      const uint32_t* layout, const float* centers,
-                                                      float* multipoles, ryo_stream_t stream)
+template<class Tc, class Tm, class Tf, class Tmp>
+ryo_status leafMultipoles(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const int* leafToInternal,
+                          int numLeaves, const uint32_t* layout, const Tf* centers, Tmp* multipoles, bool mdq,
+                          ryo_stream_t stream)
 {
     return guarded(tlsError,
                    [&]
                    {
-                       launchLeafMultipoles(x, y, z, m, leafToInternal, numLeaves, layout,
-                                            reinterpret_cast<const float4*>(centers), multipoles, stream);
+                       REQUIRE(numLeaves == 0 || (x && y && z && m && leafToInternal && layout && centers &&
+                                                  multipoles),
+                               "compute_leaf_multipoles: null argument");
+                       launchLeafMultipoles(x, y, z, m, leafToInternal, numLeaves, layout, centers, multipoles, mdq,
+                                            stream);
                    });
 }
 
-extern "C" ryo_status ryo_upsweep_multipoles_f32(int firstCell, int lastCell, const int* childOffsets,
-                                                 const float* centers, float* multipoles, ryo_stream_t stream)
+template<class Tf, class Tmp>
+ryo_status upsweepMultipoles(int firstCell, int lastCell, const int* childOffsets, const Tf* centers, Tmp* multipoles,
+                             bool mdq, ryo_stream_t stream)
 {
     return guarded(tlsError,
                    [&]
                    {
-                       launchUpsweepMultipoles(firstCell, lastCell, childOffsets,
-                                               reinterpret_cast<const float4*>(centers), multipoles, stream);
+                       REQUIRE(lastCell <= firstCell || (childOffsets && centers && multipoles),
+                               "upsweep_multipoles: null argument");
+                       launchUpsweepMultipoles(firstCell, lastCell, childOffsets, centers, multipoles, mdq, stream);
                    });
 }
 
-extern "C" ryo_status ryo_compute_leaf_multipoles_mdq_f32(const float* x, const float* y, const float* z,
-                                                          const float* m, const int* leafToInternal, int numLeaves,
-                                                          const uint32_t* layout, const float* centers,
-                                                          float* multipoles, ryo_stream_t stream)
-{
-    return guarded(tlsError,
-                   [&]
-                   {
-                       launchLeafMultipolesMDQ(x, y, z, m, leafToInternal, numLeaves, layout,
-                                               reinterpret_cast<const float4*>(centers), multipoles, stream);
-                   });
-}
-
-extern "C" ryo_status ryo_upsweep_multipoles_mdq_f32(int firstCell, int lastCell, const int* childOffsets,
-                                                     const float* centers, float* multipoles, ryo_stream_t stream)
-{
-    return guarded(tlsError,
-                   [&]
-                   {
-                       launchUpsweepMultipolesMDQ(firstCell, lastCell, childOffsets,
-                                                  reinterpret_cast<const float4*>(centers), multipoles, stream);
-                   });
-}
-
-extern "C" ryo_status ryo_set_mac_f32(const uint64_t* prefixes, int numNodes, float* centers, float invTheta,
-                                      const ryo_box_f32* box, ryo_stream_t stream)
+template<class T, class Box>
+ryo_status setMac(const uint64_t* prefixes, int numNodes, T* centers, float invTheta, const Box* box,
+                  ryo_stream_t stream)
 {
     return guarded(tlsError,
                    [&]
                    {
                        REQUIRE(box, "set_mac: null box");
                        checkBox(box->limits);
-                       launchSetMac(prefixes, numNodes, reinterpret_cast<float4*>(centers), invTheta, boxOf(box),
-                                    stream);
+                       launchSetMac(prefixes, numNodes, centers, invTheta, boxOf(box), stream);
                    });
+}
+} // namespace
+
+extern "C" ryo_status ryo_compute_leaf_source_center_f32(const float* x, const float* y, const float* z,
+                                                         const float* m, const int* leafToInternal, int numLeaves,
+                                                         const uint32_t* layout, float* centers, ryo_stream_t stream)
+{
+    return leafSourceCenter(x, y, z, m, leafToInternal, numLeaves, layout, centers, stream);
+}
+extern "C" ryo_status ryo_compute_leaf_source_center_f64(const double* x, const double* y, const double* z,
+                                                         const double* m, const int* leafToInternal, int numLeaves,
+                                                         const uint32_t* layout, double* centers, ryo_stream_t stream)
+{
+    return leafSourceCenter(x, y, z, m, leafToInternal, numLeaves, layout, centers, stream);
+}
+extern "C" ryo_status ryo_compute_leaf_source_center_mixed(const double* x, const double* y, const double* z,
+                                                           const float* m, const int* leafToInternal, int numLeaves,
+                                                           const uint32_t* layout, double* centers,
+                                                           ryo_stream_t stream)
+{
+    return leafSourceCenter(x, y, z, m, leafToInternal, numLeaves, layout, centers, stream);
+}
+
+extern "C" ryo_status ryo_upsweep_centers_f32(int numLevels, const int* levelRange, const int* childOffsets,
+                                              float* centers, ryo_stream_t stream)
+{
+    return upsweepCenters(numLevels, levelRange, childOffsets, centers, stream);
+}
+extern "C" ryo_status ryo_upsweep_centers_f64(int numLevels, const int* levelRange, const int* childOffsets,
+                                              double* centers, ryo_stream_t stream)
+{
+    return upsweepCenters(numLevels, levelRange, childOffsets, centers, stream);
+}
+
+#define RYO_LEAF_MULTIPOLES(NAME, Tc, Tm, Tf, Tmp, MDQ)                                                               \
+    extern "C" ryo_status NAME(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const int* leafToInternal,         \
+                               int numLeaves, const uint32_t* layout, const Tf* centers, Tmp* multipoles,             \
+                               ryo_stream_t stream)                                                                   \
+    {                                                                                                                  \
+        return leafMultipoles(x, y, z, m, leafToInternal, numLeaves, layout, centers, multipoles, MDQ, stream);      \
+    }
+RYO_LEAF_MULTIPOLES(ryo_compute_leaf_multipoles_f32, float, float, float, float, false)
+RYO_LEAF_MULTIPOLES(ryo_compute_leaf_multipoles_f64, double, double, double, double, false)
+RYO_LEAF_MULTIPOLES(ryo_compute_leaf_multipoles_mixed, double, float, double, float, false)
+RYO_LEAF_MULTIPOLES(ryo_compute_leaf_multipoles_mdq_f32, float, float, float, float, true)
+RYO_LEAF_MULTIPOLES(ryo_compute_leaf_multipoles_mdq_f64, double, double, double, double, true)
+RYO_LEAF_MULTIPOLES(ryo_compute_leaf_multipoles_mdq_mixed, double, float, double, float, true)
+#undef RYO_LEAF_MULTIPOLES
+
+#define RYO_UPSWEEP_MULTIPOLES(NAME, Tf, Tmp, MDQ)                                                                    \
+    extern "C" ryo_status NAME(int firstCell, int lastCell, const int* childOffsets, const Tf* centers,              \
+                               Tmp* multipoles, ryo_stream_t stream)                                                  \
+    {                                                                                                                  \
+        return upsweepMultipoles(firstCell, lastCell, childOffsets, centers, multipoles, MDQ, stream);               \
+    }
+RYO_UPSWEEP_MULTIPOLES(ryo_upsweep_multipoles_f32, float, float, false)
+RYO_UPSWEEP_MULTIPOLES(ryo_upsweep_multipoles_f64, double, double, false)
+RYO_UPSWEEP_MULTIPOLES(ryo_upsweep_multipoles_mixed, double, float, false)
+RYO_UPSWEEP_MULTIPOLES(ryo_upsweep_multipoles_mdq_f32, float, float, true)
+RYO_UPSWEEP_MULTIPOLES(ryo_upsweep_multipoles_mdq_f64, double, double, true)
+RYO_UPSWEEP_MULTIPOLES(ryo_upsweep_multipoles_mdq_mixed, double, float, true)
+#undef RYO_UPSWEEP_MULTIPOLES
+
+extern "C" ryo_status ryo_set_mac_f32(const uint64_t* prefixes, int numNodes, float* centers, float invTheta,
+                                      const ryo_box_f32* box, ryo_stream_t stream)
+{
+    return setMac(prefixes, numNodes, centers, invTheta, box, stream);
+}
+extern "C" ryo_status ryo_set_mac_f64(const uint64_t* prefixes, int numNodes, double* centers, float invTheta,
+                                      const ryo_box_f64* box, ryo_stream_t stream)
+{
+    return setMac(prefixes, numNodes, centers, invTheta, box, stream);
 }
 
 // ==================================================================================================== traversal
@@ -505,6 +565,24 @@ int heavyParts(uint32_t numHeavy, int smCount)
 {
     uint32_t want = (uint32_t(smCount) * 20u + numHeavy - 1) / numHeavy;
     return int(std::max(2u, std::min(16u, want)));
+}
+
+/*! the groups of a traverse call are the caller's: each must hold 1 to 64 targets inside [firstBody, lastBody). A
+ *  warp evaluates at most 64 targets, and an empty group would read before its start. The reference refuses
+ *  unsupported group sizes too (cstone/traversal/groups_gpu.cu:150). The check reads the group arrays back, so the
+ *  call synchronises its stream. */
+void checkCallerGroups(const ryo_group_view* grp, cudaStream_t stream)
+{
+    if (grp->numGroups == 0) return;
+    REQUIRE(grp->groupStart && grp->groupEnd, "traverse: null group arrays");
+    std::vector<uint32_t> gs(grp->numGroups), ge(grp->numGroups);
+    RYO_CUDA(cudaMemcpyAsync(gs.data(), grp->groupStart, gs.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             stream));
+    RYO_CUDA(cudaMemcpyAsync(ge.data(), grp->groupEnd, ge.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    RYO_CUDA(cudaStreamSynchronize(stream));
+    for (size_t g = 0; g < gs.size(); ++g)
+        REQUIRE(gs[g] >= grp->firstBody && ge[g] <= grp->lastBody && ge[g] > gs[g] && ge[g] - gs[g] <= 64,
+                "traverse: every group needs 1 to 64 targets within [firstBody, lastBody)");
 }
 
 void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potentialOut)
@@ -618,23 +696,7 @@ extern "C" ryo_status ryo_traverse_ex_f32(ryo_ctx_t* ctx, const ryo_group_view* 
                                    internalToLeaf && layout && sourceCenter && multipoles && ax && ay && az,
                                "traverse: null argument");
                        REQUIRE(numShells >= 0 && (numShells == 0 || boxL), "traverse: replicas need boxL");
-                       // the groups are the caller's: each must hold 1 to 64 targets inside [firstBody, lastBody). A
-                       // warp evaluates at most 64 targets, and an empty group would read before its start. The
-                       // reference refuses unsupported group sizes too (cstone/traversal/groups_gpu.cu:150).
-                       if (grp->numGroups > 0)
-                       {
-                           REQUIRE(grp->groupStart && grp->groupEnd, "traverse: null group arrays");
-                           std::vector<uint32_t> gs(grp->numGroups), ge(grp->numGroups);
-                           RYO_CUDA(cudaMemcpyAsync(gs.data(), grp->groupStart, gs.size() * sizeof(uint32_t),
-                                                    cudaMemcpyDeviceToHost, stream));
-                           RYO_CUDA(cudaMemcpyAsync(ge.data(), grp->groupEnd, ge.size() * sizeof(uint32_t),
-                                                    cudaMemcpyDeviceToHost, stream));
-                           RYO_CUDA(cudaStreamSynchronize(stream));
-                           for (size_t g = 0; g < gs.size(); ++g)
-                               REQUIRE(gs[g] >= grp->firstBody && ge[g] <= grp->lastBody && ge[g] > gs[g] &&
-                                           ge[g] - gs[g] <= 64,
-                                       "traverse: every group needs 1 to 64 targets within [firstBody, lastBody)");
-                       }
+                       checkCallerGroups(grp, stream);
                        TraverseLaunch t{};
                        t.groupStart     = grp->groupStart;
                        t.groupEnd       = grp->groupEnd;
@@ -681,6 +743,89 @@ extern "C" ryo_status ryo_traverse_f32(ryo_ctx_t* ctx, const ryo_group_view* grp
     return ryo_traverse_ex_f32(ctx, grp, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
                                internalToLeaf, layout, sourceCenter, multipoles, G, numShells, boxL, p, ax, ay, az,
                                totalPotential, nullptr, stream);
+}
+
+namespace
+{
+//! the double-coordinate instantiations of traverse (traversal_gpu.cu:637-638): Th softenings, Tm masses, Ta
+//! outputs, Tmp multipole values; centres are 4 doubles per node
+template<class Th, class Tm, class Ta, class Tmp>
+ryo_status traverseDouble(ryo_ctx_t* ctx, int precision, const ryo_group_view* grp, int initNodeIdx, const double* xt,
+                          const double* yt, const double* zt, const Tm* mt, const Th* ht, const double* xs,
+                          const double* ys, const double* zs, const Tm* ms, const Th* hs, const int* childOffsets,
+                          const int* internalToLeaf, const uint32_t* layout, const double* sourceCenter,
+                          const Tmp* multipoles, double G, int numShells, const double* boxL, Ta* p, Ta* ax, Ta* ay,
+                          Ta* az, double* totalPotential, const ryo_traverse_options* options, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guardedCtx(ctx,
+                   [&]
+                   {
+                       REQUIRE(grp && xt && yt && zt && mt && ht && xs && ys && zs && ms && hs && childOffsets &&
+                                   internalToLeaf && layout && sourceCenter && multipoles && ax && ay && az,
+                               "traverse: null argument");
+                       REQUIRE(numShells >= 0 && (numShells == 0 || boxL), "traverse: replicas need boxL");
+                       checkCallerGroups(grp, stream);
+                       TraverseLaunch t{};
+                       t.precision      = precision;
+                       t.groupStart     = grp->groupStart;
+                       t.groupEnd       = grp->groupEnd;
+                       t.numGroups      = int(grp->numGroups);
+                       t.initNode       = initNodeIdx;
+                       t.numNodes       = initNodeIdx == 0 ? 1 : 2;
+                       t.childOffsets   = childOffsets;
+                       t.internalToLeaf = internalToLeaf;
+                       t.layout         = layout;
+                       t.xt64 = xt, t.yt64 = yt, t.zt64 = zt, t.mt64 = mt, t.ht64 = ht;
+                       t.xs64 = xs, t.ys64 = ys, t.zs64 = zs, t.ms64 = ms, t.hs64 = hs;
+                       t.centers64    = sourceCenter;
+                       t.multipoles64 = multipoles;
+                       t.G64          = G;
+                       t.G            = float(G);
+                       t.numShells    = numShells;
+                       for (int d = 0; d < 3; ++d)
+                           t.boxL64[d] = numShells > 0 ? boxL[d] : 0.0;
+                       t.p64 = p, t.ax64 = ax, t.ay64 = ay, t.az64 = az;
+                       t.groupM2P      = options ? options->groupM2P : nullptr;
+                       t.groupP2P      = options ? options->groupP2P : nullptr;
+                       t.stackCapacity = options ? options->stackCapacity : 0;
+                       t.mdqArrays     = options && options->multipole == RYO_MULTIPOLE_MDQ ? 1 : 0;
+                       double pot      = 0;
+                       runTraversal(ctx, t, stream, &pot);
+                       if (totalPotential) *totalPotential = 0.5 * G * pot;
+                       if (ctx->hostStats[kMaxP2P] == 0xFFFFFFFFull)
+                           throw ApiError{RYO_ERR_STACK_OVERFLOW_UNSPLITTABLE,
+                                          "traverse: a single target overflowed the stack"};
+                   });
+}
+} // namespace
+
+extern "C" ryo_status ryo_traverse_f64(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const double* xt,
+                                       const double* yt, const double* zt, const double* mt, const double* ht,
+                                       const double* xs, const double* ys, const double* zs, const double* ms,
+                                       const double* hs, const int* childOffsets, const int* internalToLeaf,
+                                       const uint32_t* layout, const double* sourceCenter, const double* multipoles,
+                                       double G, int numShells, const double* boxL, double* p, double* ax, double* ay,
+                                       double* az, double* totalPotential, const ryo_traverse_options* options,
+                                       ryo_stream_t stream)
+{
+    return traverseDouble(ctx, kPrecisionF64, grp, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
+                          internalToLeaf, layout, sourceCenter, multipoles, G, numShells, boxL, p, ax, ay, az,
+                          totalPotential, options, stream);
+}
+
+extern "C" ryo_status ryo_traverse_mixed(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const double* xt,
+                                         const double* yt, const double* zt, const float* mt, const float* ht,
+                                         const double* xs, const double* ys, const double* zs, const float* ms,
+                                         const float* hs, const int* childOffsets, const int* internalToLeaf,
+                                         const uint32_t* layout, const double* sourceCenter, const float* multipoles,
+                                         double G, int numShells, const double* boxL, float* p, float* ax, float* ay,
+                                         float* az, double* totalPotential, const ryo_traverse_options* options,
+                                         ryo_stream_t stream)
+{
+    return traverseDouble(ctx, kPrecisionMixed, grp, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs,
+                          childOffsets, internalToLeaf, layout, sourceCenter, multipoles, G, numShells, boxL, p, ax,
+                          ay, az, totalPotential, options, stream);
 }
 
 extern "C" ryo_status ryo_read_bh_stats(ryo_ctx_t* ctx, uint64_t* stats5)

@@ -212,20 +212,23 @@ void linkOctree(ryo_ctx* ctx, const uint64_t* leaves, int numLeaves, const Octre
 void launchFixedGroups(uint32_t first, uint32_t last, unsigned groupSize, uint32_t* groups, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- upsweep.cu
-void launchLeafCenters(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
-                       int numLeaves, const uint32_t* layout, float4* centers, cudaStream_t s);
-void launchUpsweepCenters(int first, int last, const int* childOffsets, float4* centers, cudaStream_t s);
-void launchLeafMultipoles(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
-                          int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
+// The reference-signature steps, for the reference's type sets: (Tc, Tm, Tf, Tmp) = (float, float, float, float),
+// (double, double, double, double) and (double, float, double, float). Centres are 4 values of Tf per node,
+// multipoles 8 (12 with mdq) values of Tmp per node.
+template<class Tc, class Tm, class Tf>
+void launchLeafCenters(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const int* leafToInternal, int numLeaves,
+                       const uint32_t* layout, Tf* centers, cudaStream_t s);
+template<class Tf>
+void launchUpsweepCenters(int first, int last, const int* childOffsets, Tf* centers, cudaStream_t s);
+template<class Tc, class Tm, class Tf, class Tmp>
+void launchLeafMultipoles(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const int* leafToInternal,
+                          int numLeaves, const uint32_t* layout, const Tf* centers, Tmp* multipoles, bool mdq,
                           cudaStream_t s);
-void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const float4* centers, float* multipoles,
+template<class Tf, class Tmp>
+void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const Tf* centers, Tmp* multipoles, bool mdq,
                              cudaStream_t s);
-void launchLeafMultipolesMDQ(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
-                             int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
-                             cudaStream_t s);
-void launchUpsweepMultipolesMDQ(int first, int last, const int* childOffsets, const float4* centers,
-                                float* multipoles, cudaStream_t s);
-void launchSetMac(const uint64_t* prefixes, int numNodes, float4* centers, float invTheta, const DevBox<float>& box,
+template<class T>
+void launchSetMac(const uint64_t* prefixes, int numNodes, T* centers, float invTheta, const DevBox<T>& box,
                   cudaStream_t s);
 
 //! node record used by the traversal: 64 bytes, one cache line half per node
@@ -310,7 +313,23 @@ struct TraverseLaunch
     // min and max softening of every target and source as ordered bits (null: not known). Equal values let the
     // direct sums skip staging and comparing the sources' softening.
     const uint32_t* softeningRange;
+    // double coordinates (traverse64.cu): kPrecisionF64 (everything double) or kPrecisionMixed (double coordinates
+    // and centres; float softenings, masses, multipoles and outputs). The float fields above are unused then; the
+    // untyped pointers hold double (f64) or float (mixed) arrays.
+    int precision;
+    const double *xt64, *yt64, *zt64, *xs64, *ys64, *zs64;
+    const void *mt64, *ht64, *ms64, *hs64;
+    const double* centers64;   // 4 per node
+    const void* multipoles64;  // 8 or 12 per node
+    double G64;
+    double boxL64[3];
+    void *p64, *ax64, *ay64, *az64;
 };
+
+constexpr int kPrecisionF32   = 0;
+constexpr int kPrecisionF64   = 1;
+constexpr int kPrecisionMixed = 2;
+void launchTraverse64(const TraverseLaunch& t, int smCount, cudaStream_t s);
 
 //! per-system traversal parameters of a batched solve
 struct SysTrav

@@ -983,6 +983,11 @@ static void launchTyped(const TraverseLaunch& t, const Nodes& nodes, const Targe
 void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s)
 {
     if (t.numGroups <= 0 || (t.parts > 0 && t.numHeavy == 0)) return;
+    if (t.precision != kPrecisionF32)
+    {
+        launchTraverse64(t, smCount, s);
+        return;
+    }
     if (t.nodes)
     {
         PackedBodies tgt{t.tgtXYZH, t.tgtM}, src{t.srcXYZM, t.srcH};

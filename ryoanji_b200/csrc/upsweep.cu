@@ -28,11 +28,31 @@ __device__ inline T groupSum8(T v)
 }
 
 // ------------------------------------------------------------------------------------------------ reference steps
+//
+// The reference instantiates its step functions for three type sets (coordinates Tc, masses Tm, centres Tf,
+// multipole values Tmp): all float, all double, and double coordinates and centres with float masses and multipoles
+// (cstone/include/cstone/focus/source_center_gpu.cu:164-170, ryoanji/src/ryoanji/nbody/upsweep_gpu.cu:134-143). The
+// kernels below take the same sets; their sums run in double in every set and are rounded once per stored value.
 
-__global__ void leafCentersKernel(const float* __restrict__ x, const float* __restrict__ y,
-                                  const float* __restrict__ z, const float* __restrict__ m,
-                                  const int* __restrict__ leafToInternal, int numLeaves,
-                                  const uint32_t* __restrict__ layout, float4* __restrict__ centers)
+//! a node centre (x, y, z, |m| or MAC r^2) of type T: float4 for float, four aligned doubles otherwise
+template<class T>
+struct alignas(4 * sizeof(T)) Center4
+{
+    T x, y, z, w;
+};
+template<class T>
+using CenterOf = std::conditional_t<std::is_same_v<T, float>, float4, Center4<T>>;
+
+template<class T>
+__device__ __forceinline__ CenterOf<T> makeCenter(double x, double y, double z, double w)
+{
+    return CenterOf<T>{T(x), T(y), T(z), T(w)};
+}
+
+template<class Tc, class Tm, class Tf>
+__global__ void leafCentersKernel(const Tc* __restrict__ x, const Tc* __restrict__ y, const Tc* __restrict__ z,
+                                  const Tm* __restrict__ m, const int* __restrict__ leafToInternal, int numLeaves,
+                                  const uint32_t* __restrict__ layout, CenterOf<Tf>* __restrict__ centers)
 {
     int tid  = blockIdx.x * blockDim.x + threadIdx.x;
     int leaf = tid / kTpl;
@@ -54,12 +74,12 @@ __global__ void leafCentersKernel(const float* __restrict__ x, const float* __re
     if (leaf < numLeaves && tid % kTpl == 0)
     {
         double inv = c[3] != 0.0 ? 1.0 / c[3] : 1.0;
-        centers[leafToInternal[leaf]] = make_float4(float(c[0] * inv), float(c[1] * inv), float(c[2] * inv),
-                                                    float(c[3]));
+        centers[leafToInternal[leaf]] = makeCenter<Tf>(c[0] * inv, c[1] * inv, c[2] * inv, c[3]);
     }
 }
 
-__global__ void upsweepCentersKernel(int first, int last, const int* __restrict__ childOffsets, float4* centers)
+template<class Tf>
+__global__ void upsweepCentersKernel(int first, int last, const int* __restrict__ childOffsets, CenterOf<Tf>* centers)
 {
     int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= last) return;
@@ -68,45 +88,48 @@ __global__ void upsweepCentersKernel(int first, int last, const int* __restrict_
     double c[4] = {0, 0, 0, 0};
     for (int k = fc; k < fc + 8; ++k)
     {
-        float4 ck = centers[k];
-        double w  = fabs(double(ck.w));
+        CenterOf<Tf> ck = centers[k];
+        double w        = fabs(double(ck.w));
         c[0] += w * ck.x;
         c[1] += w * ck.y;
         c[2] += w * ck.z;
         c[3] += w;
     }
     double inv = c[3] != 0.0 ? 1.0 / c[3] : 1.0;
-    centers[i] = make_float4(float(c[0] * inv), float(c[1] * inv), float(c[2] * inv), float(c[3]));
+    centers[i] = makeCenter<Tf>(c[0] * inv, c[1] * inv, c[2] * inv, c[3]);
 }
 
 //! traceless x3 form with the trace in the last slot (cartesian_qpole.hpp:92-108)
-__device__ inline void finalizeQuad(const double raw[7], float* out)
+template<class Tmp>
+__device__ inline void finalizeQuad(const double raw[7], Tmp* out)
 {
     double tr = raw[1] + raw[4] + raw[6];
-    out[0]    = float(raw[0]);
-    out[1]    = float(3 * raw[1] - tr);
-    out[2]    = float(3 * raw[2]);
-    out[3]    = float(3 * raw[3]);
-    out[4]    = float(3 * raw[4] - tr);
-    out[5]    = float(3 * raw[5]);
-    out[6]    = float(3 * raw[6] - tr);
-    out[7]    = float(tr);
+    out[0]    = Tmp(raw[0]);
+    out[1]    = Tmp(3 * raw[1] - tr);
+    out[2]    = Tmp(3 * raw[2]);
+    out[3]    = Tmp(3 * raw[3]);
+    out[4]    = Tmp(3 * raw[4] - tr);
+    out[5]    = Tmp(3 * raw[5]);
+    out[6]    = Tmp(3 * raw[6] - tr);
+    out[7]    = Tmp(tr);
 }
 
-__global__ void leafMultipolesKernel(const float* __restrict__ x, const float* __restrict__ y,
-                                     const float* __restrict__ z, const float* __restrict__ m,
-                                     const int* __restrict__ leafToInternal, int numLeaves,
-                                     const uint32_t* __restrict__ layout, const float4* __restrict__ centers,
-                                     float* __restrict__ multipoles)
+//! leaf expansions (P2M_add / P2M_finalize, cartesian_qpole.hpp:67-108; with kMDQ the dipole of :237-303 too)
+template<class Tc, class Tm, class Tf, class Tmp, bool kMDQ>
+__global__ void leafMultipolesKernel(const Tc* __restrict__ x, const Tc* __restrict__ y, const Tc* __restrict__ z,
+                                     const Tm* __restrict__ m, const int* __restrict__ leafToInternal, int numLeaves,
+                                     const uint32_t* __restrict__ layout, const CenterOf<Tf>* __restrict__ centers,
+                                     Tmp* __restrict__ multipoles)
 {
+    constexpr int kTerms = kMDQ ? 10 : 7; // mass, xx, xy, xz, yy, yz, zz (, px, py, pz)
     int tid  = blockIdx.x * blockDim.x + threadIdx.x;
     int leaf = tid / kTpl;
-    double q[7] = {0, 0, 0, 0, 0, 0, 0}; // mass, xx, xy, xz, yy, yz, zz
-    int node    = 0;
+    double q[kTerms] = {};
+    int node         = 0;
     if (leaf < numLeaves)
     {
-        node     = leafToInternal[leaf];
-        float4 c = centers[node];
+        node           = leafToInternal[leaf];
+        CenterOf<Tf> c = centers[node];
         for (uint32_t i = layout[leaf] + tid % kTpl; i < layout[leaf + 1]; i += kTpl)
         {
             double rx = double(x[i]) - c.x, ry = double(y[i]) - c.y, rz = double(z[i]) - c.z, mi = m[i];
@@ -117,202 +140,170 @@ __global__ void leafMultipolesKernel(const float* __restrict__ x, const float* _
             q[4] += ry * ry * mi;
             q[5] += ry * rz * mi;
             q[6] += rz * rz * mi;
+            if constexpr (kMDQ)
+            {
+                q[7] += mi * rx;
+                q[8] += mi * ry;
+                q[9] += mi * rz;
+            }
         }
     }
 #pragma unroll
-    for (int k = 0; k < 7; ++k)
-        q[k] = groupSum8(q[k]);
-    if (leaf < numLeaves && tid % kTpl == 0) finalizeQuad(q, multipoles + 8 * size_t(node));
-}
-
-//! M2M of cells [first, last) from their eight children (cartesian_qpole.hpp:187-235), double sums
-__global__ void upsweepMultipolesKernel(int first, int last, const int* __restrict__ childOffsets,
-                                        const float4* __restrict__ centers, float* multipoles)
-{
-    int i = first + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= last) return;
-    int fc = childOffsets[i];
-    if (!fc) return;
-    float4 cp = centers[i];
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int k = fc; k < fc + 8; ++k)
-    {
-        float4 ck      = centers[k];
-        const float* a = multipoles + 8 * size_t(k);
-        double rx = double(cp.x) - ck.x, ry = double(cp.y) - ck.y, rz = double(cp.z) - ck.z;
-        double r2 = (rx * rx + ry * ry + rz * rz) * (1.0 / 3.0);
-        double ml = double(a[0]) * 3;
-        acc[7] += a[7] + ml * r2;
-        acc[0] += a[0];
-        acc[1] += a[1] + ml * (rx * rx - r2);
-        acc[2] += a[2] + ml * rx * ry;
-        acc[3] += a[3] + ml * rx * rz;
-        acc[4] += a[4] + ml * (ry * ry - r2);
-        acc[5] += a[5] + ml * ry * rz;
-        acc[6] += a[6] + ml * (rz * rz - r2);
-    }
-    float* o = multipoles + 8 * size_t(i);
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-        o[k] = float(acc[k]);
-}
-
-//! leaf CartesianMDQpole expansions (P2M_add / P2M_finalize, cartesian_qpole.hpp:237-303), double sums
-__global__ void leafMultipolesMDQKernel(const float* __restrict__ x, const float* __restrict__ y,
-                                        const float* __restrict__ z, const float* __restrict__ m,
-                                        const int* __restrict__ leafToInternal, int numLeaves,
-                                        const uint32_t* __restrict__ layout, const float4* __restrict__ centers,
-                                        float* __restrict__ multipoles)
-{
-    int tid  = blockIdx.x * blockDim.x + threadIdx.x;
-    int leaf = tid / kTpl;
-    double q[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0}; // mass, xx, xy, xz, yy, yz, zz, px, py, pz
-    int node     = 0;
-    if (leaf < numLeaves)
-    {
-        node     = leafToInternal[leaf];
-        float4 c = centers[node];
-        for (uint32_t i = layout[leaf] + tid % kTpl; i < layout[leaf + 1]; i += kTpl)
-        {
-            double rx = double(x[i]) - c.x, ry = double(y[i]) - c.y, rz = double(z[i]) - c.z, mi = m[i];
-            q[0] += mi;
-            q[1] += rx * rx * mi;
-            q[2] += rx * ry * mi;
-            q[3] += rx * rz * mi;
-            q[4] += ry * ry * mi;
-            q[5] += ry * rz * mi;
-            q[6] += rz * rz * mi;
-            q[7] += mi * rx;
-            q[8] += mi * ry;
-            q[9] += mi * rz;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < 10; ++k)
+    for (int k = 0; k < kTerms; ++k)
         q[k] = groupSum8(q[k]);
     if (leaf < numLeaves && tid % kTpl == 0)
     {
-        float* o = multipoles + 12 * size_t(node);
+        Tmp* o = multipoles + (kMDQ ? 12 : 8) * size_t(node);
         finalizeQuad(q, o);
-        o[8]  = float(q[7]);
-        o[9]  = float(q[8]);
-        o[10] = float(q[9]);
-        o[11] = 0.f;
+        if constexpr (kMDQ)
+        {
+            o[8]  = Tmp(q[7]);
+            o[9]  = Tmp(q[8]);
+            o[10] = Tmp(q[9]);
+            o[11] = Tmp(0);
+        }
     }
 }
 
-//! M2M of CartesianMDQpole cells [first, last) from their eight children (addQuadrupole, cartesian_qpole.hpp:352-418)
-__global__ void upsweepMultipolesMDQKernel(int first, int last, const int* __restrict__ childOffsets,
-                                           const float4* __restrict__ centers, float* multipoles)
+/*! M2M of cells [first, last) from their eight children, double sums: the quadrupole's parallel-axis theorem
+ *  (addQuadrupole, cartesian_qpole.hpp:187-235) and, with kMDQ, the dipole terms of cartesian_qpole.hpp:352-418 */
+template<class Tf, class Tmp, bool kMDQ>
+__global__ void upsweepMultipolesKernel(int first, int last, const int* __restrict__ childOffsets,
+                                        const CenterOf<Tf>* __restrict__ centers, Tmp* multipoles)
 {
+    constexpr int kVals = kMDQ ? 12 : 8;
     int i = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= last) return;
     int fc = childOffsets[i];
     if (!fc) return;
-    float4 cp = centers[i];
-    double acc[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    CenterOf<Tf> cp = centers[i];
+    double acc[11]  = {};
     for (int k = fc; k < fc + 8; ++k)
     {
-        float4 ck      = centers[k];
-        const float* a = multipoles + 12 * size_t(k);
+        CenterOf<Tf> ck = centers[k];
+        const Tmp* a    = multipoles + kVals * size_t(k);
         double rx = double(cp.x) - ck.x, ry = double(cp.y) - ck.y, rz = double(cp.z) - ck.z;
-        double r2  = (rx * rx + ry * ry + rz * rz) * (1.0 / 3.0);
-        double ml  = double(a[0]) * 3;
-        double px = a[8], py = a[9], pz = a[10];
-        double dip = rx * px + ry * py + rz * pz;
-        acc[7] += a[7] + ml * r2 - 2.0 * dip;
-        acc[0] += a[0];
-        acc[8] += px - double(a[0]) * rx;
-        acc[9] += py - double(a[0]) * ry;
-        acc[10] += pz - double(a[0]) * rz;
-        acc[1] += a[1] + ml * (rx * rx - r2) - 6.0 * rx * px + 2.0 * dip;
-        acc[2] += a[2] + ml * rx * ry - 3.0 * (rx * py + ry * px);
-        acc[3] += a[3] + ml * rx * rz - 3.0 * (rx * pz + rz * px);
-        acc[4] += a[4] + ml * (ry * ry - r2) - 6.0 * ry * py + 2.0 * dip;
-        acc[5] += a[5] + ml * ry * rz - 3.0 * (ry * pz + rz * py);
-        acc[6] += a[6] + ml * (rz * rz - r2) - 6.0 * rz * pz + 2.0 * dip;
+        double r2 = (rx * rx + ry * ry + rz * rz) * (1.0 / 3.0);
+        double ml = double(a[0]) * 3;
+        if constexpr (!kMDQ)
+        {
+            acc[7] += a[7] + ml * r2;
+            acc[0] += a[0];
+            acc[1] += a[1] + ml * (rx * rx - r2);
+            acc[2] += a[2] + ml * rx * ry;
+            acc[3] += a[3] + ml * rx * rz;
+            acc[4] += a[4] + ml * (ry * ry - r2);
+            acc[5] += a[5] + ml * ry * rz;
+            acc[6] += a[6] + ml * (rz * rz - r2);
+        }
+        else
+        {
+            double px = a[8], py = a[9], pz = a[10];
+            double dip = rx * px + ry * py + rz * pz;
+            acc[7] += a[7] + ml * r2 - 2.0 * dip;
+            acc[0] += a[0];
+            acc[8] += px - double(a[0]) * rx;
+            acc[9] += py - double(a[0]) * ry;
+            acc[10] += pz - double(a[0]) * rz;
+            acc[1] += a[1] + ml * (rx * rx - r2) - 6.0 * rx * px + 2.0 * dip;
+            acc[2] += a[2] + ml * rx * ry - 3.0 * (rx * py + ry * px);
+            acc[3] += a[3] + ml * rx * rz - 3.0 * (rx * pz + rz * px);
+            acc[4] += a[4] + ml * (ry * ry - r2) - 6.0 * ry * py + 2.0 * dip;
+            acc[5] += a[5] + ml * ry * rz - 3.0 * (ry * pz + rz * py);
+            acc[6] += a[6] + ml * (rz * rz - r2) - 6.0 * rz * pz + 2.0 * dip;
+        }
     }
-    float* o = multipoles + 12 * size_t(i);
+    Tmp* o = multipoles + kVals * size_t(i);
 #pragma unroll
-    for (int k = 0; k < 11; ++k)
-        o[k] = float(acc[k]);
-    o[11] = 0.f;
+    for (int k = 0; k < (kMDQ ? 11 : 8); ++k)
+        o[k] = Tmp(acc[k]);
+    if constexpr (kMDQ) o[11] = Tmp(0);
 }
 
-__global__ void setMacKernel(const uint64_t* __restrict__ prefixes, int numNodes, float4* centers, float invTheta,
-                             DevBox<float> box)
+template<class T>
+__global__ void setMacKernel(const uint64_t* __restrict__ prefixes, int numNodes, CenterOf<T>* centers, float invTheta,
+                             DevBox<T> box)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= numNodes) return;
-    float4 c      = centers[i];
-    float com[3]  = {c.x, c.y, c.z};
-    float mac     = vecMacR2(prefixes[i], com, invTheta, box);
-    centers[i].w  = (c.w != 0.f) ? mac : 0.f;
+    CenterOf<T> c = centers[i];
+    T com[3]      = {c.x, c.y, c.z};
+    T mac         = vecMacR2(prefixes[i], com, invTheta, box);
+    centers[i].w  = (c.w != T(0)) ? mac : T(0);
 }
 
-void launchLeafCenters(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
-                       int numLeaves, const uint32_t* layout, float4* centers, cudaStream_t s)
+template<class Tc, class Tm, class Tf>
+void launchLeafCenters(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const int* leafToInternal, int numLeaves,
+                       const uint32_t* layout, Tf* centers, cudaStream_t s)
 {
     if (numLeaves <= 0) return;
-    leafCentersKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(x, y, z, m, leafToInternal, numLeaves,
-                                                                              layout, centers);
+    leafCentersKernel<Tc, Tm, Tf><<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(
+        x, y, z, m, leafToInternal, numLeaves, layout, reinterpret_cast<CenterOf<Tf>*>(centers));
     RYO_LAUNCH_CHECK();
 }
 
-void launchUpsweepCenters(int first, int last, const int* childOffsets, float4* centers, cudaStream_t s)
+template<class Tf>
+void launchUpsweepCenters(int first, int last, const int* childOffsets, Tf* centers, cudaStream_t s)
 {
     if (last <= first) return;
-    upsweepCentersKernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets, centers);
+    upsweepCentersKernel<Tf><<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets,
+                                                                        reinterpret_cast<CenterOf<Tf>*>(centers));
     RYO_LAUNCH_CHECK();
 }
 
-void launchLeafMultipoles(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
-                          int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
+template<class Tc, class Tm, class Tf, class Tmp>
+void launchLeafMultipoles(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const int* leafToInternal,
+                          int numLeaves, const uint32_t* layout, const Tf* centers, Tmp* multipoles, bool mdq,
                           cudaStream_t s)
 {
     if (numLeaves <= 0) return;
-    leafMultipolesKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(x, y, z, m, leafToInternal,
-                                                                                 numLeaves, layout, centers,
-                                                                                 multipoles);
+    auto kernel = mdq ? leafMultipolesKernel<Tc, Tm, Tf, Tmp, true> : leafMultipolesKernel<Tc, Tm, Tf, Tmp, false>;
+    kernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(
+        x, y, z, m, leafToInternal, numLeaves, layout, reinterpret_cast<const CenterOf<Tf>*>(centers), multipoles);
     RYO_LAUNCH_CHECK();
 }
 
-void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const float4* centers, float* multipoles,
+template<class Tf, class Tmp>
+void launchUpsweepMultipoles(int first, int last, const int* childOffsets, const Tf* centers, Tmp* multipoles, bool mdq,
                              cudaStream_t s)
 {
     if (last <= first) return;
-    upsweepMultipolesKernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets, centers,
-                                                                       multipoles);
+    auto kernel = mdq ? upsweepMultipolesKernel<Tf, Tmp, true> : upsweepMultipolesKernel<Tf, Tmp, false>;
+    kernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets,
+                                                      reinterpret_cast<const CenterOf<Tf>*>(centers), multipoles);
     RYO_LAUNCH_CHECK();
 }
 
-void launchLeafMultipolesMDQ(const float* x, const float* y, const float* z, const float* m, const int* leafToInternal,
-                             int numLeaves, const uint32_t* layout, const float4* centers, float* multipoles,
-                             cudaStream_t s)
-{
-    if (numLeaves <= 0) return;
-    leafMultipolesMDQKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(x, y, z, m, leafToInternal,
-                                                                                  numLeaves, layout, centers,
-                                                                                  multipoles);
-    RYO_LAUNCH_CHECK();
-}
-
-void launchUpsweepMultipolesMDQ(int first, int last, const int* childOffsets, const float4* centers,
-                                float* multipoles, cudaStream_t s)
-{
-    if (last <= first) return;
-    upsweepMultipolesMDQKernel<<<ceilDiv(last - first, 256), 256, 0, s>>>(first, last, childOffsets, centers,
-                                                                          multipoles);
-    RYO_LAUNCH_CHECK();
-}
-
-void launchSetMac(const uint64_t* prefixes, int numNodes, float4* centers, float invTheta, const DevBox<float>& box,
+template<class T>
+void launchSetMac(const uint64_t* prefixes, int numNodes, T* centers, float invTheta, const DevBox<T>& box,
                   cudaStream_t s)
 {
     if (numNodes <= 0) return;
-    setMacKernel<<<ceilDiv(numNodes, 256), 256, 0, s>>>(prefixes, numNodes, centers, invTheta, box);
+    setMacKernel<T><<<ceilDiv(numNodes, 256), 256, 0, s>>>(prefixes, numNodes,
+                                                           reinterpret_cast<CenterOf<T>*>(centers), invTheta, box);
     RYO_LAUNCH_CHECK();
 }
+
+// the reference's three type sets (coordinates, masses, centres, multipole values)
+template void launchLeafCenters(const float*, const float*, const float*, const float*, const int*, int,
+                                const uint32_t*, float*, cudaStream_t);
+template void launchLeafCenters(const double*, const double*, const double*, const double*, const int*, int,
+                                const uint32_t*, double*, cudaStream_t);
+template void launchLeafCenters(const double*, const double*, const double*, const float*, const int*, int,
+                                const uint32_t*, double*, cudaStream_t);
+template void launchUpsweepCenters(int, int, const int*, float*, cudaStream_t);
+template void launchUpsweepCenters(int, int, const int*, double*, cudaStream_t);
+template void launchLeafMultipoles(const float*, const float*, const float*, const float*, const int*, int,
+                                   const uint32_t*, const float*, float*, bool, cudaStream_t);
+template void launchLeafMultipoles(const double*, const double*, const double*, const double*, const int*, int,
+                                   const uint32_t*, const double*, double*, bool, cudaStream_t);
+template void launchLeafMultipoles(const double*, const double*, const double*, const float*, const int*, int,
+                                   const uint32_t*, const double*, float*, bool, cudaStream_t);
+template void launchUpsweepMultipoles(int, int, const int*, const float*, float*, bool, cudaStream_t);
+template void launchUpsweepMultipoles(int, int, const int*, const double*, double*, bool, cudaStream_t);
+template void launchUpsweepMultipoles(int, int, const int*, const double*, float*, bool, cudaStream_t);
+template void launchSetMac(const uint64_t*, int, float*, float, const DevBox<float>&, cudaStream_t);
+template void launchSetMac(const uint64_t*, int, double*, float, const DevBox<double>&, cudaStream_t);
 
 // ------------------------------------------------------------------------------------------------ fused path
 

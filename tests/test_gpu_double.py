@@ -1,0 +1,184 @@
+"""The double-coordinate type sets of the boundary against the reference's own GPU code.
+
+The reference instantiates its upward pass and its traversal for three type sets (source_center_gpu.cu:164-170,
+upsweep_gpu.cu:134-143, traversal_gpu.cu:635-641): all float, all double ("f64") and double coordinates and centres
+with float masses, softenings, multipoles and outputs ("mixed"). For the two double sets this file runs the
+reference's TreeBuilder<uint64_t>::update<double>, its upsweep and its traverse (compiled from its sources into
+oracle/_ref/libryo_ref_gpu.so) beside this library's steps and traversal on the same tree and groups:
+
+- centres and MAC radii: the reference sums in its centre type, this library in double and rounds once;
+- multipoles: float round-off (mixed) or double round-off (f64) of the node's largest moment;
+- readBhStats sums and maxima equal;
+- accelerations: 1e-9 relative at the 99th percentile for f64 (both sides sum in double with the same
+  single-precision rsqrt, only the order and the contraction of the arithmetic differ), 1e-5 for mixed (float
+  outputs).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from ryoanji_b200 import datasets as ds
+from test_gpu_ref_traverse import _ptr, host, ref_fixed_groups, ref_lib, rel_err, sorted_bodies
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref64_lib():
+    lib = ref_lib()
+    lib.ref_gpu_build_f64.restype = C.c_int
+    lib.ref_gpu_build_f64.argtypes = [C.c_void_p] * 4 + [C.c_size_t, C.c_void_p]
+    lib.ref_gpu_upsweep_f64.argtypes = [C.c_void_p] * 6 + [C.c_float, C.c_void_p, C.c_void_p, C.c_int]
+    lib.ref_gpu_upsweep_mixed.argtypes = [C.c_void_p] * 6 + [C.c_float, C.c_void_p, C.c_void_p, C.c_int]
+    for name in ("ref_gpu_traverse_f64", "ref_gpu_traverse_mixed"):
+        fn = getattr(lib, name)
+        fn.restype = C.c_double
+        fn.argtypes = ([C.c_uint32] * 3 + [C.c_void_p] * 2 + [C.c_int] + [C.c_void_p] * 15 + [C.c_double, C.c_int] +
+                       [C.c_void_p] * 7 + [C.c_int])
+    return lib
+
+
+class RefFlow64:
+    """the reference's double build and upsweep of one type set on Hilbert-sorted bodies"""
+
+    def __init__(self, kind, x, y, z, m, h, box, bucket, theta, mdq=False):
+        lib = _ref64_lib()
+        mt = torch.float64 if kind == "f64" else torch.float32
+        d = lambda a, t=torch.float64: torch.from_numpy(np.ascontiguousarray(a)).to("cuda", t)  # noqa: E731
+        self.kind, self.mdq = kind, mdq
+        self.x, self.y, self.z = d(x), d(y), d(z)
+        self.m, self.h = d(m, mt), d(h, mt)
+        self.n = len(x)
+        self.box = np.ascontiguousarray(box, np.float64)
+        torch.cuda.synchronize()
+        self.handle = lib.ref_gpu_create(bucket)
+        self.num_nodes = lib.ref_gpu_build_f64(self.handle, _ptr(self.x), _ptr(self.y), _ptr(self.z), self.n,
+                                               self.box.ctypes.data_as(C.c_void_p))
+        lr, nl = (C.c_int * 23)(), C.c_int(0)
+        lib.ref_gpu_tree(self.handle, lr, C.byref(nl))
+        self.num_leaves, self.level_range = nl.value, list(lr)
+        i32 = lambda k: torch.empty(k, dtype=torch.int32, device="cuda")  # noqa: E731
+        self.layout, self.child_offsets = i32(self.num_leaves + 1), i32(self.num_nodes)
+        self.leaf_to_internal, self.internal_to_leaf = i32(self.num_leaves), i32(self.num_nodes)
+        self.prefixes = torch.empty(self.num_nodes, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        assert lib.ref_gpu_tree_copy(self.handle, _ptr(self.layout), _ptr(self.prefixes), _ptr(self.child_offsets),
+                                     _ptr(self.leaf_to_internal), _ptr(self.internal_to_leaf)) == 0
+        self.centers = torch.zeros(self.num_nodes, 4, dtype=torch.float64, device="cuda")
+        self.multipoles = torch.zeros(self.num_nodes, 12 if mdq else 8, dtype=mt, device="cuda")
+        up = lib.ref_gpu_upsweep_f64 if kind == "f64" else lib.ref_gpu_upsweep_mixed
+        up(self.handle, _ptr(self.x), _ptr(self.y), _ptr(self.z), _ptr(self.m), self.box.ctypes.data_as(C.c_void_p),
+           C.c_float(theta), _ptr(self.centers), _ptr(self.multipoles), int(mdq))
+        assert lib.ref_gpu_last_error() == 0
+
+    def close(self):
+        ref_lib().ref_gpu_destroy(self.handle)
+
+
+def ref_traverse64(f, groups, shells=0, boxL=(0.0, 0.0, 0.0), G=1.0):
+    lib = _ref64_lib()
+    at = torch.float64 if f.kind == "f64" else torch.float32
+    p, ax, ay, az = (torch.zeros(f.n, dtype=at, device="cuda") for _ in range(4))
+    stats, retries = (C.c_uint64 * 5)(), C.c_uint64(0)
+    bl = np.asarray(boxL, np.float64)
+    gs, ge = groups[:-1].contiguous(), groups[1:].contiguous()
+    fn = lib.ref_gpu_traverse_f64 if f.kind == "f64" else lib.ref_gpu_traverse_mixed
+    torch.cuda.synchronize()
+    pot = fn(0, f.n, int(gs.numel()), _ptr(gs), _ptr(ge), 1, _ptr(f.x), _ptr(f.y), _ptr(f.z), _ptr(f.m), _ptr(f.h),
+             _ptr(f.x), _ptr(f.y), _ptr(f.z), _ptr(f.m), _ptr(f.h), _ptr(f.child_offsets), _ptr(f.internal_to_leaf),
+             _ptr(f.layout), _ptr(f.centers), _ptr(f.multipoles), C.c_double(G), shells,
+             bl.ctypes.data_as(C.c_void_p), _ptr(p), _ptr(ax), _ptr(ay), _ptr(az), stats, C.byref(retries),
+             int(f.mdq))
+    assert lib.ref_gpu_last_error() == 0
+    return pot, list(stats), p, ax, ay, az
+
+
+def _bodies(oracle, kind_of_set):
+    if kind_of_set == "plummer":
+        p = ds.plummer(1 << 16, seed=31, velocities=False)
+    else:
+        p = ds.uniform_cube(1 << 16, seed=32, eps=0.01)
+    box = np.array(ds.cube_box(p, pad=1e-6), np.float64)
+    # double coordinates that are not float values: a jitter far below the spacing
+    rng = np.random.default_rng(33)
+    x, y, z = (a.astype(np.float64) + rng.uniform(-1e-9, 1e-9, p.n) for a in (p.x, p.y, p.z))
+    return sorted_bodies(oracle, x, y, z, p.m.astype(np.float64), p.h.astype(np.float64), box) + (box,)
+
+
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
+@pytest.mark.parametrize("mdq", [False, True])
+def test_double_upsweep_steps_match_reference(oracle, kind, mdq):
+    import ryoanji_b200 as ryo
+    x, y, z, m, h, box = _bodies(oracle, "plummer")
+    f = RefFlow64(kind, x, y, z, m, h, box, 64, 0.5, mdq=mdq)
+    try:
+        centers = torch.zeros_like(f.centers)
+        mp = torch.zeros_like(f.multipoles)
+        ryo.compute_leaf_source_center(f.x, f.y, f.z, f.m, f.leaf_to_internal, f.layout, centers)
+        nlev = max(i for i in range(22) if f.level_range[i + 1] > f.level_range[i]) + 1
+        ryo.upsweep_centers(nlev, f.level_range, f.child_offsets, centers)
+        ryo.compute_leaf_multipoles(f.x, f.y, f.z, f.m, f.leaf_to_internal, f.layout, centers, mp, mdq=mdq)
+        for level in range(nlev - 1, 0, -1):
+            ryo.upsweep_multipoles(f.level_range[level], f.level_range[level + 1], f.child_offsets, centers, mp,
+                                   mdq=mdq)
+        b = ryo.Box(*[float(v) for v in box])
+        ryo.set_mac(f.prefixes, centers, 2.0, b)
+        c, rc = host(centers), host(f.centers)
+        scale = np.abs(rc[:, :3]).max()
+        assert np.abs(c[:, :3] - rc[:, :3]).max() <= 1e-13 * scale
+        assert np.allclose(c[:, 3], rc[:, 3], rtol=1e-12, atol=0)
+        q, rq = host(mp).astype(np.float64), host(f.multipoles).astype(np.float64)
+        tol = 1e-11 if kind == "f64" else 2e-5  # the reference accumulates float multipoles in float
+        big = np.maximum(np.abs(rq[:, 1:]).max(axis=1), np.abs(q[:, 1:]).max(axis=1)) + 1e-300
+        assert np.all(np.abs(q[:, 1:] - rq[:, 1:]).max(axis=1) <= tol * big)
+        assert np.allclose(q[:, 0], rq[:, 0], rtol=tol, atol=0)
+    finally:
+        f.close()
+
+
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
+@pytest.mark.parametrize("dataset,mdq", [("plummer", False), ("cube", False), ("plummer", True)])
+def test_double_traverse_matches_reference(oracle, kind, dataset, mdq):
+    import ryoanji_b200 as ryo
+    x, y, z, m, h, box = _bodies(oracle, dataset)
+    f = RefFlow64(kind, x, y, z, m, h, box, 64, 0.5, mdq=mdq)
+    try:
+        groups = torch.from_numpy(ref_fixed_groups(f.n).view(np.int32)).cuda()
+        rpot, rst, rp, rax, ray, raz = ref_traverse64(f, groups)
+        at = torch.float64 if kind == "f64" else torch.float32
+        p, ax, ay, az = (torch.zeros(f.n, dtype=at, device="cuda") for _ in range(4))
+        pot, gm, gp = ryo.traverse(groups, 1, f.x, f.y, f.z, f.m, f.h, f.x, f.y, f.z, f.m, f.h, f.child_offsets,
+                                   f.internal_to_leaf, f.layout, f.centers, f.multipoles, 1.0, 0, None, p, ax, ay,
+                                   az, group_counts=True, mdq=mdq)
+        st = ryo.read_bh_stats()
+        assert st[:4] == rst[:4], (st, rst)
+        e = rel_err(host(ax), host(ay), host(az), host(rax), host(ray), host(raz))
+        tol = 1e-9 if kind == "f64" else 1e-5
+        assert np.percentile(e, 99) <= tol and e.max() <= 50 * tol, (np.percentile(e, 99), e.max())
+        assert abs(pot - rpot) <= 1e-5 * abs(rpot)
+    finally:
+        f.close()
+
+
+def test_mixed_traverse_agrees_with_float_traverse(oracle):
+    """the mixed instantiation on float-representable inputs equals the float one to float round-off"""
+    import ryoanji_b200 as ryo
+    p = ds.plummer(1 << 15, seed=34, velocities=False)
+    box = np.array(ds.cube_box(p, pad=1e-6), np.float64)
+    x, y, z, m, h = sorted_bodies(oracle, p.x.astype(np.float64), p.y.astype(np.float64), p.z.astype(np.float64),
+                                  p.m.astype(np.float64), p.h.astype(np.float64), box)
+    f = RefFlow64("mixed", x, y, z, m, h, box, 32, 0.5)
+    try:
+        groups = torch.from_numpy(ref_fixed_groups(f.n).view(np.int32)).cuda()
+        out = {}
+        for label, cast in (("mixed", lambda t: t), ("f32", lambda t: t.float())):
+            acc = [torch.zeros(f.n, device="cuda") for _ in range(4)]
+            ryo.traverse(groups, 1, *(cast(t) for t in (f.x, f.y, f.z)), f.m, f.h, *(cast(t) for t in (f.x, f.y, f.z)),
+                         f.m, f.h, f.child_offsets, f.internal_to_leaf, f.layout, cast(f.centers), f.multipoles, 1.0,
+                         0, None, *acc)
+            out[label] = [host(a) for a in acc]
+        e = rel_err(*out["f32"][1:], *out["mixed"][1:])
+        assert np.percentile(e, 99) < 1e-4
+    finally:
+        f.close()
