@@ -4,11 +4,14 @@
  * Re-creates the template signatures that the reference's callers use (ryoanji/src/ryoanji/interface/
  * treebuilder.cuh:34-125, ryoanji/src/ryoanji/nbody/traversal_gpu.h:51-70, upsweep_gpu.h:24-41,
  * interface/ewald.cuh:24-27, and the cstone execution::Gpu functions) for the instantiations that the B200 library
- * implements: 64-bit keys, float coordinates, CartesianQuadrupole<float> multipoles (8 floats per node) and
- * Vec4<float> source centres (4 floats per node). Device arrays are device pointers, as in the reference.
+ * implements: 64-bit keys and the reference's three type sets of the upward pass and the traversal: all float, all
+ * double, and double coordinates and centres with float masses, softenings, multipoles and outputs (its "mixed"
+ * instantiation). Multipoles are CartesianQuadrupole<T> (8 values per node) or CartesianMDQpole<T> (12), source
+ * centres Vec4<T> (4 values per node). Device arrays are device pointers, as in the reference.
  *
  * Differences a caller sees:
- *   - everything lives in namespace ryo (a caller switches with `namespace ryoanji = ryo;` or by renaming);
+ *   - everything lives in namespace ryo; ryoanji_b200/compat.hpp adds the reference's namespaces and spellings
+ *     (cstone::, ryoanji::, execution::Gpu first arguments) on top of this header;
  *   - failures throw ryo::Error (status + message) instead of exiting the process;
  *   - each function takes an optional stream (last argument) and an optional ryo::Context; the default context
  *     is the current device's;
@@ -156,11 +159,56 @@ struct Vec3
     T x, y, z;
 };
 
-//! the reference's multipole types (ryoanji/src/ryoanji/nbody/cartesian_qpole.hpp:24-48): float instantiations
+//! the reference's multipole types (ryoanji/src/ryoanji/nbody/cartesian_qpole.hpp:24-48)
 template<class T>
 using CartesianQuadrupole = std::array<T, 8>;
 template<class T>
 using CartesianMDQpole = std::array<T, 12>;
+//! a source centre: x, y, z and the squared MAC radius (cstone::SourceCenterType / Vec4<T>)
+template<class T>
+using Vec4 = std::array<T, 4>;
+
+namespace detail
+{
+//! the value type of a multipole array element, and whether it is a CartesianMDQpole
+template<class M>
+struct Mpole
+{
+    using value                = M;
+    static constexpr bool mdq  = false;
+};
+template<class T>
+struct Mpole<std::array<T, 8>>
+{
+    using value               = T;
+    static constexpr bool mdq = false;
+};
+template<class T>
+struct Mpole<std::array<T, 12>>
+{
+    using value               = T;
+    static constexpr bool mdq = true;
+};
+//! the value type of a centre array element (T or Vec4<T>)
+template<class C>
+struct Center
+{
+    using value = C;
+};
+template<class T>
+struct Center<std::array<T, 4>>
+{
+    using value = T;
+};
+template<class Tc, class Tm>
+inline constexpr bool isF32 = std::is_same_v<Tc, float> && std::is_same_v<Tm, float>;
+template<class Tc, class Tm>
+inline constexpr bool isF64 = std::is_same_v<Tc, double> && std::is_same_v<Tm, double>;
+template<class Tc, class Tm>
+inline constexpr bool isMixed = std::is_same_v<Tc, double> && std::is_same_v<Tm, float>;
+template<class>
+inline constexpr bool alwaysFalse = false;
+} // namespace detail
 
 //! ryoanji::TreeBuilder (ryoanji/src/ryoanji/interface/treebuilder.cuh:34-125); the returned pointers stay valid
 //! until the next update
@@ -315,74 +363,104 @@ void buildOctreeGpu(const KeyType* cstoneTree, OctreeView<KeyType> d, Context& c
           ctx.get());
 }
 
-//! cstone::computeLeafSourceCenterGpu (cstone/include/cstone/focus/source_center_gpu.h)
-inline void computeLeafSourceCenterGpu(const float* x, const float* y, const float* z, const float* m,
-                                       const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
-                                       const LocalIndex* layout, float* centers /* Vec4<float> */,
-                                       ryo_stream_t stream = nullptr)
+/*! cstone::computeLeafSourceCenterGpu (cstone/include/cstone/focus/source_center_gpu.h:65-80) for the type sets
+ *  (Tc, Tm, Tf) = (float, float, float), (double, double, double), (double, float, double); @p centers holds 4
+ *  values per node (Tf or Vec4<Tf> elements) */
+template<class Tc, class Tm, class C>
+void computeLeafSourceCenterGpu(const Tc* x, const Tc* y, const Tc* z, const Tm* m,
+                                const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
+                                const LocalIndex* layout, C* centers, ryo_stream_t stream = nullptr)
 {
-    check(ryo_compute_leaf_source_center_f32(x, y, z, m, leafToInternal, numLeaves, layout, centers, stream));
+    using Tf = typename detail::Center<C>::value;
+    auto* c  = reinterpret_cast<Tf*>(centers);
+    if constexpr (detail::isF32<Tc, Tm> && std::is_same_v<Tf, float>)
+        check(ryo_compute_leaf_source_center_f32(x, y, z, m, leafToInternal, numLeaves, layout, c, stream));
+    else if constexpr (detail::isF64<Tc, Tm> && std::is_same_v<Tf, double>)
+        check(ryo_compute_leaf_source_center_f64(x, y, z, m, leafToInternal, numLeaves, layout, c, stream));
+    else if constexpr (detail::isMixed<Tc, Tm> && std::is_same_v<Tf, double>)
+        check(ryo_compute_leaf_source_center_mixed(x, y, z, m, leafToInternal, numLeaves, layout, c, stream));
+    else
+        static_assert(detail::alwaysFalse<C>, "not an instantiated type set");
 }
 
 //! cstone::upsweepCentersGpu; levelRange is a host pointer as in the reference
-inline void upsweepCentersGpu(int numLevels, const TreeNodeIndex* levelRange, const TreeNodeIndex* childOffsets,
-                              float* centers, ryo_stream_t stream = nullptr)
+template<class C>
+void upsweepCentersGpu(int numLevels, const TreeNodeIndex* levelRange, const TreeNodeIndex* childOffsets, C* centers,
+                       ryo_stream_t stream = nullptr)
 {
-    check(ryo_upsweep_centers_f32(numLevels, levelRange, childOffsets, centers, stream));
+    using Tf = typename detail::Center<C>::value;
+    auto* c  = reinterpret_cast<Tf*>(centers);
+    if constexpr (std::is_same_v<Tf, float>) check(ryo_upsweep_centers_f32(numLevels, levelRange, childOffsets, c, stream));
+    else check(ryo_upsweep_centers_f64(numLevels, levelRange, childOffsets, c, stream));
 }
 
-//! cstone::setMacGpu with the vector MAC
-inline void setMacGpu(const uint64_t* prefixes, TreeNodeIndex numNodes, float* centers, float invTheta,
-                      const Box<float>& box, ryo_stream_t stream = nullptr)
+//! cstone::setMacGpu with the vector MAC (float or double centres and box)
+template<class C, class T>
+void setMacGpu(const uint64_t* prefixes, TreeNodeIndex numNodes, C* centers, float invTheta, const Box<T>& box,
+               ryo_stream_t stream = nullptr)
 {
-    ryo_box_f32 b = box.abiF32();
-    check(ryo_set_mac_f32(prefixes, numNodes, centers, invTheta, &b, stream));
+    using Tf = typename detail::Center<C>::value;
+    static_assert(std::is_same_v<Tf, T>, "centres and box of one type");
+    auto* c = reinterpret_cast<Tf*>(centers);
+    if constexpr (std::is_same_v<T, float>)
+    {
+        ryo_box_f32 b = box.abiF32();
+        check(ryo_set_mac_f32(prefixes, numNodes, c, invTheta, &b, stream));
+    }
+    else
+    {
+        ryo_box_f64 b = box.abiF64();
+        check(ryo_set_mac_f64(prefixes, numNodes, c, invTheta, &b, stream));
+    }
 }
 
-//! ryoanji::computeLeafMultipoles (upsweep_gpu.h:24-28), CartesianQuadrupole<float>
-inline void computeLeafMultipoles(const float* x, const float* y, const float* z, const float* m,
-                                  const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
-                                  const LocalIndex* layout, const float* centers, float* multipoles,
-                                  ryo_stream_t stream = nullptr)
+/*! ryoanji::computeLeafMultipoles (upsweep_gpu.h:24-31) for the type sets (Tc, Tm, Tf, MType) = (float, float,
+ *  float, M<float>), (double, double, double, M<double>), (double, float, double, M<float>), M = CartesianQuadrupole
+ *  or CartesianMDQpole; a plain value pointer means CartesianQuadrupole */
+template<class Tc, class Tm, class C, class M>
+void computeLeafMultipoles(const Tc* x, const Tc* y, const Tc* z, const Tm* m, const TreeNodeIndex* leafToInternal,
+                           TreeNodeIndex numLeaves, const LocalIndex* layout, const C* centers, M* multipoles,
+                           ryo_stream_t stream = nullptr)
 {
-    check(ryo_compute_leaf_multipoles_f32(x, y, z, m, leafToInternal, numLeaves, layout, centers, multipoles,
-                                          stream));
-}
-
-//! ryoanji::computeLeafMultipoles with typed expansions (CartesianQuadrupole or CartesianMDQpole)
-inline void computeLeafMultipoles(const float* x, const float* y, const float* z, const float* m,
-                                  const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
-                                  const LocalIndex* layout, const float* centers,
-                                  CartesianQuadrupole<float>* multipoles, ryo_stream_t stream = nullptr)
-{
-    computeLeafMultipoles(x, y, z, m, leafToInternal, numLeaves, layout, centers, multipoles->data(), stream);
-}
-inline void computeLeafMultipoles(const float* x, const float* y, const float* z, const float* m,
-                                  const TreeNodeIndex* leafToInternal, TreeNodeIndex numLeaves,
-                                  const LocalIndex* layout, const float* centers, CartesianMDQpole<float>* multipoles,
-                                  ryo_stream_t stream = nullptr)
-{
-    check(ryo_compute_leaf_multipoles_mdq_f32(x, y, z, m, leafToInternal, numLeaves, layout, centers,
-                                              multipoles->data(), stream));
+    using Tf  = typename detail::Center<C>::value;
+    using Tmp = typename detail::Mpole<M>::value;
+    constexpr bool mdq = detail::Mpole<M>::mdq;
+    const Tf* c        = reinterpret_cast<const Tf*>(centers);
+    Tmp* q             = reinterpret_cast<Tmp*>(multipoles);
+    if constexpr (detail::isF32<Tc, Tm> && std::is_same_v<Tf, float> && std::is_same_v<Tmp, float>)
+        check(mdq ? ryo_compute_leaf_multipoles_mdq_f32(x, y, z, m, leafToInternal, numLeaves, layout, c, q, stream)
+                  : ryo_compute_leaf_multipoles_f32(x, y, z, m, leafToInternal, numLeaves, layout, c, q, stream));
+    else if constexpr (detail::isF64<Tc, Tm> && std::is_same_v<Tf, double> && std::is_same_v<Tmp, double>)
+        check(mdq ? ryo_compute_leaf_multipoles_mdq_f64(x, y, z, m, leafToInternal, numLeaves, layout, c, q, stream)
+                  : ryo_compute_leaf_multipoles_f64(x, y, z, m, leafToInternal, numLeaves, layout, c, q, stream));
+    else if constexpr (detail::isMixed<Tc, Tm> && std::is_same_v<Tf, double> && std::is_same_v<Tmp, float>)
+        check(mdq ? ryo_compute_leaf_multipoles_mdq_mixed(x, y, z, m, leafToInternal, numLeaves, layout, c, q, stream)
+                  : ryo_compute_leaf_multipoles_mixed(x, y, z, m, leafToInternal, numLeaves, layout, c, q, stream));
+    else
+        static_assert(detail::alwaysFalse<M>, "not an instantiated type set");
 }
 
 //! ryoanji::upsweepMultipoles (upsweep_gpu.h:39-41) for cells [firstCell, lastCell) of one level
-inline void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
-                              const float* centers, float* multipoles, ryo_stream_t stream = nullptr)
+template<class C, class M>
+void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
+                       const C* centers, M* multipoles, ryo_stream_t stream = nullptr)
 {
-    check(ryo_upsweep_multipoles_f32(firstCell, lastCell, childOffsets, centers, multipoles, stream));
-}
-
-inline void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
-                              const float* centers, CartesianQuadrupole<float>* multipoles,
-                              ryo_stream_t stream = nullptr)
-{
-    upsweepMultipoles(firstCell, lastCell, childOffsets, centers, multipoles->data(), stream);
-}
-inline void upsweepMultipoles(TreeNodeIndex firstCell, TreeNodeIndex lastCell, const TreeNodeIndex* childOffsets,
-                              const float* centers, CartesianMDQpole<float>* multipoles, ryo_stream_t stream = nullptr)
-{
-    check(ryo_upsweep_multipoles_mdq_f32(firstCell, lastCell, childOffsets, centers, multipoles->data(), stream));
+    using Tf  = typename detail::Center<C>::value;
+    using Tmp = typename detail::Mpole<M>::value;
+    constexpr bool mdq = detail::Mpole<M>::mdq;
+    const Tf* c        = reinterpret_cast<const Tf*>(centers);
+    Tmp* q             = reinterpret_cast<Tmp*>(multipoles);
+    if constexpr (std::is_same_v<Tf, float> && std::is_same_v<Tmp, float>)
+        check(mdq ? ryo_upsweep_multipoles_mdq_f32(firstCell, lastCell, childOffsets, c, q, stream)
+                  : ryo_upsweep_multipoles_f32(firstCell, lastCell, childOffsets, c, q, stream));
+    else if constexpr (std::is_same_v<Tf, double> && std::is_same_v<Tmp, double>)
+        check(mdq ? ryo_upsweep_multipoles_mdq_f64(firstCell, lastCell, childOffsets, c, q, stream)
+                  : ryo_upsweep_multipoles_f64(firstCell, lastCell, childOffsets, c, q, stream));
+    else if constexpr (std::is_same_v<Tf, double> && std::is_same_v<Tmp, float>)
+        check(mdq ? ryo_upsweep_multipoles_mdq_mixed(firstCell, lastCell, childOffsets, c, q, stream)
+                  : ryo_upsweep_multipoles_mixed(firstCell, lastCell, childOffsets, c, q, stream));
+    else
+        static_assert(detail::alwaysFalse<M>, "not an instantiated type set");
 }
 
 /*! cstone::computeGroupSplits (groups_gpu.cu:60-151): spatial target groups of SFC-sorted bodies [first, last) into
@@ -405,44 +483,46 @@ inline LocalIndex computeGroupSplits(LocalIndex first, LocalIndex last, const fl
 inline int bhMaxTargetSize() { return ryo_bh_max_target_size(); }
 inline LocalIndex stackSize(LocalIndex numGroups) { return ryo_stack_size(numGroups); }
 
-/*! ryoanji::traverse (traversal_gpu.h:51-56) for Tc = Th = Tm = Ta = Tf = float, MType = CartesianQuadrupole<float>.
+/*! ryoanji::traverse (traversal_gpu.h:51-56) for the instantiated type sets (traversal_gpu.cu:635-641): (Tc, Th,
+ *  Tm, Ta, Tf) = all float, all double, or (double, float, float, float, double); MType = CartesianQuadrupole or
+ *  CartesianMDQpole of float (double in the all-double set), or a plain value pointer for CartesianQuadrupole.
  *  Accumulates into p (may be null), ax, ay, az and returns the total potential 0.5 G sum m phi. */
-inline double traverse(GroupView grp, int initNodeIdx, const float* xt, const float* yt, const float* zt,
-                       const float* mt, const float* ht, const float* xs, const float* ys, const float* zs,
-                       const float* ms, const float* hs, const TreeNodeIndex* childOffsets,
-                       const TreeNodeIndex* internalToLeaf, const LocalIndex* layout, const float* sourceCenter,
-                       const float* multipoles, float G, int numShells, Vec3<float> boxL, float* p, float* ax,
-                       float* ay, float* az, int* /* gmPool: unused */, Context& ctx = defaultContext(),
-                       ryo_stream_t stream = nullptr)
+template<class Tc, class Th, class Tm, class Ta, class C, class M>
+double traverse(GroupView grp, int initNodeIdx, const Tc* xt, const Tc* yt, const Tc* zt, const Tm* mt, const Th* ht,
+                const Tc* xs, const Tc* ys, const Tc* zs, const Tm* ms, const Th* hs,
+                const TreeNodeIndex* childOffsets, const TreeNodeIndex* internalToLeaf, const LocalIndex* layout,
+                const C* sourceCenter, const M* multipoles, Tc G, int numShells, Vec3<Tc> boxL, Ta* p, Ta* ax, Ta* ay,
+                Ta* az, int* /* gmPool: unused */, Context& ctx = defaultContext(), ryo_stream_t stream = nullptr)
 {
+    using Tf  = typename detail::Center<C>::value;
+    using Tmp = typename detail::Mpole<M>::value;
     ryo_group_view g = grp.abi();
-    float L[3]       = {boxL.x, boxL.y, boxL.z};
-    double total     = 0;
-    check(ryo_traverse_f32(ctx.get(), &g, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
-                           internalToLeaf, layout, sourceCenter, multipoles, G, numShells, L, p, ax, ay, az, &total,
-                           stream),
-          ctx.get());
-    return total;
-}
-
-//! ryoanji::traverse with CartesianMDQpole multipoles (TRAVERSE_MPOLE(CartesianMDQpole), traversal_gpu.cu:641)
-inline double traverse(GroupView grp, int initNodeIdx, const float* xt, const float* yt, const float* zt,
-                       const float* mt, const float* ht, const float* xs, const float* ys, const float* zs,
-                       const float* ms, const float* hs, const TreeNodeIndex* childOffsets,
-                       const TreeNodeIndex* internalToLeaf, const LocalIndex* layout, const float* sourceCenter,
-                       const CartesianMDQpole<float>* multipoles, float G, int numShells, Vec3<float> boxL, float* p,
-                       float* ax, float* ay, float* az, int* /* gmPool: unused */, Context& ctx = defaultContext(),
-                       ryo_stream_t stream = nullptr)
-{
-    ryo_group_view g = grp.abi();
-    float L[3]       = {boxL.x, boxL.y, boxL.z};
     double total     = 0;
     ryo_traverse_options opt{};
-    opt.multipole = RYO_MULTIPOLE_MDQ;
-    check(ryo_traverse_ex_f32(ctx.get(), &g, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
-                              internalToLeaf, layout, sourceCenter, multipoles->data(), G, numShells, L, p, ax, ay,
-                              az, &total, &opt, stream),
-          ctx.get());
+    opt.multipole = detail::Mpole<M>::mdq ? RYO_MULTIPOLE_MDQ : RYO_MULTIPOLE_QUADRUPOLE;
+    const Tf* c   = reinterpret_cast<const Tf*>(sourceCenter);
+    const Tmp* q  = reinterpret_cast<const Tmp*>(multipoles);
+    Tc L[3]       = {boxL.x, boxL.y, boxL.z};
+    constexpr bool f32 = detail::isF32<Tc, Tm> && std::is_same_v<Th, float> && std::is_same_v<Ta, float> &&
+                         std::is_same_v<Tf, float> && std::is_same_v<Tmp, float>;
+    constexpr bool f64 = detail::isF64<Tc, Tm> && std::is_same_v<Th, double> && std::is_same_v<Ta, double> &&
+                         std::is_same_v<Tf, double> && std::is_same_v<Tmp, double>;
+    constexpr bool mixed = detail::isMixed<Tc, Tm> && std::is_same_v<Th, float> && std::is_same_v<Ta, float> &&
+                           std::is_same_v<Tf, double> && std::is_same_v<Tmp, float>;
+    if constexpr (f32)
+        check(ryo_traverse_ex_f32(ctx.get(), &g, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
+                                  internalToLeaf, layout, c, q, G, numShells, L, p, ax, ay, az, &total, &opt, stream),
+              ctx.get());
+    else if constexpr (f64)
+        check(ryo_traverse_f64(ctx.get(), &g, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
+                               internalToLeaf, layout, c, q, G, numShells, L, p, ax, ay, az, &total, &opt, stream),
+              ctx.get());
+    else if constexpr (mixed)
+        check(ryo_traverse_mixed(ctx.get(), &g, initNodeIdx, xt, yt, zt, mt, ht, xs, ys, zs, ms, hs, childOffsets,
+                                 internalToLeaf, layout, c, q, G, numShells, L, p, ax, ay, az, &total, &opt, stream),
+              ctx.get());
+    else
+        static_assert(detail::alwaysFalse<M>, "not an instantiated type set");
     return total;
 }
 

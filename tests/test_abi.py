@@ -141,3 +141,16 @@ def test_public_api_is_exported():
     own = [n for n, v in vars(ryo).items() if not n.startswith("_") and (inspect.isfunction(v) or inspect.isclass(v))
            and getattr(v, "__module__", "") == ryo.__name__]
     assert set(own) <= set(ryo.__all__), set(own) - set(ryo.__all__)
+
+
+def test_compat_demo_flow_compiles_and_links(tmp_path):
+    """the reference demo's flow in the reference's own spellings (cstone::, ryoanji::, execution::Gpu) builds against
+    ryoanji_b200/compat.hpp and this library, for all three type sets"""
+    from ryoanji_b200._abi import LIB_PATH
+    exe = tmp_path / "demo_flow"
+    libdir = os.path.dirname(LIB_PATH)
+    r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I",
+                        "/usr/local/cuda/include", os.path.join(ROOT, "tests", "cpp", "demo_flow.cpp"), "-o", str(exe),
+                        "-L", libdir, "-lryoanji_b200", "-L", "/usr/local/cuda/lib64", "-lcudart",
+                        f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
