@@ -337,6 +337,22 @@ extern "C"
                                                      const float* z, const float* m, const ryo_box_f32* box, float G,
                                                      float* ugrav, float* ax, float* ay, float* az, double* ugravTot,
                                                      const ryo_ewald_settings* settings, ryo_stream_t stream);
+    /* the double-coordinate instantiations (COMPUTE_GRAVITY_EWALD_GPU, ewald.cu:101-110): _f64 is
+     * (CartesianQuadrupole<double or float>, double, double, double, double), the root expansion given as 8 doubles;
+     * _mixed is (CartesianQuadrupole<float>, double, float, float, double). The real-space images run in double
+     * there, as the reference's run in its coordinate type. */
+    RYO_API ryo_status ryo_compute_gravity_ewald_f64(ryo_ctx_t* ctx, const double* rootCenter, const double* Mroot,
+                                                     const ryo_group_view* grp, const double* x, const double* y,
+                                                     const double* z, const double* m, const ryo_box_f64* box,
+                                                     float G, double* ugrav, double* ax, double* ay, double* az,
+                                                     double* ugravTot, const ryo_ewald_settings* settings,
+                                                     ryo_stream_t stream);
+    RYO_API ryo_status ryo_compute_gravity_ewald_mixed(ryo_ctx_t* ctx, const double* rootCenter, const float* Mroot,
+                                                       const ryo_group_view* grp, const double* x, const double* y,
+                                                       const double* z, const float* m, const ryo_box_f64* box,
+                                                       float G, float* ugrav, float* ax, float* ay, float* az,
+                                                       double* ugravTot, const ryo_ewald_settings* settings,
+                                                       ryo_stream_t stream);
 
     /* ------------------------------------------------------------------------------------------ direct sums */
 

@@ -235,13 +235,12 @@ inline LocalIndex stackSize(LocalIndex numGroups) { return ryo::stackSize(numGro
 inline std::array<uint64_t, 5> readBhStats() { return ryo::readBhStats(); }
 inline uint64_t readTraversalRetries() { return ryo::readTraversalRetries(); }
 
-/*! ryoanji::computeGravityEwaldGpu (ryoanji/src/ryoanji/interface/ewald.cuh:24-27) for the float set
- *  (CartesianQuadrupole<float>, float, float, float, float) */
-template<class Tu>
-void computeGravityEwaldGpu(const Vec3<float>& rootCenter, const CartesianQuadrupole<float>& Mroot,
-                            cstone::GroupView grp, const float* x, const float* y, const float* z, const float* m,
-                            const cstone::Box<float>& box, float G, float* ugrav, float* ax, float* ay, float* az,
-                            Tu* ugravTot, EwaldSettings settings)
+/*! ryoanji::computeGravityEwaldGpu (ryoanji/src/ryoanji/interface/ewald.cuh:24-27) for the reference's instantiated
+ *  sets (ewald.cu:101-110) */
+template<class MType, class Tc, class Ta, class Tm, class Tu>
+void computeGravityEwaldGpu(const Vec3<Tc>& rootCenter, const MType& Mroot, cstone::GroupView grp, const Tc* x,
+                            const Tc* y, const Tc* z, const Tm* m, const cstone::Box<Tc>& box, float G, Ta* ugrav,
+                            Ta* ax, Ta* ay, Ta* az, Tu* ugravTot, EwaldSettings settings)
 {
     ryo_ewald_settings s{settings.numReplicaShells, settings.lCut, settings.hCut, settings.alpha_scale,
                          settings.small_R_scale_factor};

@@ -558,20 +558,44 @@ inline ryo_ewald_settings defaultEwaldSettings()
     return e;
 }
 
-/*! ryoanji::computeGravityEwaldGpu (interface/ewald.cuh:24-27) for MType = CartesianQuadrupole<float>; Mroot is
- *  the root's 8 multipole floats (host). Adds the Ewald correction to ugrav, ax, ay, az and to *ugravTot. */
-inline void computeGravityEwaldGpu(const Vec3<float>& rootCenter, const float* Mroot, GroupView grp, const float* x,
-                                   const float* y, const float* z, const float* m, const Box<float>& box, float G,
-                                   float* ugrav, float* ax, float* ay, float* az, double* ugravTot,
-                                   const ryo_ewald_settings& settings, Context& ctx = defaultContext(),
-                                   ryo_stream_t stream = nullptr)
+/*! ryoanji::computeGravityEwaldGpu (interface/ewald.cuh:24-27) for the instantiated sets (ewald.cu:101-110): float
+ *  coordinates, masses and outputs with float Mroot; double everything (Mroot double or float); double coordinates
+ *  with float masses and outputs and float Mroot. Mroot is the root's 8 multipole values (host). Adds the Ewald
+ *  correction to ugrav, ax, ay, az and to *ugravTot. */
+template<class Tc, class Tr, class Tm, class Ta>
+void computeGravityEwaldGpu(const Vec3<Tc>& rootCenter, const Tr* Mroot, GroupView grp, const Tc* x, const Tc* y,
+                            const Tc* z, const Tm* m, const Box<Tc>& box, float G, Ta* ugrav, Ta* ax, Ta* ay, Ta* az,
+                            double* ugravTot, const ryo_ewald_settings& settings, Context& ctx = defaultContext(),
+                            ryo_stream_t stream = nullptr)
 {
     ryo_group_view g = grp.abi();
-    ryo_box_f32 b    = box.abiF32();
-    float rc[3]      = {rootCenter.x, rootCenter.y, rootCenter.z};
-    check(ryo_compute_gravity_ewald_f32(ctx.get(), rc, Mroot, &g, x, y, z, m, &b, G, ugrav, ax, ay, az, ugravTot,
-                                        &settings, stream),
-          ctx.get());
+    Tc rc[3]         = {rootCenter.x, rootCenter.y, rootCenter.z};
+    if constexpr (detail::isF32<Tc, Tm> && std::is_same_v<Ta, float> && std::is_same_v<Tr, float>)
+    {
+        ryo_box_f32 b = box.abiF32();
+        check(ryo_compute_gravity_ewald_f32(ctx.get(), rc, Mroot, &g, x, y, z, m, &b, G, ugrav, ax, ay, az, ugravTot,
+                                            &settings, stream),
+              ctx.get());
+    }
+    else if constexpr (detail::isF64<Tc, Tm> && std::is_same_v<Ta, double>)
+    {
+        ryo_box_f64 b = box.abiF64();
+        double mr[8];
+        for (int i = 0; i < 8; ++i)
+            mr[i] = double(Mroot[i]);
+        check(ryo_compute_gravity_ewald_f64(ctx.get(), rc, mr, &g, x, y, z, m, &b, G, ugrav, ax, ay, az, ugravTot,
+                                            &settings, stream),
+              ctx.get());
+    }
+    else if constexpr (detail::isMixed<Tc, Tm> && std::is_same_v<Ta, float> && std::is_same_v<Tr, float>)
+    {
+        ryo_box_f64 b = box.abiF64();
+        check(ryo_compute_gravity_ewald_mixed(ctx.get(), rc, Mroot, &g, x, y, z, m, &b, G, ugrav, ax, ay, az,
+                                              ugravTot, &settings, stream),
+              ctx.get());
+    }
+    else
+        static_assert(detail::alwaysFalse<Tr>, "not an instantiated type set");
 }
 
 //! ryoanji::directSum (interface/multipole_holder.cuh:91-93): exact sums for targets [first, last)

@@ -20,6 +20,7 @@
 #include "cstone/cuda/device_vector.h"
 #include "cstone/focus/source_center_gpu.h"
 #include "cstone/traversal/groups_gpu.h"
+#include "ryoanji/interface/ewald.cuh"
 #include "ryoanji/interface/treebuilder.cuh"
 #include "ryoanji/nbody/cartesian_qpole.hpp"
 #include "ryoanji/nbody/traversal_gpu.h"
@@ -303,6 +304,60 @@ extern "C"
         for (auto& e : ev)
             cudaEventDestroy(e);
         return pot;
+    }
+
+    /*! ryoanji::computeGravityEwaldGpu (ryoanji/src/ryoanji/interface/ewald.cu:64-99) over the groups [gStart, gEnd)
+     *  (device) of a cubic box (box6 host); settings5 = numReplicaShells, lCut, hCut, alpha_scale,
+     *  small_R_scale_factor; returns the increment of *ugravTot. kind 0: (Quad<float>, float, float, float, float);
+     *  1: (Quad<double>, double, double, double, double); 2: (Quad<float>, double, float, float, double). Coordinates,
+     *  masses and outputs follow the kind; rootCenter and Mroot are host doubles. */
+    double ref_gpu_ewald(int kind, const double* rootCenter3, const double* mroot8, uint32_t first, uint32_t last,
+                         uint32_t numGroups, const uint32_t* gStart, const uint32_t* gEnd, const void* x, const void* y,
+                         const void* z, const void* m, const double* box6, float G, void* ugrav, void* ax, void* ay,
+                         void* az, const double* settings5)
+    {
+        if (numGroups == 0) return 0.0;
+        cstone::GroupView grp{first, last, numGroups, gStart, gEnd};
+        ryoanji::EwaldSettings es{int(settings5[0]), settings5[1], settings5[2], settings5[3], settings5[4]};
+        double total = 0;
+        if (kind == 0)
+        {
+            cstone::Vec3<float> rc{float(rootCenter3[0]), float(rootCenter3[1]), float(rootCenter3[2])};
+            ryoanji::CartesianQuadrupole<float> M;
+            for (int i = 0; i < 8; ++i)
+                M[i] = float(mroot8[i]);
+            float tot = 0;
+            cstone::Box<float> box(box6[0], box6[1], box6[2], box6[3], box6[4], box6[5]);
+            ryoanji::computeGravityEwaldGpu(rc, M, grp, (const float*)x, (const float*)y, (const float*)z,
+                                            (const float*)m, box, G, (float*)ugrav, (float*)ax, (float*)ay,
+                                            (float*)az, &tot, es);
+            total = tot;
+        }
+        else
+        {
+            cstone::Vec3<double> rc{rootCenter3[0], rootCenter3[1], rootCenter3[2]};
+            cstone::Box<double> box(box6[0], box6[1], box6[2], box6[3], box6[4], box6[5]);
+            if (kind == 1)
+            {
+                ryoanji::CartesianQuadrupole<double> M;
+                for (int i = 0; i < 8; ++i)
+                    M[i] = mroot8[i];
+                ryoanji::computeGravityEwaldGpu(rc, M, grp, (const double*)x, (const double*)y, (const double*)z,
+                                                (const double*)m, box, G, (double*)ugrav, (double*)ax, (double*)ay,
+                                                (double*)az, &total, es);
+            }
+            else
+            {
+                ryoanji::CartesianQuadrupole<float> M;
+                for (int i = 0; i < 8; ++i)
+                    M[i] = float(mroot8[i]);
+                ryoanji::computeGravityEwaldGpu(rc, M, grp, (const double*)x, (const double*)y, (const double*)z,
+                                                (const float*)m, box, G, (float*)ugrav, (float*)ax, (float*)ay,
+                                                (float*)az, &total, es);
+            }
+        }
+        cudaDeviceSynchronize();
+        return total;
     }
 
     //! the last CUDA error of this library's runtime (0 = none); clears it

@@ -400,14 +400,16 @@ def compute_gravity_ewald(root_center, m_root, groups: torch.Tensor, x, y, z, m,
     settings = settings or EwaldSettings()
     ng = groups.numel() - 1
     gv = _abi.GroupView(0, x.numel(), ng, C.c_void_p(groups.data_ptr()), C.c_void_p(groups.data_ptr() + 4))
-    rc = (C.c_float * 3)(*[float(v) for v in root_center])
-    mr = (C.c_float * 8)(*[float(v) for v in m_root])
-    b = box.f32()
+    kind = _type_set(x, m)  # f32, f64 (double everything) or mixed (double coordinates, float masses and outputs)
+    real = C.c_float if kind == "f32" else C.c_double
+    rc = (real * 3)(*[float(v) for v in root_center])
+    mr = ((C.c_double if kind == "f64" else C.c_float) * 8)(*[float(v) for v in m_root])
+    b = box.f32() if kind == "f32" else box.f64()
     tot = C.c_double(0)
     s = settings.c()
-    _check(lib.ryo_compute_gravity_ewald_f32(ctx.handle, rc, mr, C.byref(gv), _ptr(x), _ptr(y), _ptr(z), _ptr(m),
-                                             C.byref(b), C.c_float(G), _ptr(ugrav), _ptr(ax), _ptr(ay), _ptr(az),
-                                             C.byref(tot), C.byref(s), _stream(stream, ctx)), ctx)
+    fn = getattr(lib, "ryo_compute_gravity_ewald_" + kind)
+    _check(fn(ctx.handle, rc, mr, C.byref(gv), _ptr(x), _ptr(y), _ptr(z), _ptr(m), C.byref(b), C.c_float(G),
+              _ptr(ugrav), _ptr(ax), _ptr(ay), _ptr(az), C.byref(tot), C.byref(s), _stream(stream, ctx)), ctx)
     return tot.value
 
 

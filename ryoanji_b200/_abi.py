@@ -170,6 +170,12 @@ SIGNATURES = {
     "ryo_compute_gravity_ewald_f32": (_i, [_p, C.POINTER(_f), C.POINTER(_f), C.POINTER(GroupView), _p, _p, _p, _p,
                                            C.POINTER(BoxF32), _f, _p, _p, _p, _p, C.POINTER(_d),
                                            C.POINTER(EwaldSettings), _p]),
+    "ryo_compute_gravity_ewald_f64": (_i, [_p, C.POINTER(_d), C.POINTER(_d), C.POINTER(GroupView), _p, _p, _p, _p,
+                                           C.POINTER(BoxF64), _f, _p, _p, _p, _p, C.POINTER(_d),
+                                           C.POINTER(EwaldSettings), _p]),
+    "ryo_compute_gravity_ewald_mixed": (_i, [_p, C.POINTER(_d), C.POINTER(_f), C.POINTER(GroupView), _p, _p, _p, _p,
+                                             C.POINTER(BoxF64), _f, _p, _p, _p, _p, C.POINTER(_d),
+                                             C.POINTER(EwaldSettings), _p]),
     "ryo_direct_sum_f32": (_i, [_sz, _sz, _sz, C.POINTER(_f), _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "ryo_direct_sum_f64": (_i, [_sz, _sz, _sz, C.POINTER(_d), _i, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
     "ryo_direct_targets_f64": (_i, [_p, _sz, _p, _p, _p, _p, _p, _sz, _d, C.POINTER(_d), _i, _p, _p, _p, _p, _p]),

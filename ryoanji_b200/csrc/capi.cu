@@ -840,11 +840,14 @@ extern "C" uint64_t ryo_read_traversal_retries(ryo_ctx_t* ctx) { return ctx ? ct
 
 // ==================================================================================================== Ewald
 
-extern "C" ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float* rootCenter, const float* Mroot,
-                                                    const ryo_group_view* grp, const float* x, const float* y,
-                                                    const float* z, const float* m, const ryo_box_f32* box, float G,
-                                                    float* ugrav, float* ax, float* ay, float* az, double* ugravTot,
-                                                    const ryo_ewald_settings* settings, ryo_stream_t stream)
+namespace
+{
+//! computeGravityEwaldGpu for one type set: Tr the root expansion's values, Tc coordinates and box, Tm masses, Ta
+//! outputs (ryoanji/src/ryoanji/interface/ewald.cu:31-110)
+template<class Tr, class Tc, class Tm, class Ta, class Box>
+ryo_status gravityEwald(ryo_ctx_t* ctx, const Tc* rootCenter, const Tr* Mroot, const ryo_group_view* grp, const Tc* x,
+                        const Tc* y, const Tc* z, const Tm* m, const Box* box, float G, Ta* ugrav, Ta* ax, Ta* ay,
+                        Ta* az, double* ugravTot, const ryo_ewald_settings* settings, ryo_stream_t stream)
 {
     if (!ctx) return RYO_ERR_BAD_ARG;
     return guardedCtx(ctx,
@@ -853,14 +856,14 @@ extern "C" ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float*
                        checkEwald(settings);
                        REQUIRE(rootCenter && Mroot && grp && x && y && z && m && box && ax && ay && az && settings,
                                "compute_gravity_ewald: null argument");
-                       float lx = box->limits[1] - box->limits[0], ly = box->limits[3] - box->limits[2],
-                             lz = box->limits[5] - box->limits[4];
+                       Tc lx = box->limits[1] - box->limits[0], ly = box->limits[3] - box->limits[2],
+                          lz = box->limits[5] - box->limits[4];
                        if (!(lx == ly && ly == lz)) throw ApiError{RYO_ERR_NOT_CUBIC, "Ewald needs a cubic box"};
                        double mr[8], c[3];
                        for (int i = 0; i < 8; ++i)
-                           mr[i] = Mroot[i];
+                           mr[i] = double(Mroot[i]);
                        for (int i = 0; i < 3; ++i)
-                           c[i] = rootCenter[i];
+                           c[i] = double(rootCenter[i]);
                        EwaldHost e = ewaldSetup(mr, c, settings->numReplicaShells, double(lx), settings->lCut,
                                                 settings->hCut, settings->alpha_scale,
                                                 settings->small_R_scale_factor);
@@ -873,6 +876,39 @@ extern "C" ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float*
                        RYO_CUDA(cudaStreamSynchronize(stream));
                        if (ugravTot) *ugravTot += 0.5 * double(G) * h;
                    });
+}
+} // namespace
+
+extern "C" ryo_status ryo_compute_gravity_ewald_f32(ryo_ctx_t* ctx, const float* rootCenter, const float* Mroot,
+                                                    const ryo_group_view* grp, const float* x, const float* y,
+                                                    const float* z, const float* m, const ryo_box_f32* box, float G,
+                                                    float* ugrav, float* ax, float* ay, float* az, double* ugravTot,
+                                                    const ryo_ewald_settings* settings, ryo_stream_t stream)
+{
+    return gravityEwald(ctx, rootCenter, Mroot, grp, x, y, z, m, box, G, ugrav, ax, ay, az, ugravTot, settings,
+                        stream);
+}
+
+extern "C" ryo_status ryo_compute_gravity_ewald_f64(ryo_ctx_t* ctx, const double* rootCenter, const double* Mroot,
+                                                    const ryo_group_view* grp, const double* x, const double* y,
+                                                    const double* z, const double* m, const ryo_box_f64* box, float G,
+                                                    double* ugrav, double* ax, double* ay, double* az,
+                                                    double* ugravTot, const ryo_ewald_settings* settings,
+                                                    ryo_stream_t stream)
+{
+    return gravityEwald(ctx, rootCenter, Mroot, grp, x, y, z, m, box, G, ugrav, ax, ay, az, ugravTot, settings,
+                        stream);
+}
+
+extern "C" ryo_status ryo_compute_gravity_ewald_mixed(ryo_ctx_t* ctx, const double* rootCenter, const float* Mroot,
+                                                      const ryo_group_view* grp, const double* x, const double* y,
+                                                      const double* z, const float* m, const ryo_box_f64* box,
+                                                      float G, float* ugrav, float* ax, float* ay, float* az,
+                                                      double* ugravTot, const ryo_ewald_settings* settings,
+                                                      ryo_stream_t stream)
+{
+    return gravityEwald(ctx, rootCenter, Mroot, grp, x, y, z, m, box, G, ugrav, ax, ay, az, ugravTot, settings,
+                        stream);
 }
 
 // ==================================================================================================== direct sums

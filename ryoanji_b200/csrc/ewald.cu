@@ -16,12 +16,14 @@
 namespace ryo
 {
 
+//! kernel constants; R is the real-space type (float for float coordinates, double otherwise)
+template<class R>
 struct EwaldKernelParams
 {
-    float mroot[8];
-    float center[3];
+    R mroot[8];
+    R center[3];
     double centerD[3];
-    float L, lCut2, alpha, alpha2, k1, ka, smallR2;
+    R L, lCut2, alpha, alpha2, k1, ka, smallR2;
     int replicaShells, ewaldShells;
     int numK;
     double twoPiOverL;
@@ -103,10 +105,24 @@ EwaldHost ewaldSetup(const double* mroot, const double* center, int replicaShell
 
 __device__ inline double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 
-__global__ void ewaldKernel(const __grid_constant__ EwaldKernelParams E, const uint32_t* __restrict__ groupStart,
-                            const uint32_t* __restrict__ groupEnd, uint32_t numGroups, const float* __restrict__ x,
-                            const float* __restrict__ y, const float* __restrict__ z, const float* __restrict__ m,
-                            float G, float* ugrav, float* ax, float* ay, float* az, double* potential)
+// the real-space functions in the real-space type
+__device__ inline float rsSqrt(float v) { return sqrtf(v); }
+__device__ inline double rsSqrt(double v) { return sqrt(v); }
+__device__ inline float rsExp(float v) { return expf(v); }
+__device__ inline double rsExp(double v) { return exp(v); }
+__device__ inline float rsErf(float v) { return erff(v); }
+__device__ inline double rsErf(double v) { return erf(v); }
+__device__ inline float rsErfc(float v) { return erfcf(v); }
+__device__ inline double rsErfc(double v) { return erfc(v); }
+
+/*! one warp per target group. R is the real-space type: float for the reference's float instantiation, double for its
+ *  double-coordinate ones (ryoanji/src/ryoanji/interface/ewald.cu:101-110), where the reference's real space runs in
+ *  its coordinate type; the reciprocal sum is double in every set. Tc, Tm, Ta: coordinates, masses, outputs. */
+template<class R, class Tc, class Tm, class Ta>
+__global__ void ewaldKernel(const __grid_constant__ EwaldKernelParams<R> E, const uint32_t* __restrict__ groupStart,
+                            const uint32_t* __restrict__ groupEnd, uint32_t numGroups, const Tc* __restrict__ x,
+                            const Tc* __restrict__ y, const Tc* __restrict__ z, const Tm* __restrict__ m, float G,
+                            Ta* ugrav, Ta* ax, Ta* ay, Ta* az, double* potential)
 {
     int warpGlobal = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
     int lane       = laneId();
@@ -116,41 +132,41 @@ __global__ void ewaldKernel(const __grid_constant__ EwaldKernelParams E, const u
         uint32_t b = groupStart[warpGlobal], e = groupEnd[warpGlobal];
         for (uint32_t i = b + lane; i < e; i += kWarp)
         {
-            float pos[3]  = {x[i], y[i], z[i]};
-            float acc[4]  = {E.k1 * E.mroot[0], 0.f, 0.f, 0.f};
-            float r[3]    = {pos[0] - E.center[0], pos[1] - E.center[1], pos[2] - E.center[2]};
-            int S         = E.ewaldShells, Rs = E.replicaShells;
+            R pos[3]  = {R(x[i]), R(y[i]), R(z[i])};
+            R acc[4]  = {E.k1 * E.mroot[0], R(0), R(0), R(0)};
+            R r[3]    = {pos[0] - E.center[0], pos[1] - E.center[1], pos[2] - E.center[2]};
+            int S     = E.ewaldShells, Rs = E.replicaShells;
             // real space (ewald.hpp:200-301)
             for (int ix = -S; ix <= S; ++ix)
                 for (int iy = -S; iy <= S; ++iy)
                     for (int iz = -S; iz <= S; ++iz)
                     {
-                        bool pre  = (-Rs <= ix && ix <= Rs) && (-Rs <= iy && iy <= Rs) && (-Rs <= iz && iz <= Rs);
-                        float R[3] = {r[0] + ix * E.L, r[1] + iy * E.L, r[2] + iz * E.L};
-                        float R2   = R[0] * R[0] + (R[1] * R[1] + R[2] * R[2]);
+                        bool pre = (-Rs <= ix && ix <= Rs) && (-Rs <= iy && iy <= Rs) && (-Rs <= iz && iz <= Rs);
+                        R Rv[3]  = {r[0] + ix * E.L, r[1] + iy * E.L, r[2] + iz * E.L};
+                        R R2     = Rv[0] * Rv[0] + (Rv[1] * Rv[1] + Rv[2] * Rv[2]);
                         if (R2 > E.lCut2 && !pre) continue;
-                        float g[6];
-                        if (R2 < E.smallR2 && E.ka > 0.f)
+                        R g[6];
+                        if (R2 < E.smallR2 && E.ka > R(0))
                         {
-                            float c0 = E.ka, a2 = R2 * E.alpha2;
-                            g[0] = c0 * (a2 / 3.f - 1.f);
+                            R c0 = E.ka, a2 = R2 * E.alpha2;
+                            g[0] = c0 * (a2 / R(3) - R(1));
                             c0 *= 2 * E.alpha2;
-                            g[1] = c0 * (a2 / 5.f - 1.f / 3.f);
+                            g[1] = c0 * (a2 / R(5) - R(1) / R(3));
                             c0 *= 2 * E.alpha2;
-                            g[2] = c0 * (a2 / 7.f - 1.f / 5.f);
+                            g[2] = c0 * (a2 / R(7) - R(1) / R(5));
                             c0 *= 2 * E.alpha2;
-                            g[3] = c0 * (a2 / 9.f - 1.f / 7.f);
+                            g[3] = c0 * (a2 / R(9) - R(1) / R(7));
                             c0 *= 2 * E.alpha2;
-                            g[4] = c0 * (a2 / 11.f - 1.f / 9.f);
+                            g[4] = c0 * (a2 / R(11) - R(1) / R(9));
                             c0 *= 2 * E.alpha2;
-                            g[5] = c0 * (a2 / 13.f - 1.f / 11.f);
+                            g[5] = c0 * (a2 / R(13) - R(1) / R(11));
                         }
                         else
                         {
-                            float Rm = sqrtf(R2), iR = 1.f / Rm, iR2 = iR * iR;
-                            float a  = expf(-R2 * E.alpha2) * E.ka * iR2;
-                            float an = 1.f;
-                            float fn = pre ? -erff(E.alpha * Rm) : erfcf(E.alpha * Rm);
+                            R Rm = rsSqrt(R2), iR = R(1) / Rm, iR2 = iR * iR;
+                            R a  = rsExp(-R2 * E.alpha2) * E.ka * iR2;
+                            R an = R(1);
+                            R fn = pre ? -rsErf(E.alpha * Rm) : rsErfc(E.alpha * Rm);
                             g[0] = fn * iR;
                             g[1] = g[0] * iR2 + a;
                             an *= 2 * E.alpha2;
@@ -162,7 +178,7 @@ __global__ void ewaldKernel(const __grid_constant__ EwaldKernelParams E, const u
                             an *= 2 * E.alpha2;
                             g[5] = 9 * g[4] * iR2 + an * a;
                         }
-                        ewaldEval<float>(acc, R, g, E.mroot);
+                        ewaldEval<R>(acc, Rv, g, E.mroot);
                     }
             // reciprocal space (ewald.hpp:303-327), double, exp(i k.r) from powers of the per-axis phases
             double dr[3] = {double(pos[0]) - E.centerD[0], double(pos[1]) - E.centerD[1],
@@ -198,37 +214,38 @@ __global__ void ewaldKernel(const __grid_constant__ EwaldKernelParams E, const u
             double phi = double(acc[0]) + kp;
             double mi  = m[i];
             upot += phi * mi;
-            if (ugrav) ugrav[i] += float(G * phi * mi);
-            ax[i] += float(G * (double(acc[1]) + ka3[0]));
-            ay[i] += float(G * (double(acc[2]) + ka3[1]));
-            az[i] += float(G * (double(acc[3]) + ka3[2]));
+            if (ugrav) ugrav[i] += Ta(G * phi * mi);
+            ax[i] += Ta(G * (double(acc[1]) + ka3[0]));
+            ay[i] += Ta(G * (double(acc[2]) + ka3[1]));
+            az[i] += Ta(G * (double(acc[3]) + ka3[2]));
         }
     }
     upot = warpSum(upot);
     if (lane == 0 && upot != 0.0) atomicAdd(potential, upot);
 }
 
-void launchEwaldGroups(const EwaldHost& h, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
-                       const float* x, const float* y, const float* z, const float* m, float G, float* ugrav,
-                       float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s)
+template<class R, class Tc, class Tm, class Ta>
+static void launchEwaldTyped(const EwaldHost& h, const uint32_t* groupStart, const uint32_t* groupEnd,
+                             uint32_t numGroups, const Tc* x, const Tc* y, const Tc* z, const Tm* m, float G, Ta* ugrav,
+                             Ta* ax, Ta* ay, Ta* az, double* potentialOut, cudaStream_t s)
 {
     if (h.ewaldShells == 0 || numGroups == 0) return;
-    EwaldKernelParams E{};
+    EwaldKernelParams<R> E{};
     for (int i = 0; i < 8; ++i)
-        E.mroot[i] = float(h.mroot[i]);
+        E.mroot[i] = R(h.mroot[i]);
     for (int i = 0; i < 3; ++i)
     {
-        E.center[i]  = float(h.center[i]);
+        E.center[i]  = R(h.center[i]);
         E.centerD[i] = h.center[i];
     }
     double alpha    = h.alphaScale / h.L;
-    E.L             = float(h.L);
-    E.lCut2         = float(h.lCut * h.lCut * h.L * h.L);
-    E.alpha         = float(alpha);
-    E.alpha2        = float(alpha * alpha);
-    E.k1            = float(M_PI / (alpha * alpha * h.L * h.L * h.L));
-    E.ka            = float(2.0 * alpha / std::sqrt(M_PI));
-    E.smallR2       = float(h.smallR * h.L * h.L);
+    E.L             = R(h.L);
+    E.lCut2         = R(h.lCut * h.lCut * h.L * h.L);
+    E.alpha         = R(alpha);
+    E.alpha2        = R(alpha * alpha);
+    E.k1            = R(M_PI / (alpha * alpha * h.L * h.L * h.L));
+    E.ka            = R(2.0 * alpha / std::sqrt(M_PI));
+    E.smallR2       = R(h.smallR * h.L * h.L);
     E.replicaShells = h.replicaShells;
     E.ewaldShells   = h.ewaldShells;
     E.numK          = h.numK;
@@ -242,9 +259,30 @@ void launchEwaldGroups(const EwaldHost& h, const uint32_t* groupStart, const uin
     }
     unsigned threads = 128;
     unsigned blocks  = ceilDiv(size_t(numGroups) * kWarp, threads);
-    ewaldKernel<<<blocks, threads, 0, s>>>(E, groupStart, groupEnd, numGroups, x, y, z, m, G, ugrav, ax, ay, az,
-                                           potentialOut);
+    ewaldKernel<R, Tc, Tm, Ta><<<blocks, threads, 0, s>>>(E, groupStart, groupEnd, numGroups, x, y, z, m, G, ugrav,
+                                                           ax, ay, az, potentialOut);
     RYO_LAUNCH_CHECK();
+}
+
+void launchEwaldGroups(const EwaldHost& h, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
+                       const float* x, const float* y, const float* z, const float* m, float G, float* ugrav,
+                       float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s)
+{
+    launchEwaldTyped<float>(h, groupStart, groupEnd, numGroups, x, y, z, m, G, ugrav, ax, ay, az, potentialOut, s);
+}
+
+void launchEwaldGroups(const EwaldHost& h, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
+                       const double* x, const double* y, const double* z, const double* m, float G, double* ugrav,
+                       double* ax, double* ay, double* az, double* potentialOut, cudaStream_t s)
+{
+    launchEwaldTyped<double>(h, groupStart, groupEnd, numGroups, x, y, z, m, G, ugrav, ax, ay, az, potentialOut, s);
+}
+
+void launchEwaldGroups(const EwaldHost& h, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
+                       const double* x, const double* y, const double* z, const float* m, float G, float* ugrav,
+                       float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s)
+{
+    launchEwaldTyped<double>(h, groupStart, groupEnd, numGroups, x, y, z, m, G, ugrav, ax, ay, az, potentialOut, s);
 }
 
 // ------------------------------------------------------------------------------------------------ FP64 oracle

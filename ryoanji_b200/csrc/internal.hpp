@@ -404,6 +404,13 @@ void launchEwaldTargetsF64(ryo_ctx* ctx, const int64_t* targets, size_t numTarge
 void launchEwaldGroups(const EwaldHost& e, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
                        const float* x, const float* y, const float* z, const float* m, float G, float* ugrav,
                        float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s);
+//! the double-coordinate instantiations: all double, and double coordinates with float masses and outputs
+void launchEwaldGroups(const EwaldHost& e, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
+                       const double* x, const double* y, const double* z, const double* m, float G, double* ugrav,
+                       double* ax, double* ay, double* az, double* potentialOut, cudaStream_t s);
+void launchEwaldGroups(const EwaldHost& e, const uint32_t* groupStart, const uint32_t* groupEnd, uint32_t numGroups,
+                       const double* x, const double* y, const double* z, const float* m, float G, float* ugrav,
+                       float* ax, float* ay, float* az, double* potentialOut, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- probe.cu
 void measurePeaks(int smCount, double* fp32, double* fp32x2, double* copyGBs, cudaStream_t s);

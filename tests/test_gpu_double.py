@@ -182,3 +182,56 @@ def test_mixed_traverse_agrees_with_float_traverse(oracle):
         assert np.percentile(e, 99) < 1e-4
     finally:
         f.close()
+
+
+def _root_expansion(x, y, z, m):
+    """the root's CartesianQuadrupole about its centre of mass (P2M, cartesian_qpole.hpp:67-108), in double"""
+    w = np.abs(m)
+    c = np.array([np.sum(w * a) / w.sum() for a in (x, y, z)])
+    r = [a - ci for a, ci in zip((x, y, z), c)]
+    raw = [np.sum(m * r[i] * r[j]) for i, j in ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))]
+    tr = raw[0] + raw[3] + raw[5]
+    q = [m.sum(), 3 * raw[0] - tr, 3 * raw[1], 3 * raw[2], 3 * raw[3] - tr, 3 * raw[4], 3 * raw[5] - tr, tr]
+    return c, np.array(q)
+
+
+@pytest.mark.parametrize("kind", ["f32", "f64", "mixed"])
+def test_ewald_matches_reference_gpu(kind):
+    """computeGravityEwaldGpu for the three type sets of the reference (ewald.cu:101-110) against the reference's own
+    GPU kernel on the same groups: the correction's accelerations and potentials to the round-off of the set (the
+    reference sums its reciprocal space in the coordinate type, this library in double), and the energy increment"""
+    import ryoanji_b200 as ryo
+    lib = ref_lib()
+    lib.ref_gpu_ewald.restype = C.c_double
+    lib.ref_gpu_ewald.argtypes = ([C.c_int, C.c_void_p, C.c_void_p] + [C.c_uint32] * 3 + [C.c_void_p] * 7 +
+                                  [C.c_void_p, C.c_float] + [C.c_void_p] * 5)
+    p = ds.periodic_box(4096, seed=51, eps=0.01)
+    rng = np.random.default_rng(52)
+    m64 = rng.uniform(0.5, 1.5, p.n) / p.n
+    c, q = _root_expansion(p.x.astype(np.float64), p.y.astype(np.float64), p.z.astype(np.float64), m64)
+    ct = torch.float32 if kind == "f32" else torch.float64
+    mt = torch.float64 if kind == "f64" else torch.float32
+    x, y, z = (torch.from_numpy(a).to("cuda", ct) for a in (p.x, p.y, p.z))
+    m = torch.from_numpy(m64).to("cuda", mt)
+    groups = torch.from_numpy(ref_fixed_groups(p.n).view(np.int32)).cuda()
+    gs, ge = groups[:-1].contiguous(), groups[1:].contiguous()
+    box6 = np.array([0, 1, 0, 1, 0, 1], np.float64)
+    settings = np.array([1, 2.6, 2.8, 2.0, 3.0e-3], np.float64)
+    ref = [torch.zeros(p.n, dtype=mt, device="cuda") for _ in range(4)]
+    torch.cuda.synchronize()
+    rtot = lib.ref_gpu_ewald({"f32": 0, "f64": 1, "mixed": 2}[kind], c.ctypes.data_as(C.c_void_p),
+                             q.ctypes.data_as(C.c_void_p), 0, p.n, int(gs.numel()), _ptr(gs), _ptr(ge), _ptr(x),
+                             _ptr(y), _ptr(z), _ptr(m), box6.ctypes.data_as(C.c_void_p), C.c_float(1.0),
+                             *[_ptr(t) for t in ref], settings.ctypes.data_as(C.c_void_p))
+    assert lib.ref_gpu_last_error() == 0
+    ours = [torch.zeros(p.n, dtype=mt, device="cuda") for _ in range(4)]
+    box = ryo.Box(0.0, 1.0, 0.0, 1.0, 0.0, 1.0, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
+    tot = ryo.compute_gravity_ewald(c, q, groups, x, y, z, m, box, 1.0, *ours)
+    a_ref = np.stack([host(t).astype(np.float64) for t in ref[1:]])
+    a_our = np.stack([host(t).astype(np.float64) for t in ours[1:]])
+    scale = np.abs(a_ref).max()
+    tol = {"f32": 2e-5, "f64": 1e-9, "mixed": 2e-6}[kind]
+    assert np.abs(a_our - a_ref).max() <= tol * scale, (np.abs(a_our - a_ref).max() / scale)
+    u_ref, u_our = host(ref[0]).astype(np.float64), host(ours[0]).astype(np.float64)
+    assert np.abs(u_our - u_ref).max() <= tol * np.abs(u_ref).max()
+    assert abs(tot - rtot) <= 1e-5 * abs(rtot)
