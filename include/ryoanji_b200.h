@@ -321,6 +321,26 @@ extern "C"
                                           float* p, float* ax, float* ay, float* az, double* totalPotential,
                                           const ryo_traverse_options* options, ryo_stream_t stream);
 
+    /* The locally essential tree of the last ryo_solve_f32 on this context for another rank's domain, the exchange
+     * step of a system spread over several GPUs (cstone/include/cstone/focus/octree_focus_mpi.hpp:629, globalExchange,
+     * and the peer exchange it feeds). peerBox6 (host: xmin, xmax, ymin, ymax, zmin, zmax) bounds the other rank's
+     * bodies. A node is exported iff every strict ancestor below the root fails the MAC against that box; a node
+     * that fails it keeps its eight children (internal) or sends its bodies (leaf); one that passes is sent as a
+     * multipole without children or bodies. The export is one packed buffer of 32-bit words (counts->words of them;
+     * N nodes, L leaves with bodies, B bodies): centres [0, 4N), multipoles [4N, 12N) (8 floats), childOffsets
+     * [12N, 13N), internalToLeaf [13N, 14N), layout [14N, 14N + L + 2), then x, y, z, m, h of the bodies (B each).
+     * ryo_traverse_f32 evaluates it as the source tree of the other rank's targets (initNodeIdx 1, or 0 if N is 1).
+     * Writes *counts always; RYO_ERR_CAPACITY (nothing written to @p buffer) if capacityWords is too small. Open
+     * boundaries and quadrupole expansions only. The call synchronises its stream to read the sizes. Not in the
+     * reference's single-GPU interface. */
+    typedef struct ryo_let_counts
+    {
+        uint32_t numNodes, numLeaves, numBodies, pad;
+        uint64_t words;
+    } ryo_let_counts;
+    RYO_API ryo_status ryo_let_export_f32(ryo_ctx_t* ctx, const float* peerBox6, uint32_t* buffer,
+                                          size_t capacityWords, ryo_let_counts* counts, ryo_stream_t stream);
+
     /* ryoanji::readBhStats (traversal_gpu.h:64-65): {sumP2P, maxP2P, sumM2P, maxM2P, maxStack} of the last
      * traversal on this context; maxP2P is 0xFFFFFFFF if a single target could not be traversed */
     RYO_API ryo_status ryo_read_bh_stats(ryo_ctx_t* ctx, uint64_t* stats5);

@@ -117,6 +117,11 @@ _f = C.c_float
 _d = C.c_double
 
 # name -> (restype, argtypes); every symbol declared in include/ryoanji_b200.h
+class LetCounts(C.Structure):
+    _fields_ = [("numNodes", C.c_uint32), ("numLeaves", C.c_uint32), ("numBodies", C.c_uint32), ("pad", C.c_uint32),
+                ("words", C.c_uint64)]
+
+
 SIGNATURES = {
     "ryo_status_string": (C.c_char_p, [_i]),
     "ryo_version": (C.c_char_p, []),
@@ -165,6 +170,7 @@ SIGNATURES = {
     "ryo_traverse_mixed": (_i, [_p, C.POINTER(GroupView), _i] + [_p] * 15 + [_d, _i, C.POINTER(_d), _p, _p, _p, _p,
                                                                              C.POINTER(_d), C.POINTER(TraverseOptions),
                                                                              _p]),
+    "ryo_let_export_f32": (_i, [_p, C.POINTER(_f), _p, C.c_size_t, C.POINTER(LetCounts), _p]),
     "ryo_read_bh_stats": (_i, [_p, C.POINTER(C.c_uint64)]),
     "ryo_read_traversal_retries": (C.c_uint64, [_p]),
     "ryo_compute_gravity_ewald_f32": (_i, [_p, C.POINTER(_f), C.POINTER(_f), C.POINTER(GroupView), _p, _p, _p, _p,

@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libryoanji_b200.so")
 
-SOURCES = ["sfc.cu", "sort.cu", "octree.cu", "upsweep.cu", "traverse.cu", "traverse64.cu", "ewald.cu", "direct.cu", "probe.cu", "batch.cu", "engine.cu", "groups.cu",
+SOURCES = ["sfc.cu", "sort.cu", "octree.cu", "upsweep.cu", "traverse.cu", "traverse64.cu", "ewald.cu", "direct.cu", "probe.cu", "batch.cu", "engine.cu", "groups.cu", "let.cu",
            "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off",

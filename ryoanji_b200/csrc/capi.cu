@@ -828,6 +828,40 @@ extern "C" ryo_status ryo_traverse_mixed(ryo_ctx_t* ctx, const ryo_group_view* g
                           ay, az, totalPotential, options, stream);
 }
 
+extern "C" ryo_status ryo_let_export_f32(ryo_ctx_t* ctx, const float* peerBox6, uint32_t* buffer,
+                                         size_t capacityWords, ryo_let_counts* counts, ryo_stream_t stream)
+{
+    if (!ctx) return RYO_ERR_BAD_ARG;
+    return guardedCtx(ctx,
+                   [&]
+                   {
+                       const auto& S = ctx->solveState;
+                       REQUIRE(peerBox6 && counts, "let_export: null argument");
+                       REQUIRE(S.valid && S.nodes, "let_export: needs a preceding ryo_solve_f32 on this context");
+                       REQUIRE(!S.periodic, "let_export: open boundaries only");
+                       REQUIRE(!S.dipoles, "let_export: quadrupole expansions only");
+                       for (int d = 0; d < 3; ++d)
+                           REQUIRE(peerBox6[2 * d + 1] >= peerBox6[2 * d], "let_export: box max below min");
+                       LetBox box;
+                       for (int d = 0; d < 3; ++d)
+                       {
+                           float lo = peerBox6[2 * d], hi = peerBox6[2 * d + 1];
+                           box.tc[d] = (hi + lo) * 0.5f; // the traversal's group box, rounded the same way
+                           box.ts[d] = (hi - lo) * 0.5f;
+                       }
+                       const NodeRecord* nodes = static_cast<const NodeRecord*>(S.nodes);
+                       LetCounts c = letSelect(ctx, nodes, ctx->lastSolve.parents, S.numNodes, box, stream);
+                       counts->numNodes  = c.numNodes;
+                       counts->numLeaves = c.numLeaves;
+                       counts->numBodies = c.numBodies;
+                       counts->words     = c.words();
+                       if (!buffer || capacityWords < c.words())
+                           throw ApiError{RYO_ERR_CAPACITY, "let_export: the buffer needs counts->words words"};
+                       letWrite(c, nodes, S.numNodes, static_cast<const float4*>(S.xyzm), S.srcH, box, buffer,
+                                stream);
+                   });
+}
+
 extern "C" ryo_status ryo_read_bh_stats(ryo_ctx_t* ctx, uint64_t* stats5)
 {
     if (!ctx || !stats5) return RYO_ERR_BAD_ARG;

@@ -231,6 +231,19 @@ template<class T>
 void launchSetMac(const uint64_t* prefixes, int numNodes, T* centers, float invTheta, const DevBox<T>& box,
                   cudaStream_t s);
 
+//! the reference's applyMAC (traversal_gpu.cu:77-84) with every operation rounded once: true if the cell of centre
+//! c (MAC r^2 in c.w) is too close to the box of centre tc and half-size ts for its multipole
+__device__ __forceinline__ bool macFails(float4 c, const float tc[3], const float ts[3])
+{
+    float dx = __fsub_rn(fabsf(__fsub_rn(tc[0], c.x)), ts[0]);
+    float dy = __fsub_rn(fabsf(__fsub_rn(tc[1], c.y)), ts[1]);
+    float dz = __fsub_rn(fabsf(__fsub_rn(tc[2], c.z)), ts[2]);
+    dx       = __fmul_rn(__fadd_rn(dx, fabsf(dx)), 0.5f);
+    dy       = __fmul_rn(__fadd_rn(dy, fabsf(dy)), 0.5f);
+    dz       = __fmul_rn(__fadd_rn(dz, fabsf(dz)), 0.5f);
+    return norm2Exact(dx, dy, dz) < c.w;
+}
+
 //! node record used by the traversal: 64 bytes, one cache line half per node
 struct alignas(16) NodeRecord
 {
@@ -239,6 +252,33 @@ struct alignas(16) NodeRecord
     float4 q1;     // qyy, qyz, qzz, trace
     int4 link;     // child (global node index, 0 = leaf), first body, body count, unused
 };
+
+// ---------------------------------------------------------------------------------------------------- let.cu
+//! a box as the traversal sees a target group: centre and half-size, rounded as the traversal rounds them
+struct LetBox
+{
+    float tc[3], ts[3];
+};
+//! where the packed export buffer keeps each array
+struct LetLayout
+{
+    float *centers, *multipoles;
+    int *childOffsets, *internalToLeaf;
+    uint32_t* layout;
+    float *x, *y, *z, *m, *h;
+    uint32_t numLeaves, numBodies;
+};
+//! sizes of one export and its per-node offsets (scratch of the context)
+struct LetCounts
+{
+    uint32_t numNodes, numLeaves, numBodies;
+    const uint32_t *keepIdx, *leafIdx, *bodyOff;
+    size_t words() const { return 14 * size_t(numNodes) + numLeaves + 2 + 5 * size_t(numBodies); }
+};
+LetCounts letSelect(ryo_ctx* ctx, const NodeRecord* nodes, const int* parents, int numNodes, const LetBox& box,
+                    cudaStream_t s);
+void letWrite(const LetCounts& c, const NodeRecord* nodes, int numNodes, const float4* xyzm, const float* h,
+              const LetBox& box, uint32_t* buffer, cudaStream_t s);
 
 /*! fused upsweep of the solver path: per leaf FP64 centre of mass and P2M in one pass over the bodies, then M2M
  *  bottom-up by last-arriving child, MAC radius, and the traversal node records. Also writes the reference-layout

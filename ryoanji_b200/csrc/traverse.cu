@@ -119,18 +119,6 @@ __device__ __forceinline__ float rsqrtApprox(float x)
     return y;
 }
 
-//! the reference's applyMAC (traversal_gpu.cu:77-84) with every operation rounded once
-__device__ __forceinline__ bool macFails(float4 c, const float tc[3], const float ts[3])
-{
-    float dx = __fsub_rn(fabsf(__fsub_rn(tc[0], c.x)), ts[0]);
-    float dy = __fsub_rn(fabsf(__fsub_rn(tc[1], c.y)), ts[1]);
-    float dz = __fsub_rn(fabsf(__fsub_rn(tc[2], c.z)), ts[2]);
-    dx       = __fmul_rn(__fadd_rn(dx, fabsf(dx)), 0.5f);
-    dy       = __fmul_rn(__fadd_rn(dy, fabsf(dy)), 0.5f);
-    dz       = __fmul_rn(__fadd_rn(dz, fabsf(dz)), 0.5f);
-    return norm2Exact(dx, dy, dz) < c.w;
-}
-
 __device__ __forceinline__ f2 rsqrt2(f2 v)
 {
     float a, b;
