@@ -550,6 +550,11 @@ extern "C"
         int maxSystems;         /* resident requests at most (default and upper limit RYO_BATCH_MAX_SYSTEMS) */
         uint64_t reserveBodies; /* resident bodies the arenas hold from creation on (default 0: grown on demand,
                                    doubling, which waits for the device at each growth) */
+        uint64_t maxStepBodies; /* bodies one step advances at most (default 2^22; 0: every resident request each
+                                   step). The resident requests are kept in the order of their remaining work
+                                   (bodies x steps left), and each step advances the longest prefix of that order
+                                   that fits (at least one request): short requests are not held to the pace of the
+                                   long ones. The order is renewed when requests are admitted or retire. */
     } ryo_engine_params;
     typedef struct ryo_engine_request
     {

@@ -695,7 +695,9 @@ class Engine:
 
     def __init__(self, params: SolveParams | None = None, hbm_budget_bytes: float = 120e9,
                  bytes_per_body: float = 256.0, max_systems: int = MAX_BATCH_SYSTEMS, ctx: Context | None = None,
-                 reserve_bodies: int = 0):
+                 reserve_bodies: int = 0, max_step_bodies: int | None = None):
+        """max_step_bodies: bodies one step advances at most (None: the library default, 2^22; 0: every resident
+        request every step); the requests with the least remaining work go first"""
         self.ctx = ctx or default_context()
         ep = _abi.EngineParams()
         lib.ryo_engine_params_default(C.byref(ep))
@@ -704,6 +706,8 @@ class Engine:
         ep.bytesPerBody = bytes_per_body
         ep.maxSystems = max_systems
         ep.reserveBodies = reserve_bodies
+        if max_step_bodies is not None:
+            ep.maxStepBodies = max_step_bodies
         h = C.c_void_p()
         _check(lib.ryo_engine_create(self.ctx.handle, C.byref(ep), C.byref(h)), self.ctx)
         self.handle = h

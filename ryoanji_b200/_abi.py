@@ -85,7 +85,7 @@ class System(C.Structure):
 
 class EngineParams(C.Structure):
     _fields_ = [("solve", SolveParams), ("hbmBudgetBytes", C.c_double), ("bytesPerBody", C.c_double),
-                ("maxSystems", C.c_int), ("reserveBodies", C.c_uint64)]
+                ("maxSystems", C.c_int), ("reserveBodies", C.c_uint64), ("maxStepBodies", C.c_uint64)]
 
 
 class EngineRequest(C.Structure):

@@ -70,21 +70,26 @@ struct ArenaPtrs
     uint32_t* id;
 };
 
-//! copy the bodies of the surviving requests: destination range r starts at dstFirst[r], source at srcFirst[r]
-__global__ void engineCompact(ArenaPtrs src, ArenaPtrs dst, const uint64_t* __restrict__ dstFirst,
-                              const uint64_t* __restrict__ srcFirst, uint32_t numReq, uint64_t total)
+/*! copy the bodies of the surviving requests: request r's bodies are the range [virtFirst[r], virtFirst[r + 1]) of
+ *  the survivors taken in their new order; they move from srcFirst[r] to dstFirst[r] (newly admitted requests may
+ *  sit between the destination ranges) */
+__global__ void engineCompact(ArenaPtrs src, ArenaPtrs dst, const uint64_t* __restrict__ virtFirst,
+                              const uint64_t* __restrict__ dstFirst, const uint64_t* __restrict__ srcFirst,
+                              uint32_t numReq, uint64_t total)
 {
     size_t stride = size_t(gridDim.x) * blockDim.x;
-    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += stride)
+    for (size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x; v < total; v += stride)
     {
         uint32_t lo = 0, hi = numReq - 1;
         while (lo < hi)
         {
             uint32_t mid = (lo + hi + 1) >> 1;
-            if (dstFirst[mid] <= i) lo = mid;
+            if (virtFirst[mid] <= v) lo = mid;
             else hi = mid - 1;
         }
-        size_t j = srcFirst[lo] + (i - dstFirst[lo]);
+        size_t off = v - virtFirst[lo];
+        size_t j   = srcFirst[lo] + off;
+        size_t i   = dstFirst[lo] + off;
 #pragma unroll
         for (int k = 0; k < kArenaArrays; ++k)
             dst.a[k][i] = src.a[k][j];
@@ -235,6 +240,7 @@ struct ryo_engine
     double budget;
     double bytesPerBody;
     int maxSystems;
+    uint64_t maxStepBodies = 0; // 0: every resident request steps every step
     double used = 0;
     std::deque<Request> queue;
     std::vector<Request> resident;
@@ -270,53 +276,70 @@ unsigned gridFor(size_t n, int sms)
     return unsigned(std::max<size_t>(1, std::min(want, cap)));
 }
 
-//! rebuild the arena: survivors compacted to the front, newly admitted requests copied in behind them
+//! the work a request has left: bodies times the force evaluations still to come
+double remainingWork(const Request& q) { return double(q.n) * double(q.stepsLeft + (q.haveForces ? 0 : 1)); }
+
+/*! rebuild the arena with the survivors and the newly admitted requests in one order: by remaining work, least
+ *  first, when steps are capped (so that a step's prefix holds the requests closest to completion), else survivors
+ *  first, then the admitted in arrival order. Survivors are compacted on the device, admitted ones copied in. */
 void rebuildArena(ryo_engine* E, std::vector<Request>& admitted, cudaStream_t s)
 {
     Arena& src = E->arenas.buf[E->arenas.cur];
     Arena& dst = E->arenas.buf[1 - E->arenas.cur];
-    uint64_t total = 0;
+    std::vector<std::pair<Request, bool>> all; // (request, admitted now)
     for (auto& r : E->resident)
-        total += r.n;
-    uint64_t survivors = total;
+        all.emplace_back(r, false);
     for (auto& r : admitted)
-        total += r.n;
+        all.emplace_back(r, true);
+    if (E->maxStepBodies > 0)
+        std::stable_sort(all.begin(), all.end(), [](const auto& a, const auto& b)
+                         { return remainingWork(a.first) < remainingWork(b.first); });
+    uint64_t total = 0;
+    for (auto& r : all)
+        total += r.first.n;
     dst.ensure(std::max<uint64_t>(total, 1));
-    if (!E->resident.empty())
+    std::vector<uint64_t> vf, df, sf; // survivors: virtual, destination and source offsets
+    uint64_t o = 0, survivors = 0;
+    for (auto& [q, fresh] : all)
     {
-        std::vector<uint64_t> df(E->resident.size()), sf(E->resident.size());
-        uint64_t o = 0;
-        for (size_t k = 0; k < E->resident.size(); ++k)
+        if (!fresh)
         {
-            df[k] = o;
-            sf[k] = E->resident[k].arenaFirst;
-            o += E->resident[k].n;
+            vf.push_back(survivors);
+            df.push_back(o);
+            sf.push_back(q.arenaFirst);
+            survivors += q.n;
         }
-        uint64_t* d = E->ctx->scratch<uint64_t>("eng.compact", 2 * df.size(), s);
-        RYO_CUDA(cudaMemcpyAsync(d, df.data(), df.size() * 8, cudaMemcpyHostToDevice, s));
-        RYO_CUDA(cudaMemcpyAsync(d + df.size(), sf.data(), sf.size() * 8, cudaMemcpyHostToDevice, s));
-        engineCompact<<<gridFor(survivors, E->ctx->smCount), 256, 0, s>>>(ptrsOf(src), ptrsOf(dst), d, d + df.size(),
-                                                                         uint32_t(df.size()), survivors);
-        RYO_LAUNCH_CHECK();
-        for (size_t k = 0; k < E->resident.size(); ++k)
-            E->resident[k].arenaFirst = df[k];
+        q.arenaFirst = o;
+        o += q.n;
     }
-    uint64_t o = survivors;
-    for (auto& r : admitted)
+    if (survivors > 0)
     {
-        r.arenaFirst = o;
+        size_t k     = vf.size();
+        uint64_t* d = E->ctx->scratch<uint64_t>("eng.compact", 3 * k, s);
+        RYO_CUDA(cudaMemcpyAsync(d, vf.data(), k * 8, cudaMemcpyHostToDevice, s));
+        RYO_CUDA(cudaMemcpyAsync(d + k, df.data(), k * 8, cudaMemcpyHostToDevice, s));
+        RYO_CUDA(cudaMemcpyAsync(d + 2 * k, sf.data(), k * 8, cudaMemcpyHostToDevice, s));
+        engineCompact<<<gridFor(survivors, E->ctx->smCount), 256, 0, s>>>(ptrsOf(src), ptrsOf(dst), d, d + k,
+                                                                         d + 2 * k, uint32_t(k), survivors);
+        RYO_LAUNCH_CHECK();
+    }
+    for (auto& [r, fresh] : all)
+    {
+        if (!fresh) continue;
         for (int k = 0; k < 8; ++k)
         {
             if (r.in[k])
-                RYO_CUDA(cudaMemcpyAsync(dst.a[k] + o, r.in[k], r.n * sizeof(float), cudaMemcpyHostToDevice, s));
+                RYO_CUDA(cudaMemcpyAsync(dst.a[k] + r.arenaFirst, r.in[k], r.n * sizeof(float),
+                                         cudaMemcpyHostToDevice, s));
             else
-                RYO_CUDA(cudaMemsetAsync(dst.a[k] + o, 0, r.n * sizeof(float), s));
+                RYO_CUDA(cudaMemsetAsync(dst.a[k] + r.arenaFirst, 0, r.n * sizeof(float), s));
         }
-        engineIota<<<ceilDiv(r.n, 256), 256, 0, s>>>(dst.id, o, r.n);
+        engineIota<<<ceilDiv(r.n, 256), 256, 0, s>>>(dst.id, r.arenaFirst, r.n);
         RYO_LAUNCH_CHECK();
-        o += r.n;
-        E->resident.push_back(r);
     }
+    E->resident.clear();
+    for (auto& r : all)
+        E->resident.push_back(r.first);
     E->arenas.cur     = 1 - E->arenas.cur;
     E->residentBodies = total;
 }
@@ -374,6 +397,7 @@ extern "C" void ryo_engine_params_default(ryo_engine_params* p)
     p->bytesPerBody   = 256.0;
     p->maxSystems     = RYO_BATCH_MAX_SYSTEMS;
     p->reserveBodies  = 0;
+    p->maxStepBodies  = uint64_t(1) << 22;
 }
 
 extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params* p, ryo_engine_t** out)
@@ -392,6 +416,7 @@ extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params*
         E->budget       = p->hbmBudgetBytes;
         E->bytesPerBody = p->bytesPerBody;
         E->maxSystems   = p->maxSystems;
+        E->maxStepBodies = p->maxStepBodies;
         if (p->reserveBodies > 0)
         {
             E->arenas.buf[0].ensure(p->reserveBodies);
@@ -534,10 +559,20 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                                if (info) *info = st;
                                return;
                            }
-                           const uint32_t ns = uint32_t(E->resident.size());
-                           Arena& A          = E->arenas.buf[E->arenas.cur];
-                           ArenaPtrs P       = ptrsOf(A);
-                           const uint64_t n  = E->residentBodies;
+                           // the requests this step advances: all, or the longest prefix of the resident order
+                           // (least remaining work first) within maxStepBodies, at least one
+                           const uint32_t nsAll = uint32_t(E->resident.size());
+                           uint32_t ns          = nsAll;
+                           uint64_t n           = E->residentBodies;
+                           if (E->maxStepBodies > 0)
+                           {
+                               ns = 0;
+                               n  = 0;
+                               while (ns < nsAll && (ns == 0 || n + E->resident[ns].n <= E->maxStepBodies))
+                                   n += E->resident[ns++].n;
+                           }
+                           Arena& A    = E->arenas.buf[E->arenas.cur];
+                           ArenaPtrs P = ptrsOf(A);
 
                            std::vector<ryo_system> sys(ns);
                            std::vector<EngineSys> es(ns);
@@ -650,6 +685,8 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                                ++st.retired;
                                E->changed = true;
                            }
+                           for (uint32_t k = ns; k < nsAll; ++k)
+                               keep.push_back(E->resident[k]); // not advanced this step
                            if (outAt) RYO_CUDA(cudaStreamSynchronize(s));
                            E->resident.swap(keep);
                            st.hostMs[3] = since(t3);

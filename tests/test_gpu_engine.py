@@ -163,3 +163,36 @@ def test_submit_rejects_bad_periodic_requests():
     done = _drain(eng)
     assert sorted(done) == [1]
     eng.close()
+
+
+def test_capped_steps_keep_results_and_favour_short_requests():
+    """with a step cap, each step advances the requests with the least remaining work that fit; the results stay the
+    uncapped engine's, the least-work request retires first, and some steps leave requests waiting"""
+    import ryoanji_b200 as ryo
+    reqs = _requests()
+    params = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32)
+    capped = ryo.Engine(params, max_step_bodies=4000)
+    for r in reqs:
+        _submit(capped, r)
+    finished, partial_steps = {}, 0
+    for step in range(500):
+        info = capped.step()
+        partial_steps += info["solved"] < info["resident"]
+        for d in capped.poll():
+            finished[d["tag"]] = (step, d)
+        if len(finished) == len(reqs):
+            break
+    assert len(finished) == len(reqs) and partial_steps > 0
+    ref = ryo.Engine(params, max_step_bodies=0)
+    for r in reqs:
+        _submit(ref, r)
+    full = _drain(ref)
+    for r in reqs:
+        sa, sb = full[r["tag"]]["state"], finished[r["tag"]][1]["state"]
+        scale = np.abs(sa).max(axis=1, keepdims=True) + 1e-30
+        assert float((np.abs(sa - sb) / scale).max()) <= 1e-5, r["tag"]
+    work = {r["tag"]: r["p"].n * (r["steps"] + 1) for r in reqs}
+    first = min(finished, key=lambda t: (finished[t][0], work[t]))
+    assert work[first] == min(work.values())
+    capped.close()
+    ref.close()
