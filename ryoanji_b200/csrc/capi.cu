@@ -1292,7 +1292,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     float4* rec      = ctx->scratch<float4>("solve.bodyRecords", 2 * n, s);
     float4* xyzm     = ctx->scratch<float4>("solve.xyzm", n, s);
     float4* xyzh     = ctx->scratch<float4>("solve.xyzh", n, s);
-    uint32_t* hRange = ctx->scratch<uint32_t>("solve.softeningRange", 2, s);
+    uint32_t* hRange = ctx->scratch<uint32_t>("solve.softeningRange", 4, s);
     auto permute     = [&]()
     {
         if (pipe) RYO_CUDA(cudaStreamWaitEvent(s, pipe->massReady, 0));
@@ -1402,6 +1402,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     t.stackCapacity = P->stackCapacity;
     t.dipoles       = dipoles;
     t.softeningRange = hRange;
+    t.massRange      = dipoles ? nullptr : hRange + 2; // signed-mass expansions keep the per-source mass
     uint32_t* gm2p  = ctx->scratch<uint32_t>("solve.groupM2P", numGroups, s);
     uint32_t* gp2p  = ctx->scratch<uint32_t>("solve.groupP2P", numGroups, s);
     RYO_CUDA(cudaMemsetAsync(gm2p, 0, sizeof(uint32_t) * numGroups, s));
@@ -1703,7 +1704,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        float4* xyzm           = ctx->scratch<float4>("solve.xyzm", n, s);
                        float4* xyzh           = ctx->scratch<float4>("solve.xyzh", n, s);
                        launchPackRecords(x, y, z, m, h, vx, vy, vz, n, rec, s);
-                       uint32_t* hRange       = ctx->scratch<uint32_t>("solve.softeningRange", 2, s);
+                       uint32_t* hRange       = ctx->scratch<uint32_t>("solve.softeningRange", 4, s);
                        launchGatherRecords(order, rec, n, x, y, z, m, h, vx, vy, vz, xyzm, xyzh, hRange, s);
                        if (orderOut)
                            RYO_CUDA(cudaMemcpyAsync(orderOut, order, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));

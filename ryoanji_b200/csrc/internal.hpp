@@ -169,7 +169,8 @@ void launchGatherT(const uint32_t* order, const T* in, T* out, size_t n, cudaStr
 void launchPackRecords(const float* x, const float* y, const float* z, const float* m, const float* h,
                        const float* vx, const float* vy, const float* vz, size_t n, float4* rec, cudaStream_t s);
 //! body i of the output is record order[i]: the per-body arrays (null ones skipped) and xyzm / xyzh (may be null);
-//! hRange (may be null) receives the min and max softening as ordered bits (orderedBits)
+//! hRange (may be null, else 4 entries) receives the min and max softening, then the min and max mass, as ordered
+//! bits (orderedBits)
 void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, float* x, float* y, float* z, float* m,
                          float* h, float* vx, float* vy, float* vz, float4* xyzm, float4* xyzh, uint32_t* hRange,
                          cudaStream_t s);
@@ -353,6 +354,9 @@ struct TraverseLaunch
     // min and max softening of every target and source as ordered bits (null: not known). Equal values let the
     // direct sums skip staging and comparing the sources' softening.
     const uint32_t* softeningRange;
+    // min and max mass of every source as ordered bits (null: not known). Equal values let the direct sums apply
+    // the mass once per batch instead of once per source.
+    const uint32_t* massRange;
     // double coordinates (traverse64.cu): kPrecisionF64 (everything double) or kPrecisionMixed (double coordinates
     // and centres; float softenings, masses, multipoles and outputs). The float fields above are unused then; the
     // untyped pointers hold double (f64) or float (mixed) arrays.

@@ -295,13 +295,15 @@ __global__ void gatherRecordsKernel(const uint32_t* __restrict__ order, const fl
                                     float4* __restrict__ xyzh, uint32_t* __restrict__ hRange)
 {
     size_t stride = size_t(gridDim.x) * blockDim.x;
-    uint32_t lo = 0xffffffffu, hi = 0u;
+    uint32_t lo = 0xffffffffu, hi = 0u, mlo = 0xffffffffu, mhi = 0u;
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
     {
         size_t j = order[i];
         float4 a = rec[2 * j], b = rec[2 * j + 1]; // one 32-byte sector
         lo       = min(lo, orderedBits(b.x));
         hi       = max(hi, orderedBits(b.x));
+        mlo      = min(mlo, orderedBits(a.w));
+        mhi      = max(mhi, orderedBits(a.w));
         x[i]     = a.x;
         y[i]     = a.y;
         z[i]     = a.z;
@@ -313,7 +315,11 @@ __global__ void gatherRecordsKernel(const uint32_t* __restrict__ order, const fl
         if (xyzm) xyzm[i] = a;
         if (xyzh) xyzh[i] = make_float4(a.x, a.y, a.z, b.x);
     }
-    if (hRange) foldRange(lo, hi, hRange);
+    if (hRange)
+    {
+        foldRange(lo, hi, hRange);
+        foldRange(mlo, mhi, hRange + 2);
+    }
 }
 
 //! gatherRecordsKernel for four consecutive sorted bodies per thread: one 16-byte load of their indices, 16-byte
@@ -325,7 +331,7 @@ __global__ void gatherRecordsKernel4(const uint4* __restrict__ order, const floa
                                      float4* __restrict__ xyzh, uint32_t* __restrict__ hRange)
 {
     size_t stride = size_t(gridDim.x) * blockDim.x;
-    uint32_t lo = 0xffffffffu, hi = 0u;
+    uint32_t lo = 0xffffffffu, hi = 0u, mlo = 0xffffffffu, mhi = 0u;
     for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < n4; t += stride)
     {
         uint4 j = order[t];
@@ -335,6 +341,8 @@ __global__ void gatherRecordsKernel4(const uint4* __restrict__ order, const floa
         float4 a3 = rec[2 * size_t(j.w)], b3 = rec[2 * size_t(j.w) + 1];
         lo = min(min(min(lo, orderedBits(b0.x)), orderedBits(b1.x)), min(orderedBits(b2.x), orderedBits(b3.x)));
         hi = max(max(max(hi, orderedBits(b0.x)), orderedBits(b1.x)), max(orderedBits(b2.x), orderedBits(b3.x)));
+        mlo = min(min(min(mlo, orderedBits(a0.w)), orderedBits(a1.w)), min(orderedBits(a2.w), orderedBits(a3.w)));
+        mhi = max(max(max(mhi, orderedBits(a0.w)), orderedBits(a1.w)), max(orderedBits(a2.w), orderedBits(a3.w)));
         x[t] = make_float4(a0.x, a1.x, a2.x, a3.x);
         y[t] = make_float4(a0.y, a1.y, a2.y, a3.y);
         z[t] = make_float4(a0.z, a1.z, a2.z, a3.z);
@@ -360,7 +368,11 @@ __global__ void gatherRecordsKernel4(const uint4* __restrict__ order, const floa
             o[3] = make_float4(a3.x, a3.y, a3.z, b3.x);
         }
     }
-    if (hRange) foldRange(lo, hi, hRange);
+    if (hRange)
+    {
+        foldRange(lo, hi, hRange);
+        foldRange(mlo, mhi, hRange + 2);
+    }
 }
 
 namespace
@@ -390,8 +402,11 @@ void launchGatherRecords(const uint32_t* order, const float4* rec, size_t n, flo
 {
     if (hRange)
     {
-        RYO_CUDA(cudaMemsetAsync(hRange, 0xff, sizeof(uint32_t), s)); // min
-        RYO_CUDA(cudaMemsetAsync(hRange + 1, 0, sizeof(uint32_t), s)); // max
+        // softening (min, max), then mass (min, max)
+        RYO_CUDA(cudaMemsetAsync(hRange, 0xff, sizeof(uint32_t), s));
+        RYO_CUDA(cudaMemsetAsync(hRange + 1, 0, sizeof(uint32_t), s));
+        RYO_CUDA(cudaMemsetAsync(hRange + 2, 0xff, sizeof(uint32_t), s));
+        RYO_CUDA(cudaMemsetAsync(hRange + 3, 0, sizeof(uint32_t), s));
     }
     if (n == 0) return;
     size_t done = 0;

@@ -52,7 +52,11 @@ struct WarpSmem
     // (batch j when j % parts == part; parts is 1 outside the split second pass)
     int batchNext, part, parts, item;
     // 1 if every target and source of the launch has the softening of the group's targets (T.h0)
-    int allUniform, pad[3];
+    int allUniform;
+    // 1 if every source of the launch has the mass massU: the direct sums then apply it once per batch
+    int uniformMass;
+    float massU;
+    int pad;
 };
 
 //! true if the walk's next evaluation batch belongs to this warp; counts the batch either way. Outside the split
@@ -199,6 +203,22 @@ __device__ __forceinline__ void p2p2u(Acc2& A, f2 tx, f2 ty, f2 tz, float hh, f2
     A.x    = fma2(dx, m3, A.x);
     A.y    = fma2(dy, m3, A.y);
     A.z    = fma2(dz, m3, A.z);
+}
+
+/*! p2p2u for sources of one common mass, which the caller applies to the batch's sums: a packed multiply less
+ *  per interaction */
+__device__ __forceinline__ void p2p2um(Acc2& A, f2 tx, f2 ty, f2 tz, float hh, f2 sx, f2 sy, f2 sz)
+{
+    f2 dx  = sub2(sx, tx), dy = sub2(sy, ty), dz = sub2(sz, tz);
+    f2 r2  = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+    float r0, r1;
+    upk(r2, r0, r1);
+    f2 ir  = pk(rsqrtApprox(fmaxf(r0, hh)), rsqrtApprox(fmaxf(r1, hh)));
+    f2 i3  = mul2(ir, mul2(ir, ir));
+    A.p    = fma2(i3, r2, A.p);
+    A.x    = fma2(dx, i3, A.x);
+    A.y    = fma2(dy, i3, A.y);
+    A.z    = fma2(dz, i3, A.z);
 }
 
 /*! P2P (kernel.hpp:99-120) for both targets against one source; s* are duplicated pairs, th the targets' h */
@@ -516,31 +536,53 @@ __device__ int evalP2P(WarpSmem& S, int numLeaves, bool all, const Sources& src,
                 float hij = __fadd_rn(T.h0, hj0);
                 float hh  = __fmul_rn(hij, hij);
                 Acc2 pb   = zero2();
-                auto oneU = [&](Acc2& pp, int j)
+                // two accumulation chains over the batch's sources
+                auto batch = [&](auto&& oneU)
                 {
-                    ulonglong2 a = st[2 * j], c = st[2 * j + 1];
-                    p2p2u(pp, T.tx, T.ty, T.tz, hh, a.x, a.y, c.x, c.y);
-                };
-                if (nvalid == kP2PBatch)
-                {
-#pragma unroll 8
-                    for (int j = 0; j < kP2PBatch; j += 2)
+                    if (nvalid == kP2PBatch)
                     {
-                        oneU(part, j);
-                        oneU(pb, j + 1);
+#pragma unroll 8
+                        for (int j = 0; j < kP2PBatch; j += 2)
+                        {
+                            oneU(part, j);
+                            oneU(pb, j + 1);
+                        }
                     }
+                    else
+                    {
+                        int j = 0;
+                        for (; j + 1 < nvalid; j += 2)
+                        {
+                            oneU(part, j);
+                            oneU(pb, j + 1);
+                        }
+                        if (j < nvalid) oneU(part, j);
+                    }
+                };
+                if (S.uniformMass)
+                {
+                    batch([&](Acc2& pp, int j)
+                          {
+                              ulonglong2 a = st[2 * j], c = st[2 * j + 1];
+                              p2p2um(pp, T.tx, T.ty, T.tz, hh, a.x, a.y, c.x);
+                          });
+                    Acc2 sum = sum2(part, pb);
+                    f2 mm    = pk(S.massU, S.massU);
+                    sum.p    = mul2(sum.p, mm);
+                    sum.x    = mul2(sum.x, mm);
+                    sum.y    = mul2(sum.y, mm);
+                    sum.z    = mul2(sum.z, mm);
+                    addBatchS(S, sum);
                 }
                 else
                 {
-                    int j = 0;
-                    for (; j + 1 < nvalid; j += 2)
-                    {
-                        oneU(part, j);
-                        oneU(pb, j + 1);
-                    }
-                    if (j < nvalid) oneU(part, j);
+                    batch([&](Acc2& pp, int j)
+                          {
+                              ulonglong2 a = st[2 * j], c = st[2 * j + 1];
+                              p2p2u(pp, T.tx, T.ty, T.tz, hh, a.x, a.y, c.x, c.y);
+                          });
+                    addBatchS(S, sum2(part, pb));
                 }
-                addBatchS(S, sum2(part, pb));
                 __syncwarp();
                 continue;
             }
@@ -728,8 +770,12 @@ __global__ void __launch_bounds__(kTravThreads, 5)
         T.h0       = __shfl_sync(0xffffffffu, t0.w, 0);
         T.uniformH = __all_sync(0xffffffffu, t0.w == T.h0 && t1.w == T.h0);
         if (lane == 0)
+        {
             S.allUniform = P.softeningRange && T.uniformH && P.softeningRange[0] == P.softeningRange[1] &&
                            orderedFloat(P.softeningRange[0]) == T.h0;
+            S.uniformMass = P.massRange && !P.groupSys && P.massRange[0] == P.massRange[1];
+            S.massU       = S.uniformMass ? orderedFloat(P.massRange[0]) : 0.f;
+        }
 #pragma unroll
         for (int c = 0; c < 4; ++c)
             S.sums[0][c][lane] = S.sums[1][c][lane] = 0ull;
