@@ -40,11 +40,24 @@ def _deps() -> list[str]:
         os.path.join(ROOT, "include", "ryoanji_b200.h")]
 
 
-def _stale(target: str, inputs: list[str]) -> bool:
-    if not os.path.exists(target):
+def _digest(inputs: list[str], cmd: list[str]) -> str:
+    """hash of the inputs' contents and the compile command"""
+    import hashlib
+    h = hashlib.sha256(" ".join(cmd).encode())
+    for path in sorted(inputs):
+        with open(path, "rb") as f:
+            h.update(path.encode() + b"\0" + f.read())
+    return h.hexdigest()
+
+
+def _stale(target: str, inputs: list[str], cmd: list[str]) -> bool:
+    """an object is rebuilt unless it exists and was compiled from exactly these contents with this command (file
+    times are not enough: a source edited while its compile runs would leave an object newer than the edit)"""
+    stamp = target + ".sha256"
+    if not (os.path.exists(target) and os.path.exists(stamp)):
         return True
-    t = os.path.getmtime(target)
-    return any(os.path.getmtime(i) > t for i in inputs)
+    with open(stamp) as f:
+        return f.read().strip() != _digest(inputs, cmd)
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
@@ -57,15 +70,22 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(obj)
-        if force or _stale(obj, [path] + deps):
-            cmd = [cc, *FLAGS, "-c", path, "-o", obj]
+        cmd = [cc, *FLAGS, "-c", path, "-o", obj]
+        if force or _stale(obj, [path] + deps, cmd):
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
-            jobs.append((src, cmd))
+            # the digest is taken before compiling: an edit during the compile makes the next build redo it
+            jobs.append((src, cmd, obj, _digest([path] + deps, [cc, *FLAGS, "-c", path, "-o", obj])))
 
     def run(job):
-        src, cmd = job
+        src, cmd, obj, digest = job
+        stamp = obj + ".sha256"
+        if os.path.exists(stamp):
+            os.remove(stamp)
         r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode == 0:
+            with open(stamp, "w") as f:
+                f.write(digest)
         return src, r
 
     failed = []
@@ -77,7 +97,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
                 failed.append(src)
     if failed:
         raise RuntimeError(f"nvcc failed for {failed}")
-    if force or jobs or _stale(LIB, objs):
+    if force or jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [cc, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fPIC"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
