@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--no-plummer", action="store_true", help="skip the 2^24 Plummer sphere leg")
     ap.add_argument("--served-requests", type=int, default=48)
     ap.add_argument("--served-rate", type=float, default=24.0, help="Poisson arrival rate, requests per second")
+    ap.add_argument("--served-max-step-bodies", type=int, default=None,
+                    help="engine step cap in bodies (default: the library's; 0: every resident request each step)")
     ap.add_argument("--no-accuracy-matched", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the precision-study leg (halos, periodic box)")
     ap.add_argument("--precision", action="store_true",
@@ -451,7 +453,7 @@ def summarize(line: dict) -> dict:
         s["acc_theta_0.5"] = {"p99": a["err_p99_1st_pct"], "max": a["err_max"]}
     if "accuracy_matched" in line:
         a = line["accuracy_matched"]
-        s["acc_matched"] = {k: a.get(k) for k in ("theta", "mparticles_per_s", "err_p99_1st_pct")}
+        s["acc_matched"] = {"theta": a.get("theta"), "mps": a.get("value"), "p99": a.get("err_p99_1st_pct")}
     if "ensemble" in line:
         e = line["ensemble"]
         s["ensemble"] = {"batched_sps": e.get("batched", {}).get("solves_per_s"),
@@ -649,7 +651,8 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
 
     # served: the engine admits what has arrived at every step. Its two arenas are reserved at creation for 2^25
     # resident bodies (the stream peaks near 2.5e7), as a server sizes them at start-up.
-    eng = ryo.Engine(params, hbm_budget_bytes=120e9, ctx=ctx, reserve_bodies=1 << 25)
+    eng = ryo.Engine(params, hbm_budget_bytes=120e9, ctx=ctx, reserve_bodies=1 << 25,
+                     max_step_bodies=args.served_max_step_bodies)
     outs = {}
     done = {}
     i = 0
@@ -676,6 +679,8 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
             outs[d["tag"]] = d
     served = summary(done, max(done.values(), default=0.0))
     served["engine_steps"] = steps
+    served["max_step_bodies"] = ("library default" if args.served_max_step_bodies is None
+                                 else args.served_max_step_bodies)
     drift = [abs(d["kinetic"] + d["potential"] - d["initial"]) / abs(d["initial"]) for d in outs.values()
              if d["initial"] != 0]
     served["energy_drift_median"] = float(np.median(drift)) if drift else None

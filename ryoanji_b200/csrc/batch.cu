@@ -176,9 +176,10 @@ __global__ void batchRootsKernel(uint32_t numSystems, const uint64_t* __restrict
     t.boxL[0]   = boxes[s].len[0];
     t.boxL[1]   = boxes[s].len[1];
     t.boxL[2]   = boxes[s].len[2];
-    t.pad       = 0;
     t.hLo       = 0xffffffffu; // filled by batchSofteningRange
     t.hHi       = 0u;
+    t.mLo       = 0xffffffffu;
+    t.mHi       = 0u;
     out[s]      = t;
 }
 
@@ -228,45 +229,58 @@ void launchBatchKeys(const float* x, const float* y, const float* z, size_t n, c
     RYO_LAUNCH_CHECK();
 }
 
-//! one block per system: min and max softening of its bodies (systems are contiguous runs of bodies)
-__global__ void __launch_bounds__(256) batchSofteningRange(const float* __restrict__ h,
+//! one block per system: min and max softening and mass of its bodies (systems are contiguous runs of bodies)
+__global__ void __launch_bounds__(256) batchSofteningRange(const float* __restrict__ h, const float* __restrict__ m,
                                                            const uint64_t* __restrict__ first, SysTrav* trav)
 {
-    __shared__ uint32_t sLo[8], sHi[8];
+    __shared__ uint32_t sLo[2][8], sHi[2][8];
     const uint32_t s = blockIdx.x;
-    uint32_t lo = 0xffffffffu, hi = 0u;
+    uint32_t lo[2] = {0xffffffffu, 0xffffffffu}, hi[2] = {0u, 0u};
     for (uint64_t i = first[s] + threadIdx.x; i < first[s + 1]; i += blockDim.x)
     {
         uint32_t b = orderedBits(h[i]);
-        lo         = min(lo, b);
-        hi         = max(hi, b);
+        lo[0]      = min(lo[0], b);
+        hi[0]      = max(hi[0], b);
+        if (m)
+        {
+            uint32_t c = orderedBits(m[i]);
+            lo[1]      = min(lo[1], c);
+            hi[1]      = max(hi[1], c);
+        }
     }
-    lo = __reduce_min_sync(0xffffffffu, lo);
-    hi = __reduce_max_sync(0xffffffffu, hi);
     const unsigned warp = threadIdx.x / kWarp;
-    if (laneId() == 0)
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
     {
-        sLo[warp] = lo;
-        sHi[warp] = hi;
+        lo[k] = __reduce_min_sync(0xffffffffu, lo[k]);
+        hi[k] = __reduce_max_sync(0xffffffffu, hi[k]);
+        if (laneId() == 0)
+        {
+            sLo[k][warp] = lo[k];
+            sHi[k][warp] = hi[k];
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0)
     {
         for (unsigned w = 1; w < blockDim.x / kWarp; ++w)
-        {
-            lo = min(lo, sLo[w]);
-            hi = max(hi, sHi[w]);
-        }
-        trav[s].hLo = lo;
-        trav[s].hHi = hi;
+            for (int k = 0; k < 2; ++k)
+            {
+                lo[k] = min(lo[k], sLo[k][w]);
+                hi[k] = max(hi[k], sHi[k][w]);
+            }
+        trav[s].hLo = lo[0];
+        trav[s].hHi = hi[0];
+        trav[s].mLo = lo[1];
+        trav[s].mHi = hi[1];
     }
 }
 
-void launchBatchSofteningRange(const float* h, const uint64_t* first, uint32_t numSystems, SysTrav* trav,
-                               cudaStream_t s)
+void launchBatchSofteningRange(const float* h, const float* m, const uint64_t* first, uint32_t numSystems,
+                               SysTrav* trav, cudaStream_t s)
 {
     if (numSystems == 0) return;
-    batchSofteningRange<<<numSystems, 256, 0, s>>>(h, first, trav);
+    batchSofteningRange<<<numSystems, 256, 0, s>>>(h, m, first, trav);
     RYO_LAUNCH_CHECK();
 }
 

@@ -1502,6 +1502,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
         st.box        = box;
         st.ewald      = P->ewald;
         st.dipoles    = dipoles;
+        st.massRange  = dipoles ? nullptr : hRange + 2;
         ryo_solve_arrays& a = ctx->lastSolve;
         a.numLeaves         = nl;
         a.numNodes          = nn;
@@ -1782,7 +1783,9 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        RYO_CUDA(cudaMemsetAsync(rootErr, 0, sizeof(unsigned int), s));
                        launchBatchRoots(ns, oct.prefixes, levelRange[sysLevel], levelRange[sysLevel + 1],
                                         oct.childOffsets, sysLevel, dBx, dShells, dTrav, dRootNode, rootErr, s);
-                       launchBatchSofteningRange(h, dFirst, ns, dTrav, s);
+                       // the mass range only where quadrupoles are summed (signed-mass expansions keep the
+                       // per-source mass)
+                       launchBatchSofteningRange(h, dipoles ? nullptr : m, dFirst, ns, dTrav, s);
                        double* sysPot = ctx->scratch<double>("batch.pot", 2 * size_t(ns), s); // tree, Ewald
                        RYO_CUDA(cudaMemsetAsync(sysPot, 0, sizeof(double) * 2 * ns, s));
                        for (float* a : {p, ax, ay, az})
@@ -1997,6 +2000,7 @@ extern "C" ryo_status ryo_solve_targets_f32(ryo_ctx_t* ctx, const float* xt, con
                        t.tgtM          = sorted + 3 * n;
                        t.srcXYZM       = static_cast<const float4*>(S.xyzm);
                        t.srcH          = S.srcH;
+                       t.massRange     = S.massRange; // the solve's sources: the same direct-sum arithmetic
                        t.G             = S.G;
                        t.numShells     = S.numShells;
                        for (int d = 0; d < 3; ++d)

@@ -91,6 +91,7 @@ struct ryo_ctx
         const void* xyzm   = nullptr; // float4 per source body
         const float* srcH  = nullptr; // the caller's h array of the solve (sorted)
         const void* dipoles = nullptr; // float4 per node for dipole expansions, else null
+        const uint32_t* massRange = nullptr; // min and max source mass (ordered bits), null if not known
         int numNodes       = 0;
         unsigned groupSize = 64;
         float G            = 1.f;
@@ -382,11 +383,12 @@ struct SysTrav
     int numShells; // periodic replicas per dimension
     float boxL[3];
     uint32_t hLo, hHi; // min and max softening of the system's bodies as ordered bits (hLo > hHi: not known)
-    int pad;
+    uint32_t mLo, mHi; // min and max mass of the system's bodies as ordered bits (mLo > mHi: not known)
 };
-//! per-system softening range of a batched solve into trav[s].hLo / hHi (one block per system)
-void launchBatchSofteningRange(const float* h, const uint64_t* first, uint32_t numSystems, SysTrav* trav,
-                               cudaStream_t s);
+//! per-system softening and mass ranges of a batched solve into trav[s].hLo / hHi / mLo / mHi (one block per
+//! system); m may be null (the mass range then stays unknown)
+void launchBatchSofteningRange(const float* h, const float* m, const uint64_t* first, uint32_t numSystems,
+                               SysTrav* trav, cudaStream_t s);
 void launchTraverse(const TraverseLaunch& t, int smCount, cudaStream_t s);
 /*! after a second pass: per queued group, the parts' partial sums added in part order into the outputs (and the
  *  potential); a group whose walk overflowed the stack goes to t.failedGroups instead. @p mass: target masses */

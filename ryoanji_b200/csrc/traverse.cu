@@ -802,7 +802,11 @@ __global__ void __launch_bounds__(kTravThreads, 5)
             rootEntry         = st.entry;
             // a system's groups meet only its own bodies: its own softening range decides
             if (lane == 0)
-                S.allUniform = T.uniformH && st.hLo == st.hHi && orderedFloat(st.hLo) == T.h0;
+            {
+                S.allUniform  = T.uniformH && st.hLo == st.hHi && orderedFloat(st.hLo) == T.h0;
+                S.uniformMass = st.mLo == st.mHi;
+                S.massU       = S.uniformMass ? orderedFloat(st.mLo) : 0.f;
+            }
             shells            = st.numShells;
             boxL[0]           = st.boxL[0];
             boxL[1]           = st.boxL[1];

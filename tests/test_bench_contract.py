@@ -74,7 +74,7 @@ def test_summary_is_last_and_fits_the_kept_tail():
             "phase_ms": {k: 12.3456789 for k in ("sort", "tree", "upsweep", "traverse", "total")},
             "interactions": {"p2p_per_body": 3788.123456, "m2p_per_body": 1291.987654},
             "accuracy": {"err_p99_1st_pct": 7.3456789e-4, "err_max": 1.23456e-2},
-            "accuracy_matched": {"theta": 0.43, "mparticles_per_s": 197.123456, "err_p99_1st_pct": 4.7123e-4},
+            "accuracy_matched": {"theta": 0.43, "value": 197.123456, "err_p99_1st_pct": 4.7123e-4},
             "ensemble": {"batched": leg, "plain_loop": leg, "speedup_solves_per_s": 9.3456},
             "served": {"served": leg, "plain": leg, "speedup_solves_per_s": 1.3345},
             "plummer_2e24": {"fixed_groups": {"mparticles_per_s": 161.7123, "err_p99_1st_pct": 4.47e-4,
@@ -90,4 +90,5 @@ def test_summary_is_last_and_fits_the_kept_tail():
     assert text.endswith(tail[1:])
     s = line["summary"]
     assert s["acc_theta_0.5"]["p99"] == 7.346e-4 and s["acc_matched"]["theta"] == 0.43
+    assert s["acc_matched"]["mps"] == 197.1
     assert s["ensemble"]["x"] == 9.346 and s["served"]["served_latency_p99_s"] == 2.346

@@ -178,7 +178,11 @@ def sorted_bodies(oracle, x, y, z, m, h, box):
     return tuple(np.ascontiguousarray(a[order]) for a in (x, y, z, m, h))
 
 
-def compare(oracle, x, y, z, m, h, box, bucket=64, theta=0.5, shells=0, mdq=False, force_tol=1e-5):
+def compare(oracle, x, y, z, m, h, box, bucket=64, theta=0.5, shells=0, mdq=False, force_tol=1e-5, rms_norm=False):
+    """both traversals on the same tree; with rms_norm the force and potential differences are measured against the
+    rms of the reference's field instead of each target's own: in a periodic box without its Ewald correction, and
+    with masses of both signs, a target's net field is a small difference of large terms, so a summation-order
+    difference far below the terms' round-off is a large fraction of it"""
     xs, ys, zs, ms, hs = sorted_bodies(oracle, x, y, z, m, h, box)
     f = RefFlow(xs, ys, zs, ms, hs, box, bucket, theta, mdq=mdq)
     try:
@@ -193,10 +197,18 @@ def compare(oracle, x, y, z, m, h, box, bucket=64, theta=0.5, shells=0, mdq=Fals
             pytest.fail(f"readBhStats differ: reference {rst[:4]} ours {ost[:4]}; first groups: {diff}")
         e = rel_err(host(ax), host(ay), host(az), host(rax), host(ray), host(raz))
         ep = np.abs(host(p) - host(rp)) / np.maximum(np.abs(host(rp)), 1e-30)
+        if rms_norm:
+            ra = np.stack([host(rax), host(ray), host(raz)]).astype(np.float64)
+            oa = np.stack([host(ax), host(ay), host(az)]).astype(np.float64)
+            e = np.linalg.norm(oa - ra, axis=0) / np.sqrt((ra * ra).sum(0).mean())
+            rpv = host(rp).astype(np.float64)
+            ep = np.abs(host(p) - rpv) / np.sqrt((rpv * rpv).mean())
         assert np.percentile(e, 99) <= force_tol, (np.percentile(e, 99), e.max())
         assert e.max() <= 50 * force_tol, e.max()
         assert np.percentile(ep, 99) <= force_tol, np.percentile(ep, 99)
-        assert abs(opot - rpot) <= 1e-5 * abs(rpot), (opot, rpot)
+        # the total against the sum of its terms' magnitudes where the terms cancel, else against itself
+        scale = 0.5 * float(np.abs(host(rp).astype(np.float64)).sum()) if rms_norm else abs(rpot)
+        assert abs(opot - rpot) <= 1e-5 * scale, (opot, rpot)
         return dict(stats=ost, ref_stats=rst, err_p99=float(np.percentile(e, 99)), err_max=float(e.max()),
                     retries=rretry)
     finally:
@@ -209,7 +221,7 @@ def test_golden_cases_match_reference_gpu(oracle, path):
     periodic = "ewald_u" in c
     box = c["box"]
     compare(oracle, c["x"], c["y"], c["z"], c["m"], c["h"], box, bucket=int(c["bucket"]), theta=float(c["theta"]),
-            shells=1 if periodic else 0)
+            shells=1 if periodic else 0, rms_norm=periodic)
 
 
 def test_uniform_cube_2e18_matches_reference_gpu(oracle):
@@ -237,4 +249,4 @@ def test_signed_masses_mdq_match_reference_gpu(oracle):
     m = (rng.choice([-1.0, 1.0], len(p.x)) / len(p.x)).astype(np.float32)
     h = np.full_like(p.x, 1e-3)
     box = np.array(ds.cube_box(p, pad=1e-6), np.float32)
-    compare(oracle, p.x, p.y, p.z, m, h, box, theta=0.3, mdq=True)
+    compare(oracle, p.x, p.y, p.z, m, h, box, theta=0.3, mdq=True, rms_norm=True)
