@@ -551,10 +551,10 @@ extern "C"
         uint64_t reserveBodies; /* resident bodies the arenas hold from creation on (default 0: grown on demand,
                                    doubling, which waits for the device at each growth) */
         uint64_t maxStepBodies; /* bodies one step advances at most (default 2^22; 0: every resident request each
-                                   step). The resident requests are kept in the order of their remaining work
-                                   (bodies x steps left), and each step advances the longest prefix of that order
-                                   that fits (at least one request): short requests are not held to the pace of the
-                                   long ones. The order is renewed when requests are admitted or retire. */
+                                   step). Taken in the order of their remaining work (bodies x steps left, least
+                                   first), the resident requests that still fit join the step (the first always
+                                   does): short requests are not held to the pace of the long ones. The choice is
+                                   renewed when requests are admitted or retire. */
     } ryo_engine_params;
     typedef struct ryo_engine_request
     {

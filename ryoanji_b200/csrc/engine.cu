@@ -241,6 +241,7 @@ struct ryo_engine
     double bytesPerBody;
     int maxSystems;
     uint64_t maxStepBodies = 0; // 0: every resident request steps every step
+    uint32_t stepping      = 0; // with a cap: the resident requests (a prefix of the arena) the steps advance
     double used = 0;
     std::deque<Request> queue;
     std::vector<Request> resident;
@@ -279,9 +280,10 @@ unsigned gridFor(size_t n, int sms)
 //! the work a request has left: bodies times the force evaluations still to come
 double remainingWork(const Request& q) { return double(q.n) * double(q.stepsLeft + (q.haveForces ? 0 : 1)); }
 
-/*! rebuild the arena with the survivors and the newly admitted requests in one order: by remaining work, least
- *  first, when steps are capped (so that a step's prefix holds the requests closest to completion), else survivors
- *  first, then the admitted in arrival order. Survivors are compacted on the device, admitted ones copied in. */
+/*! rebuild the arena with the survivors and the newly admitted requests in one order. When steps are capped, the
+ *  requests the next steps advance come first: taken in the order of their remaining work (least first), each one
+ *  that still fits the cap joins (the first always does); the rest follow. Without a cap: survivors first, then the
+ *  admitted in arrival order. Survivors are compacted on the device, admitted ones copied in. */
 void rebuildArena(ryo_engine* E, std::vector<Request>& admitted, cudaStream_t s)
 {
     Arena& src = E->arenas.buf[E->arenas.cur];
@@ -291,9 +293,26 @@ void rebuildArena(ryo_engine* E, std::vector<Request>& admitted, cudaStream_t s)
         all.emplace_back(r, false);
     for (auto& r : admitted)
         all.emplace_back(r, true);
+    E->stepping = uint32_t(all.size());
     if (E->maxStepBodies > 0)
+    {
         std::stable_sort(all.begin(), all.end(), [](const auto& a, const auto& b)
                          { return remainingWork(a.first) < remainingWork(b.first); });
+        std::vector<char> take(all.size(), 0);
+        uint64_t bodies = 0;
+        for (size_t k = 0; k < all.size(); ++k)
+            if (k == 0 || bodies + all[k].first.n <= E->maxStepBodies)
+            {
+                take[k] = 1;
+                bodies += all[k].first.n;
+            }
+        std::vector<std::pair<Request, bool>> ordered;
+        for (int pass = 1; pass >= 0; --pass)
+            for (size_t k = 0; k < all.size(); ++k)
+                if (take[k] == pass) ordered.push_back(all[k]);
+        all.swap(ordered);
+        E->stepping = uint32_t(std::count(take.begin(), take.end(), 1));
+    }
     uint64_t total = 0;
     for (auto& r : all)
         total += r.first.n;
@@ -559,17 +578,17 @@ extern "C" ryo_status ryo_engine_step(ryo_engine_t* E, ryo_engine_step_info* inf
                                if (info) *info = st;
                                return;
                            }
-                           // the requests this step advances: all, or the longest prefix of the resident order
-                           // (least remaining work first) within maxStepBodies, at least one
+                           // the requests this step advances: all, or those the last rebuild chose (the arena's
+                           // first E->stepping requests; while none of them retires the choice stands)
                            const uint32_t nsAll = uint32_t(E->resident.size());
                            uint32_t ns          = nsAll;
                            uint64_t n           = E->residentBodies;
                            if (E->maxStepBodies > 0)
                            {
-                               ns = 0;
+                               ns = std::min(E->stepping, nsAll);
                                n  = 0;
-                               while (ns < nsAll && (ns == 0 || n + E->resident[ns].n <= E->maxStepBodies))
-                                   n += E->resident[ns++].n;
+                               for (uint32_t k = 0; k < ns; ++k)
+                                   n += E->resident[k].n;
                            }
                            Arena& A    = E->arenas.buf[E->arenas.cur];
                            ArenaPtrs P = ptrsOf(A);

@@ -1,6 +1,7 @@
 """The reference demo's flow written in the reference's spellings (tests/cpp/demo_flow.cpp, compiled against
 ryoanji_b200/compat.hpp) runs on the GPU for the three type sets and gives exactly what the same steps give through
-the Python API: the same readBhStats, potential and accelerations, bit for bit (one library, one order of work)."""
+the Python API: the same readBhStats and accelerations bit for bit (one library, one order of work), and the same total
+potential to the round-off of its atomic sum."""
 import json
 import os
 import subprocess
@@ -60,7 +61,8 @@ def test_compat_demo_flow_equals_python_api(tmp_path):
                                ("mixed", torch.float64, torch.float32)):
         stats, pot, acc = _python_flow(xyz, dtype, mtype)
         assert lines[name]["stats"] == list(stats), (name, lines[name]["stats"], stats)
-        assert lines[name]["potential"] == pot, name
+        # the total is an FP64 atomic sum over groups: its last bit depends on their order
+        assert abs(lines[name]["potential"] - pot) <= 1e-13 * abs(pot), name
         cpp = np.fromfile(tmp_path / f"acc.{name}.bin", np.float64).reshape(3, n)
         assert np.array_equal(cpp, acc), name
     # the type sets differ only by precision: float-representable inputs give nearly the same field

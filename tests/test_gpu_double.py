@@ -99,10 +99,13 @@ def _bodies(oracle, kind_of_set):
         p = ds.plummer(1 << 16, seed=31, velocities=False)
     else:
         p = ds.uniform_cube(1 << 16, seed=32, eps=0.01)
-    box = np.array(ds.cube_box(p, pad=1e-6), np.float64)
     # double coordinates that are not float values: a jitter far below the spacing
     rng = np.random.default_rng(33)
     x, y, z = (a.astype(np.float64) + rng.uniform(-1e-9, 1e-9, p.n) for a in (p.x, p.y, p.z))
+    # the cube enclosing the jittered bodies (the reference asserts that every body lies in the box)
+    lo = np.array([x.min(), y.min(), z.min()])
+    ext = float((np.array([x.max(), y.max(), z.max()]) - lo).max()) * (1 + 1e-6)
+    box = np.array([lo[0], lo[0] + ext, lo[1], lo[1] + ext, lo[2], lo[2] + ext], np.float64)
     return sorted_bodies(oracle, x, y, z, p.m.astype(np.float64), p.h.astype(np.float64), box) + (box,)
 
 
