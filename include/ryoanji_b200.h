@@ -142,6 +142,12 @@ extern "C"
     RYO_API ryo_status ryo_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, uint64_t* keyBuf,
                                               uint32_t* valueBuf, ryo_stream_t stream);
 
+    /* Failure-detection self-test, no counterpart in the reference: one onesweep tile runs while the tile before it
+     * never publishes its counts, so the tile's bounded look-back wait (2^22 polls, a few seconds) runs out. Returns
+     * RYO_ERR_TIMEOUT, as a sort whose wait ran out does, and leaves the context usable; RYO_ERR_INTERNAL if the
+     * wait did not report. Allocates and frees its own small buffers. */
+    RYO_API ryo_status ryo_sort_wait_timeout_selftest(ryo_stream_t stream);
+
     /* cstone::computeOctree / updateOctreeGpu to convergence (cstone/include/cstone/tree/csarray.hpp:409-440,
      * update_gpu.cuh:43-68): the cornerstone leaf array of sorted keys with at most @p bucketSize particles per
      * leaf. Built in one pass (no host-synchronised rebalance loop); identical to the reference's fixed point.

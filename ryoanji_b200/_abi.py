@@ -135,6 +135,7 @@ SIGNATURES = {
     "ryo_sort_by_key_temp_bytes": (_sz, [_sz]),
     "ryo_sort_by_key": (_i, [_p, _p, _sz, _p, _p, _p, _sz, _p]),
     "ryo_sort_by_key_static": (_i, [_p, _p, _sz, _p, _p, _p]),
+    "ryo_sort_wait_timeout_selftest": (_i, [_p]),
     "ryo_compute_octree": (_i, [_p, _p, _sz, _u, _p, _p, _i, C.POINTER(_i), _p]),
     "ryo_build_octree": (_i, [_p, _p, _i, _p, _p, _p, C.POINTER(_i), _p, _p, _p, _p]),
     "ryo_compute_fixed_groups": (_i, [_u32, _u32, _u, _p, _p]),

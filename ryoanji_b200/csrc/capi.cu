@@ -300,6 +300,18 @@ extern "C" ryo_status ryo_sort_by_key_static(uint64_t* keys, uint32_t* values, s
                    });
 }
 
+extern "C" ryo_status ryo_sort_wait_timeout_selftest(ryo_stream_t stream)
+{
+    return guarded(tlsError,
+                   [&]
+                   {
+                       if (!sortWaitTimeoutSelfTest(stream))
+                           throw ApiError{RYO_ERR_INTERNAL, "sort_wait_timeout_selftest: the look-back wait of a "
+                                                            "tile whose predecessor never published did not report"};
+                       throw ApiError{RYO_ERR_TIMEOUT, "sort_wait_timeout_selftest: look-back wait timed out"};
+                   });
+}
+
 extern "C" ryo_status ryo_compute_octree(ryo_ctx_t* ctx, const uint64_t* sortedKeys, size_t n, unsigned bucketSize,
                                          uint64_t* leaves, uint32_t* counts, int capacity, int* numLeaves,
                                          ryo_stream_t stream)

@@ -191,6 +191,8 @@ size_t sortTempBytes(size_t n);
 bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_t* valuesAlt, size_t n, int beginBit,
                     int endBit, void* tmp, size_t tmpBytes, unsigned int* errorFlag, cudaStream_t s,
                     bool iotaValues = false);
+//! runs one onesweep tile whose predecessor never publishes; true if its bounded look-back wait ran out and said so
+bool sortWaitTimeoutSelfTest(cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------------- octree.cu
 //! cornerstone leaves of sorted keys; returns numLeaves (host), writes only if numLeaves <= capacity

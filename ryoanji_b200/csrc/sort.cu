@@ -419,6 +419,49 @@ bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_
     return inAlt;
 }
 
+/*! failure-detection self-test of the look-back wait. One pass over two tiles of zero keys is launched with a single
+ *  block whose tile ticket starts at 1: the block takes tile 1, and tile 0's status words are never published, so
+ *  each digit thread's bounded wait runs out after kSpinLimit polls and raises the flag. The accesses stay inside the
+ *  buffers: every key has digit 0 (base 0), so the lone tile scatters to positions [0, kSortTile) of the 2 x
+ *  kSortTile outputs. Returns whether the flag was raised. */
+bool sortWaitTimeoutSelfTest(cudaStream_t s)
+{
+    const size_t n = 2 * size_t(kSortTile);
+    struct Buffers
+    {
+        void* p[5] = {};
+        ~Buffers()
+        {
+            for (void* q : p)
+                if (q) cudaFree(q);
+        }
+    } b;
+    const size_t bytes[5] = {n * sizeof(uint64_t), n * sizeof(uint64_t), n * sizeof(uint32_t), sortTempBytes(n),
+                             sizeof(unsigned int)};
+    for (int i = 0; i < 5; ++i)
+        RYO_CUDA(cudaMalloc(&b.p[i], bytes[i]));
+    auto* keys = static_cast<uint64_t*>(b.p[0]);
+    auto* kout = static_cast<uint64_t*>(b.p[1]);
+    auto* vout = static_cast<uint32_t*>(b.p[2]);
+    auto* flag = static_cast<unsigned int*>(b.p[4]);
+    SortTemp t = sortLayout(b.p[3], n);
+    RYO_CUDA(cudaMemsetAsync(keys, 0, bytes[0], s));
+    RYO_CUDA(cudaMemsetAsync(b.p[3], 0, bytes[3], s));
+    RYO_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned int), s));
+    const unsigned int one = 1;
+    RYO_CUDA(cudaMemcpyAsync(t.tile, &one, sizeof(one), cudaMemcpyHostToDevice, s));
+    digitHistogram<<<1, 256, 0, s>>>(keys, n, 0, 1, t.hist);
+    RYO_LAUNCH_CHECK();
+    digitBases<<<1, kDigits, 0, s>>>(t.hist, t.base, 1);
+    RYO_LAUNCH_CHECK();
+    onesweepPass<<<1, kSortBlock, 0, s>>>(keys, nullptr, kout, vout, n, 0, 8, t.base, t.status, t.tile, 1u, flag);
+    RYO_LAUNCH_CHECK();
+    unsigned int raised = 0;
+    RYO_CUDA(cudaMemcpyAsync(&raised, flag, sizeof(raised), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaStreamSynchronize(s));
+    return raised != 0;
+}
+
 
 // ------------------------------------------------------------------------------------------------ fixed scratch
 

@@ -206,7 +206,9 @@ def test_ewald_matches_reference_gpu(kind):
     import ryoanji_b200 as ryo
     lib = ref_lib()
     lib.ref_gpu_ewald.restype = C.c_double
-    lib.ref_gpu_ewald.argtypes = ([C.c_int, C.c_void_p, C.c_void_p] + [C.c_uint32] * 3 + [C.c_void_p] * 7 +
+    # kind, root centre, root multipole; first, last, numGroups; gStart, gEnd, x, y, z, m; box6, G; ugrav, ax, ay,
+    # az, settings
+    lib.ref_gpu_ewald.argtypes = ([C.c_int, C.c_void_p, C.c_void_p] + [C.c_uint32] * 3 + [C.c_void_p] * 6 +
                                   [C.c_void_p, C.c_float] + [C.c_void_p] * 5)
     p = ds.periodic_box(4096, seed=51, eps=0.01)
     rng = np.random.default_rng(52)

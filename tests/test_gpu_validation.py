@@ -134,3 +134,19 @@ def test_bounding_box_is_the_exact_min_and_max():
         b = ryo.compute_bounding_box(*(torch.from_numpy(a).cuda() for a in xyz))
         want = [v for a in xyz for v in (float(a.min()), float(a.max()))]
         assert list(b) == want, (n, list(b), want)
+
+
+def test_sort_look_back_wait_runs_out_and_reports():
+    """the onesweep look-back's bounded wait: a tile whose predecessor never publishes gives up after its poll limit,
+    raises the flag the host reads (RYO_ERR_TIMEOUT), and leaves the context usable for the next sort"""
+    import ryoanji_b200 as ryo
+    torch.cuda.synchronize()
+    status = ryo.lib.ryo_sort_wait_timeout_selftest(None)
+    msg = (ryo.lib.ryo_ctx_last_error(None) or b"").decode()
+    assert status == ryo._abi.ERR_TIMEOUT and "timed out" in msg, (status, msg)
+    rng = np.random.default_rng(19)
+    keys = torch.from_numpy(rng.integers(0, 2**63, 100003, dtype=np.int64)).cuda()
+    vals = torch.arange(keys.numel(), dtype=torch.int32, device="cuda")
+    want = np.argsort(keys.cpu().numpy(), kind="stable")
+    ryo.sort_by_key(keys, vals)
+    assert np.array_equal(vals.cpu().numpy(), want)
