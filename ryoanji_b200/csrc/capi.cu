@@ -1762,7 +1762,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        DevBox<float> unused = hbox[0];
                        launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
                                           oct.parents, oct.prefixes, 1.0f / P->theta, unused, records, nullptr, nullptr,
-                                          nullptr, s, dBx, sysLevel, sysRoots, dipoles);
+                                          nullptr, s, dBx, sysLevel, sysRoots, dipoles, ns);
                        mark(ctx, P, 3, s);
 
                        // groups inside systems, system roots, traversal

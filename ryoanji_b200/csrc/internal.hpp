@@ -292,7 +292,7 @@ void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int num
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
                         float4* centers, float* multipoles, double* rootCenterMultipole, cudaStream_t s,
                         const DevBox<float>* sysBoxes = nullptr, int sysLevel = 0, double* sysRoots = nullptr,
-                        float4* dipoles = nullptr);
+                        float4* dipoles = nullptr, uint32_t numSystems = 0);
 
 //! pack reference-layout tree arrays into node records (for the reference-signature traverse)
 void launchPackNodes(int numNodes, const float4* centers, const float* multipoles, const int* childOffsets,

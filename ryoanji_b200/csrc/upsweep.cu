@@ -374,6 +374,7 @@ struct FusedArgs
     // s, and sysRoots (11 doubles per system) receives the FP64 expansion of every system's root node
     const DevBox<float>* sysBoxes;
     int sysLevel;
+    uint32_t numSystems; // system prefixes at or above this index belong to no system: their nodes are empty
     double* sysRoots;
     // monopole + dipole + quadrupole expansions: node dipoles (px, py, pz, 0) are written here when not null, and
     // the second moments are combined with the dipole terms of the parallel-axis theorem
@@ -420,8 +421,13 @@ __device__ void emitNode(const FusedArgs& A, int node, const double c[3], double
             uint32_t sys      = uint32_t(start >> (63 - sysBits));
             uint64_t local    = (start << sysBits) & (kKeyEnd - 1);
             uint64_t localPre = encodePrefix(local, 3 * (lvl - A.sysLevel));
-            if (w != 0.0 && float(w) != 0.f) mac = vecMacR2(localPre, com, A.invTheta, A.sysBoxes[sys]);
-            if (lvl == A.sysLevel && A.sysRoots) writeRootExpansion(A.sysRoots + 11 * size_t(sys), c, raw);
+            // the tree holds all 8^sysLevel system-level nodes; those past the last system are empty leaves, and
+            // sysBoxes and sysRoots have entries for real systems only
+            if (sys < A.numSystems)
+            {
+                if (w != 0.0 && float(w) != 0.f) mac = vecMacR2(localPre, com, A.invTheta, A.sysBoxes[sys]);
+                if (lvl == A.sysLevel && A.sysRoots) writeRootExpansion(A.sysRoots + 11 * size_t(sys), c, raw);
+            }
         }
     }
     float qf[8];
@@ -599,13 +605,15 @@ void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int num
                         const int* leafToInternal, const int* childOffsets, const int* parents,
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
                         float4* centers, float* multipoles, double* root, cudaStream_t s,
-                        const DevBox<float>* sysBoxes, int sysLevel, double* sysRoots, float4* dipoles)
+                        const DevBox<float>* sysBoxes, int sysLevel, double* sysRoots, float4* dipoles,
+                        uint32_t numSystems)
 {
     FusedArgs A;
     A.dipoles        = dipoles;
     A.sysBoxes       = sysBoxes;
     A.sysLevel       = sysLevel;
     A.sysRoots       = sysRoots;
+    A.numSystems     = numSystems;
     A.xyzm           = xyzm;
     A.layout         = layout;
     A.leafToInternal = leafToInternal;

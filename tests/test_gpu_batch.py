@@ -140,3 +140,32 @@ def test_batch_rejects_bad_descriptions():
     bad = ryo.Box(0, 1, 0, 2, 0, 1, boundary=(ryo.BOUNDARY_PERIODIC,) * 3)
     with pytest.raises(ryo.RyoError):
         ryo.solve_batch([ryo.BatchSystem(10, bad)], x, x, x, x, x, x, x, x, x)
+
+
+def test_batch_system_counts_between_powers_of_eight():
+    """a batch of ns systems builds one tree whose system level holds 8^L >= ns nodes; the nodes past the last system
+    are empty and own no per-system entry (box, root expansion). Batches of 9 and 65 systems (55 and 447 empty
+    system-level nodes), solved one after the other so that each batch's per-system tables follow the previous one's
+    in memory, each equal their systems' single solves"""
+    import ryoanji_b200 as ryo
+    rng = np.random.default_rng(23)
+    params = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=64, group_tolerance=2.0)
+    for ns in (65, 9, 65):
+        sizes = [int(v) for v in rng.integers(200, 3000, ns)]
+        systems = [(f"s{i}", ds.plummer(s, seed=300 + i, velocities=False, center=tuple(rng.uniform(-5, 5, 3))),
+                    None) for i, s in enumerate(sizes)]
+        res, B = _run_batch(systems, params)
+        assert len(res.energies) == ns
+        first = 0
+        for (name, p, _), e_batch in zip(systems, res.energies):
+            sl = slice(first, first + p.n)
+            first += p.n
+            x, y, z, m, h = (_dev(a) for a in (p.x, p.y, p.z, p.m, p.h))
+            pot, ax, ay, az = (torch.empty(p.n, device="cuda") for _ in range(4))
+            sp = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=64, group_tolerance=2.0)
+            r = ryo.solve(x, y, z, m, h, pot, ax, ay, az, sp)
+            assert torch.equal(B["x"][sl], x), (ns, name)
+            amag = torch.sqrt(ax * ax + ay * ay + az * az) + 1e-30
+            for k, ref in (("ax", ax), ("ay", ay), ("az", az)):
+                assert float(((B[k][sl] - ref).abs() / amag).max()) <= 1e-6, (ns, name, k)
+            assert e_batch == pytest.approx(r.potential_energy, rel=1e-9, abs=1e-12), (ns, name)
