@@ -206,6 +206,9 @@ int buildLeaves(ryo_ctx* ctx, const uint64_t* keys, size_t n64, unsigned bucket,
 
 // ------------------------------------------------------------------------------------------------ links
 
+constexpr uint64_t kEmptySlot = 31; // sort key of a slot without a node: after every level (0 .. 21)
+constexpr int kLevelBits      = 5;  // bits of a slot's sort key
+
 //! weight of the digits on levels 1..level+1 in the binary-radix-tree to octree index map (octree.hpp:55-65)
 __device__ inline int treeIndexWeight(uint64_t key, unsigned level)
 {
@@ -219,21 +222,45 @@ __device__ inline int treeIndexWeight(uint64_t key, unsigned level)
 }
 
 /*! unsorted node layout: internal nodes first, numbered as in the reference's binary-radix-tree map (node of the
- *  leaf pair whose common prefix ends on a level boundary), then the leaves (octree_gpu.cu:41-64) */
+ *  leaf pair whose common prefix ends on a level boundary), then the leaves (octree_gpu.cu:41-64). Beside it, the
+ *  sort slots of the level-major order: slot 2t holds the internal node of leaf pair t, if there is one, and slot
+ *  2t + 1 leaf t; a slot's key is its node's level (31 for an empty slot) and its value the node's unsorted index.
+ *  Nodes of one level appear in the slots in key order: two nodes of a level cover disjoint key ranges, and the leaf
+ *  indices that stand for them (t for the node of pair t, which holds leaves t and t + 1; j for leaf j) are ordered
+ *  as the ranges are. A stable sort of the slots by level is therefore the sort of the placeholder-bit prefixes. */
 __global__ void unsortedLayout(const uint64_t* __restrict__ leaves, int numInternal, int numLeaves,
-                               uint64_t* __restrict__ prefixes)
+                               uint64_t* __restrict__ prefixes, uint64_t* __restrict__ slotLevel,
+                               uint32_t* __restrict__ slotNode)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= numLeaves) return;
     uint64_t key              = leaves[t];
     uint64_t next             = leaves[t + 1];
-    prefixes[t + numInternal] = encodePrefix(key, 3 * int(rangeLevel(next - key)));
+    unsigned leafLevel        = rangeLevel(next - key);
+    prefixes[t + numInternal] = encodePrefix(key, 3 * int(leafLevel));
+    slotLevel[2 * t + 1]      = leafLevel;
+    slotNode[2 * t + 1]       = uint32_t(numInternal + t);
     int common                = commonBits(key, next);
     if (t < numLeaves - 1 && common % 3 == 0)
     {
-        int at       = (t + treeIndexWeight(key, common / 3)) / 7;
-        prefixes[at] = encodePrefix(key, common);
+        int at           = (t + treeIndexWeight(key, common / 3)) / 7;
+        prefixes[at]     = encodePrefix(key, common);
+        slotLevel[2 * t] = uint64_t(common / 3);
+        slotNode[2 * t]  = uint32_t(at);
     }
+    else
+    {
+        slotLevel[2 * t] = kEmptySlot;
+        slotNode[2 * t]  = 0;
+    }
+}
+
+//! prefixes in the level-major order: sorted[i] = unsorted[order[i]]
+__global__ void gatherPrefixes(const uint64_t* __restrict__ unsorted, const uint32_t* __restrict__ order, int numNodes,
+                               uint64_t* __restrict__ sorted)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < numNodes) sorted[i] = unsorted[order[i]];
 }
 
 __global__ void invertOrder(const uint32_t* __restrict__ order, int numNodes, int numInternal,
@@ -296,20 +323,23 @@ void linkOctree(ryo_ctx* ctx, const uint64_t* leaves, int numLeaves, const Octre
 {
     int numInternal = (numLeaves - 1) / 7;
     int numNodes    = numLeaves + numInternal;
+    size_t slots    = 2 * size_t(numLeaves);
     uint64_t* pre   = ctx->scratch<uint64_t>("link.prefix", numNodes, s);
-    uint64_t* preB  = ctx->scratch<uint64_t>("link.prefixB", numNodes, s);
-    uint32_t* ord   = ctx->scratch<uint32_t>("link.order", numNodes, s);
-    uint32_t* ordB  = ctx->scratch<uint32_t>("link.orderB", numNodes, s);
-    size_t tmpBytes = sortTempBytes(numNodes);
+    uint64_t* lvl   = ctx->scratch<uint64_t>("link.slotLevel", slots, s);
+    uint64_t* lvlB  = ctx->scratch<uint64_t>("link.slotLevelB", slots, s);
+    uint32_t* ord   = ctx->scratch<uint32_t>("link.order", slots, s);
+    uint32_t* ordB  = ctx->scratch<uint32_t>("link.orderB", slots, s);
+    size_t tmpBytes = sortTempBytes(slots);
     void* tmp       = ctx->scratch<char>("link.sorttmp", tmpBytes, s);
 
-    unsortedLayout<<<ceilDiv(numLeaves, 256), 256, 0, s>>>(leaves, numInternal, numLeaves, pre);
+    unsortedLayout<<<ceilDiv(numLeaves, 256), 256, 0, s>>>(leaves, numInternal, numLeaves, pre, lvl, ord);
     RYO_LAUNCH_CHECK();
-    // prefixes are unique, so any correct sort gives the reference's order
-    bool alt = radixSortPairs(pre, ord, preB, ordB, numNodes, 0, 64, tmp, tmpBytes, &ctx->ctl->error, s, true);
-    const uint64_t* sortedPre = alt ? preB : pre;
-    const uint32_t* order     = alt ? ordB : ord;
-    RYO_CUDA(cudaMemcpyAsync(out.prefixes, sortedPre, sizeof(uint64_t) * numNodes, cudaMemcpyDeviceToDevice, s));
+    // one stable pass over the 5-bit levels; the empty slots sort behind the numNodes nodes
+    bool alt              = radixSortPairs(lvl, ord, lvlB, ordB, slots, 0, kLevelBits, tmp, tmpBytes,
+                                           &ctx->ctl->error, s, false);
+    const uint32_t* order = alt ? ordB : ord;
+    gatherPrefixes<<<ceilDiv(numNodes, 256), 256, 0, s>>>(pre, order, numNodes, out.prefixes);
+    RYO_LAUNCH_CHECK();
     invertOrder<<<ceilDiv(numNodes, 256), 256, 0, s>>>(order, numNodes, numInternal, out.internalToLeaf,
                                                         out.leafToInternal);
     RYO_LAUNCH_CHECK();
