@@ -274,7 +274,8 @@ extern "C"
      * receives 0.5 G sum(m phi) over the traversed targets. Groups whose traversal overflows the stack are split
      * and traversed again (ryoanji/src/ryoanji/nbody/traversal_gpu.cu:582-618). Every group must hold 1 to 64
      * targets within [firstBody, lastBody) (RYO_ERR_BAD_ARG otherwise; the call reads the group arrays back to check
-     * them). */
+     * them). The call synchronises its stream (the group check, the split passes, the statistics), so it cannot be
+     * captured in a CUDA graph. */
     RYO_API ryo_status ryo_traverse_f32(ryo_ctx_t* ctx, const ryo_group_view* grp, int initNodeIdx, const float* xt,
                                         const float* yt, const float* zt, const float* mt, const float* ht,
                                         const float* xs, const float* ys, const float* zs, const float* ms,
@@ -395,7 +396,8 @@ extern "C"
                                           double* az, ryo_stream_t stream);
     /* accuracy reference: double-precision direct sum for selected targets of float data, exact 1/sqrt
      * (the P2P<true> form, ryoanji/src/ryoanji/nbody/kernel.hpp:55-120); writes G m phi and G a per target. Every
-     * target index must be a body (the call reads the indices back to check them; RYO_ERR_BAD_ARG otherwise). */
+     * target index must be a body (the call reads the indices back to check them, synchronising its stream;
+     * RYO_ERR_BAD_ARG otherwise). */
     RYO_API ryo_status ryo_direct_targets_f64(const int64_t* targets, size_t numTargets, const float* x,
                                               const float* y, const float* z, const float* m, const float* h,
                                               size_t numBodies, double G, const double* boxL, int numShells,
