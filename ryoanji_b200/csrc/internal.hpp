@@ -347,6 +347,8 @@ struct TraverseLaunch
     // (direct bodies + 2 x approximated cells) passes heavyCost stops and is queued in heavyGroups. Second pass
     // (parts > 0): item i walks group heavyGroups[i / parts] in full but evaluates only every parts-th batch,
     // starting at batch i % parts, and writes its compensated partial sums to partials[i][64] for the combine step.
+    uint32_t balanceGroups; // group count the split threshold follows (0: the launch's); a solve traversed in several
+                            // launches passes its total, so that its groups split as in one launch
     uint32_t* heavyGroups;
     uint32_t heavyCapacity;
     unsigned heavyCost;
