@@ -19,6 +19,7 @@ reference sources) on the host cores for a bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import subprocess
@@ -654,8 +655,10 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
     def serve_once():
         # served: the engine admits what has arrived at every step. Its two arenas are reserved at creation for 2^25
         # resident bodies (the stream peaks near 2.5e7), as a server sizes them at start-up.
-        eng = ryo.Engine(params, hbm_budget_bytes=120e9, ctx=ctx, reserve_bodies=1 << 25,
-                         max_step_bodies=args.served_max_step_bodies)
+        # the engine's solves record their phase times (CUDA events), to show where a step's device time goes
+        eng = ryo.Engine(dataclasses.replace(params, timing=True), hbm_budget_bytes=120e9, ctx=ctx,
+                         reserve_bodies=1 << 25, max_step_bodies=args.served_max_step_bodies)
+        phase = np.zeros(6)
         outs = {}
         done = {}
         i = 0
@@ -675,13 +678,20 @@ def run_served(args, ctx, dev, rank=0, world=1, dist=None) -> dict:
             if st["queued"] == 0 and st["resident"] == 0:
                 time.sleep(max(0.0, reqs[i]["arrival"] - (time.perf_counter() - t0)))
                 continue
-            eng.step()
+            info = eng.step()
+            phase += np.array(info["ms"][:6])
             steps += 1
             for d in eng.poll():
                 done[d["tag"]] = time.perf_counter() - t0
                 outs[d["tag"]] = d
         served = summary(done, max(done.values(), default=0.0))
         served["engine_steps"] = steps
+        # device time of the engine's batched solves by phase, summed over the steps: keys + sort + gather, leaves +
+        # links, upsweep, groups + traversal, Ewald; share of the solves' total
+        names = ("sort", "tree", "upsweep", "traverse", "ewald")
+        served["solve_phase_ms"] = {k: round(float(v), 1) for k, v in zip(names + ("total",), phase)}
+        served["solve_phase_share"] = {k: round(float(v / phase[5]), 4) if phase[5] > 0 else None
+                                       for k, v in zip(names, phase)}
         served["max_step_bodies"] = ("library default" if args.served_max_step_bodies is None
                                      else args.served_max_step_bodies)
         drift = [abs(d["kinetic"] + d["potential"] - d["initial"]) / abs(d["initial"]) for d in outs.values()
