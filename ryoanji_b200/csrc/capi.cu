@@ -1382,7 +1382,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
                               : nullptr;
     launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
                        oct.parents, oct.prefixes, 1.0f / P->theta, dbox, records, nullptr, nullptr,
-                       root, s, nullptr, 0, nullptr, dipoles);
+                       root, s, nullptr, 0, nullptr, dipoles, 0, levelRange);
 
     mark(ctx, P, 3, s);
     // groups and traversal
@@ -1780,7 +1780,7 @@ extern "C" ryo_status ryo_solve_batch_f32(ryo_ctx_t* ctx, const ryo_solve_params
                        DevBox<float> unused = hbox[0];
                        launchFusedUpsweep(ctx, xyzm, nl, nn, layout, oct.leafToInternal + ni, oct.childOffsets,
                                           oct.parents, oct.prefixes, 1.0f / P->theta, unused, records, nullptr, nullptr,
-                                          nullptr, s, dBx, sysLevel, sysRoots, dipoles, ns);
+                                          nullptr, s, dBx, sysLevel, sysRoots, dipoles, ns, levelRange);
                        mark(ctx, P, 3, s);
 
                        // groups inside systems, system roots, traversal

@@ -284,15 +284,16 @@ LetCounts letSelect(ryo_ctx* ctx, const NodeRecord* nodes, const int* parents, i
 void letWrite(const LetCounts& c, const NodeRecord* nodes, int numNodes, const float4* xyzm, const float* h,
               const LetBox& box, uint32_t* buffer, cudaStream_t s);
 
-/*! fused upsweep of the solver path: per leaf FP64 centre of mass and P2M in one pass over the bodies, then M2M
- *  bottom-up by last-arriving child, MAC radius, and the traversal node records. Also writes the reference-layout
- *  centers (4 floats) and multipoles (8 floats) if not null. */
+/*! upsweep of the solver path: per leaf FP64 centre of mass and P2M in one pass over the bodies, then M2M level by
+ *  level from the deepest (one launch per level, @p hostLevelRange the host copy of the level-major ranges), MAC
+ *  radius, and the traversal node records. Also writes the reference-layout centers (4 floats) and multipoles (8
+ *  floats) if not null. */
 void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
                         const int* leafToInternal, const int* childOffsets, const int* parents,
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
                         float4* centers, float* multipoles, double* rootCenterMultipole, cudaStream_t s,
                         const DevBox<float>* sysBoxes = nullptr, int sysLevel = 0, double* sysRoots = nullptr,
-                        float4* dipoles = nullptr, uint32_t numSystems = 0);
+                        float4* dipoles = nullptr, uint32_t numSystems = 0, const int* hostLevelRange = nullptr);
 
 //! pack reference-layout tree arrays into node records (for the reference-signature traverse)
 void launchPackNodes(int numNodes, const float4* centers, const float* multipoles, const int* childOffsets,

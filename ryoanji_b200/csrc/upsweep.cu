@@ -365,7 +365,6 @@ struct FusedArgs
     float invTheta;
     DevBox<float> box;
     DNode* dn;
-    unsigned int* arrivals;
     NodeRecord* records;
     float4* centers;
     float* multipoles;
@@ -496,8 +495,8 @@ __device__ void combineChildren(const FusedArgs& A, int node, int fc, int sub, u
     }
 }
 
-/*! eight lanes per leaf: one pass over the bodies, then the group of the last-arriving sibling climbs and combines
- *  each parent with one child per lane (small register footprint, so many leaf groups stay resident per SM) */
+/*! eight lanes per leaf: one pass over the bodies, P2M of the leaf (small register footprint, so many leaf groups
+ *  stay resident per SM). The internal nodes follow level by level (levelCombineKernel). */
 __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
 {
     int tid     = blockIdx.x * blockDim.x + threadIdx.x;
@@ -582,23 +581,21 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
         emitNode(A, node, c, W, M, q, dp, 0, b0, b1 - b0);
     }
 
-    // climb: the group of the eighth sibling to arrive combines the parent, one child per lane
+}
+
+/*! the internal nodes of one tree level, [first, last) in the level-major order: eight lanes per node combine its
+ *  eight children (one per lane), which the leaf pass or the previous (deeper) level wrote. Leaves of the level are
+ *  skipped. */
+__global__ void __launch_bounds__(256) levelCombineKernel(FusedArgs A, int first, int last)
+{
+    const int tid  = blockIdx.x * blockDim.x + threadIdx.x;
+    const int node = first + tid / kTpl;
+    const int sub  = tid % kTpl;
+    if (node >= last) return;                // whole groups of eight leave together
+    const int fc = A.childOffsets[node];
+    if (fc == 0) return;                     // a leaf: written by the leaf pass
     const unsigned gmask = 0xFFu << (threadIdx.x & 24u);
-    while (node > 0)
-    {
-        int parent = A.parents[(node - 1) / 8];
-        int last   = 0;
-        if (sub == 0)
-        {
-            __threadfence();
-            last = atomicAdd(A.arrivals + parent, 1u) == 7u;
-        }
-        last = __shfl_sync(gmask, last, 0, kTpl);
-        if (!last) break;
-        __threadfence();
-        combineChildren(A, parent, A.childOffsets[parent], sub, gmask);
-        node = parent;
-    }
+    combineChildren(A, node, fc, sub, gmask);
 }
 
 void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
@@ -606,7 +603,7 @@ void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int num
                         const uint64_t* prefixes, float invTheta, const DevBox<float>& box, NodeRecord* records,
                         float4* centers, float* multipoles, double* root, cudaStream_t s,
                         const DevBox<float>* sysBoxes, int sysLevel, double* sysRoots, float4* dipoles,
-                        uint32_t numSystems)
+                        uint32_t numSystems, const int* hostLevelRange)
 {
     FusedArgs A;
     A.dipoles        = dipoles;
@@ -625,14 +622,21 @@ void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int num
     A.invTheta       = invTheta;
     A.box            = box;
     A.dn             = ctx->scratch<DNode>("up.dnode", numNodes, s);
-    A.arrivals       = ctx->scratch<unsigned int>("up.arrivals", numNodes, s);
     A.records        = records;
     A.centers        = centers;
     A.multipoles     = multipoles;
     A.root           = root;
-    RYO_CUDA(cudaMemsetAsync(A.arrivals, 0, sizeof(unsigned int) * numNodes, s));
     fusedUpsweepKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(A);
     RYO_LAUNCH_CHECK();
+    // internal nodes bottom-up, one launch per level that holds nodes (level-major order: level l is
+    // [levelRange[l], levelRange[l + 1]))
+    for (int l = kMaxLevel - 1; l >= 0; --l)
+    {
+        const int first = hostLevelRange[l], last = hostLevelRange[l + 1];
+        if (last <= first) continue;
+        levelCombineKernel<<<ceilDiv(size_t(last - first) * kTpl, 256), 256, 0, s>>>(A, first, last);
+        RYO_LAUNCH_CHECK();
+    }
 }
 
 // ------------------------------------------------------------------------------------------------ packing
