@@ -284,9 +284,9 @@ LetCounts letSelect(ryo_ctx* ctx, const NodeRecord* nodes, const int* parents, i
 void letWrite(const LetCounts& c, const NodeRecord* nodes, int numNodes, const float4* xyzm, const float* h,
               const LetBox& box, uint32_t* buffer, cudaStream_t s);
 
-/*! upsweep of the solver path: per leaf FP64 centre of mass and P2M in one pass over the bodies, then M2M level by
- *  level from the deepest (one launch per level, @p hostLevelRange the host copy of the level-major ranges), MAC
- *  radius, and the traversal node records. Also writes the reference-layout centers (4 floats) and multipoles (8
+/*! upsweep of the solver path: per leaf FP64 centre of mass and P2M in one pass over the bodies, then M2M bottom-up
+ *  (by last-arriving-child counters, or for large trees level by level from the deepest, one launch per level, with
+ *  @p hostLevelRange the host copy of the level-major ranges), MAC radius, and the traversal node records. Also writes the reference-layout centers (4 floats) and multipoles (8
  *  floats) if not null. */
 void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
                         const int* leafToInternal, const int* childOffsets, const int* parents,

@@ -369,6 +369,8 @@ struct FusedArgs
     float4* centers;
     float* multipoles;
     double* root; // 11 doubles: centre (3) + finalized multipole (8)
+    // internal nodes by the climb (arrival counters, non-null) or by level launches (null)
+    unsigned int* arrivals;
     // batched systems: node keys carry a system prefix of sysLevel octree levels; sysBoxes[s] is the box of system
     // s, and sysRoots (11 doubles per system) receives the FP64 expansion of every system's root node
     const DevBox<float>* sysBoxes;
@@ -496,7 +498,8 @@ __device__ void combineChildren(const FusedArgs& A, int node, int fc, int sub, u
 }
 
 /*! eight lanes per leaf: one pass over the bodies, P2M of the leaf (small register footprint, so many leaf groups
- *  stay resident per SM). The internal nodes follow level by level (levelCombineKernel). */
+ *  stay resident per SM). The internal nodes follow by the climb (A.arrivals set: the group of the eighth sibling to
+ *  arrive combines the parent, one child per lane, and goes on up) or level by level (levelCombineKernel). */
 __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
 {
     int tid     = blockIdx.x * blockDim.x + threadIdx.x;
@@ -580,7 +583,24 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
         storeDNode(A.dn + node, c, W, M, q, dp);
         emitNode(A, node, c, W, M, q, dp, 0, b0, b1 - b0);
     }
+    if (!A.arrivals) return;
 
+    const unsigned gmask = 0xFFu << (threadIdx.x & 24u);
+    while (node > 0)
+    {
+        int parent = A.parents[(node - 1) / 8];
+        int last   = 0;
+        if (sub == 0)
+        {
+            __threadfence();
+            last = atomicAdd(A.arrivals + parent, 1u) == 7u;
+        }
+        last = __shfl_sync(gmask, last, 0, kTpl);
+        if (!last) break;
+        __threadfence();
+        combineChildren(A, parent, A.childOffsets[parent], sub, gmask);
+        node = parent;
+    }
 }
 
 /*! the internal nodes of one tree level, [first, last) in the level-major order: eight lanes per node combine its
@@ -597,6 +617,9 @@ __global__ void __launch_bounds__(256) levelCombineKernel(FusedArgs A, int first
     const unsigned gmask = 0xFFu << (threadIdx.x & 24u);
     combineChildren(A, node, fc, sub, gmask);
 }
+
+//! trees of at least this many nodes combine their internal nodes level by level (a 2^26-body cube has about 5M)
+constexpr int kLevelUpsweepNodes = 1 << 21;
 
 void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
                         const int* leafToInternal, const int* childOffsets, const int* parents,
@@ -622,12 +645,18 @@ void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int num
     A.invTheta       = invTheta;
     A.box            = box;
     A.dn             = ctx->scratch<DNode>("up.dnode", numNodes, s);
+    // the climb leaves the other leaf groups of a climbing warp idle, which large trees pay for; each level launch
+    // costs a few microseconds, which small and deep trees pay for. The results are the same either way.
+    const bool byLevels = hostLevelRange && numNodes >= kLevelUpsweepNodes;
+    A.arrivals          = byLevels ? nullptr : ctx->scratch<unsigned int>("up.arrivals", numNodes, s);
     A.records        = records;
     A.centers        = centers;
     A.multipoles     = multipoles;
     A.root           = root;
+    if (A.arrivals) RYO_CUDA(cudaMemsetAsync(A.arrivals, 0, sizeof(unsigned int) * numNodes, s));
     fusedUpsweepKernel<<<ceilDiv(size_t(numLeaves) * kTpl, 256), 256, 0, s>>>(A);
     RYO_LAUNCH_CHECK();
+    if (!byLevels) return;
     // internal nodes bottom-up, one launch per level that holds nodes (level-major order: level l is
     // [levelRange[l], levelRange[l + 1]))
     for (int l = kMaxLevel - 1; l >= 0; --l)
