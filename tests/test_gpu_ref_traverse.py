@@ -250,3 +250,41 @@ def test_signed_masses_mdq_match_reference_gpu(oracle):
     h = np.full_like(p.x, 1e-3)
     box = np.array(ds.cube_box(p, pad=1e-6), np.float32)
     compare(oracle, p.x, p.y, p.z, m, h, box, theta=0.3, mdq=True, rms_norm=True)
+
+
+def test_varied_softening_and_masses_match_reference_gpu(oracle):
+    """every body its own softening and mass: the general direct sums (the per-pair softening floor (h_i + h_j)^2 and
+    the per-source mass) instead of the one-softening and one-mass forms"""
+    p = ds.gaussian(1 << 16, seed=21, sigma=0.3)
+    rng = np.random.default_rng(21)
+    m = (rng.uniform(0.2, 1.8, len(p.x)) / len(p.x)).astype(np.float32)
+    h = rng.uniform(1e-4, 1e-2, len(p.x)).astype(np.float32)
+    box = np.array(ds.cube_box(p, pad=1e-6), np.float32)
+    compare(oracle, p.x, p.y, p.z, m, h, box)
+
+
+def test_clustered_halos_theta_0_7_bucket_16_match_reference_gpu(oracle):
+    """a clustered set at a coarse opening angle and small leaves: many approximated cells and many small leaves per
+    group"""
+    p = ds.hernquist_halos(1 << 17, num_halos=16, seed=22, eps=1e-3)
+    box = np.array(ds.cube_box(p, pad=1e-6), np.float32)
+    compare(oracle, p.x, p.y, p.z, p.m, p.h, box, theta=0.7, bucket=16)
+
+
+def test_ragged_small_set_matches_reference_gpu(oracle):
+    """fewer bodies than one group of 64 plus a ragged tail: a tree of a few leaves and a partial last group"""
+    p = ds.uniform_cube(100, seed=23, eps=1e-3)
+    compare(oracle, p.x, p.y, p.z, p.m, p.h, np.array(p.box, np.float32), bucket=8)
+
+
+def test_periodic_replicas_of_a_cluster_match_reference_gpu(oracle):
+    """one shell of periodic replicas (27 images per group) without the Ewald correction, on a cluster inside the unit
+    box: its field does not cancel, so each target's own field is the scale (in a uniform box the net field is a small
+    remainder of the images' terms). The interaction counts must be equal. The forces differ by more than in an open
+    box: the reference moves its targets into each image and back (traversal_gpu.cu:484-505), which leaves residues
+    of about one float ulp of the coordinates in the later images, where this library adds each image's shift to the
+    original positions. Near the softening length (h = 1e-3) such a residue is about 6e-5 of the force."""
+    p = ds.gaussian(1 << 15, seed=24, sigma=0.1, eps=2e-3)
+    x, y, z = (np.mod(a + 0.5, 1.0).astype(np.float32) for a in (p.x, p.y, p.z))
+    box = np.array([0, 1, 0, 1, 0, 1], np.float32)
+    compare(oracle, x, y, z, p.m, p.h, box, shells=1, force_tol=1e-4)
