@@ -196,3 +196,33 @@ def test_capped_steps_keep_results_and_favour_short_requests():
     assert work[first] == min(work.values())
     capped.close()
     ref.close()
+
+
+def test_capped_step_takes_every_request_that_fits_in_priority_order():
+    """a capped step goes down the priority order (least remaining work first) and takes each request that still
+    fits: a request too large for the cap does not keep the smaller ones behind it out of the step"""
+    import ryoanji_b200 as ryo
+    params = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32)
+    # remaining work (bodies x force evaluations to come): a 1000 x 3, b 3500 x 1, c 2500 x 5; order a, b, c
+    reqs = [dict(tag=1, p=ds.plummer(1000, seed=31), steps=2, box=None),
+            dict(tag=2, p=ds.plummer(3500, seed=32), steps=0, box=None),
+            dict(tag=3, p=ds.plummer(2500, seed=33), steps=4, box=None)]
+    eng = ryo.Engine(params, max_step_bodies=4000)
+    for r in reqs:
+        _submit(eng, r)
+    info = eng.step()
+    # a (1000) fits, b (1000 + 3500) does not, c (1000 + 2500) does
+    assert info["resident"] == 3 and info["solved"] == 2 and info["residentBodies"] == 7000, info
+    done = _drain(eng)
+    for d in eng.poll():
+        done[d["tag"]] = d
+    ref = ryo.Engine(params, max_step_bodies=0)
+    for r in reqs:
+        _submit(ref, r)
+    full = _drain(ref)
+    for r in reqs:
+        sa, sb = full[r["tag"]]["state"], done[r["tag"]]["state"]
+        scale = np.abs(sa).max(axis=1, keepdims=True) + 1e-30
+        assert float((np.abs(sa - sb) / scale).max()) <= 1e-5, r["tag"]
+    eng.close()
+    ref.close()
