@@ -505,7 +505,9 @@ extern "C"
      * xs, ys, zs (may be NULL) receive the positions in SFC order, p, ax, ay, az the potential and acceleration in
      * that order, order (may be NULL) the original index of each sorted body. The copies overlap the solve: m and h
      * upload during the key sort and the leaf and link construction, the order downloads while the tree is built and
-     * the sorted positions during the upsweep, and for an open box with fixed groups the traversal runs in 8
+     * the sorted positions during the upsweep. For an open box, when p, ax, ay and az are page-locked and mapped
+     * (cudaHostAlloc, cudaMallocHost, or cudaHostRegister with cudaHostRegisterMapped), the traversal stores its
+     * results straight into them while it runs. Otherwise, for an open box with fixed groups the traversal runs in 8
      * launches whose results download while the next one runs.
      * Returns when every output is in host memory. Device buffers are context scratch. */
     RYO_API ryo_status ryo_solve_host_f32(ryo_ctx_t* ctx, const ryo_solve_params* params, const float* x,

@@ -617,8 +617,8 @@ def solve_host(x, y, z, m, h, p, ax, ay, az, params: SolveParams | None = None, 
     """The fused solve from and to host memory (ryo_solve_host_f32): x, y, z, m, h are contiguous host float32
     arrays (CPU tensors, pinned for the fastest copies), left unchanged; p, ax, ay, az (host float32) receive G m phi
     and G a in SFC order, sorted_xyz (three host arrays, optional) the positions in that order and order (host
-    int32, optional) the original index of each sorted body. Host copies overlap the solve; returns when every
-    output is in host memory."""
+    int32, optional) the original index of each sorted body. Host copies overlap the solve; pinned p, ax, ay, az
+    of an open system receive the traversal's results directly. Returns when every output is in host memory."""
     ctx = ctx or default_context()
     params = params or SolveParams()
     for a in (x, y, z, m, h, p, ax, ay, az) + tuple(sorted_xyz or ()) + ((order,) if order is not None else ()):

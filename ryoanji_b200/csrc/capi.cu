@@ -1255,6 +1255,34 @@ void d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
     if (dst && bytes) RYO_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
 }
 
+/*! the device's address of the host array [@p h, @p h + n): non-null when the array is page-locked and mapped into
+ *  this device's address space from its first to its last element, in one contiguous mapping */
+float* mappedHostArray(float* h, size_t n)
+{
+    if (!h || n == 0) return nullptr;
+    cudaPointerAttributes a0{}, a1{};
+    cudaError_t e0 = cudaPointerGetAttributes(&a0, h);
+    cudaError_t e1 = cudaPointerGetAttributes(&a1, h + (n - 1));
+    if (e0 != cudaSuccess || e1 != cudaSuccess)
+    {
+        (void)cudaGetLastError(); // an address the runtime does not know is an answer here, not a failure
+        return nullptr;
+    }
+    if (a0.type != cudaMemoryTypeHost || a1.type != cudaMemoryTypeHost || !a0.devicePointer || !a1.devicePointer)
+        return nullptr;
+    float* d0 = static_cast<float*>(a0.devicePointer);
+    return static_cast<float*>(a1.devicePointer) == d0 + (n - 1) ? d0 : nullptr;
+}
+
+//! the device addresses of a host solve's four output arrays, if all four are mapped
+bool mappedHostOutputs(const HostPipe* pipe, size_t n, float* out[4])
+{
+    float* h[4] = {pipe->hp, pipe->hax, pipe->hay, pipe->haz};
+    for (int k = 0; k < 4; ++k)
+        if (!(out[k] = mappedHostArray(h[k], n))) return false;
+    return true;
+}
+
 /*! the fused single-system solve (ryo_solve_f32); with @p pipe, the host copies of ryo_solve_host_f32 are issued on
  *  its copy stream as soon as their data is final */
 void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, float* z, float* m, float* h, float* vx,
@@ -1407,8 +1435,13 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
         groups = ctx->scratch<uint32_t>("solve.groups", size_t(numGroups) + 1, s);
         launchFixedGroups(0, uint32_t(n), P->groupSize, groups, s);
     }
-    for (float* a : {p, ax, ay, az})
-        RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
+    // a host solve of an open system whose output arrays are page-locked and mapped stores the traversal's results
+    // straight into them: the results cross the link while the traversal runs, and no download follows it
+    float* mapped[4]  = {nullptr, nullptr, nullptr, nullptr};
+    const bool direct = pipe && !periodic && mappedHostOutputs(pipe, n, mapped);
+    if (!direct)
+        for (float* a : {p, ax, ay, az})
+            RYO_CUDA(cudaMemsetAsync(a, 0, n * sizeof(float), s));
     TraverseLaunch t{};
     t.groupStart    = groups;
     t.groupEnd      = groups + 1;
@@ -1424,10 +1457,11 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     t.numShells     = periodic ? P->numShells : 0;
     for (int d = 0; d < 3; ++d)
         t.boxL[d] = dbox.len[d];
-    t.p  = p;
-    t.ax = ax;
-    t.ay = ay;
-    t.az = az;
+    t.p  = direct ? mapped[0] : p;
+    t.ax = direct ? mapped[1] : ax;
+    t.ay = direct ? mapped[2] : ay;
+    t.az = direct ? mapped[3] : az;
+    t.overwrite     = direct ? 1 : 0;
     t.stackCapacity = P->stackCapacity;
     t.dipoles       = dipoles;
     t.softeningRange = hRange;
@@ -1439,9 +1473,9 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
     t.groupM2P      = gm2p;
     t.groupP2P      = gp2p;
     double pot = 0;
-    // a host solve of an open system with fixed groups traverses in chunks of groups and copies each chunk's results
-    // to the host while the next chunk runs
-    const bool chunked = pipe && pipe->chunks > 1 && !periodic && !(P->groupTolerance > 0.f) &&
+    // otherwise, a host solve of an open system with fixed groups traverses in chunks of groups and copies each
+    // chunk's results to the host while the next chunk runs
+    const bool chunked = pipe && !direct && pipe->chunks > 1 && !periodic && !(P->groupTolerance > 0.f) &&
                          numGroups >= uint32_t(pipe->chunks);
     if (!chunked) runTraversal(ctx, t, s, &pot);
     else
@@ -1500,7 +1534,7 @@ void solveSingle(ryo_ctx* ctx, const ryo_solve_params* P, float* x, float* y, fl
         RYO_CUDA(cudaStreamSynchronize(s));
         energy += 0.5 * double(P->G) * he;
     }
-    if (pipe && !chunked)
+    if (pipe && !chunked && !direct)
     {
         streamAfter(ctx, pipe->copy, s, 0);
         d2h(pipe->hp, p, n * sizeof(float), pipe->copy);

@@ -363,6 +363,9 @@ struct TraverseLaunch
     // min and max mass of every source as ordered bits (null: not known). Equal values let the direct sums apply
     // the mass once per batch instead of once per source.
     const uint32_t* massRange;
+    // 1: p, ax, ay, az receive the group's results instead of adding them (0 + result, the same bits as an add to a
+    // zeroed array) and are never read. The host-memory solve points them at the caller's mapped host arrays.
+    int overwrite;
     // double coordinates (traverse64.cu): kPrecisionF64 (everything double) or kPrecisionMixed (double coordinates
     // and centres; float softenings, masses, multipoles and outputs). The float fields above are unused then; the
     // untyped pointers hold double (f64) or float (mixed) arrays.

@@ -670,6 +670,17 @@ void launchTraversalReset(Control* ctl, bool resetStats, cudaStream_t s)
     RYO_LAUNCH_CHECK();
 }
 
+/*! a target's G m phi and G a: added to the outputs (the reference's accumulation), or with P.overwrite stored as
+ *  0 + value without reading them, which gives the bits an add to a zeroed output gives */
+__device__ __forceinline__ void storeResult(const TraverseLaunch& P, int idx, float p, float x, float y, float z)
+{
+    const bool add = !P.overwrite;
+    if (P.p) P.p[idx] = (add ? P.p[idx] : 0.f) + p;
+    P.ax[idx] = (add ? P.ax[idx] : 0.f) + x;
+    P.ay[idx] = (add ? P.ay[idx] : 0.f) + y;
+    P.az[idx] = (add ? P.az[idx] : 0.f) + z;
+}
+
 //! one warp per queued group: add the parts' partial sums in part order (FP64) and write the group's results
 __global__ void combineHeavyKernel(TraverseLaunch P, const float* __restrict__ mass)
 {
@@ -711,10 +722,7 @@ __global__ void combineHeavyKernel(TraverseLaunch P, const float* __restrict__ m
             float phi = float(s0), gx = float(s1), gy = float(s2), gz = float(s3);
             float mi  = mass[idx];
             pot += double(mi) * double(phi);
-            if (P.p) P.p[idx] += P.G * mi * phi;
-            P.ax[idx] += P.G * gx;
-            P.ay[idx] += P.G * gy;
-            P.az[idx] += P.G * gz;
+            storeResult(P, idx, P.G * mi * phi, P.G * gx, P.G * gy, P.G * gz);
         }
     }
     pot = warpSum(pot);
@@ -973,10 +981,7 @@ __global__ void __launch_bounds__(kTravThreads, 5)
                 {
                     float mi = tgt.scalar(idx);
                     pot += double(mi) * double(phi[k]);
-                    if (P.p) P.p[idx] += P.G * mi * phi[k];
-                    P.ax[idx] += P.G * gx[k];
-                    P.ay[idx] += P.G * gy[k];
-                    P.az[idx] += P.G * gz[k];
+                    storeResult(P, idx, P.G * mi * phi[k], P.G * gx[k], P.G * gy[k], P.G * gz[k]);
                 }
             }
             pot = warpSum(pot);

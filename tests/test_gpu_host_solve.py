@@ -1,9 +1,12 @@
 """Solve from and to host memory (ryo_solve_host_f32): the same results as the device solve.
 
 Inputs come from pinned host tensors and are left unchanged; outputs (sorted positions, order, potential and
-acceleration in SFC order) land in host tensors. The traversal of an open system runs in chunks of groups whose
-results download while the next chunk runs: every group is computed by the same kernel code as in one launch, so
-the results are bit-identical, except for groups split over several warps, whose part count may differ (rounding).
+acceleration in SFC order) land in host tensors.
+- Pinned output arrays: the traversal of an open system stores its results straight into them. It is the device
+  solve's launch, so the results are bit-identical.
+- Pageable output arrays: the traversal runs in chunks of groups whose results download while the next chunk runs.
+  Every group is computed by the same kernel code as in one launch, so the results are bit-identical, except for
+  groups split over several warps, whose part count may differ (rounding).
 """
 import numpy as np
 import pytest
@@ -18,12 +21,12 @@ def _pinned(a):
     return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
 
 
-def _compare(pset, params, exact):
+def _compare(pset, params, exact, pinned_out=True):
     import ryoanji_b200 as ryo
     n = pset.n
     hin = [_pinned(a) for a in (pset.x, pset.y, pset.z, pset.m, pset.h)]
     before = [t.clone() for t in hin]
-    hout = [torch.empty(n).pin_memory() for _ in range(4)]
+    hout = [torch.empty(n).pin_memory() if pinned_out else torch.empty(n) for _ in range(4)]
     hxyz = [torch.empty(n).pin_memory() for _ in range(3)]
     hord = torch.empty(n, dtype=torch.int32).pin_memory()
     ctx = ryo.Context()
@@ -57,8 +60,18 @@ def test_host_solve_equals_device_solve_cube():
 
 def test_host_solve_equals_device_solve_with_split_groups():
     import ryoanji_b200 as ryo
-    r = _compare(ds.plummer(100000, seed=1, velocities=False), ryo.SolveParams(theta=0.5), exact=False)
+    pset = ds.plummer(100000, seed=1, velocities=False)
+    r = _compare(pset, ryo.SolveParams(theta=0.5), exact=True)
     assert r.max_p2p > 16384  # the sparse outskirts took the split path
+    _compare(pset, ryo.SolveParams(theta=0.5), exact=False, pinned_out=False)
+
+
+def test_host_solve_into_pageable_outputs():
+    import ryoanji_b200 as ryo
+    pset = ds.uniform_cube(300000, seed=3)
+    _compare(pset, ryo.SolveParams(theta=0.5), exact=True, pinned_out=False)
+    _compare(pset, ryo.SolveParams(theta=0.5, group_tolerance=2.0), exact=True, pinned_out=False)
+    _compare(pset, ryo.SolveParams(theta=0.5, group_tolerance=2.0), exact=True)  # spatial groups, stored directly
 
 
 def test_host_solve_periodic_and_small():
