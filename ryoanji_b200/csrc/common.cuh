@@ -237,6 +237,57 @@ constexpr HilbertLut makeHilbertLut()
     return t;
 }
 
+/*! the inverse of the state table: for every state and Hilbert digit, the original octant bits and the next state.
+ *  A key then decodes from its top level down, one lookup per level, and a node's corner needs only the node's own
+ *  levels. */
+struct HilbertDecodeLut
+{
+    uint16_t one[48 * 8]; // (octant bits x4 y2 z1) | (next state << 3)
+};
+
+constexpr HilbertDecodeLut makeHilbertDecodeLut()
+{
+    HilbertDecodeLut t{};
+    for (int st = 0; st < 48; ++st)
+        for (unsigned o = 0; o < 8; ++o)
+        {
+            unsigned d = 0;
+            int nx     = 0;
+            hilbertStep(st, o, d, nx);
+            t.one[st * 8 + d] = uint16_t(o | (unsigned(nx) << 3));
+        }
+    return t;
+}
+
+#ifdef __CUDACC__
+static __device__ const HilbertDecodeLut kHilbertDecodeDev = makeHilbertDecodeLut();
+#endif
+
+/*! integer coordinates of the lower corner of the node at octree level @p levels whose keys start at @p key, for a
+ *  box whose three axes use all kMaxLevel levels: the top @p levels bits of each coordinate, lower bits zero */
+__host__ __device__ inline void hilbertCorner(uint64_t key, unsigned levels, unsigned p[3])
+{
+#ifdef __CUDA_ARCH__
+    const uint16_t* dec = kHilbertDecodeDev.one;
+#else
+    static constexpr HilbertDecodeLut host = makeHilbertDecodeLut();
+    const uint16_t* dec = host.one;
+#endif
+    unsigned st = 0, x = 0, y = 0, z = 0;
+    for (unsigned l = 0; l < levels; ++l)
+    {
+        unsigned e = dec[st * 8 + (unsigned(key >> (3 * (kMaxLevel - 1 - l))) & 7u)];
+        x          = (x << 1) | ((e >> 2) & 1u);
+        y          = (y << 1) | ((e >> 1) & 1u);
+        z          = (z << 1) | (e & 1u);
+        st         = e >> 3;
+    }
+    const unsigned sh = kMaxLevel - levels;
+    p[0]              = x << sh;
+    p[1]              = y << sh;
+    p[2]              = z << sh;
+}
+
 //! bits 0..20 of v spread to every third bit (v_i at bit 3 i)
 __host__ __device__ inline uint64_t spreadBits3(uint32_t v)
 {
@@ -651,7 +702,10 @@ __host__ __device__ inline void nodeGeometry(uint64_t key, unsigned level, const
     }
     unsigned fromRight = kMaxLevel - level;
     unsigned p[3];
-    unhilbertKey(key, box.bits, p);
+    if (box.bits[0] == unsigned(kMaxLevel) && box.bits[1] == unsigned(kMaxLevel) && box.bits[2] == unsigned(kMaxLevel))
+        hilbertCorner(key, level, p); // the node's levels only; the bits below are masked off next
+    else
+        unhilbertKey(key, box.bits, p);
     const T unit = T(1.) / T(1u << kMaxLevel);
 #pragma unroll
     for (int d = 0; d < 3; ++d)

@@ -399,21 +399,20 @@ __device__ inline void writeRootExpansion(double* out, const double c[3], const 
     out[10]   = tr;
 }
 
-//! write the float outputs of a finished node
-__device__ void emitNode(const FusedArgs& A, int node, const double c[3], double w, double m, const double q[6],
-                         const double dp[3], int child, uint32_t firstBody, uint32_t count)
+//! write the float outputs of a finished node; @p prefix is the node's, loaded by the caller ahead of its sums
+__device__ void emitNode(const FusedArgs& A, int node, uint64_t prefix, const double c[3], double w, double m,
+                         const double q[6], const double dp[3], int child, uint32_t firstBody, uint32_t count)
 {
     if (A.dipoles) A.dipoles[node] = make_float4(float(dp[0]), float(dp[1]), float(dp[2]), 0.f);
     float com[3] = {float(c[0]), float(c[1]), float(c[2])};
     double raw[7] = {m, q[0], q[1], q[2], q[3], q[4], q[5]};
     float mac     = 0.f;
     if (!A.sysBoxes)
-        mac = w != 0.0 && float(w) != 0.f ? vecMacR2(A.prefixes[node], com, A.invTheta, A.box) : 0.f;
+        mac = w != 0.0 && float(w) != 0.f ? vecMacR2(prefix, com, A.invTheta, A.box) : 0.f;
     else
     {
         // a node inside a system: its geometry is the system-local node (prefix without the system bits) in the
         // system's box; nodes above the system level mix systems and are never traversed
-        uint64_t prefix = A.prefixes[node];
         int lvl         = prefixLength(prefix) / 3;
         if (lvl >= A.sysLevel)
         {
@@ -462,6 +461,7 @@ __device__ __forceinline__ double groupSum8(double v, unsigned gmask)
 //! combine the eight children of @p node (parallel-axis theorem, double): lane @p sub of the group holds child sub
 __device__ void combineChildren(const FusedArgs& A, int node, int fc, int sub, unsigned gmask)
 {
+    const uint64_t prefix = sub == 0 ? A.prefixes[node] : 0; // in flight with the children
     double cc[3], cw, cm, cq[6], cp[3];
     loadDNode(A.dn + fc + sub, cc, cw, cm, cq, cp);
     double w  = fabs(cw);
@@ -493,32 +493,42 @@ __device__ void combineChildren(const FusedArgs& A, int node, int fc, int sub, u
     if (sub == 0)
     {
         storeDNode(A.dn + node, c, W, M, q, dp);
-        emitNode(A, node, c, W, M, q, dp, fc, 0, 0);
+        emitNode(A, node, prefix, c, W, M, q, dp, fc, 0, 0);
     }
 }
 
 /*! eight lanes per leaf: one pass over the bodies, P2M of the leaf (small register footprint, so many leaf groups
  *  stay resident per SM). The internal nodes follow by the climb (A.arrivals set: the group of the eighth sibling to
  *  arrive combines the parent, one child per lane, and goes on up) or level by level (levelCombineKernel). */
-__global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
+__global__ void __launch_bounds__(256, 4) fusedUpsweepKernel(FusedArgs A)
 {
     int tid     = blockIdx.x * blockDim.x + threadIdx.x;
     int leaf    = tid / kTpl;
     int sub     = tid % kTpl;
     bool active = leaf < A.numLeaves;
+    // two dependent rounds of loads: the leaf's range and node, then its bodies and the node's prefix. The sums are
+    // taken relative to the leaf's first body, which lane 0 of the group loads as its own first body.
     uint32_t b0 = 0, b1 = 0;
-    float4 p0   = make_float4(0.f, 0.f, 0.f, 0.f);
+    int node    = 0;
     if (active)
     {
-        b0 = A.layout[leaf];
-        b1 = A.layout[leaf + 1];
-        if (b1 > b0) p0 = A.xyzm[b0];
+        b0   = A.layout[leaf];
+        b1   = A.layout[leaf + 1];
+        node = A.leafToInternal[leaf];
     }
+    const uint64_t prefix = active && sub == 0 ? A.prefixes[node] : 0;
+    float4 b              = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t i            = b0 + sub;
+    if (i < b1) b = A.xyzm[i];
+    float4 p0;
+    p0.x = __shfl_sync(0xFFFFFFFFu, b.x, 0, kTpl);
+    p0.y = __shfl_sync(0xFFFFFFFFu, b.y, 0, kTpl);
+    p0.z = __shfl_sync(0xFFFFFFFFu, b.z, 0, kTpl);
     // sums relative to the first body: sum|m|, sum|m|d, sum m, sum m d, sum m d d^T
     double s[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t i = b0 + sub; i < b1; i += kTpl)
+    for (; i < b1; i += kTpl)
     {
-        float4 b  = A.xyzm[i];
+        if (i != b0 + sub) b = A.xyzm[i];
         double dx = double(b.x) - p0.x, dy = double(b.y) - p0.y, dz = double(b.z) - p0.z;
         double mi = b.w, wi = fabs(mi);
         s[0] += wi;
@@ -541,7 +551,6 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
         s[k] = groupSum8(s[k]);
     if (!active) return; // the eight lanes of a leaf group leave together
 
-    int node = A.leafToInternal[leaf];
     double W = s[0], M = s[4];
     double c[3], q[6], dp[3];
     if (W != 0.0)
@@ -581,7 +590,7 @@ __global__ void __launch_bounds__(256) fusedUpsweepKernel(FusedArgs A)
     if (sub == 0)
     {
         storeDNode(A.dn + node, c, W, M, q, dp);
-        emitNode(A, node, c, W, M, q, dp, 0, b0, b1 - b0);
+        emitNode(A, node, prefix, c, W, M, q, dp, 0, b0, b1 - b0);
     }
     if (!A.arrivals) return;
 

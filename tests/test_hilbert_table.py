@@ -1,8 +1,10 @@
-"""The table-driven Hilbert index (two levels per lookup) against the bitwise encoder, on the host (no GPU).
+"""The table-driven Hilbert index (two levels per lookup) against the bitwise encoder, and the table-driven node
+corner decoder against the bitwise decoder, on the host (no GPU).
 
-The cubic-box key kernels use the table; the GPU key parity tests compare their keys with the oracle. This check
-compiles the shared header for the host and compares the two encoders on edge cases, 2M random cells and every
-combination of the six lowest bits.
+The cubic-box key kernels use the encoding table, and the node geometry of cubic boxes (MAC radii, group boxes) the
+decoding table; the GPU parity tests compare keys and MAC radii with the oracle. This check compiles the shared
+header for the host and compares the encoders on edge cases, 2M random cells and every combination of the six
+lowest bits, and the decoders at every level on edge cases and 200k random cells.
 """
 import os
 import shutil
