@@ -23,21 +23,28 @@ namespace ryo
 
 constexpr int kLeafBlock = 256;
 
-/*! level of the leaf that contains each sorted particle
+/*! level of the leaf that contains each sorted particle, and where each particle starts a new non-empty leaf
  *
  * w[j] = min(commonLevel(k[j], k[j+B]), 20) is the level of the deepest internal node holding the window j; the
- * particle's leaf is one level below the deepest window level among the windows that contain it.
+ * particle's leaf is one level below the deepest window level among the windows that contain it. The windows of
+ * particle i are j in [i - B, i]; those outside [0, n - B) hold level 0 here, which leaves every maximum unchanged.
+ * The maximum over B + 1 consecutive windows comes from a sparse table built by doubling in shared memory:
+ * m_2P[t] = max(m_P[t], m_P[t + P]), and the window [a, a + K) is max(m_P[a], m_P[a + K - P]) for the largest power
+ * of two P <= K. A block also computes the level of the particle before its first, so head[i] (1 where particle i
+ * starts a non-empty leaf: its leaf's start differs from particle i - 1's) needs no second pass.
  */
 __global__ void __launch_bounds__(kLeafBlock) leafLevels(const uint64_t* __restrict__ keys, uint32_t n,
                                                          uint32_t bucket, uint32_t minLevel,
-                                                         uint8_t* __restrict__ level)
+                                                         uint8_t* __restrict__ level, uint32_t* __restrict__ head)
 {
     extern __shared__ unsigned char smem[];
-    uint8_t* w = smem; // window levels for j in [i0 - B, i0 + blockDim)
-    const uint32_t i0     = blockIdx.x * kLeafBlock;
-    const int64_t jFirst  = int64_t(i0) - int64_t(bucket);
-    const uint32_t span   = kLeafBlock + bucket;
-    const int64_t numWin  = int64_t(n) - int64_t(bucket); // windows j in [0, n - B)
+    __shared__ uint8_t leafLvl[kLeafBlock + 1]; // particles i0 - 1 .. i0 + kLeafBlock - 1
+    const uint32_t i0    = blockIdx.x * kLeafBlock;
+    const uint32_t span  = kLeafBlock + bucket + 1;             // windows j in [i0 - B - 1, i0 + kLeafBlock)
+    const int64_t jFirst = int64_t(i0) - int64_t(bucket) - 1;
+    const int64_t numWin = int64_t(n) - int64_t(bucket);        // windows j in [0, n - B)
+    uint8_t* src         = smem;
+    uint8_t* dst         = smem + span;
     for (uint32_t t = threadIdx.x; t < span; t += kLeafBlock)
     {
         int64_t j = jFirst + t;
@@ -48,37 +55,43 @@ __global__ void __launch_bounds__(kLeafBlock) leafLevels(const uint64_t* __restr
             int lvl = cb / 3;
             v       = uint8_t(lvl < kMaxLevel - 1 ? lvl : kMaxLevel - 1);
         }
-        w[t] = v;
+        src[t] = v;
     }
     __syncthreads();
-    uint32_t i = i0 + threadIdx.x;
-    if (i >= n) return;
-    // windows covering i: j in [max(0, i - B), min(i, n - B - 1)], at w[j - jFirst]
-    int64_t jlo = int64_t(i) - bucket;
-    if (jlo < 0) jlo = 0;
-    int64_t jhi = int64_t(i) < numWin - 1 ? int64_t(i) : numWin - 1;
-    uint8_t mx  = 0;
-    for (int64_t j = jlo; j <= jhi; ++j)
+    const uint32_t K = bucket + 1;
+    uint32_t P       = 1;
+    for (; 2 * P <= K; P *= 2)
     {
-        uint8_t v = w[j - jFirst];
-        mx        = v > mx ? v : mx;
+        for (uint32_t t = threadIdx.x; t + 2 * P <= span; t += kLeafBlock)
+        {
+            uint8_t a = src[t], b = src[t + P];
+            dst[t]    = a > b ? a : b;
+        }
+        __syncthreads();
+        uint8_t* tmp = src;
+        src          = dst;
+        dst          = tmp;
     }
-    uint32_t lv = uint32_t(mx) + 1;
-    level[i]    = uint8_t(lv > minLevel ? lv : minLevel);
-}
-
-//! 1 where a particle starts a new non-empty leaf
-__global__ void leafHeads(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ level, uint32_t n,
-                          uint32_t* __restrict__ head)
-{
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // particle i0 + tid covers the windows at [tid + 1, tid + 1 + K); the particle before the block, [0, K)
+    auto leafLevel = [&](uint32_t a) -> uint32_t
+    {
+        uint8_t x = src[a], y = src[a + K - P];
+        uint32_t lv = uint32_t(x > y ? x : y) + 1;
+        return lv > minLevel ? lv : minLevel;
+    };
+    const uint32_t i = i0 + threadIdx.x;
+    uint32_t lv      = leafLevel(threadIdx.x + 1);
+    leafLvl[threadIdx.x + 1] = uint8_t(lv);
+    if (threadIdx.x == 0) leafLvl[0] = uint8_t(leafLevel(0));
+    __syncthreads();
     if (i >= n) return;
-    uint64_t s = keys[i] & ~(nodeRange(level[i]) - 1);
+    level[i]   = uint8_t(lv);
     uint32_t h = 1;
     if (i > 0)
     {
-        uint64_t sp = keys[i - 1] & ~(nodeRange(level[i - 1]) - 1);
-        h           = sp != s;
+        uint64_t st = keys[i] & ~(nodeRange(lv) - 1);
+        uint64_t sp = keys[i - 1] & ~(nodeRange(leafLvl[threadIdx.x]) - 1);
+        h           = sp != st;
     }
     head[i] = h;
 }
@@ -171,12 +184,10 @@ int buildLeaves(ryo_ctx* ctx, const uint64_t* keys, size_t n64, unsigned bucket,
 
     uint8_t* level  = ctx->scratch<uint8_t>("leaf.level", n, s);
     uint32_t* head  = ctx->scratch<uint32_t>("leaf.head", size_t(n) + 1, s);
-    size_t smemBytes = kLeafBlock + bucket;
+    size_t smemBytes = 2 * (size_t(kLeafBlock) + bucket + 1); // two window-level buffers of the sparse table
     if (smemBytes > 48 * 1024)
         RYO_CUDA(cudaFuncSetAttribute(leafLevels, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemBytes)));
-    leafLevels<<<ceilDiv(n, kLeafBlock), kLeafBlock, smemBytes, s>>>(keys, n, bucket, minLevel, level);
-    RYO_LAUNCH_CHECK();
-    leafHeads<<<ceilDiv(n, 256), 256, 0, s>>>(keys, level, n, head);
+    leafLevels<<<ceilDiv(n, kLeafBlock), kLeafBlock, smemBytes, s>>>(keys, n, bucket, minLevel, level, head);
     RYO_LAUNCH_CHECK();
     exclusiveScanU32(ctx, head, head, n, s);
     uint32_t numNE = 0;
