@@ -165,9 +165,12 @@ size_t sortTempBytes(size_t n)
     return 2 * kMaxPasses * kDigits * sizeof(uint32_t) + 256 + (tiles + 1) * kDigits * sizeof(unsigned long long);
 }
 
+constexpr int kHistKeys = 4; // keys per thread and round of the histogram, loaded before any is counted
+
 //! all digit histograms in one read of the keys: two shared-memory copies per block (each shared by four warps),
 //! plain shared atomics, and one aggregated add when a whole warp holds the same digit (top digits of clustered or
-//! presorted keys)
+//! presorted keys). A round loads kHistKeys keys per thread before counting them, so that enough loads are in
+//! flight to cover the memory latency.
 __global__ void __launch_bounds__(256) digitHistogram(const uint64_t* __restrict__ keys, size_t n, int beginBit,
                                                       int numPasses, uint32_t* hist)
 {
@@ -177,25 +180,35 @@ __global__ void __launch_bounds__(256) digitHistogram(const uint64_t* __restrict
     __syncthreads();
     uint32_t(*mine)[kDigits] = sh[(threadIdx.x >> 7) & 1];
     const unsigned lane      = laneId();
-    size_t stride            = size_t(gridDim.x) * blockDim.x;
-    for (size_t i0 = size_t(blockIdx.x) * blockDim.x; i0 < n; i0 += stride)
+    const size_t round       = size_t(blockDim.x) * kHistKeys;
+    const size_t stride      = size_t(gridDim.x) * round;
+    for (size_t i0 = size_t(blockIdx.x) * round; i0 < n; i0 += stride)
     {
-        size_t i       = i0 + threadIdx.x;
-        bool valid     = i < n;
-        uint64_t key   = valid ? keys[i] : 0;
-        unsigned vmask = __ballot_sync(0xffffffffu, valid);
-        if (vmask == 0) continue;
-        int lead = __ffs(vmask) - 1;
-        for (int p = 0; p < numPasses; ++p)
+        uint64_t key[kHistKeys];
+#pragma unroll
+        for (int k = 0; k < kHistKeys; ++k)
         {
-            unsigned d  = unsigned(key >> (beginBit + 8 * p)) & 255u;
-            unsigned d0 = __shfl_sync(0xffffffffu, d, lead);
-            if (__all_sync(0xffffffffu, !valid || d == d0))
+            size_t i = i0 + size_t(k) * blockDim.x + threadIdx.x;
+            key[k]   = i < n ? keys[i] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < kHistKeys; ++k)
+        {
+            bool valid     = i0 + size_t(k) * blockDim.x + threadIdx.x < n;
+            unsigned vmask = __ballot_sync(0xffffffffu, valid);
+            if (vmask == 0) continue;
+            int lead = __ffs(vmask) - 1;
+            for (int p = 0; p < numPasses; ++p)
             {
-                if (lane == unsigned(lead)) atomicAdd(&mine[p][d0], __popc(vmask));
+                unsigned d  = unsigned(key[k] >> (beginBit + 8 * p)) & 255u;
+                unsigned d0 = __shfl_sync(0xffffffffu, d, lead);
+                if (__all_sync(0xffffffffu, !valid || d == d0))
+                {
+                    if (lane == unsigned(lead)) atomicAdd(&mine[p][d0], __popc(vmask));
+                }
+                else if (valid)
+                    atomicAdd(&mine[p][d], 1u);
             }
-            else if (valid)
-                atomicAdd(&mine[p][d], 1u);
         }
     }
     __syncthreads();
@@ -390,7 +403,7 @@ bool radixSortPairs(uint64_t* keys, uint32_t* values, uint64_t* keysAlt, uint32_
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    size_t hb = (n + 255) / 256;
+    size_t hb = (n + 256 * kHistKeys - 1) / (256 * kHistKeys);
     unsigned histBlocks = unsigned(hb < size_t(sms) * 4 ? hb : size_t(sms) * 4);
     digitHistogram<<<histBlocks, 256, 0, s>>>(keys, n, beginBit, numPasses, t.hist);
     RYO_LAUNCH_CHECK();

@@ -92,12 +92,20 @@ def test_leaves_bit_exact(case):
     assert np.array_equal(host(counts).view(np.uint32), case["counts"])
 
 
-@pytest.mark.parametrize("kind,bucket", [("plummer", 64), ("halos", 16), ("cube", 1), ("dup", 4), ("tiny", 64)])
+# buckets that are and are not one less than a power of two: the window maximum over bucket + 1 windows comes from
+# power-of-two spans, and 16384 is the largest bucket the leaf construction takes
+@pytest.mark.parametrize("kind,bucket", [("plummer", 64), ("halos", 16), ("cube", 1), ("dup", 4), ("tiny", 64),
+                                         ("cube", 7), ("halos", 100), ("plummer", 1000), ("big", 16384),
+                                         ("edge", 64)])
 def test_leaves_against_oracle(oracle, kind, bucket):
     import ryoanji_b200 as ryo
     from ryoanji_b200 import datasets as ds
     if kind == "plummer":
         p = ds.plummer(150000, seed=3, velocities=False)
+    elif kind == "big":
+        p = ds.plummer(120000, seed=8, velocities=False)
+    elif kind == "edge":
+        p = ds.uniform_cube(65, seed=9)  # one window of bucket + 1 keys
     elif kind == "halos":
         p = ds.hernquist_halos(60000, num_halos=8, seed=4)
     elif kind == "cube":
