@@ -560,7 +560,7 @@ extern "C"
         int maxSystems;         /* resident requests at most (default and upper limit RYO_BATCH_MAX_SYSTEMS) */
         uint64_t reserveBodies; /* resident bodies the arenas hold from creation on (default 0: grown on demand,
                                    doubling, which waits for the device at each growth) */
-        uint64_t maxStepBodies; /* bodies one step advances at most (default 2^23; 0: every resident request each
+        uint64_t maxStepBodies; /* bodies one step advances at most (default 7 x 2^20; 0: every resident request each
                                    step). Taken in the order of their remaining work (bodies x steps left, least
                                    first), the resident requests that still fit join the step (the first always
                                    does): short requests are not held to the pace of the long ones. The choice is

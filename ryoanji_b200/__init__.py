@@ -696,7 +696,7 @@ class Engine:
     def __init__(self, params: SolveParams | None = None, hbm_budget_bytes: float = 120e9,
                  bytes_per_body: float = 256.0, max_systems: int = MAX_BATCH_SYSTEMS, ctx: Context | None = None,
                  reserve_bodies: int = 0, max_step_bodies: int | None = None):
-        """max_step_bodies: bodies one step advances at most (None: the library default, 2^23; 0: every resident
+        """max_step_bodies: bodies one step advances at most (None: the library default, 7 x 2^20; 0: every resident
         request every step); the requests with the least remaining work go first"""
         self.ctx = ctx or default_context()
         ep = _abi.EngineParams()

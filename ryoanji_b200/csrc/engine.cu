@@ -416,7 +416,7 @@ extern "C" void ryo_engine_params_default(ryo_engine_params* p)
     p->bytesPerBody   = 256.0;
     p->maxSystems     = RYO_BATCH_MAX_SYSTEMS;
     p->reserveBodies  = 0;
-    p->maxStepBodies  = uint64_t(1) << 23;
+    p->maxStepBodies  = uint64_t(7) << 20;
 }
 
 extern "C" ryo_status ryo_engine_create(ryo_ctx_t* ctx, const ryo_engine_params* p, ryo_engine_t** out)
