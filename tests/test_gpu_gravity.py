@@ -181,6 +181,38 @@ def test_solve_matches_oracle_path(oracle):
     assert res.sum_m2p == int((m2p.astype(np.int64) * np.diff(g)).sum())
 
 
+def test_solve_upsweep_by_levels_matches_double_oracle(oracle):
+    """a tree of more than 2^17 nodes (188k here), whose internal nodes the fused upsweep combines one level per
+    launch instead of by the climb: links bit-exact, centres, MAC radii and multipoles against the FP64 oracle"""
+    import ryoanji_b200 as ryo
+    from ryoanji_b200 import datasets as ds
+    pset = ds.plummer(400000, seed=22, velocities=False)
+    x, y, z, m, h = (dev(a) for a in (pset.x, pset.y, pset.z, pset.m, pset.h))
+    n = x.numel()
+    p, ax, ay, az = (torch.empty(n, device="cuda") for _ in range(4))
+    ctx = ryo.Context()
+    res = ryo.solve(x, y, z, m, h, p, ax, ay, az, ryo.SolveParams(theta=0.5, bucket_size=8), ctx=ctx)
+    assert res.num_nodes > 1 << 17
+    arr = ryo.solve_arrays(ctx)
+    box = np.array(res.box, np.float32)
+    sk, o = oracle.sort_keys(oracle.sfc_keys(pset.x, pset.y, pset.z, box))
+    l_ref, c_ref = oracle.octree_leaves(sk, 8)
+    t_ref = oracle.octree_link(l_ref)
+    for k in ("prefixes", "childOffsets", "internalToLeaf", "parents"):
+        assert np.array_equal(host(arr[k]).view(t_ref[k].dtype), t_ref[k]), k
+    layout = np.concatenate([[0], np.cumsum(c_ref)]).astype(np.uint32)
+    c_dbl, m_dbl = oracle.upsweep(pset.x[o], pset.y[o], pset.z[o], pset.m[o], layout, t_ref, 0.5, box, mode=1)
+    cg, mg = host(arr["centers"]), host(arr["multipoles"])
+    assert np.abs(cg[:, :3] - c_dbl[:, :3]).max() <= 4e-7 * np.abs(c_dbl[:, :3]).max()
+    same = np.all(cg[:, :3] == c_dbl[:, :3], axis=1)
+    assert same.mean() > 0.9 and np.array_equal(cg[same, 3], c_dbl[same, 3])
+    L = float(max(box[1::2] - box[0::2]))
+    scale = np.maximum(np.abs(mg[:, 1:]).max(axis=1), np.abs(m_dbl[:, 1:]).max(axis=1))
+    tol = 2e-6 * scale + 1e-9 * np.abs(m_dbl[:, 0]) * L * L
+    assert np.all(np.abs(mg[:, 1:] - m_dbl[:, 1:]).max(axis=1) <= tol)
+    assert np.allclose(mg[:, 0], m_dbl[:, 0], rtol=1e-6, atol=0)
+
+
 SPLIT_COST = 32768  # direct bodies + 2 x approximated cells past which the traversal splits a group over warps
 
 
