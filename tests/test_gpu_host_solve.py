@@ -87,3 +87,31 @@ def test_host_solve_rejects_device_tensors():
     x = torch.zeros(16, device="cuda")
     with pytest.raises(ValueError):
         ryo.solve_host(x, x, x, x, x, x, x, x, x)
+
+
+def test_host_solve_into_registered_outputs():
+    """outputs in host memory page-locked by cudaHostRegister (default flags) rather than allocated pinned"""
+    import ryoanji_b200 as ryo
+    cudart = torch._C._cudart
+    pset = ds.uniform_cube(200000, seed=5)
+    n = pset.n
+    outs = [np.empty(n, np.float32) for _ in range(4)]
+    registered = []
+    try:
+        for a in outs:
+            assert int(cudart.cudaHostRegister(a.ctypes.data, a.nbytes, 0)) == 0
+            registered.append(a)
+        hin = [_pinned(a) for a in (pset.x, pset.y, pset.z, pset.m, pset.h)]
+        hout = [torch.from_numpy(a) for a in outs]
+        hord = torch.empty(n, dtype=torch.int32)
+        ctx = ryo.Context()
+        params = ryo.SolveParams(theta=0.5)
+        ryo.solve_host(*hin, *hout, params=params, order=hord, ctx=ctx)
+        d = [t.cuda() for t in hin]
+        dout = [torch.empty(n, device="cuda") for _ in range(4)]
+        ryo.solve(*d, *dout, params=params, ctx=ctx)
+        for a, b in zip(hout, dout):
+            assert torch.equal(a, b.cpu())
+    finally:
+        for a in registered:
+            cudart.cudaHostUnregister(a.ctypes.data)
