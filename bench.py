@@ -88,59 +88,97 @@ def parse():
 # ------------------------------------------------------------------------------------------------------ clocks
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons while the timed region runs"""
+    """SM clocks and clock-event (throttle) reasons sampled while the timed region runs: NVML read queries every
+    100 ms from a thread, or, where NVML is missing, an nvidia-smi subprocess at 200 ms. Nothing is set."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    # NVML clock-event reason bits of NAMES
+    BITS = (0x8, 0x40, 0x20, 0x4)
 
     def __init__(self, gpu_id: str):
         self.gpu_id = gpu_id
         self.proc = None
+        self.source = None
+        self.samples: list[tuple[float, float, set]] = []  # (sm MHz, max sm MHz, active reasons)
         self.lines: list[str] = []
+        self._stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            handle = pynvml.nvmlDeviceGetHandleByUUID(self.gpu_id)
+            self.source = "nvml"
+            self.thread = threading.Thread(target=self._poll_nvml, args=(pynvml, handle), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:  # no NVML binding or library: fall back to nvidia-smi
+            self.source = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi"
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
 
+    def _poll_nvml(self, pynvml, handle):
+        events = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        try:
+            mx = float(pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM))
+            while not self._stop.is_set():
+                sm = float(pynvml.nvmlDeviceGetClockInfo(handle, pynvml.NVML_CLOCK_SM))
+                bits = int(events(handle))
+                self.samples.append((sm, mx, {n for n, b in zip(self.NAMES, self.BITS) if bits & b}))
+                self._stop.wait(0.1)
+        except Exception:
+            pass
+        finally:
+            try:
+                pynvml.nvmlShutdown()
+            except Exception:
+                pass
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self._stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        samples = list(self.samples)
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 8:
                 continue
             try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
+                sm, mx = float(parts[0]), float(parts[1])
             except ValueError:
                 continue
-            for name, v in zip(names, parts[4:8]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+            samples.append((sm, mx, {n for n, v in zip(self.NAMES, parts[4:8]) if v.lower().startswith("active")}))
+        if not samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": self.source}
+        reasons = set().union(*(r for _, _, r in samples))
+        return {"sm_mhz": float(np.median([s for s, _, _ in samples])),
+                "sm_max_mhz": float(max(m for _, m, _ in samples)), "reasons": sorted(reasons),
+                "samples": len(samples), "source": self.source}
 
 
 # ------------------------------------------------------------------------------------------------------ arms
