@@ -92,3 +92,24 @@ def test_summary_is_last_and_fits_the_kept_tail():
     assert s["acc_theta_0.5"]["p99"] == 7.346e-4 and s["acc_matched"]["theta"] == 0.43
     assert s["acc_matched"]["mps"] == 197.1
     assert s["ensemble"]["x"] == 9.346 and s["served"]["served_latency_p99_s"] == 2.346
+
+
+def _bench_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_clock_summary_reads_samples_and_reasons():
+    """the clock record: median SM clock, the maximum, and every throttle reason seen active in any sample, from
+    NVML samples and from nvidia-smi lines alike"""
+    b = _bench_module()
+    c = b.ClockSampler("GPU-unused")
+    c.samples = [(1965.0, 1965.0, set()), (1950.0, 1965.0, {"sw_power_cap"})]
+    c.lines = ["1800, 1965, 700.5, Active, Active, Not Active, Not Active, Not Active", "garbage"]
+    s = c.summary()
+    assert s["samples"] == 3 and s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["hw_slowdown", "sw_power_cap"]
+    assert b.ClockSampler("GPU-unused").summary()["samples"] == 0
