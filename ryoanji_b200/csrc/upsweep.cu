@@ -627,9 +627,9 @@ __global__ void __launch_bounds__(256) levelCombineKernel(FusedArgs A, int first
     combineChildren(A, node, fc, sub, gmask);
 }
 
-//! trees of at least this many nodes combine their internal nodes level by level (a 2^26-body cube has about 5M, a
-//! 2^22-body cube 300k, a 2^20-body cube 37k nodes: at those sizes the levels took 1.04, 0.144 and 0.051 ms, the
-//! climb 1.55, 0.194 and 0.047 ms)
+//! trees of at least this many nodes combine their internal nodes level by level. A 2^22-body cube has 300k nodes, a
+//! 2^20-body cube 37k: the levels took 0.144 and 0.051 ms there, the climb 0.194 and 0.047 ms. A 2^26-body cube has
+//! about 5M.
 constexpr int kLevelUpsweepNodes = 1 << 17;
 
 void launchFusedUpsweep(ryo_ctx* ctx, const float4* xyzm, int numLeaves, int numNodes, const uint32_t* layout,
