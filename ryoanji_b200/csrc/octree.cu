@@ -31,11 +31,13 @@ constexpr int kLeafBlock = 256;
  * The maximum over B + 1 consecutive windows comes from a sparse table built by doubling in shared memory:
  * m_2P[t] = max(m_P[t], m_P[t + P]), and the window [a, a + K) is max(m_P[a], m_P[a + K - P]) for the largest power
  * of two P <= K. A block also computes the level of the particle before its first, so head[i] (1 where particle i
- * starts a non-empty leaf: its leaf's start differs from particle i - 1's) needs no second pass.
+ * starts a non-empty leaf: its leaf's start differs from particle i - 1's) needs no second pass. blockHeads[b]
+ * receives the number of heads in block b, whose scan places each block's leaves.
  */
 __global__ void __launch_bounds__(kLeafBlock) leafLevels(const uint64_t* __restrict__ keys, uint32_t n,
                                                          uint32_t bucket, uint32_t minLevel,
-                                                         uint8_t* __restrict__ level, uint32_t* __restrict__ head)
+                                                         uint8_t* __restrict__ level, uint8_t* __restrict__ head,
+                                                         uint32_t* __restrict__ blockHeads)
 {
     extern __shared__ unsigned char smem[];
     __shared__ uint8_t leafLvl[kLeafBlock + 1]; // particles i0 - 1 .. i0 + kLeafBlock - 1
@@ -84,31 +86,57 @@ __global__ void __launch_bounds__(kLeafBlock) leafLevels(const uint64_t* __restr
     leafLvl[threadIdx.x + 1] = uint8_t(lv);
     if (threadIdx.x == 0) leafLvl[0] = uint8_t(leafLevel(0));
     __syncthreads();
-    if (i >= n) return;
-    level[i]   = uint8_t(lv);
-    uint32_t h = 1;
-    if (i > 0)
+    int h = 0;
+    if (i < n)
     {
-        uint64_t st = keys[i] & ~(nodeRange(lv) - 1);
-        uint64_t sp = keys[i - 1] & ~(nodeRange(leafLvl[threadIdx.x]) - 1);
-        h           = sp != st;
+        h = 1;
+        if (i > 0)
+        {
+            uint64_t st = keys[i] & ~(nodeRange(lv) - 1);
+            uint64_t sp = keys[i - 1] & ~(nodeRange(leafLvl[threadIdx.x]) - 1);
+            h           = sp != st;
+        }
     }
-    head[i] = h;
+    const int count = __syncthreads_count(h);
+    if (threadIdx.x == 0) blockHeads[blockIdx.x] = uint32_t(count);
+    if (i >= n) return;
+    level[i] = uint8_t(lv);
+    head[i]  = uint8_t(h);
 }
 
-__global__ void leafCompact(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ level,
-                            const uint32_t* __restrict__ rank, uint32_t n, uint64_t* __restrict__ leafStart,
-                            uint8_t* __restrict__ leafLvl, uint32_t* __restrict__ leafFirst)
+/*! the start, level and first particle of every non-empty leaf, in particle order: block b of leafLevels' blocks
+ *  writes its heads from blockOffset[b] on, ranked within the block by warp ballots */
+__global__ void __launch_bounds__(kLeafBlock) leafCompact(const uint64_t* __restrict__ keys,
+                                                          const uint8_t* __restrict__ level,
+                                                          const uint8_t* __restrict__ head,
+                                                          const uint32_t* __restrict__ blockOffset, uint32_t n,
+                                                          uint64_t* __restrict__ leafStart,
+                                                          uint8_t* __restrict__ leafLvl,
+                                                          uint32_t* __restrict__ leafFirst)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (rank[i + 1] != rank[i])
+    __shared__ uint32_t warpBase[kLeafBlock / kWarp];
+    const uint32_t i      = blockIdx.x * kLeafBlock + threadIdx.x;
+    const bool h          = i < n && head[i] != 0;
+    const unsigned ballot = __ballot_sync(0xffffffffu, h);
+    const unsigned warp   = threadIdx.x / kWarp;
+    if (laneId() == 0) warpBase[warp] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0)
     {
-        uint32_t q   = rank[i];
-        leafStart[q] = keys[i] & ~(nodeRange(level[i]) - 1);
-        leafLvl[q]   = level[i];
-        leafFirst[q] = i;
+        uint32_t run = 0;
+        for (int w = 0; w < kLeafBlock / kWarp; ++w)
+        {
+            uint32_t c  = warpBase[w];
+            warpBase[w] = run;
+            run += c;
+        }
     }
+    __syncthreads();
+    if (!h) return;
+    const uint32_t q = blockOffset[blockIdx.x] + warpBase[warp] + __popc(ballot & lanemaskLt());
+    leafStart[q]     = keys[i] & ~(nodeRange(level[i]) - 1);
+    leafLvl[q]       = level[i];
+    leafFirst[q]     = i;
 }
 
 //! number of output leaves contributed by non-empty leaf q: the gap before it plus itself (q == numNE: final gap)
@@ -182,23 +210,25 @@ int buildLeaves(ryo_ctx* ctx, const uint64_t* keys, size_t n64, unsigned bucket,
     }
     if (bucket > 16384) throw CudaError{cudaErrorInvalidValue, "bucket size above 16384 is not supported"};
 
-    uint8_t* level  = ctx->scratch<uint8_t>("leaf.level", n, s);
-    uint32_t* head  = ctx->scratch<uint32_t>("leaf.head", size_t(n) + 1, s);
+    const uint32_t numBlocks = uint32_t(ceilDiv(n, kLeafBlock));
+    uint8_t* level       = ctx->scratch<uint8_t>("leaf.level", n, s);
+    uint8_t* head        = ctx->scratch<uint8_t>("leaf.head8", n, s);
+    uint32_t* blockHeads = ctx->scratch<uint32_t>("leaf.blockHeads", size_t(numBlocks) + 1, s);
     size_t smemBytes = 2 * (size_t(kLeafBlock) + bucket + 1); // two window-level buffers of the sparse table
     if (smemBytes > 48 * 1024)
         RYO_CUDA(cudaFuncSetAttribute(leafLevels, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemBytes)));
-    leafLevels<<<ceilDiv(n, kLeafBlock), kLeafBlock, smemBytes, s>>>(keys, n, bucket, minLevel, level, head);
+    leafLevels<<<numBlocks, kLeafBlock, smemBytes, s>>>(keys, n, bucket, minLevel, level, head, blockHeads);
     RYO_LAUNCH_CHECK();
-    exclusiveScanU32(ctx, head, head, n, s);
+    exclusiveScanU32(ctx, blockHeads, blockHeads, numBlocks, s);
     uint32_t numNE = 0;
-    RYO_CUDA(cudaMemcpyAsync(&numNE, head + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    RYO_CUDA(cudaMemcpyAsync(&numNE, blockHeads + numBlocks, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     RYO_CUDA(cudaStreamSynchronize(s));
 
     uint64_t* leafStart = ctx->scratch<uint64_t>("leaf.start", numNE, s);
     uint8_t* leafLvl    = ctx->scratch<uint8_t>("leaf.lvl", numNE, s);
     uint32_t* leafFirst = ctx->scratch<uint32_t>("leaf.first", numNE, s);
     uint32_t* slots     = ctx->scratch<uint32_t>("leaf.slots", size_t(numNE) + 2, s);
-    leafCompact<<<ceilDiv(n, 256), 256, 0, s>>>(keys, level, head, n, leafStart, leafLvl, leafFirst);
+    leafCompact<<<numBlocks, kLeafBlock, 0, s>>>(keys, level, head, blockHeads, n, leafStart, leafLvl, leafFirst);
     RYO_LAUNCH_CHECK();
     leafSlots<<<ceilDiv(numNE + 1, 256), 256, 0, s>>>(leafStart, leafLvl, numNE, slots);
     RYO_LAUNCH_CHECK();
