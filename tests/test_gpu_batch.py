@@ -107,6 +107,42 @@ def test_batch_equals_single_solves(tol):
     assert res.stats.num_groups == groups
 
 
+def test_batch_mdq_signed_masses_equals_single_solves():
+    """monopole + dipole + quadrupole expansions of signed masses (node dipoles, and an FP64 dipole in every system
+    root): each system of the batch gets its single solve's result"""
+    import ryoanji_b200 as ryo
+    systems = []
+    for i, (n, sigma) in enumerate(((20000, 0.2), (5000, 0.1), (700, 0.3))):
+        p = ds.gaussian(n, seed=40 + i, sigma=sigma)
+        m = np.full(n, 1.0 / n)
+        m[1::2] *= -1.0
+        p.m = m.astype(np.float32)
+        p.h = np.full(n, 0.002, np.float32)
+        systems.append((f"signed{i}", p, None))
+    params = ryo.SolveParams(theta=0.5, bucket_size=32, group_size=32, multipole="mdq")
+    res, B = _run_batch(systems, params)
+    first = 0
+    for (name, p, _), e_batch, box in zip(systems, res.energies, res.boxes):
+        n = p.n
+        sl = slice(first, first + n)
+        first += n
+        x, y, z, m, h = (_dev(a) for a in (p.x, p.y, p.z, p.m, p.h))
+        pot, ax, ay, az = (torch.empty(n, device="cuda") for _ in range(4))
+        order = torch.empty(n, dtype=torch.int32, device="cuda")
+        r = ryo.solve(x, y, z, m, h, pot, ax, ay, az, params, order=order)
+        assert r.box == pytest.approx(box, rel=0, abs=0), name
+        assert torch.equal(B["order"][sl] - (first - n), order), name
+        assert torch.equal(B["x"][sl], x) and torch.equal(B["m"][sl], m), name
+        # groups split over warps in one solve and not in the other move sums by a few ulps of their value
+        amax = float(torch.sqrt(ax * ax + ay * ay + az * az).max()) + 1e-30
+        for k, ref in (("ax", ax), ("ay", ay), ("az", az)):
+            d = (B[k][sl] - ref).abs() / amax
+            assert float(d.max()) <= 1e-6, (name, k, float(d.max()))
+        dp = (B["p"][sl] - pot).abs() / (float(pot.abs().max()) + 1e-30)
+        assert float(dp.max()) <= 1e-6, (name, float(dp.max()))
+        assert e_batch == pytest.approx(r.potential_energy, rel=1e-6, abs=1e-9), name
+
+
 def test_batch_many_small_systems_against_direct_sums():
     import ryoanji_b200 as ryo
     rng = np.random.default_rng(11)
